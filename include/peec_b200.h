@@ -1,0 +1,189 @@
+/*
+ * peec_b200.h — C ABI of the B200 frequency-sweep library (libpeec_b200.so).
+ *
+ * Two layers are exported from the same shared library:
+ *
+ *   1. The batched core ("pb_*"): plain C structs, pointers and sizes. The caller hands
+ *      over the discretised geometry once (current cells, charge cells, nodes, ports)
+ *      and then asks for partial-element matrices or a whole frequency sweep. All device
+ *      memory is owned by an opaque context; every call is synchronous on return.
+ *
+ *   2. The reference-compatible entry points (lp_fill, pot_fill, solve, lu_decomp, ...):
+ *      declared in peec_abi.h with the reference's own prototypes, implemented on top of
+ *      layer 1. A program built from the reference's host files (parser, geometry,
+ *      outputs, main) links against this library instead of the reference's
+ *      partial.c / potential.c / surface.c / volume.c / polygon.c / skin.c / mna.c /
+ *      lu.c / solve.c.
+ *
+ * Return convention of the core: 0 = success, non-zero = error; pb_last_error() returns a
+ * message for the calling thread's last failure. There is no host fallback: if no CUDA
+ * device is usable every compute entry point fails with PB_ERR_CUDA.
+ *
+ * Complex numbers cross the ABI as interleaved double pairs {re, im}, matching the
+ * reference's d_complex_t (include/complex.h:13).
+ */
+#ifndef PEEC_B200_H
+#define PEEC_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PB_OK            0
+#define PB_ERR_ARG       1   /* invalid argument / size                              */
+#define PB_ERR_CUDA      2   /* CUDA runtime or library failure (no device, OOM, ...) */
+#define PB_ERR_SINGULAR  3   /* zero pivot in an LU factorisation                     */
+#define PB_ERR_NOCONV    4   /* refinement / GMRES did not reach the tolerance        */
+#define PB_ERR_UNSUP     5   /* input uses a feature this build does not implement    */
+
+/* Cell shape codes, identical to the reference's SHAPE_* (include/peec.h:50-53). */
+#define PB_SHAPE_ROUND 0
+#define PB_SHAPE_BAR   1
+#define PB_SHAPE_PLATE 2
+#define PB_SHAPE_POLY  3
+
+/*
+ * One discretised cell (current cell or charge cell). Field meanings follow the
+ * reference's seg_t (include/peec.h:108-136); the polygon vertex ring is not stored
+ * inline (seg_t carries pv[3*64]) but in a shared pool addressed by pvoff/npv.
+ * 256 bytes, no padding.
+ */
+typedef struct {
+    double x1[3], x2[3];   /* axis end points [m]                                   */
+    double len;            /* |x2 - x1|                                             */
+    double wid;            /* ribbon width (0 = thin filament); polygons: area/len  */
+    double thick;          /* thickness (volume bars, skin formula)                 */
+    double wv[3];          /* in-plane transverse unit vector (ribbons, bars)       */
+    double papex[3];       /* fan apex of a polygon cell                            */
+    double aL, aP;         /* equivalent radius for inductance / potential          */
+    double radius;         /* round-wire radius                                     */
+    double area, perim;    /* cross-section area and perimeter                      */
+    double sigma, res;     /* conductivity, DC resistance                           */
+    double cexc, gexc, gfac, epss, epsinf, frelax; /* dielectric branch parameters  */
+    int    n1, n2;         /* node ids of the two ends (current cells)              */
+    int    shape;          /* PB_SHAPE_*                                            */
+    int    vol;            /* 1 = volume bar (Hoer-Love pairs)                      */
+    int    diel;           /* 1 = dielectric branch                                 */
+    int    npv;            /* polygon vertex count (0 = not a polygon)              */
+    int    pvoff;          /* first vertex of the ring in the vertex pool           */
+    int    pad_;
+} pb_cell_t;
+
+typedef struct { int n1, n2; double z0; } pb_port_t;
+
+/* Lumped element kinds (reference rc_t / ind_t / src_t, include/peec.h:40-44). */
+#define PB_LUMP_R 0          /* resistor  val = ohm                     */
+#define PB_LUMP_C 1          /* capacitor val = farad                   */
+#define PB_LUMP_L 2          /* inductor  val = henry (branch current)  */
+#define PB_LUMP_V 3          /* ideal voltage source (branch current)   */
+typedef struct { int kind, n1, n2; double val; } pb_lump_t;
+
+/* Mutual coupling between two inductors (indices into the PB_LUMP_L elements in
+ * order of appearance), M = k sqrt(L1 L2) (reference mut_t, include/peec.h:42). */
+typedef struct { int l1, l2; double k; } pb_mutual_t;
+
+typedef struct {
+    int nseg;  const pb_cell_t *seg;     /* current cells, reference p->seg order      */
+    int nchg;  const pb_cell_t *chg;     /* charge sub-cells, reference p->chg order   */
+    const int *chgnode;                  /* [nchg] node id of each charge sub-cell     */
+    int npv;   const double *pv;         /* polygon vertex pool [3*npv]                */
+    int maxid;                           /* largest node id in use                     */
+    int nport; const pb_port_t *port;
+    int nlump; const pb_lump_t *lump;
+    int nmut;  const pb_mutual_t *mut;
+    int capacitance, retardation, skin, gp;
+    double gpz, gmin;
+} pb_problem_t;
+
+typedef struct pb_ctx pb_ctx;
+
+/* Precision of the partial-element fill / the dense solve. */
+#define PB_PREC_FP64   0     /* plain path: FP64 everywhere, static part re-evaluated   */
+#define PB_PREC_MIXED  1     /* FP64 static part (cached) + FP32 retardation correction */
+
+/* Dense factorisation used inside the sweep. */
+#define PB_LU_FP64     0     /* FP64 panels + FP64 trailing updates                      */
+#define PB_LU_FP32     1     /* FP32 panels + FP32 SIMT trailing updates, FP64 refinement */
+#define PB_LU_TC       2     /* FP32 panels + tensor-core trailing updates, FP64 refinement */
+
+/* MNA formulation inside the sweep. */
+#define PB_FORM_AUTO    0    /* reduced when applicable, else full                       */
+#define PB_FORM_FULL    1    /* the reference's dense MNA with C = P^-1 (mna.c:175-297)   */
+#define PB_FORM_REDUCED 2    /* branch-current Schur form (requires every node = a cell) */
+
+typedef struct {
+    int    fill_prec;       /* PB_PREC_*                                               */
+    int    lu;              /* PB_LU_*                                                 */
+    int    form;            /* PB_FORM_*                                               */
+    int    batch;           /* frequencies per device batch (0 = automatic)            */
+    double refine_tol;      /* target relative FP64 residual (0 = 1e-12)               */
+    int    refine_maxit;    /* max refinement / GMRES iterations (0 = 30)              */
+    int    verbose;
+} pb_sweep_opts;
+
+typedef struct {
+    double t_static_ms, t_corr_ms, t_assemble_ms, t_lu_ms, t_refine_ms, t_total_ms;
+    double corr_samples;    /* retardation-correction quadrature samples evaluated    */
+    double lu_flops;        /* (8/3) n^3 per frequency, summed                       */
+    double max_resid;       /* largest final relative FP64 residual over the sweep   */
+    int    max_iters;       /* largest refinement iteration count                    */
+    int    form_used;       /* PB_FORM_FULL or PB_FORM_REDUCED                       */
+    int    n_system;        /* order of the factorised system                        */
+    int    static_refreshes;/* how many times the cached static part was rebuilt     */
+    int    kernel_launches; /* kernels launched by the last pb_sweep call            */
+} pb_sweep_stats;
+
+const char *pb_last_error(void);
+int  pb_device_count(void);
+
+/* Context lifetime. pb_create copies the geometry to the device. */
+int  pb_create(const pb_problem_t *prob, pb_ctx **out);
+void pb_destroy(pb_ctx *ctx);
+int  pb_sizes(const pb_ctx *ctx, int *nseg, int *nchg, int *ncell, int *nnode, int *nunknown);
+
+/*
+ * Dense partial-inductance matrix at wavenumber kw (0 = quasi-static), both triangles,
+ * row-major [nseg*nseg] complex. Entry (i,j) equals the reference's lp_entry(p,i,j,kw)
+ * (src/partial.c:371-424) including the ground-plane image term.
+ */
+int  pb_lp_fill(pb_ctx *ctx, double kw, int prec, double *lp_host);
+
+/*
+ * Dense potential-coefficient matrix P at cell level (ncell x ncell, complex), entry
+ * (i,j) equal to the reference's pot_entry(p,i,j,kw) (src/potential.c:124-150).
+ */
+int  pb_pot_fill(pb_ctx *ctx, double kw, int prec, double *p_host);
+
+/*
+ * Frequency sweep (reference solve(), src/solve.c:171-430, dense path): for every
+ * frequency fill Lp/P (retardation) or reuse them (quasi-static), assemble, factorise,
+ * solve one 1 A excitation per port. Output zmat [nfreq*nport*nport] complex with the
+ * reference's ZIDX layout (include/peec.h:234). Any output pointer may be NULL.
+ * segi [nfreq*nport*nseg] receives the segment currents (reference DIDX layout).
+ */
+int  pb_sweep(pb_ctx *ctx, int nfreq, const double *freq, const pb_sweep_opts *opts,
+              double *zmat, double *segi, pb_sweep_stats *stats);
+
+/*
+ * Dense complex LU with partial pivoting on a host matrix, executed on the GPU
+ * (reference lu_decomp, src/lu.c:16-66): row-major a[n*n] complex is replaced by L\U,
+ * piv[k] = row swapped with row k at step k. Returns -1 on success or the 0-based row of
+ * the first zero pivot (max |re|+|im| < 1e-30), exactly like the reference; returns -2
+ * on a CUDA error.
+ */
+int  pb_lu_decomp(int n, double *a, int *piv);
+/* Forward/back substitution with the factors of pb_lu_decomp (reference lu_solve,
+ * src/lu.c:68-96). b[n] complex is overwritten by the solution. Returns 0 or PB_ERR_*. */
+int  pb_lu_solve(int n, const double *a, const int *piv, double *b);
+
+/*
+ * Batched variant operating on device memory: nb matrices of order n, row-major,
+ * complex FP64, stride n*n, factorised in place with the same pivot rule.
+ * info[b] = -1 or the zero-pivot row of matrix b. Device pointers (cudaMalloc'd).
+ */
+int  pb_lu_decomp_batched_dev(int n, int nb, double *a_dev, int *piv_dev, int *info_host);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PEEC_B200_H */
