@@ -1,0 +1,97 @@
+"""Python binding of the batched core of libpeec_b200.so (include/peec_b200.h).
+
+    from openpeec_b200 import geometry, api
+    prob = geometry.load_peec("dipole.peec")
+    with api.Context(prob) as ctx:
+        z, stats = ctx.sweep(prob.freqs())           # Z matrices per frequency
+
+Every compute call runs on the GPU; a missing library or device raises.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+
+
+class PbError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("libpeec_b200 error %d: %s" % (code, msg))
+        self.code = code
+
+
+def _check(code):
+    if code != abi.PB_OK:
+        raise PbError(code, abi.last_error())
+
+
+class Context:
+    """Device-resident discretisation of one structure (pb_create / pb_destroy)."""
+
+    def __init__(self, prob):
+        self.prob = prob
+        self._s = abi.problem_struct(prob)
+        h = C.c_void_p()
+        _check(abi.lib().pb_create(C.byref(self._s), C.byref(h)))
+        self.h = h
+        ns, nh, nc, nn, nu = (C.c_int() for _ in range(5))
+        _check(abi.lib().pb_sizes(self.h, C.byref(ns), C.byref(nh), C.byref(nc), C.byref(nn),
+                                  C.byref(nu)))
+        self.nseg, self.nchg, self.ncell = ns.value, nh.value, nc.value
+        self.nnode, self.nunknown = nn.value, nu.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            abi.lib().pb_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def lp_fill(self, kw, prec=abi.PREC_MIXED):
+        out = np.zeros((self.nseg, self.nseg), np.complex128)
+        _check(abi.lib().pb_lp_fill(self.h, float(kw), int(prec), out.ctypes.data))
+        return out
+
+    def pot_fill(self, kw, prec=abi.PREC_MIXED):
+        out = np.zeros((self.ncell, self.ncell), np.complex128)
+        _check(abi.lib().pb_pot_fill(self.h, float(kw), int(prec), out.ctypes.data))
+        return out
+
+    def sweep(self, freqs, fill_prec=abi.PREC_MIXED, lu=abi.LU_TC, form=abi.FORM_AUTO,
+              batch=0, refine_tol=0.0, refine_maxit=0, want_segi=False, zmat_out=None):
+        freqs = np.ascontiguousarray(freqs, np.float64)
+        npt = len(self.prob.port)
+        z = zmat_out if zmat_out is not None else np.zeros((len(freqs), npt, npt), np.complex128)
+        segi = np.zeros((len(freqs), npt, self.nseg), np.complex128) if want_segi else None
+        o = abi.PbSweepOpts(int(fill_prec), int(lu), int(form), int(batch), float(refine_tol),
+                            int(refine_maxit), 0)
+        st = abi.PbSweepStats()
+        _check(abi.lib().pb_sweep(self.h, len(freqs), freqs.ctypes.data, C.byref(o),
+                                  z.ctypes.data, None if segi is None else segi.ctypes.data,
+                                  C.byref(st)))
+        if want_segi:
+            return z, segi, st.as_dict()
+        return z, st.as_dict()
+
+
+def lu_decomp(a):
+    """GPU LU with the reference's contract (src/lu.c:16-66): returns (info, LU, piv)."""
+    a = np.ascontiguousarray(a, np.complex128).copy()
+    piv = np.zeros(a.shape[0], np.int32)
+    r = abi.lib().pb_lu_decomp(a.shape[0], a.ctypes.data, piv.ctypes.data)
+    if r == -2:
+        raise PbError(abi.PB_ERR_CUDA, abi.last_error())
+    return r, a, piv
+
+
+def lu_solve(lu, piv, b):
+    b = np.ascontiguousarray(b, np.complex128).copy()
+    _check(abi.lib().pb_lu_solve(lu.shape[0], np.ascontiguousarray(lu).ctypes.data,
+                                 np.ascontiguousarray(piv, np.int32).ctypes.data, b.ctypes.data))
+    return b

@@ -1,0 +1,414 @@
+// pb_api.cu — C entry points of the batched core (include/peec_b200.h).
+#include "pb_ctx.cuh"
+#include <algorithm>
+#include <cstdarg>
+#include <cstring>
+#include <map>
+#include <string>
+
+static thread_local std::string g_err;
+
+void pb_set_error(const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+}
+
+int pb_cuda_fail(cudaError_t e, const char *what, const char *file, int line)
+{
+    pb_set_error("CUDA error %s (%s) in %s at %s:%d", cudaGetErrorName(e), cudaGetErrorString(e), what, file, line);
+    return PB_ERR_CUDA;
+}
+
+int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts *opts,
+                  double *zmat, double *segi, pb_sweep_stats *stats);
+
+extern "C" const char *pb_last_error(void) { return g_err.c_str(); }
+
+extern "C" int pb_device_count(void)
+{
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
+    return n;
+}
+
+static int need_device()
+{
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) {
+        pb_set_error("no CUDA device available (%s); libpeec_b200 has no host fallback",
+                     e != cudaSuccess ? cudaGetErrorString(e) : "0 devices");
+        return PB_ERR_CUDA;
+    }
+    return PB_OK;
+}
+
+template <typename T> static int upload(T **d, const T *h, size_t n, cudaStream_t s)
+{
+    PB_CUDA(cudaMalloc(d, sizeof(T) * (n > 0 ? n : 1)));
+    if (n > 0 && h) PB_CUDA(cudaMemcpyAsync(*d, h, sizeof(T) * n, cudaMemcpyHostToDevice, s));
+    return PB_OK;
+}
+
+static int build(pb_ctx *c)
+{
+    const int nh = (int)c->chg.size(), ns = (int)c->seg.size();
+    // potential.c:29-62 : cells in order of first appearance of the node id
+    c->cellof.assign(nh, 0);
+    c->cellid.clear();
+    std::map<int, int> seen;
+    for (int h = 0; h < nh; h++) {
+        auto it = seen.find(c->chgnode[h]);
+        int id;
+        if (it == seen.end()) { id = (int)c->cellid.size(); seen[c->chgnode[h]] = id; c->cellid.push_back(c->chgnode[h]); }
+        else id = it->second;
+        c->cellof[h] = id;
+    }
+    c->ncell = (int)c->cellid.size();
+    c->carea.assign(c->ncell, 0.0);
+    for (int h = 0; h < nh; h++) c->carea[c->cellof[h]] += c->chg[h].len;
+    c->csoff.assign(c->ncell + 1, 0);                    // potential.c:72-97
+    for (int h = 0; h < nh; h++) c->csoff[c->cellof[h] + 1]++;
+    for (int i = 0; i < c->ncell; i++) c->csoff[i + 1] += c->csoff[i];
+    c->csidx.assign(nh, 0);
+    {
+        std::vector<int> fill(c->csoff);
+        for (int h = 0; h < nh; h++) c->csidx[fill[c->cellof[h]]++] = h;
+    }
+    // mna.c:16-84 : numbering
+    const int nid = c->maxid + 1;
+    auto bad = [&](int id) { return id < 0 || id >= nid; };
+    std::vector<int> used(nid, 0);
+    for (auto &l : c->lump) { if (bad(l.n1) || bad(l.n2)) return PB_ERR_ARG; used[l.n1] = used[l.n2] = 1; }
+    for (auto &p : c->port) { if (bad(p.n1) || bad(p.n2)) return PB_ERR_ARG; used[p.n1] = used[p.n2] = 1; }
+    for (auto &s : c->seg) { if (bad(s.n1) || bad(s.n2)) return PB_ERR_ARG; used[s.n1] = used[s.n2] = 1; }
+    for (int h = 0; h < nh; h++) if (bad(c->chgnode[h])) return PB_ERR_ARG;
+    const int usecap = c->capacitance && c->ncell > 0;
+    c->refnode = (usecap || used[0]) ? 0 : c->port[0].n2;
+    c->nodemap.assign(nid, -2);
+    int idx = 0;
+    for (int id = 0; id < nid; id++) {
+        if (id == c->refnode) c->nodemap[id] = -1;
+        else if (used[id]) c->nodemap[id] = idx++;
+    }
+    c->nnode = idx;
+    c->nind = c->nvsrc = 0;
+    for (auto &l : c->lump) { c->nind += l.kind == PB_LUMP_L; c->nvsrc += l.kind == PB_LUMP_V; }
+    c->offL = c->nnode;
+    c->offV = c->offL + c->nind;
+    c->offS = c->offV + c->nvsrc;
+    c->nunknown = c->offS + ns;
+    c->cell_of_node.assign(nid, -1);
+    for (int i = 0; i < c->ncell; i++) c->cell_of_node[c->cellid[i]] = i;
+
+    // reduced form applicability
+    int ok = usecap && c->gmin == 0 && c->lump.empty() && c->mut.empty();
+    for (int id = 0; ok && id < nid; id++)
+        if (c->nodemap[id] >= 0 && c->cell_of_node[id] < 0) ok = 0;   // matrix node without a cell
+    for (int i = 0; ok && i < c->ncell; i++)
+        if (c->nodemap[c->cellid[i]] < 0) ok = 0;                       // cell on the reference node
+    c->reduced_ok = ok;
+    c->seg_ca.assign(ns, -1);
+    c->seg_cb.assign(ns, -1);
+    c->inc_off.assign(c->ncell + 1, 0);
+    c->inc_seg.clear();
+    if (ok) {
+        for (int k = 0; k < ns; k++) {
+            const pb_cell_t &s = c->seg[k];
+            c->seg_ca[k] = c->nodemap[s.n1] >= 0 ? c->cell_of_node[s.n1] : -1;
+            c->seg_cb[k] = c->nodemap[s.n2] >= 0 ? c->cell_of_node[s.n2] : -1;
+        }
+        std::vector<std::vector<int>> inc(c->ncell);
+        for (int k = 0; k < ns; k++) {
+            if (c->seg_ca[k] >= 0) inc[c->seg_ca[k]].push_back(k + 1);
+            if (c->seg_cb[k] >= 0) inc[c->seg_cb[k]].push_back(-(k + 1));
+        }
+        for (int i = 0; i < c->ncell; i++) {
+            c->inc_off[i + 1] = c->inc_off[i] + (int)inc[i].size();
+            c->inc_seg.insert(c->inc_seg.end(), inc[i].begin(), inc[i].end());
+        }
+    }
+
+    // full (augmented) form: contributions per unique entry, in the reference's
+    // stamping order (mna.c:181-241, 248-251, 277-278)
+    c->nfull = c->nunknown + (usecap ? c->ncell : 0);
+    std::map<std::pair<int, int>, std::vector<pb_stamp>> ent;
+    auto put = [&](int i, int j, int kind, double v) {
+        if (i < 0 || j < 0) return;                      // mna.c:156
+        ent[std::make_pair(i, j)].push_back(pb_stamp{kind, v});
+    };
+    const int *map = c->nodemap.data();
+    if (c->gmin > 0) for (int i = 0; i < c->nnode; i++) put(i, i, ST_CONST, c->gmin);
+    for (int pass = 0; pass < 2; pass++)
+        for (auto &l : c->lump) {
+            if (l.kind != (pass ? PB_LUMP_C : PB_LUMP_R)) continue;
+            const int i1 = map[l.n1], i2 = map[l.n2];
+            const int k = pass ? ST_JW : ST_CONST;
+            const double y = pass ? l.val : 1 / l.val;
+            put(i1, i1, k, y); put(i2, i2, k, y); put(i1, i2, k, -y); put(i2, i1, k, -y);
+        }
+    std::vector<double> lval;
+    int il = 0;
+    for (auto &l : c->lump) {
+        if (l.kind != PB_LUMP_L) continue;
+        const int i1 = map[l.n1], i2 = map[l.n2], r = c->offL + il++;
+        lval.push_back(l.val);
+        put(i1, r, ST_CONST, 1); put(r, i1, ST_CONST, 1); put(i2, r, ST_CONST, -1); put(r, i2, ST_CONST, -1);
+        put(r, r, ST_MJW, l.val);
+    }
+    for (auto &m : c->mut) {
+        if (m.l1 < 0 || m.l2 < 0 || m.l1 >= (int)lval.size() || m.l2 >= (int)lval.size()) return PB_ERR_ARG;
+        const double mm = m.k * std::sqrt(lval[m.l1] * lval[m.l2]);
+        put(c->offL + m.l1, c->offL + m.l2, ST_MJW, mm);
+        put(c->offL + m.l2, c->offL + m.l1, ST_MJW, mm);
+    }
+    int iv = 0;
+    for (auto &l : c->lump) {
+        if (l.kind != PB_LUMP_V) continue;
+        const int i1 = map[l.n1], i2 = map[l.n2], r = c->offV + iv++;
+        put(i1, r, ST_CONST, 1); put(r, i1, ST_CONST, 1); put(i2, r, ST_CONST, -1); put(r, i2, ST_CONST, -1);
+    }
+    for (int k = 0; k < ns; k++) {
+        const int i1 = map[c->seg[k].n1], i2 = map[c->seg[k].n2], rk = c->offS + k;
+        put(i1, rk, ST_CONST, 1); put(rk, i1, ST_CONST, 1); put(i2, rk, ST_CONST, -1); put(rk, i2, ST_CONST, -1);
+    }
+    if (usecap)
+        for (int i = 0; i < c->ncell; i++) {
+            const int mi = map[c->cellid[i]], ri = c->nunknown + i;
+            put(mi, ri, ST_JW, 1);
+            put(ri, mi, ST_CONST, -1);
+        }
+    c->fe_row.clear(); c->fe_col.clear(); c->fe_off.assign(1, 0); c->fe_st.clear();
+    for (auto &kv : ent) {
+        c->fe_row.push_back(kv.first.first);
+        c->fe_col.push_back(kv.first.second);
+        c->fe_st.insert(c->fe_st.end(), kv.second.begin(), kv.second.end());
+        c->fe_off.push_back((int)c->fe_st.size());
+    }
+    return PB_OK;
+}
+
+extern "C" {
+
+int pb_create(const pb_problem_t *prob, pb_ctx **out)
+{
+    if (!prob || !out) { pb_set_error("pb_create: null argument"); return PB_ERR_ARG; }
+    *out = nullptr;
+    if (prob->nseg < 0 || prob->nchg < 0 || prob->npv < 0 || prob->nport <= 0 || prob->maxid < 0 ||
+        (prob->nseg > 0 && !prob->seg) || (prob->nchg > 0 && (!prob->chg || !prob->chgnode)) ||
+        (prob->npv > 0 && !prob->pv) || !prob->port || (prob->nlump > 0 && !prob->lump) ||
+        (prob->nmut > 0 && !prob->mut)) {
+        pb_set_error("pb_create: inconsistent problem description");
+        return PB_ERR_ARG;
+    }
+    PB_TRY(need_device());
+    pb_ctx *c = new pb_ctx();
+    c->seg.assign(prob->seg, prob->seg + prob->nseg);
+    c->chg.assign(prob->chg, prob->chg + prob->nchg);
+    c->chgnode.assign(prob->chgnode, prob->chgnode + prob->nchg);
+    c->pv.assign(prob->pv, prob->pv + 3 * (size_t)prob->npv);
+    c->port.assign(prob->port, prob->port + prob->nport);
+    c->lump.assign(prob->lump, prob->lump + prob->nlump);
+    c->mut.assign(prob->mut, prob->mut + prob->nmut);
+    c->capacitance = prob->capacitance; c->retardation = prob->retardation;
+    c->skin = prob->skin; c->gp = prob->gp; c->gpz = prob->gpz; c->gmin = prob->gmin;
+    c->maxid = prob->maxid;
+    for (auto &s : c->seg)
+        if (s.npv > 0 && (s.npv > PB_POLY_MAX || s.pvoff < 0 || s.pvoff + s.npv > prob->npv)) { delete c; pb_set_error("pb_create: polygon ring out of range"); return PB_ERR_ARG; }
+    for (auto &s : c->chg)
+        if (s.npv > 0 && (s.npv > PB_POLY_MAX || s.pvoff < 0 || s.pvoff + s.npv > prob->npv)) { delete c; pb_set_error("pb_create: polygon ring out of range"); return PB_ERR_ARG; }
+    int r = build(c);
+    if (r != PB_OK) { delete c; if (r == PB_ERR_ARG) pb_set_error("pb_create: node id out of range"); return r; }
+
+    cudaGetDevice(&c->dev);
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c; pb_set_error("cudaStreamCreate failed"); return PB_ERR_CUDA;
+    }
+    const cudaStream_t s = c->stream;
+    auto fail = [&](int rr) { pb_destroy(c); return rr; };
+    pb_fill_geom &g = c->g;
+    g.gp = c->gp; g.gpz = c->gpz; g.ncell = c->ncell;
+    g.seg.n = (int)c->seg.size();
+    g.chg.n = (int)c->chg.size();
+    if ((r = upload(&g.seg.cell, c->seg.data(), c->seg.size(), s))) return fail(r);
+    if ((r = upload(&g.chg.cell, c->chg.data(), c->chg.size(), s))) return fail(r);
+    if ((r = upload(&g.pv, c->pv.data(), c->pv.size(), s))) return fail(r);
+    if ((r = upload(&g.csoff, c->csoff.data(), c->csoff.size(), s))) return fail(r);
+    if ((r = upload(&g.csidx, c->csidx.data(), c->csidx.size(), s))) return fail(r);
+    if ((r = upload(&g.carea, c->carea.data(), c->carea.size(), s))) return fail(r);
+    if ((r = upload(&g.seg_ca, c->seg_ca.data(), c->seg_ca.size(), s))) return fail(r);
+    if ((r = upload(&g.seg_cb, c->seg_cb.data(), c->seg_cb.size(), s))) return fail(r);
+    if ((r = upload(&c->d_inc_off, c->inc_off.data(), c->inc_off.size(), s))) return fail(r);
+    if ((r = upload(&c->d_inc_seg, c->inc_seg.data(), c->inc_seg.size(), s))) return fail(r);
+    if ((r = upload(&c->d_fe_row, c->fe_row.data(), c->fe_row.size(), s))) return fail(r);
+    if ((r = upload(&c->d_fe_col, c->fe_col.data(), c->fe_col.size(), s))) return fail(r);
+    if ((r = upload(&c->d_fe_off, c->fe_off.data(), c->fe_off.size(), s))) return fail(r);
+    if ((r = upload(&c->d_fe_st, c->fe_st.data(), c->fe_st.size(), s))) return fail(r);
+    int anyp = 0;
+    for (auto &x : c->seg) anyp |= x.npv > 0;
+    for (auto &x : c->chg) anyp |= x.npv > 0;
+    g.any_poly = anyp;
+    if (anyp) {
+        if ((r = pb_build_qpts(g.seg, c->seg.data(), c->pv.data(), g.pv, s))) return fail(r);
+        if ((r = pb_build_qpts(g.chg, c->chg.data(), c->pv.data(), g.pv, s))) return fail(r);
+    }
+    if ((r = pb_lu_engine_init(&c->lu, s))) return fail(r);
+    if (cudaStreamSynchronize(s) != cudaSuccess) return fail(pb_cuda_fail(cudaGetLastError(), "upload", __FILE__, __LINE__));
+    *out = c;
+    return PB_OK;
+}
+
+void pb_destroy(pb_ctx *c)
+{
+    if (!c) return;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    void *ptrs[] = {c->g.seg.cell, c->g.seg.qpt, c->g.seg.qoff, c->g.chg.cell, c->g.chg.qpt,
+                    c->g.chg.qoff, c->g.pv, c->g.csoff, c->g.csidx, c->g.carea, c->g.seg_ca,
+                    c->g.seg_cb, c->d_inc_off, c->d_inc_seg, c->d_fe_row, c->d_fe_col, c->d_fe_off,
+                    c->d_fe_st, c->d_cellnode};
+    for (void *p : ptrs) if (p) cudaFree(p);
+    pb_lu_engine_free(&c->lu);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+int pb_sizes(const pb_ctx *c, int *nseg, int *nchg, int *ncell, int *nnode, int *nunknown)
+{
+    if (!c) return PB_ERR_ARG;
+    if (nseg) *nseg = (int)c->seg.size();
+    if (nchg) *nchg = (int)c->chg.size();
+    if (ncell) *ncell = c->ncell;
+    if (nnode) *nnode = c->nnode;
+    if (nunknown) *nunknown = c->nunknown;
+    return PB_OK;
+}
+
+int pb_lp_fill(pb_ctx *c, double kw, int prec, double *lp_host)
+{
+    if (!c || !lp_host || kw < 0) { pb_set_error("pb_lp_fill: bad argument"); return PB_ERR_ARG; }
+    const int n = (int)c->seg.size();
+    if (n == 0) return PB_OK;
+    double *st = nullptr;
+    double2 *out = nullptr;
+    PB_CUDA(cudaMalloc(&st, sizeof(double) * (size_t)n * n));
+    cudaError_t e = cudaMalloc(&out, sizeof(double2) * (size_t)n * n);
+    if (e != cudaSuccess) { cudaFree(st); return pb_cuda_fail(e, "cudaMalloc", __FILE__, __LINE__); }
+    int r = pb_lp_static(c->g, kw, st, c->stream, &c->launches);
+    pb_epi_args ea;
+    ea.out = out;
+    ea.out_stride = (long long)n * n;
+    if (r == PB_OK) r = pb_lp_corr(c->g, 1, &kw, prec == PB_PREC_MIXED, st, PB_EPI_STORE, ea, c->stream, &c->launches, nullptr);
+    if (r == PB_OK) {
+        e = cudaMemcpyAsync(lp_host, out, sizeof(double2) * (size_t)n * n, cudaMemcpyDeviceToHost, c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) r = pb_cuda_fail(e, "pb_lp_fill copy", __FILE__, __LINE__);
+    }
+    cudaFree(st);
+    cudaFree(out);
+    return r;
+}
+
+int pb_pot_fill(pb_ctx *c, double kw, int prec, double *p_host)
+{
+    if (!c || !p_host || kw < 0) { pb_set_error("pb_pot_fill: bad argument"); return PB_ERR_ARG; }
+    const int n = c->ncell;
+    if (n == 0) return PB_OK;
+    double *st = nullptr;
+    double2 *out = nullptr;
+    PB_CUDA(cudaMalloc(&st, sizeof(double) * (size_t)n * n));
+    cudaError_t e = cudaMalloc(&out, sizeof(double2) * (size_t)n * n);
+    if (e != cudaSuccess) { cudaFree(st); return pb_cuda_fail(e, "cudaMalloc", __FILE__, __LINE__); }
+    int r = pb_pot_static(c->g, kw, st, c->stream, &c->launches);
+    if (r == PB_OK) r = pb_pot_corr(c->g, 1, &kw, prec == PB_PREC_MIXED, st, out, (long long)n * n, c->stream, &c->launches, nullptr);
+    if (r == PB_OK) {
+        e = cudaMemcpyAsync(p_host, out, sizeof(double2) * (size_t)n * n, cudaMemcpyDeviceToHost, c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) r = pb_cuda_fail(e, "pb_pot_fill copy", __FILE__, __LINE__);
+    }
+    cudaFree(st);
+    cudaFree(out);
+    return r;
+}
+
+int pb_sweep(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts *opts, double *zmat,
+             double *segi, pb_sweep_stats *stats)
+{
+    if (!c) { pb_set_error("pb_sweep: null context"); return PB_ERR_ARG; }
+    PB_CUDA(cudaSetDevice(c->dev));
+    return pb_sweep_impl(c, nfreq, freq, opts, zmat, segi, stats);
+}
+
+// ---------------------------------------------------------------- dense LU entry points
+int pb_lu_decomp_batched_dev(int n, int nb, double *a_dev, int *piv_dev, int *info_host)
+{
+    if (n <= 0 || nb <= 0 || !a_dev || !piv_dev || !info_host) { pb_set_error("pb_lu_decomp_batched_dev: bad argument"); return PB_ERR_ARG; }
+    PB_TRY(need_device());
+    pb_lu_engine e;
+    PB_TRY(pb_lu_engine_init(&e, nullptr));
+    e.gemm_kind = PB_GEMM_FP64;
+    int *info = nullptr;
+    cudaError_t ce = cudaMalloc(&info, sizeof(int) * nb);
+    if (ce != cudaSuccess) { pb_lu_engine_free(&e); return pb_cuda_fail(ce, "cudaMalloc", __FILE__, __LINE__); }
+    int r = pb_lu_factor<double>(&e, n, nb, (double2 *)a_dev, n, (long)n * n, piv_dev, info);
+    if (r == PB_OK) {
+        ce = cudaMemcpy(info_host, info, sizeof(int) * nb, cudaMemcpyDeviceToHost);
+        if (ce != cudaSuccess) r = pb_cuda_fail(ce, "cudaMemcpy", __FILE__, __LINE__);
+    }
+    cudaFree(info);
+    pb_lu_engine_free(&e);
+    return r;
+}
+
+int pb_lu_decomp(int n, double *a, int *piv)
+{
+    if (n <= 0 || !a || !piv) { pb_set_error("pb_lu_decomp: bad argument"); return -2; }
+    if (need_device() != PB_OK) return -2;
+    double *d = nullptr;
+    int *dp = nullptr, info = -1;
+    if (cudaMalloc(&d, sizeof(double2) * (size_t)n * n) != cudaSuccess) { pb_set_error("cudaMalloc failed"); return -2; }
+    if (cudaMalloc(&dp, sizeof(int) * n) != cudaSuccess) { cudaFree(d); pb_set_error("cudaMalloc failed"); return -2; }
+    int r = PB_OK;
+    if (cudaMemcpy(d, a, sizeof(double2) * (size_t)n * n, cudaMemcpyHostToDevice) != cudaSuccess) r = PB_ERR_CUDA;
+    if (r == PB_OK) r = pb_lu_decomp_batched_dev(n, 1, d, dp, &info);
+    if (r == PB_OK && cudaMemcpy(a, d, sizeof(double2) * (size_t)n * n, cudaMemcpyDeviceToHost) != cudaSuccess) r = PB_ERR_CUDA;
+    if (r == PB_OK && cudaMemcpy(piv, dp, sizeof(int) * n, cudaMemcpyDeviceToHost) != cudaSuccess) r = PB_ERR_CUDA;
+    cudaFree(d);
+    cudaFree(dp);
+    if (r != PB_OK) return -2;
+    return info;          // -1 = regular, else first zero-pivot row (lu.c:15-30)
+}
+
+int pb_lu_solve(int n, const double *a, const int *piv, double *b)
+{
+    if (n <= 0 || !a || !piv || !b) { pb_set_error("pb_lu_solve: bad argument"); return PB_ERR_ARG; }
+    PB_TRY(need_device());
+    pb_lu_engine e;
+    PB_TRY(pb_lu_engine_init(&e, nullptr));
+    double2 *d = nullptr, *bv = nullptr;
+    int *dp = nullptr, *perm = nullptr;
+    int r = PB_OK;
+    if (cudaMalloc(&d, sizeof(double2) * (size_t)n * n) != cudaSuccess || cudaMalloc(&bv, sizeof(double2) * n) != cudaSuccess ||
+        cudaMalloc(&dp, sizeof(int) * n) != cudaSuccess || cudaMalloc(&perm, sizeof(int) * n) != cudaSuccess) {
+        pb_set_error("cudaMalloc failed");
+        r = PB_ERR_CUDA;
+    }
+    if (r == PB_OK && (cudaMemcpy(d, a, sizeof(double2) * (size_t)n * n, cudaMemcpyHostToDevice) != cudaSuccess ||
+                       cudaMemcpy(bv, b, sizeof(double2) * n, cudaMemcpyHostToDevice) != cudaSuccess ||
+                       cudaMemcpy(dp, piv, sizeof(int) * n, cudaMemcpyHostToDevice) != cudaSuccess)) {
+        pb_set_error("cudaMemcpy failed");
+        r = PB_ERR_CUDA;
+    }
+    if (r == PB_OK) r = pb_lu_perm(&e, n, 1, dp, perm);
+    if (r == PB_OK) r = pb_lu_solve_batched<double>(&e, n, 1, 1, d, n, (long)n * n, perm, bv, bv);
+    if (r == PB_OK && cudaMemcpy(b, bv, sizeof(double2) * n, cudaMemcpyDeviceToHost) != cudaSuccess) { pb_set_error("cudaMemcpy failed"); r = PB_ERR_CUDA; }
+    cudaFree(d); cudaFree(bv); cudaFree(dp); cudaFree(perm);
+    pb_lu_engine_free(&e);
+    return r;
+}
+
+}  // extern "C"

@@ -1,0 +1,55 @@
+// pb_ctx.cuh — the opaque context behind pb_ctx* (include/peec_b200.h).
+#pragma once
+#include <vector>
+#include "pb_common.cuh"
+#include "pb_fill.cuh"
+#include "pb_lu.cuh"
+
+// One additive contribution to an MNA entry whose value scales as val * {1, jw, -jw}.
+enum { ST_CONST = 0, ST_JW = 1, ST_MJW = 2 };
+struct pb_stamp { int kind; double val; };
+
+struct pb_ctx {
+    int dev = 0;
+    cudaStream_t stream = nullptr;
+    pb_lu_engine lu;
+
+    // host copies of the problem
+    std::vector<pb_cell_t> seg, chg;
+    std::vector<int> chgnode;
+    std::vector<double> pv;
+    std::vector<pb_port_t> port;
+    std::vector<pb_lump_t> lump;
+    std::vector<pb_mutual_t> mut;
+    int capacitance = 0, retardation = 0, skin = 0, gp = 0, maxid = 0;
+    double gpz = 0, gmin = 0;
+
+    // charge-cell grouping (potential.c:29-114)
+    int ncell = 0;
+    std::vector<int> cellid, cellof, csoff, csidx;
+    std::vector<double> carea;
+    std::vector<int> cell_of_node;             // [maxid+1] -> cell index or -1
+
+    // MNA numbering (mna.c:16-113)
+    std::vector<int> nodemap;
+    int nnode = 0, refnode = 0, offL = 0, offV = 0, offS = 0, nunknown = 0, nind = 0, nvsrc = 0;
+
+    // reduced (branch-current) form
+    int reduced_ok = 0;
+    std::vector<int> seg_ca, seg_cb;           // cell of each segment end, -1 = reference
+    std::vector<int> inc_off, inc_seg;         // cell -> incident segments (signed: +k+1 / -(k+1))
+
+    // full (augmented) form: unique entries and their contributions
+    int nfull = 0;                             // order of the augmented system
+    std::vector<int> fe_row, fe_col, fe_off;   // unique entries, contributions in [fe_off[e], fe_off[e+1])
+    std::vector<pb_stamp> fe_st;
+
+    // device geometry
+    pb_fill_geom g;
+    int *d_inc_off = nullptr, *d_inc_seg = nullptr;
+    int *d_fe_row = nullptr, *d_fe_col = nullptr, *d_fe_off = nullptr;
+    pb_stamp *d_fe_st = nullptr;
+    int *d_cellnode = nullptr;                 // [ncell] matrix index of the cell's node (-1 = ref)
+
+    long launches = 0;
+};

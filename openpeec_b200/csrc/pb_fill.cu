@@ -1,0 +1,691 @@
+// pb_fill.cu — partial-inductance (Lp) and potential-coefficient (P) fill kernels.
+//
+// Each matrix entry is split as the reference splits it (partial.c:256-317):
+//   I = I_static + sum (e^{-jkR} - 1)/R   (singularity extraction).
+// * Static part: FP64, one thread per entry (k_lp_static / k_pot_static), evaluated
+//   once per quadrature level and cached across the frequency sweep.
+// * Retardation correction: one warp per entry; the 32 lanes split the quadrature
+//   samples; each sample's R is computed once and reused for up to 32 wavenumbers of
+//   the sweep (per-lane accumulators, one per frequency). FP32 in the mixed path, FP64
+//   in the plain path. The integrand is evaluated as
+//       (e^{-jkR} - 1)/R = -(2 sin(kR/2)/R) * (sin(kR/2) + j cos(kR/2)),
+//   which has no cancellation (the reference's cos(kR)-1, partial.c:168, would lose all
+//   digits in FP32 for small kR).
+// * Epilogue: store Lp / P, or assemble the reduced MNA matrix directly.
+#include "pb_fill.cuh"
+#include "pb_geom.cuh"
+#include <vector>
+
+template <typename R> __device__ __forceinline__ R XG4(int i);
+template <> __device__ __forceinline__ float XG4<float>(int i) { return (float)cXG4[i]; }
+template <> __device__ __forceinline__ double XG4<double>(int i) { return cXG4[i]; }
+template <typename R> __device__ __forceinline__ R WG4(int i);
+template <> __device__ __forceinline__ float WG4<float>(int i) { return (float)cWG4[i]; }
+template <> __device__ __forceinline__ double WG4<double>(int i) { return cWG4[i]; }
+template <typename R> __device__ __forceinline__ R XG8(int i);
+template <> __device__ __forceinline__ float XG8<float>(int i) { return (float)cXG8[i]; }
+template <> __device__ __forceinline__ double XG8<double>(int i) { return cXG8[i]; }
+template <typename R> __device__ __forceinline__ R WG8(int i);
+template <> __device__ __forceinline__ float WG8<float>(int i) { return (float)cWG8[i]; }
+template <> __device__ __forceinline__ double WG8<double>(int i) { return cWG8[i]; }
+
+__device__ __forceinline__ void sc(float x, float *s, float *c) { sincosf(x, s, c); }
+__device__ __forceinline__ void sc(double x, double *s, double *c) { sincos(x, s, c); }
+
+struct KArg {
+    double kw[PB_FMAX];
+    int nf;
+};
+
+template <typename R, int F> struct Acc {
+    R re[F], im[F];
+};
+
+// Accumulate one sample at distance r with weight w for every wavenumber.
+template <typename R, int F>
+__device__ __forceinline__ void accum(Acc<R, F> &a, const R *kh, int nf, R r, R w)
+{
+    if (r > (R)0) {
+        const R q = (R)-2 * w / r;
+#pragma unroll
+        for (int f = 0; f < F; f++) {
+            if (f < nf) {
+                R s, c;
+                sc(kh[f] * r, &s, &c);
+                const R t = q * s;
+                a.re[f] = fma(t, s, a.re[f]);
+                a.im[f] = fma(t, c, a.im[f]);
+            }
+        }
+    } else {
+        // R -> 0 limit of (e^{-jkR}-1)/R is -jk (surface.c:164-166)
+#pragma unroll
+        for (int f = 0; f < F; f++)
+            if (f < nf) a.im[f] -= (R)2 * w * kh[f];
+    }
+}
+
+// ribbon_corr (surface.c:134-178): 4^4 * nsub^2 samples; HL pairs use it too.
+template <typename R, int F>
+__device__ void corr_ribbon(const Cell &s1, const Cell &s2, int nsub, double scale,
+                            const R *kh, int nf, Acc<R, F> &a, int lane)
+{
+    double t1d[3], w1d[3], n1d[3], c1d[3], t2d[3], w2d[3], n2d[3], c2d[3];
+    frame(s1, t1d, w1d, n1d, c1d);
+    frame(s2, t2d, w2d, n2d, c2d);
+    R t1[3], w1[3], t2[3], w2[3], cd[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        t1[c] = (R)t1d[c]; w1[c] = (R)w1d[c]; t2[c] = (R)t2d[c]; w2[c] = (R)w2d[c];
+        cd[c] = (R)(c2d[c] - c1d[c]);
+    }
+    const R L1 = (R)s1.len, W1 = (R)s1.wid, L2 = (R)s2.len, W2 = (R)s2.wid;
+    const R sc_ = (R)(scale * s1.len * s2.len / (16.0 * nsub * nsub));
+    const R rn = (R)nsub;
+    const int S = 256 * nsub * nsub;
+    for (int s = lane; s < S; s += 32) {
+        const int q = s & 3, m = (s >> 2) & 3, j = (s >> 4) & 3, i = (s >> 6) & 3;
+        const int rest = s >> 8, ja = rest % nsub, ia = rest / nsub;
+        const R a1 = L1 * ((ia + (R)0.5 * (1 + XG4<R>(i))) / rn - (R)0.5);
+        const R b1 = W1 * ((R)0.5 * (1 + XG4<R>(j)) - (R)0.5);
+        const R a2 = L2 * ((ja + (R)0.5 * (1 + XG4<R>(m))) / rn - (R)0.5);
+        const R b2 = W2 * ((R)0.5 * (1 + XG4<R>(q)) - (R)0.5);
+        R d2 = 0;
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const R p1 = a1 * t1[c] + b1 * w1[c];
+            const R p2 = a2 * t2[c] + b2 * w2[c];
+            const R d = (cd[c] + p2) - p1;
+            d2 += d * d;
+        }
+        const R w = WG4<R>(i) * WG4<R>(j) * WG4<R>(m) * WG4<R>(q) * sc_;
+        accum<R, F>(a, kh, nf, sqrt(d2), w);
+    }
+}
+
+// gauss_kernel mode 1 (partial.c:61-99): 8x8 Gauss on nsub x nsub sub-squares.
+template <typename R, int F>
+__device__ void corr_wire(const Cell &s1, const Cell &s2, double aeff, int nsub, double scale,
+                          const R *kh, int nf, Acc<R, F> &a, int lane)
+{
+    R e1[3], e2[3], d0[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        e1[c] = (R)(s1.x2[c] - s1.x1[c]);
+        e2[c] = (R)(s2.x2[c] - s2.x1[c]);
+        d0[c] = (R)(s2.x1[c] - s1.x1[c]);
+    }
+    const R a2 = (R)(aeff * aeff);
+    const R sc_ = (R)(scale * s1.len * s2.len * 0.25 / ((double)nsub * nsub));
+    const R rn = (R)nsub;
+    const int S = 64 * nsub * nsub;
+    for (int s = lane; s < S; s += 32) {
+        const int j = s & 7, i = (s >> 3) & 7, rest = s >> 6, i2 = rest % nsub, i1 = rest / nsub;
+        const R u = (i1 + (R)0.5 * (1 + XG8<R>(i))) / rn;
+        const R v = (i2 + (R)0.5 * (1 + XG8<R>(j))) / rn;
+        R d2 = a2;
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const R d = (d0[c] + e2[c] * v) - e1[c] * u;
+            d2 += d * d;
+        }
+        accum<R, F>(a, kh, nf, sqrt(d2), WG8<R>(i) * WG8<R>(j) * sc_);
+    }
+}
+
+// poly_corr (polygon.c:305-334): 3-point triangle rules on both cells.
+template <typename R, int F>
+__device__ void corr_poly(const Cell &s1, const Cell &s2, const double4 *q1, int n1,
+                          const double4 *q2, int n2, double scale, const R *kh, int nf,
+                          Acc<R, F> &a, int lane)
+{
+    R cd[3];
+    const R zs = s2.mirror ? (R)-1 : (R)1;
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+        cd[c] = (R)(0.5 * (s2.x1[c] + s2.x2[c]) - 0.5 * (s1.x1[c] + s1.x2[c]));
+    const double w1 = (s1.wid > 0) ? s1.wid : 1, w2 = (s2.wid > 0) ? s2.wid : 1;
+    const R sc_ = (R)(scale / (w1 * w2));
+    const int S = n1 * n2;
+    for (int s = lane; s < S; s += 32) {
+        const int k1 = s / n2, k2 = s - k1 * n2;
+        const double4 o1 = q1[k1], o2 = q2[k2];
+        const R dx = (cd[0] + (R)o2.x) - (R)o1.x;
+        const R dy = (cd[1] + (R)o2.y) - (R)o1.y;
+        const R dz = (cd[2] + zs * (R)o2.z) - (R)o1.z;
+        accum<R, F>(a, kh, nf, sqrt(dx * dx + dy * dy + dz * dz), (R)(o1.w * o2.w) * sc_);
+    }
+}
+
+// Correction of neumann_pair_k / neumann_self_k for one (possibly mirrored) pair.
+template <typename R, int F>
+__device__ void corr_pair(const Cell &s1, const Cell &s2, int same, double a1, double a2,
+                          double scale, double kw0, const pb_dev_cells &set, int i1, int i2,
+                          const R *kh, int nf, Acc<R, F> &a, int lane)
+{
+    if (same && s1.wid <= 0 && s1.npv <= 0) {          // partial.c:320-328 (wire self)
+        corr_wire<R, F>(s1, s1, a1, corr_nsub(s1, s1, kw0), scale, kh, nf, a, lane);
+        return;
+    }
+    const int ty = pair_type(s1, s2);
+    if (ty == PT_POLY) {
+        corr_poly<R, F>(s1, s2, set.qpt + set.qoff[i1], set.qoff[i1 + 1] - set.qoff[i1],
+                        set.qpt + set.qoff[i2], set.qoff[i2 + 1] - set.qoff[i2], scale, kh, nf, a, lane);
+    } else if (ty == PT_HL || ty == PT_RIBBON) {
+        corr_ribbon<R, F>(s1, s2, ribbon_nsub(s1, s2, kw0), scale, kh, nf, a, lane);
+    } else {
+        corr_wire<R, F>(s1, s2, 0.5 * (a1 + a2), corr_nsub(s1, s2, kw0), scale, kh, nf, a, lane);
+    }
+}
+
+template <typename R, int F>
+__device__ __forceinline__ void warp_allreduce(Acc<R, F> &a)
+{
+#pragma unroll
+    for (int f = 0; f < F; f++) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            a.re[f] += __shfl_xor_sync(0xffffffffu, a.re[f], o);
+            a.im[f] += __shfl_xor_sync(0xffffffffu, a.im[f], o);
+        }
+    }
+}
+
+// ---------------------------------------------------------------- static kernels
+__global__ void __launch_bounds__(128)
+k_lp_static(pb_fill_geom g, double kw, double *st)
+{
+    const int n = g.seg.n;
+    const long long T = (long long)n * (n + 1) / 2;
+    const double coef = PB_MU0 / (4 * PB_PI);
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < T;
+         t += (long long)gridDim.x * blockDim.x) {
+        int i, j;
+        tri_index(t, n, i, j);
+        Cell si, sj, mj;
+        load_cell(si, g.seg.cell, g.pv, i, 0, g.gpz);
+        const double ai = g.seg.cell[i].aL, aj = g.seg.cell[j].aL;
+        double t1[3], t2[3];
+        tangent(si, t1);
+        double v = 0;
+        if (i == j) {                                   // partial.c:392-401
+            v = static_term(si, si, 1, ai, ai, kw);
+            if (g.gp) {
+                load_cell(mj, g.seg.cell, g.pv, i, 1, g.gpz);
+                const double tdm = t1[0] * t1[0] + t1[1] * t1[1] - t1[2] * t1[2];
+                v -= tdm * static_term(si, mj, 0, ai, ai, kw);
+            }
+        } else {                                        // partial.c:403-423
+            load_cell(sj, g.seg.cell, g.pv, j, 0, g.gpz);
+            tangent(sj, t2);
+            const double tdot = dot3(t1, t2);
+            const double tdm = t1[0] * t2[0] + t1[1] * t2[1] - t1[2] * t2[2];
+            if (tdot != 0) v = tdot * static_term(si, sj, 0, ai, aj, kw);
+            if (g.gp && tdm != 0) {
+                load_cell(mj, g.seg.cell, g.pv, j, 1, g.gpz);
+                v -= tdm * static_term(si, mj, 0, ai, aj, kw);
+            }
+        }
+        st[(long long)i * n + j] = coef * v;
+    }
+}
+
+__global__ void __launch_bounds__(128)
+k_pot_static(pb_fill_geom g, double kw, double *st)
+{
+    const int nc = g.ncell;
+    const long long T = (long long)nc * (nc + 1) / 2;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < T;
+         t += (long long)gridDim.x * blockDim.x) {
+        int ci, cj;
+        tri_index(t, nc, ci, cj);
+        double v = 0;                                   // potential.c:124-150
+        for (int e = g.csoff[ci]; e < g.csoff[ci + 1]; e++) {
+            const int h1 = g.csidx[e];
+            for (int q = g.csoff[cj]; q < g.csoff[cj + 1]; q++) {
+                const int h2 = g.csidx[q];
+                const int a = min(h1, h2), b = max(h1, h2);
+                Cell sa, sb;
+                load_cell(sa, g.chg.cell, g.pv, a, 0, g.gpz);
+                const double aa = g.chg.cell[a].aP, ab = g.chg.cell[b].aP;
+                double x;
+                if (a == b) {
+                    x = static_term(sa, sa, 1, aa, aa, kw);
+                } else {
+                    load_cell(sb, g.chg.cell, g.pv, b, 0, g.gpz);
+                    x = static_term(sa, sb, 0, aa, ab, kw);
+                }
+                if (g.gp) {
+                    load_cell(sb, g.chg.cell, g.pv, b, 1, g.gpz);
+                    x -= static_term(sa, sb, 0, aa, ab, kw);
+                }
+                v += x;
+            }
+        }
+        st[(long long)ci * nc + cj] = v / (4 * PB_PI * PB_EPS0 * g.carea[ci] * g.carea[cj]);
+    }
+}
+
+// ---------------------------------------------------------------- correction kernels
+template <typename R, int F, int EPI>
+__global__ void __launch_bounds__(256)
+k_lp_corr(pb_fill_geom g, KArg k, const double *st, pb_epi_args ea)
+{
+    const int n = g.seg.n;
+    const long long T = (long long)n * (n + 1) / 2;
+    const int lane = threadIdx.x & 31;
+    const double coef = PB_MU0 / (4 * PB_PI);
+    const double kw0 = k.kw[0];
+    const int nf = k.nf;
+    R kh[F];
+#pragma unroll
+    for (int f = 0; f < F; f++) kh[f] = (R)(0.5 * (f < nf ? k.kw[f] : 0.0));
+    const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
+    for (long long t = blockIdx.x * (long long)(blockDim.x >> 5) + (threadIdx.x >> 5); t < T; t += nwarps) {
+        int i, j;
+        tri_index(t, n, i, j);
+        Acc<R, F> acc;
+#pragma unroll
+        for (int f = 0; f < F; f++) { acc.re[f] = 0; acc.im[f] = 0; }
+        if (kw0 > 0) {
+            Cell si, sj;
+            load_cell(si, g.seg.cell, g.pv, i, 0, g.gpz);
+            const double ai = g.seg.cell[i].aL, aj = g.seg.cell[j].aL;
+            double t1[3], t2[3];
+            tangent(si, t1);
+            if (i == j) {
+                corr_pair<R, F>(si, si, 1, ai, ai, coef, kw0, g.seg, i, i, kh, nf, acc, lane);
+                if (g.gp) {
+                    load_cell(sj, g.seg.cell, g.pv, i, 1, g.gpz);
+                    const double tdm = t1[0] * t1[0] + t1[1] * t1[1] - t1[2] * t1[2];
+                    if (tdm != 0)
+                        corr_pair<R, F>(si, sj, 0, ai, ai, -tdm * coef, kw0, g.seg, i, i, kh, nf, acc, lane);
+                }
+            } else {
+                load_cell(sj, g.seg.cell, g.pv, j, 0, g.gpz);
+                tangent(sj, t2);
+                const double tdot = dot3(t1, t2);
+                const double tdm = t1[0] * t2[0] + t1[1] * t2[1] - t1[2] * t2[2];
+                if (tdot != 0)
+                    corr_pair<R, F>(si, sj, 0, ai, aj, tdot * coef, kw0, g.seg, i, j, kh, nf, acc, lane);
+                if (g.gp && tdm != 0) {
+                    load_cell(sj, g.seg.cell, g.pv, j, 1, g.gpz);
+                    corr_pair<R, F>(si, sj, 0, ai, aj, -tdm * coef, kw0, g.seg, i, j, kh, nf, acc, lane);
+                }
+            }
+            warp_allreduce<R, F>(acc);
+        }
+        const double s0 = st[(long long)i * n + j];
+#pragma unroll
+        for (int f = 0; f < F; f++) {
+            if (f == lane && f < nf) {
+                const double lr = s0 + (double)acc.re[f], li = (double)acc.im[f];
+                if (EPI == PB_EPI_STORE) {
+                    double2 *o = ea.out + f * ea.out_stride;
+                    o[(long long)i * n + j] = make_double2(lr, li);
+                    o[(long long)j * n + i] = make_double2(lr, li);
+                } else {
+                    const double om = ea.omega[f];
+                    double vr = -om * om * lr, vi = -om * om * li;
+                    if (i == j) {
+                        const double2 z = ea.zint[f * (long long)n + i];
+                        vr -= om * z.y;
+                        vi += om * z.x;
+                    }
+                    const int nc = g.ncell;
+                    const double2 *P = ea.pm + f * ea.pm_stride;
+                    const int ca = g.seg_ca[i], cb = g.seg_cb[i], da = g.seg_ca[j], db = g.seg_cb[j];
+                    if (ca >= 0 && da >= 0) { const double2 p = P[(long long)ca * nc + da]; vr += p.x; vi += p.y; }
+                    if (ca >= 0 && db >= 0) { const double2 p = P[(long long)ca * nc + db]; vr -= p.x; vi -= p.y; }
+                    if (cb >= 0 && da >= 0) { const double2 p = P[(long long)cb * nc + da]; vr -= p.x; vi -= p.y; }
+                    if (cb >= 0 && db >= 0) { const double2 p = P[(long long)cb * nc + db]; vr += p.x; vi += p.y; }
+                    double2 *m = ea.m64 + f * ea.m_stride;
+                    m[(long long)i * n + j] = make_double2(vr, vi);
+                    m[(long long)j * n + i] = make_double2(vr, vi);
+                    if (ea.m32) {
+                        float2 *m2 = ea.m32 + f * ea.m_stride;
+                        m2[(long long)i * n + j] = make_float2((float)vr, (float)vi);
+                        m2[(long long)j * n + i] = make_float2((float)vr, (float)vi);
+                    }
+                }
+            }
+        }
+    }
+}
+
+template <typename R, int F>
+__global__ void __launch_bounds__(256)
+k_pot_corr(pb_fill_geom g, KArg k, const double *st, double2 *out, long long ostride)
+{
+    const int nc = g.ncell;
+    const long long T = (long long)nc * (nc + 1) / 2;
+    const int lane = threadIdx.x & 31;
+    const double kw0 = k.kw[0];
+    const int nf = k.nf;
+    R kh[F];
+#pragma unroll
+    for (int f = 0; f < F; f++) kh[f] = (R)(0.5 * (f < nf ? k.kw[f] : 0.0));
+    const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
+    for (long long t = blockIdx.x * (long long)(blockDim.x >> 5) + (threadIdx.x >> 5); t < T; t += nwarps) {
+        int ci, cj;
+        tri_index(t, nc, ci, cj);
+        Acc<R, F> acc;
+#pragma unroll
+        for (int f = 0; f < F; f++) { acc.re[f] = 0; acc.im[f] = 0; }
+        const double scale = 1.0 / (4 * PB_PI * PB_EPS0 * g.carea[ci] * g.carea[cj]);
+        if (kw0 > 0) {
+            for (int e = g.csoff[ci]; e < g.csoff[ci + 1]; e++) {
+                const int h1 = g.csidx[e];
+                for (int q = g.csoff[cj]; q < g.csoff[cj + 1]; q++) {
+                    const int h2 = g.csidx[q];
+                    const int a = min(h1, h2), b = max(h1, h2);
+                    Cell sa, sb;
+                    load_cell(sa, g.chg.cell, g.pv, a, 0, g.gpz);
+                    const double aa = g.chg.cell[a].aP, ab = g.chg.cell[b].aP;
+                    if (a == b) {
+                        corr_pair<R, F>(sa, sa, 1, aa, aa, scale, kw0, g.chg, a, a, kh, nf, acc, lane);
+                    } else {
+                        load_cell(sb, g.chg.cell, g.pv, b, 0, g.gpz);
+                        corr_pair<R, F>(sa, sb, 0, aa, ab, scale, kw0, g.chg, a, b, kh, nf, acc, lane);
+                    }
+                    if (g.gp) {
+                        load_cell(sb, g.chg.cell, g.pv, b, 1, g.gpz);
+                        corr_pair<R, F>(sa, sb, 0, aa, ab, -scale, kw0, g.chg, a, b, kh, nf, acc, lane);
+                    }
+                }
+            }
+            warp_allreduce<R, F>(acc);
+        }
+        const double s0 = st[(long long)ci * nc + cj];
+#pragma unroll
+        for (int f = 0; f < F; f++) {
+            if (f == lane && f < nf) {
+                double2 *o = out + f * ostride;
+                const double2 v = make_double2(s0 + (double)acc.re[f], (double)acc.im[f]);
+                o[(long long)ci * nc + cj] = v;
+                o[(long long)cj * nc + ci] = v;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------- internal impedance
+__device__ double2 cdiv_d(double2 a, double2 b)                   // complex.h:40-45
+{
+    if ((fabs(b.x) <= 0) && (fabs(b.y) <= 0)) return make_double2(0, 0);
+    const double d = b.x * b.x + b.y * b.y;
+    return make_double2((a.x * b.x + a.y * b.y) / d, (a.y * b.x - a.x * b.y) / d);
+}
+__device__ __forceinline__ double cabs_d(double2 z) { return sqrt(z.x * z.x + z.y * z.y); }
+
+__device__ double2 i0_over_i1(double2 z)                          // skin.c:23-56
+{
+    if (cabs_d(z) < 15.0) {
+        const double2 z2 = cmul(z, z);
+        double2 i0 = make_double2(1, 0), t = make_double2(1, 0);
+        for (int k = 1; k <= 60; k++) {
+            const double2 u = cmul(t, z2);
+            const double f = 1.0 / (4.0 * k * k);
+            t = make_double2(f * u.x, f * u.y);
+            i0 = cadd(i0, t);
+            if (cabs_d(t) < 1e-17 * cabs_d(i0)) break;
+        }
+        double2 s = make_double2(1, 0);
+        t = make_double2(1, 0);
+        for (int k = 1; k <= 60; k++) {
+            const double2 u = cmul(t, z2);
+            const double f = 1.0 / (4.0 * k * (k + 1));
+            t = make_double2(f * u.x, f * u.y);
+            s = cadd(s, t);
+            if (cabs_d(t) < 1e-17 * cabs_d(s)) break;
+        }
+        return cdiv_d(i0, cmul(make_double2(0.5 * z.x, 0.5 * z.y), s));
+    }
+    const double2 u = cinv(z), u2 = cmul(u, u), u3 = cmul(u2, u);
+    return make_double2(1 + 0.5 * u.x + 0.375 * u2.x + 0.375 * u3.x,
+                        0.5 * u.y + 0.375 * u2.y + 0.375 * u3.y);
+}
+
+__global__ void k_zint(pb_fill_geom g, int skin, int nf, const double *freq, double2 *zint)
+{
+    const int n = g.seg.n;
+    const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (idx >= (long long)n * nf) return;
+    const int f = (int)(idx / n), k = (int)(idx - (long long)f * n);
+    const pb_cell_t *s = &g.seg.cell[k];
+    const double fr = freq[f], om = 2 * PB_PI * fr;
+    double2 z = make_double2(s->res, 0);
+    if (s->diel) {                                     // mna.c:128-138
+        if (s->frelax > 0) {
+            const double2 q = cdiv_d(make_double2(s->epss - s->epsinf, 0), make_double2(1, fr / s->frelax));
+            const double2 er = make_double2(s->epsinf + q.x, q.y);
+            z = cinv(make_double2(om * s->gfac * (-er.y), om * s->gfac * (er.x - 1)));
+        } else {
+            const double2 y = cinv(make_double2(s->gexc, s->cexc));
+            z = make_double2(y.x / om, y.y / om);
+        }
+    } else if (skin) {                                 // skin.c:112-133
+        if (s->vol) {
+            z = make_double2(s->res, 0);
+        } else if (s->shape == PB_SHAPE_ROUND) {       // skin.c:59-77
+            const double len = s->len, a = s->radius, sg = s->sigma;
+            if ((sg <= 0) || (len <= 0) || (a <= 0)) z = make_double2(0, 0);
+            else if (om <= 0) z = make_double2(len / (sg * PB_PI * a * a), 0);
+            else {
+                const double delta = sqrt(2 / (om * PB_MU0 * sg)), q = a / delta;
+                const double2 ratio = i0_over_i1(make_double2(q, q));
+                const double kf = 1 / (2 * PB_PI * a * delta * sg);
+                const double2 zz = cmul(make_double2(kf, kf), ratio);
+                z = make_double2(len * zz.x, len * zz.y);
+            }
+        } else {                                       // skin.c:91-109
+            const double len = s->len, ar = s->area, pe = s->perim, sg = s->sigma;
+            if ((sg <= 0) || (len <= 0) || (ar <= 0) || (pe <= 0)) z = make_double2(0, 0);
+            else if (om <= 0) z = make_double2(len / (sg * ar), 0);
+            else {
+                const double rdc = len / (sg * ar);
+                const double delta = sqrt(2 / (om * PB_MU0 * sg));
+                const double rhf = len / (sg * delta * pe);
+                const double ldc = PB_MU0 * len / (8 * PB_PI), lhf = rhf / om;
+                const double r = sqrt(rdc * rdc + rhf * rhf);
+                const double l = ldc * lhf / sqrt(ldc * ldc + lhf * lhf);
+                z = make_double2(r, om * l);
+            }
+        }
+    }
+    zint[idx] = z;
+}
+
+// ---------------------------------------------------------------- host launchers
+static int grid_for(long long work, int per_block, int blocks_per_sm = 8)
+{
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    long long want = (work + per_block - 1) / per_block;
+    const long long cap = (long long)nsm * blocks_per_sm * 64;
+    if (want > cap) want = cap;
+    if (want < 1) want = 1;
+    return (int)want;
+}
+
+int pb_lp_static(const pb_fill_geom &g, double kw, double *stLp, cudaStream_t s, long *launches)
+{
+    const long long T = (long long)g.seg.n * (g.seg.n + 1) / 2;
+    if (T == 0) return PB_OK;
+    k_lp_static<<<grid_for(T, 128), 128, 0, s>>>(g, kw, stLp);
+    if (launches) (*launches)++;
+    PB_CHECK_LAUNCH();
+    return PB_OK;
+}
+
+int pb_pot_static(const pb_fill_geom &g, double kw, double *stP, cudaStream_t s, long *launches)
+{
+    const long long T = (long long)g.ncell * (g.ncell + 1) / 2;
+    if (T == 0) return PB_OK;
+    k_pot_static<<<grid_for(T, 128), 128, 0, s>>>(g, kw, stP);
+    if (launches) (*launches)++;
+    PB_CHECK_LAUNCH();
+    return PB_OK;
+}
+
+template <typename R, int F>
+static int launch_lp_corr(const pb_fill_geom &g, const KArg &k, const double *st, int epi,
+                          const pb_epi_args &ea, cudaStream_t s)
+{
+    const long long T = (long long)g.seg.n * (g.seg.n + 1) / 2;
+    const int grid = grid_for(T, 8, 8);
+    if (epi == PB_EPI_STORE) k_lp_corr<R, F, PB_EPI_STORE><<<grid, 256, 0, s>>>(g, k, st, ea);
+    else k_lp_corr<R, F, PB_EPI_REDUCED><<<grid, 256, 0, s>>>(g, k, st, ea);
+    PB_CHECK_LAUNCH();
+    return PB_OK;
+}
+
+template <typename R, int F>
+static int launch_pot_corr(const pb_fill_geom &g, const KArg &k, const double *st, double2 *out,
+                           long long ostride, cudaStream_t s)
+{
+    const long long T = (long long)g.ncell * (g.ncell + 1) / 2;
+    k_pot_corr<R, F><<<grid_for(T, 8, 8), 256, 0, s>>>(g, k, st, out, ostride);
+    PB_CHECK_LAUNCH();
+    return PB_OK;
+}
+
+static int pick_f(int nf) { return nf <= 1 ? 1 : nf <= 8 ? 8 : nf <= 16 ? 16 : 32; }
+
+int pb_lp_corr(const pb_fill_geom &g, int nf, const double *kw, int use_fp32, const double *stLp,
+               int epi, const pb_epi_args &ea, cudaStream_t s, long *launches, double *samples)
+{
+    if (g.seg.n == 0) return PB_OK;
+    if (nf < 1 || nf > PB_FMAX) { pb_set_error("pb_lp_corr: bad frequency count %d", nf); return PB_ERR_ARG; }
+    KArg k;
+    for (int f = 0; f < PB_FMAX; f++) k.kw[f] = f < nf ? kw[f] : 0.0;
+    k.nf = nf;
+    const int F = pick_f(nf);
+    int r;
+    if (use_fp32) {
+        r = F == 1 ? launch_lp_corr<float, 1>(g, k, stLp, epi, ea, s)
+          : F == 8 ? launch_lp_corr<float, 8>(g, k, stLp, epi, ea, s)
+          : F == 16 ? launch_lp_corr<float, 16>(g, k, stLp, epi, ea, s)
+                    : launch_lp_corr<float, 32>(g, k, stLp, epi, ea, s);
+    } else {
+        r = F == 1 ? launch_lp_corr<double, 1>(g, k, stLp, epi, ea, s)
+          : F == 8 ? launch_lp_corr<double, 8>(g, k, stLp, epi, ea, s)
+          : F == 16 ? launch_lp_corr<double, 16>(g, k, stLp, epi, ea, s)
+                    : launch_lp_corr<double, 32>(g, k, stLp, epi, ea, s);
+    }
+    if (launches) (*launches)++;
+    (void)samples;
+    return r;
+}
+
+int pb_pot_corr(const pb_fill_geom &g, int nf, const double *kw, int use_fp32, const double *stP,
+                double2 *pout, long long pstride, cudaStream_t s, long *launches, double *samples)
+{
+    if (g.ncell == 0) return PB_OK;
+    if (nf < 1 || nf > PB_FMAX) { pb_set_error("pb_pot_corr: bad frequency count %d", nf); return PB_ERR_ARG; }
+    KArg k;
+    for (int f = 0; f < PB_FMAX; f++) k.kw[f] = f < nf ? kw[f] : 0.0;
+    k.nf = nf;
+    const int F = pick_f(nf);
+    int r;
+    if (use_fp32) {
+        r = F == 1 ? launch_pot_corr<float, 1>(g, k, stP, pout, pstride, s)
+          : F == 8 ? launch_pot_corr<float, 8>(g, k, stP, pout, pstride, s)
+          : F == 16 ? launch_pot_corr<float, 16>(g, k, stP, pout, pstride, s)
+                    : launch_pot_corr<float, 32>(g, k, stP, pout, pstride, s);
+    } else {
+        r = F == 1 ? launch_pot_corr<double, 1>(g, k, stP, pout, pstride, s)
+          : F == 8 ? launch_pot_corr<double, 8>(g, k, stP, pout, pstride, s)
+          : F == 16 ? launch_pot_corr<double, 16>(g, k, stP, pout, pstride, s)
+                    : launch_pot_corr<double, 32>(g, k, stP, pout, pstride, s);
+    }
+    if (launches) (*launches)++;
+    (void)samples;
+    return r;
+}
+
+int pb_zint(const pb_fill_geom &g, int skin, int nf, const double *freq, double2 *zint,
+            cudaStream_t s, long *launches)
+{
+    const long long T = (long long)g.seg.n * nf;
+    if (T == 0) return PB_OK;
+    k_zint<<<ceil_div(T, 128), 128, 0, s>>>(g, skin, nf, freq, zint);
+    if (launches) (*launches)++;
+    PB_CHECK_LAUNCH();
+    return PB_OK;
+}
+
+// ---------------------------------------------------------------- poly point sets
+// cell_qpts(s, nsub=1, n7=0) of polygon.c:224-268 computed on the host once per
+// geometry, stored as offsets from the cell centre 0.5*(x1+x2). Degenerate fan
+// triangles keep their slots with zero weight (their samples contribute exactly 0).
+static void host_qpts(const pb_cell_t &c, const double *pool, std::vector<double> &out)
+{
+    static const double XG4h[4] = {-0.8611363115940526, -0.3399810435848563, 0.3399810435848563, 0.8611363115940526};
+    static const double WG4h[4] = {0.3478548451374538, 0.6521451548625461, 0.6521451548625461, 0.3478548451374538};
+    static const double TB3h[3][3] = {{2.0 / 3, 1.0 / 6, 1.0 / 6}, {1.0 / 6, 2.0 / 3, 1.0 / 6}, {1.0 / 6, 1.0 / 6, 2.0 / 3}};
+    double cen[3];
+    for (int i = 0; i < 3; i++) cen[i] = 0.5 * (c.x1[i] + c.x2[i]);
+    auto push = [&](const double *p, double w) {
+        out.push_back(p[0] - cen[0]); out.push_back(p[1] - cen[1]);
+        out.push_back(p[2] - cen[2]); out.push_back(w);
+    };
+    if (c.npv > 0) {
+        const double *pv = pool + 3 * (long long)c.pvoff;
+        for (int k = 0; k < c.npv; k++) {
+            const double *b = &pv[3 * k], *cc = &pv[3 * ((k + 1) % c.npv)], *a = c.papex;
+            double u[3], v[3], w[3];
+            for (int i = 0; i < 3; i++) { u[i] = b[i] - a[i]; v[i] = cc[i] - a[i]; }
+            w[0] = u[1] * v[2] - u[2] * v[1];
+            w[1] = u[2] * v[0] - u[0] * v[2];
+            w[2] = u[0] * v[1] - u[1] * v[0];
+            const double at = 0.5 * sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+            for (int q = 0; q < 3; q++) {
+                double px[3];
+                for (int i = 0; i < 3; i++) px[i] = TB3h[q][0] * a[i] + TB3h[q][1] * b[i] + TB3h[q][2] * cc[i];
+                push(px, at > 0 ? (1.0 / 3) * at : 0.0);
+            }
+        }
+        return;
+    }
+    if (c.wid <= 0) {
+        for (int q = 0; q < 4; q++) {
+            const double u = 0.5 * (1 + XG4h[q]);
+            double px[3];
+            for (int i = 0; i < 3; i++) px[i] = c.x1[i] + (c.x2[i] - c.x1[i]) * u;
+            push(px, 0.5 * WG4h[q] * c.len);
+        }
+        return;
+    }
+    double t[3];
+    for (int i = 0; i < 3; i++) t[i] = (c.x2[i] - c.x1[i]) / c.len;
+    for (int q = 0; q < 4; q++) {
+        const double a = c.len * (0.5 * (1 + XG4h[q]) - 0.5);
+        for (int j = 0; j < 4; j++) {
+            const double b = c.wid * (0.5 * XG4h[j]);
+            double px[3];
+            for (int i = 0; i < 3; i++) px[i] = cen[i] + a * t[i] + b * c.wv[i];
+            push(px, 0.25 * WG4h[q] * WG4h[j] * c.len * c.wid);
+        }
+    }
+}
+
+int pb_build_qpts(pb_dev_cells &c, const pb_cell_t *host_cells, const double *pv_host,
+                  const double *pv_dev, cudaStream_t s)
+{
+    (void)pv_dev;
+    std::vector<double> pts;
+    std::vector<int> off(c.n + 1, 0);
+    for (int i = 0; i < c.n; i++) {
+        host_qpts(host_cells[i], pv_host, pts);
+        off[i + 1] = (int)(pts.size() / 4);
+    }
+    PB_CUDA(cudaMalloc(&c.qoff, sizeof(int) * (c.n + 1)));
+    PB_CUDA(cudaMalloc(&c.qpt, sizeof(double4) * (pts.size() / 4 + 1)));
+    PB_CUDA(cudaMemcpyAsync(c.qoff, off.data(), sizeof(int) * (c.n + 1), cudaMemcpyHostToDevice, s));
+    if (!pts.empty())
+        PB_CUDA(cudaMemcpyAsync(c.qpt, pts.data(), sizeof(double) * pts.size(), cudaMemcpyHostToDevice, s));
+    PB_CUDA(cudaStreamSynchronize(s));
+    return PB_OK;
+}

@@ -1,0 +1,67 @@
+// pb_fill.cuh — partial-element fill on the device.
+#pragma once
+#include "pb_common.cuh"
+
+// Device-resident discretisation of one structure.
+struct pb_dev_cells {
+    int n = 0;
+    pb_cell_t *cell = nullptr;      // [n]
+    double4 *qpt = nullptr;         // 3-point poly-corr point sets, offsets from centre + weight
+    int *qoff = nullptr;            // [n+1]
+};
+
+struct pb_fill_geom {
+    pb_dev_cells seg, chg;
+    double *pv = nullptr;           // shared polygon vertex pool [3*npv]
+    int gp = 0;
+    double gpz = 0;
+    int any_poly = 0;
+    // charge cells grouped by node (potential.c:29-114)
+    int ncell = 0;
+    int *csoff = nullptr, *csidx = nullptr;   // [ncell+1], [nchg]
+    double *carea = nullptr;                   // [ncell]
+    // reduced form: cell index of each segment's end nodes (-1 = reference node)
+    int *seg_ca = nullptr, *seg_cb = nullptr;  // [nseg]
+};
+
+#define PB_FMAX 32
+
+// Epilogue of the Lp correction kernel.
+enum { PB_EPI_STORE = 0, PB_EPI_REDUCED = 1 };
+
+struct pb_epi_args {
+    // STORE: out[f][i][j] (both triangles), FP64 complex, stride per frequency
+    double2 *out = nullptr;
+    long long out_stride = 0;
+    // REDUCED: M'(f) = j w zint - w^2 Lp + G^T P G (FP64 and optional FP32 copy)
+    double2 *m64 = nullptr;
+    float2 *m32 = nullptr;
+    long long m_stride = 0;
+    const double2 *pm = nullptr;    // P(f) [f][ncell][ncell]
+    long long pm_stride = 0;
+    const double2 *zint = nullptr;  // [f][nseg]
+    double omega[PB_FMAX];
+};
+
+// FP64 static tables: stLp[i*n+j] (i <= j) = coef * sum_terms weight * static;
+// stP[ci*nc+cj] (ci <= cj) likewise for P.
+int pb_lp_static(const pb_fill_geom &g, double kw, double *stLp, cudaStream_t s, long *launches);
+int pb_pot_static(const pb_fill_geom &g, double kw, double *stP, cudaStream_t s, long *launches);
+
+// Correction kernels for nf <= PB_FMAX wavenumbers (kw[f] > 0). use_fp32 selects the
+// FP32 quadrature (mixed path) or FP64 (plain path). With kw == 0 (quasi-static) pass
+// nf = 1, kw[0] = 0: only the static table is copied through the epilogue.
+int pb_lp_corr(const pb_fill_geom &g, int nf, const double *kw, int use_fp32,
+               const double *stLp, int epi, const pb_epi_args &ea, cudaStream_t s,
+               long *launches, double *samples);
+int pb_pot_corr(const pb_fill_geom &g, int nf, const double *kw, int use_fp32,
+                const double *stP, double2 *pout, long long pstride, cudaStream_t s,
+                long *launches, double *samples);
+
+// Internal impedance per segment (skin.c:112-133, mna.c:128-138, mna.c:254-258).
+int pb_zint(const pb_fill_geom &g, int skin, int nf, const double *freq, double2 *zint,
+            cudaStream_t s, long *launches);
+
+// Poly-corr point sets (cell_qpts(s, 1, 0), polygon.c:224-268) for a cell set.
+int pb_build_qpts(pb_dev_cells &c, const pb_cell_t *host_cells, const double *pv_host,
+                  const double *pv_dev, cudaStream_t s);

@@ -1,0 +1,599 @@
+// pb_lu.cu — batched dense complex LU with partial pivoting, for many frequencies at
+// once, plus the triangular solves and the FP64 residual used by iterative refinement.
+//
+// Algorithm: recursive (Toledo) right-looking LU over column halves. Leaves of up to
+// 32 columns are factored by one CTA per matrix that keeps SW columns of the panel in
+// shared memory (pivot search = block argmax of |re|+|im| with first-index tie-break,
+// the reference's rule in src/lu.c:19-30); everything above the leaves is row swaps,
+// a unit-lower triangular solve and a complex GEMM trailing update.
+// Row-major storage, like the reference (a[i*n+j]).
+#include "pb_lu.cuh"
+#include <climits>
+#include <cuComplex.h>
+
+template <typename T> using T2_t = typename cplx_t<T>::type;
+
+// ---------------------------------------------------------------- block argmax
+__device__ __forceinline__ void argmax_pair(double &m, int &i, double m2, int i2)
+{
+    if (m2 > m || (m2 == m && i2 < i)) { m = m2; i = i2; }
+}
+
+// Block-wide argmax; result broadcast to all threads. Caller must __syncthreads()
+// before reusing sm/si.
+__device__ void block_argmax(double &m, int &i, double *sm, int *si)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double m2 = __shfl_down_sync(0xffffffffu, m, o);
+        const int i2 = __shfl_down_sync(0xffffffffu, i, o);
+        argmax_pair(m, i, m2, i2);
+    }
+    if (lane == 0) { sm[warp] = m; si[warp] = i; }
+    __syncthreads();
+    if (warp == 0) {
+        m = (lane < nw) ? sm[lane] : -1.0;
+        i = (lane < nw) ? si[lane] : INT_MAX;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double m2 = __shfl_down_sync(0xffffffffu, m, o);
+            const int i2 = __shfl_down_sync(0xffffffffu, i, o);
+            argmax_pair(m, i, m2, i2);
+        }
+        if (lane == 0) { sm[32] = m; si[32] = i; }
+    }
+    __syncthreads();
+    m = sm[32];
+    i = si[32];
+}
+
+// 1/z with scaling so that |z|^2 cannot under/overflow in FP32.
+template <typename T2> __device__ __forceinline__ T2 safe_inv(T2 z)
+{
+    const auto s = fmax(fabs((double)z.x), fabs((double)z.y));
+    if (s <= 0) return mk2<T2>(0, 0);
+    const double zr = z.x / s, zi = z.y / s;
+    const double d = (zr * zr + zi * zi) * s;
+    return mk2<T2>(zr / d, -zi / d);
+}
+
+// ---------------------------------------------------------------- leaf panel
+// Factor columns [k0, k0+w) (w <= 32) over rows [k0, n) of matrix blockIdx.x, SW
+// columns at a time in shared memory. Swaps are applied to the leaf's own columns only.
+template <typename T, int SW>
+__global__ void __launch_bounds__(1024)
+k_lu_leaf(T2_t<T> *a, int n, int ld, long long stride, int k0, int w, int *piv, int *info)
+{
+    typedef T2_t<T> T2;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    __shared__ double red_m[33];
+    __shared__ int red_i[33];
+    const int m = n - k0;
+    T2 *sp = reinterpret_cast<T2 *>(smraw);       // [m][SW]
+    T2 *urow = sp + (size_t)m * SW;                // [SW][32]
+    const int b = blockIdx.x, tid = threadIdx.x, nt = blockDim.x;
+    a += (long long)b * stride;
+    piv += (long long)b * n;
+
+    for (int s0 = 0; s0 < w; s0 += SW) {
+        const int sw = min(SW, w - s0), c0 = k0 + s0;
+        for (int e = tid; e < m * sw; e += nt) {
+            const int r = e / sw, t = e - r * sw;
+            sp[r * SW + t] = a[(long long)(k0 + r) * ld + c0 + t];
+        }
+        __syncthreads();
+        for (int t = 0; t < sw; t++) {
+            const int c = c0 + t;
+            double bm = -1.0;
+            int bi = INT_MAX;
+            for (int r = c + tid; r < n; r += nt) {
+                const double mm = cmag1(sp[(r - k0) * SW + t]);
+                if (mm > bm) { bm = mm; bi = r; }
+            }
+            block_argmax(bm, bi, red_m, red_i);
+            const int ip = (bi == INT_MAX) ? c : bi;
+            if (tid == 0) {
+                piv[c] = ip;
+                if (bm < 1e-30 && info[b] < 0) info[b] = c;
+            }
+            if (ip != c) {
+                for (int e = tid; e < w; e += nt) {
+                    const int col = k0 + e;
+                    if (col >= c0 && col < c0 + sw) {
+                        T2 *x = &sp[(c - k0) * SW + (col - c0)], *y = &sp[(ip - k0) * SW + (col - c0)];
+                        const T2 tmp = *x; *x = *y; *y = tmp;
+                    } else {
+                        T2 *x = &a[(long long)c * ld + col], *y = &a[(long long)ip * ld + col];
+                        const T2 tmp = *x; *x = *y; *y = tmp;
+                    }
+                }
+            }
+            __syncthreads();
+            const T2 pinv = safe_inv(sp[(c - k0) * SW + t]);
+            for (int r = c + 1 + tid; r < n; r += nt) {
+                T2 *row = &sp[(r - k0) * SW];
+                const T2 l = cmul(row[t], pinv);
+                row[t] = l;
+                for (int tt = t + 1; tt < sw; tt++) row[tt] = cfms(row[tt], l, sp[(c - k0) * SW + tt]);
+            }
+            __syncthreads();
+        }
+        for (int e = tid; e < m * sw; e += nt) {
+            const int r = e / sw, t = e - r * sw;
+            a[(long long)(k0 + r) * ld + c0 + t] = sp[r * SW + t];
+        }
+        const int c1 = c0 + sw, nr = k0 + w - c1;
+        if (nr > 0) {
+            // U rows of this sub-panel for the remaining leaf columns
+            for (int col = c1 + tid; col < k0 + w; col += nt) {
+                for (int t = 0; t < sw; t++) {
+                    T2 v = a[(long long)(c0 + t) * ld + col];
+                    for (int tp = 0; tp < t; tp++)
+                        v = cfms(v, sp[(c0 + t - k0) * SW + tp], urow[tp * 32 + (col - c1)]);
+                    urow[t * 32 + (col - c1)] = v;
+                    a[(long long)(c0 + t) * ld + col] = v;
+                }
+            }
+            __syncthreads();
+            const long long tot = (long long)(n - c1) * nr;
+            for (long long e = tid; e < tot; e += nt) {
+                const int r = c1 + (int)(e / nr), col = c1 + (int)(e % nr);
+                T2 v = a[(long long)r * ld + col];
+#pragma unroll
+                for (int t = 0; t < SW; t++)
+                    if (t < sw) v = cfms(v, sp[(r - k0) * SW + t], urow[t * 32 + (col - c1)]);
+                a[(long long)r * ld + col] = v;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------- row swaps
+template <typename T>
+__global__ void k_swap_rows(T2_t<T> *a, int ld, long long stride, const int *piv, int n,
+                            int r0, int r1, int c0, int c1)
+{
+    typedef T2_t<T> T2;
+    const int col = c0 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= c1) return;
+    const int b = blockIdx.y;
+    a += (long long)b * stride;
+    piv += (long long)b * n;
+    for (int r = r0; r < r1; r++) {
+        const int p = piv[r];
+        if (p != r) {
+            T2 *x = &a[(long long)r * ld + col], *y = &a[(long long)p * ld + col];
+            const T2 t = *x; *x = *y; *y = t;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- small TRSM
+// X = L^-1 B, L unit lower w x w (w <= 64) at a[r0.., r0..], B = a[r0..r0+w, c0..c1).
+template <typename T>
+__global__ void __launch_bounds__(64)
+k_trsm_small(T2_t<T> *a, int ld, long long stride, int r0, int w, int c0, int c1)
+{
+    typedef T2_t<T> T2;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    T2 *L = reinterpret_cast<T2 *>(smraw);      // [w][w]
+    T2 *X = L + w * w;                            // [w][64]
+    const int b = blockIdx.y, tid = threadIdx.x;
+    a += (long long)b * stride;
+    const int cb = c0 + blockIdx.x * 64;
+    for (int e = tid; e < w * w; e += 64) {
+        const int r = e / w, c = e - r * w;
+        L[e] = (c < r) ? a[(long long)(r0 + r) * ld + r0 + c] : mk2<T2>(0, 0);
+    }
+    for (int e = tid; e < w * 64; e += 64) {
+        const int r = e / 64, c = e - r * 64;
+        X[e] = (cb + c < c1) ? a[(long long)(r0 + r) * ld + cb + c] : mk2<T2>(0, 0);
+    }
+    __syncthreads();
+    if (cb + tid < c1) {
+        for (int r = 1; r < w; r++) {
+            T2 v = X[r * 64 + tid];
+            for (int c = 0; c < r; c++) v = cfms(v, L[r * w + c], X[c * 64 + tid]);
+            X[r * 64 + tid] = v;
+        }
+        for (int r = 0; r < w; r++) a[(long long)(r0 + r) * ld + cb + tid] = X[r * 64 + tid];
+    }
+}
+
+// ---------------------------------------------------------------- GEMM wrapper
+// C(m x nc) -= A(m x k) * B(k x nc), row-major, batched with strides.
+template <typename T>
+static int gemm_sub(pb_lu_engine *e, int m, int nc, int k, const T2_t<T> *A, int lda,
+                    const T2_t<T> *B, int ldb, T2_t<T> *Cm, int ldc, long long stride, int nb);
+
+template <>
+int gemm_sub<double>(pb_lu_engine *e, int m, int nc, int k, const double2 *A, int lda,
+                     const double2 *B, int ldb, double2 *Cm, int ldc, long long stride, int nb)
+{
+    if (m <= 0 || nc <= 0 || k <= 0) return PB_OK;
+    const cuDoubleComplex alpha = make_cuDoubleComplex(-1, 0), beta = make_cuDoubleComplex(1, 0);
+    cublasStatus_t s = cublasZgemmStridedBatched(
+        e->blas, CUBLAS_OP_N, CUBLAS_OP_N, nc, m, k, &alpha,
+        (const cuDoubleComplex *)B, ldb, stride, (const cuDoubleComplex *)A, lda, stride, &beta,
+        (cuDoubleComplex *)Cm, ldc, stride, nb);
+    e->launches++;
+    if (s != CUBLAS_STATUS_SUCCESS) { pb_set_error("cublasZgemmStridedBatched failed (%d)", (int)s); return PB_ERR_CUDA; }
+    return PB_OK;
+}
+
+template <>
+int gemm_sub<float>(pb_lu_engine *e, int m, int nc, int k, const float2 *A, int lda,
+                    const float2 *B, int ldb, float2 *Cm, int ldc, long long stride, int nb)
+{
+    if (m <= 0 || nc <= 0 || k <= 0) return PB_OK;
+    const cuComplex alpha = make_cuComplex(-1, 0), beta = make_cuComplex(1, 0);
+    cublasStatus_t s;
+    if (e->gemm_kind == PB_GEMM_TC) {
+        s = cublasGemmStridedBatchedEx(
+            e->blas, CUBLAS_OP_N, CUBLAS_OP_N, nc, m, k, &alpha, B, CUDA_C_32F, ldb, stride,
+            A, CUDA_C_32F, lda, stride, &beta, Cm, CUDA_C_32F, ldc, stride, nb,
+            (cublasComputeType_t)e->tc_compute, CUBLAS_GEMM_DEFAULT);
+    } else {
+        s = cublasCgemmStridedBatched(
+            e->blas, CUBLAS_OP_N, CUBLAS_OP_N, nc, m, k, &alpha, (const cuComplex *)B, ldb,
+            stride, (const cuComplex *)A, lda, stride, &beta, (cuComplex *)Cm, ldc, stride, nb);
+    }
+    e->launches++;
+    if (s != CUBLAS_STATUS_SUCCESS) { pb_set_error("complex FP32 GEMM failed (%d)", (int)s); return PB_ERR_CUDA; }
+    return PB_OK;
+}
+
+int pb_lu_engine_init(pb_lu_engine *e, cudaStream_t s)
+{
+    e->stream = s;
+    if (cublasCreate(&e->blas) != CUBLAS_STATUS_SUCCESS) {
+        pb_set_error("cublasCreate failed");
+        return PB_ERR_CUDA;
+    }
+    cublasSetStream(e->blas, s);
+    cublasSetMathMode(e->blas, CUBLAS_PEDANTIC_MATH);
+    e->tc_compute = (int)CUBLAS_COMPUTE_32F_EMULATED_16BFX9;
+    return PB_OK;
+}
+
+void pb_lu_engine_free(pb_lu_engine *e)
+{
+    if (e->blas) cublasDestroy(e->blas);
+    e->blas = nullptr;
+}
+
+// ---------------------------------------------------------------- recursion
+template <typename T> static int leaf_sw(int m, size_t *smem)
+{
+    int dev = 0, cap = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&cap, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    const size_t avail = (size_t)cap - 1024;
+    const size_t es = sizeof(T2_t<T>);
+    for (int sw = 4; sw >= 1; sw >>= 1) {
+        const size_t need = ((size_t)m * sw + (size_t)sw * 32) * es;
+        if (need <= avail) { *smem = need; return sw; }
+    }
+    return 0;
+}
+
+template <typename T, int SW>
+static int launch_leaf(pb_lu_engine *e, T2_t<T> *a, int n, int ld, long long stride, int nb,
+                       int k0, int w, int *piv, int *info, size_t smem)
+{
+    static bool attr_set = false;
+    if (!attr_set) {
+        int dev = 0, cap = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&cap, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        PB_CUDA(cudaFuncSetAttribute(k_lu_leaf<T, SW>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap - 1024));
+        attr_set = true;
+    }
+    k_lu_leaf<T, SW><<<nb, 1024, smem, e->stream>>>(a, n, ld, stride, k0, w, piv, info);
+    e->launches++;
+    PB_CHECK_LAUNCH();
+    return PB_OK;
+}
+
+template <typename T>
+static int swap_rows(pb_lu_engine *e, T2_t<T> *a, int n, int ld, long long stride, int nb,
+                     const int *piv, int r0, int r1, int c0, int c1)
+{
+    if (c1 <= c0 || r1 <= r0) return PB_OK;
+    dim3 g(ceil_div(c1 - c0, 128), nb);
+    k_swap_rows<T><<<g, 128, 0, e->stream>>>(a, ld, stride, piv, n, r0, r1, c0, c1);
+    e->launches++;
+    PB_CHECK_LAUNCH();
+    return PB_OK;
+}
+
+template <typename T>
+static int trsm_rec(pb_lu_engine *e, T2_t<T> *a, int ld, long long stride, int nb, int r0,
+                    int w, int c0, int c1)
+{
+    if (c1 <= c0 || w <= 0) return PB_OK;
+    if (w <= 64) {
+        static bool attr_set = false;
+        if (!attr_set) {
+            PB_CUDA(cudaFuncSetAttribute(k_trsm_small<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (64 * 64 + 64 * 64) * (int)sizeof(T2_t<T>)));
+            attr_set = true;
+        }
+        const size_t smem = (size_t)(w * w + w * 64) * sizeof(T2_t<T>);
+        dim3 g(ceil_div(c1 - c0, 64), nb);
+        k_trsm_small<T><<<g, 64, smem, e->stream>>>(a, ld, stride, r0, w, c0, c1);
+        e->launches++;
+        PB_CHECK_LAUNCH();
+        return PB_OK;
+    }
+    const int w1 = ((w / 2 + 31) / 32) * 32;
+    PB_TRY(trsm_rec<T>(e, a, ld, stride, nb, r0, w1, c0, c1));
+    PB_TRY(gemm_sub<T>(e, w - w1, c1 - c0, w1, a + (long long)(r0 + w1) * ld + r0, ld,
+                       a + (long long)r0 * ld + c0, ld, a + (long long)(r0 + w1) * ld + c0, ld,
+                       stride, nb));
+    return trsm_rec<T>(e, a, ld, stride, nb, r0 + w1, w - w1, c0, c1);
+}
+
+template <typename T>
+static int lu_rec(pb_lu_engine *e, T2_t<T> *a, int n, int ld, long long stride, int nb,
+                  int k0, int w, int *piv, int *info, int sw, size_t smem)
+{
+    if (w <= 32) {
+        if (sw == 4) return launch_leaf<T, 4>(e, a, n, ld, stride, nb, k0, w, piv, info, smem);
+        if (sw == 2) return launch_leaf<T, 2>(e, a, n, ld, stride, nb, k0, w, piv, info, smem);
+        return launch_leaf<T, 1>(e, a, n, ld, stride, nb, k0, w, piv, info, smem);
+    }
+    const int w1 = ((w / 2 + 31) / 32) * 32;
+    PB_TRY(lu_rec<T>(e, a, n, ld, stride, nb, k0, w1, piv, info, sw, smem));
+    PB_TRY(swap_rows<T>(e, a, n, ld, stride, nb, piv, k0, k0 + w1, k0 + w1, k0 + w));
+    PB_TRY(trsm_rec<T>(e, a, ld, stride, nb, k0, w1, k0 + w1, k0 + w));
+    PB_TRY(gemm_sub<T>(e, n - k0 - w1, w - w1, w1, a + (long long)(k0 + w1) * ld + k0, ld,
+                       a + (long long)k0 * ld + k0 + w1, ld,
+                       a + (long long)(k0 + w1) * ld + k0 + w1, ld, stride, nb));
+    PB_TRY(lu_rec<T>(e, a, n, ld, stride, nb, k0 + w1, w - w1, piv, info, sw, smem));
+    return swap_rows<T>(e, a, n, ld, stride, nb, piv, k0 + w1, k0 + w, k0, k0 + w1);
+}
+
+__global__ void k_fill_int(int *p, int v, int n)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = v;
+}
+
+template <typename T>
+int pb_lu_factor(pb_lu_engine *e, int n, int nb, T2_t<T> *a, int ld, long stride, int *piv,
+                 int *info)
+{
+    if (n <= 0 || nb <= 0) return PB_OK;
+    k_fill_int<<<ceil_div(nb, 256), 256, 0, e->stream>>>(info, -1, nb);
+    e->launches++;
+    size_t smem = 0;
+    const int sw = leaf_sw<T>(n, &smem);
+    if (sw == 0) {
+        pb_set_error("LU order %d exceeds the shared-memory panel capacity of this build", n);
+        return PB_ERR_UNSUP;
+    }
+    return lu_rec<T>(e, a, n, ld, stride, nb, 0, n, piv, info, sw, smem);
+}
+template int pb_lu_factor<float>(pb_lu_engine *, int, int, float2 *, int, long, int *, int *);
+template int pb_lu_factor<double>(pb_lu_engine *, int, int, double2 *, int, long, int *, int *);
+
+// ---------------------------------------------------------------- permutation
+__global__ void k_perm(const int *piv, int *perm, int n, int nb)
+{
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb) return;
+    const int *p = piv + (long long)b * n;
+    int *q = perm + (long long)b * n;
+    for (int i = 0; i < n; i++) q[i] = i;
+    for (int k = 0; k < n; k++) {
+        const int j = p[k];
+        if (j != k) { const int t = q[k]; q[k] = q[j]; q[j] = t; }
+    }
+}
+
+int pb_lu_perm(pb_lu_engine *e, int n, int nb, const int *piv, int *perm)
+{
+    k_perm<<<ceil_div(nb, 64), 64, 0, e->stream>>>(piv, perm, n, nb);
+    e->launches++;
+    PB_CHECK_LAUNCH();
+    return PB_OK;
+}
+
+// ---------------------------------------------------------------- triangular solves
+// One CTA (1024 threads) per (rhs, matrix). The whole vector lives in shared memory.
+template <typename TF>
+__global__ void __launch_bounds__(1024)
+k_lu_solve(const T2_t<TF> *lu, int n, int ld, long long stride, const int *perm,
+           const double2 *r, double2 *x, int nrhs)
+{
+    typedef T2_t<TF> T2;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    T2 *xs = reinterpret_cast<T2 *>(smraw);        // [n]
+    __shared__ T2 diag[32][33];
+    __shared__ T2 tmp[32];
+    __shared__ double red[33];
+    const int rhs = blockIdx.x, b = blockIdx.y, tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    lu += (long long)b * stride;
+    perm += (long long)b * n;
+    const double2 *rv = r + ((long long)b * nrhs + rhs) * n;
+    double2 *xv = x + ((long long)b * nrhs + rhs) * n;
+
+    // scale by max |component|
+    double mx = 0;
+    for (int i = tid; i < n; i += blockDim.x) mx = fmax(mx, fmax(fabs(rv[i].x), fabs(rv[i].y)));
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, o));
+    if (lane == 0) red[warp] = mx;
+    __syncthreads();
+    if (tid == 0) {
+        double t = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t = fmax(t, red[w]);
+        red[32] = t;
+    }
+    __syncthreads();
+    const double scale = red[32] > 0 ? red[32] : 1.0;
+    for (int i = tid; i < n; i += blockDim.x) {
+        const double2 v = rv[perm[i]];
+        xs[i] = mk2<T2>(v.x / scale, v.y / scale);
+    }
+    __syncthreads();
+
+    // forward: unit lower
+    for (int r0 = 0; r0 < n; r0 += 32) {
+        const int r = r0 + warp;
+        if (r < n) {
+            const T2 *row = lu + (long long)r * ld;
+            T2 acc = mk2<T2>(0, 0);
+            for (int c = lane; c < r0; c += 32) acc = cadd(acc, cmul(row[c], xs[c]));
+            for (int o = 16; o > 0; o >>= 1) {
+                acc.x += __shfl_down_sync(0xffffffffu, acc.x, o);
+                acc.y += __shfl_down_sync(0xffffffffu, acc.y, o);
+            }
+            if (lane == 0) tmp[warp] = csub(xs[r], acc);
+            diag[warp][lane] = (r0 + lane < n) ? row[r0 + lane] : mk2<T2>(0, 0);
+        }
+        __syncthreads();
+        if (warp == 0) {
+            const int nbk = min(32, n - r0);
+            T2 xl = mk2<T2>(0, 0);               // lane l holds x[r0+l] once solved
+            for (int i = 0; i < nbk; i++) {
+                T2 p = (lane < i) ? cmul(diag[i][lane], xl) : mk2<T2>(0, 0);
+                for (int o = 16; o > 0; o >>= 1) {
+                    p.x += __shfl_xor_sync(0xffffffffu, p.x, o);
+                    p.y += __shfl_xor_sync(0xffffffffu, p.y, o);
+                }
+                const T2 v = csub(tmp[i], p);
+                if (lane == i) xl = v;
+            }
+            if (lane < nbk) xs[r0 + lane] = xl;
+        }
+        __syncthreads();
+    }
+    // backward: upper with diagonal
+    const int nblk = (n + 31) / 32;
+    for (int bk = nblk - 1; bk >= 0; bk--) {
+        const int r0 = bk * 32, nbk = min(32, n - r0);
+        const int r = r0 + warp;
+        if (warp < nbk) {
+            const T2 *row = lu + (long long)r * ld;
+            T2 acc = mk2<T2>(0, 0);
+            for (int c = r0 + 32 + lane; c < n; c += 32) acc = cadd(acc, cmul(row[c], xs[c]));
+            for (int o = 16; o > 0; o >>= 1) {
+                acc.x += __shfl_down_sync(0xffffffffu, acc.x, o);
+                acc.y += __shfl_down_sync(0xffffffffu, acc.y, o);
+            }
+            if (lane == 0) tmp[warp] = csub(xs[r], acc);
+            diag[warp][lane] = (lane < nbk) ? row[r0 + lane] : mk2<T2>(0, 0);
+        }
+        __syncthreads();
+        if (warp == 0) {
+            T2 xl = mk2<T2>(0, 0);
+            for (int i = nbk - 1; i >= 0; i--) {
+                T2 p = (lane > i && lane < nbk) ? cmul(diag[i][lane], xl) : mk2<T2>(0, 0);
+                for (int o = 16; o > 0; o >>= 1) {
+                    p.x += __shfl_xor_sync(0xffffffffu, p.x, o);
+                    p.y += __shfl_xor_sync(0xffffffffu, p.y, o);
+                }
+                const T2 v = cmul(csub(tmp[i], p), safe_inv(diag[i][i]));
+                if (lane == i) xl = v;
+            }
+            if (lane < nbk) xs[r0 + lane] = xl;
+        }
+        __syncthreads();
+    }
+    for (int i = tid; i < n; i += blockDim.x)
+        xv[i] = make_double2((double)xs[i].x * scale, (double)xs[i].y * scale);
+}
+
+template <typename TF>
+int pb_lu_solve_batched(pb_lu_engine *e, int n, int nb, int nrhs, const T2_t<TF> *lu, int ld,
+                        long stride, const int *perm, const double2 *r, double2 *x)
+{
+    const size_t smem = (size_t)n * sizeof(T2_t<TF>);
+    static bool attr_set = false;
+    if (!attr_set) {
+        int dev = 0, cap = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&cap, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        PB_CUDA(cudaFuncSetAttribute(k_lu_solve<TF>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap - 20480));
+        attr_set = true;
+    }
+    dim3 g(nrhs, nb);
+    k_lu_solve<TF><<<g, 1024, smem, e->stream>>>(lu, n, ld, stride, perm, r, x, nrhs);
+    e->launches++;
+    PB_CHECK_LAUNCH();
+    return PB_OK;
+}
+template int pb_lu_solve_batched<float>(pb_lu_engine *, int, int, int, const float2 *, int, long, const int *, const double2 *, double2 *);
+template int pb_lu_solve_batched<double>(pb_lu_engine *, int, int, int, const double2 *, int, long, const int *, const double2 *, double2 *);
+
+// ---------------------------------------------------------------- FP64 residual
+// r = b - A x ; 8 warps per block, each warp one row at a time; x staged in smem.
+__device__ __forceinline__ void atomic_max_pos(double *addr, double v)
+{
+    // non-negative doubles order like their bit patterns
+    atomicMax(reinterpret_cast<unsigned long long *>(addr), (unsigned long long)__double_as_longlong(v));
+}
+
+__global__ void __launch_bounds__(256)
+k_residual(const double2 *a, int n, int ld, long long stride, const double2 *bv,
+           const double2 *xv, double2 *rv, double *rn, double *bn, int nrhs, int rows_per_block)
+{
+    extern __shared__ __align__(16) unsigned char smraw[];
+    double2 *xs = reinterpret_cast<double2 *>(smraw);     // [nrhs][n]
+    const int b = blockIdx.y, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    a += (long long)b * stride;
+    for (int e = tid; e < nrhs * n; e += blockDim.x) xs[e] = xv[(long long)b * nrhs * n + e];
+    __syncthreads();
+    const int rbeg = blockIdx.x * rows_per_block;
+    const int rend = min(n, rbeg + rows_per_block);
+    for (int r = rbeg + warp; r < rend; r += 8) {
+        const double2 *row = a + (long long)r * ld;
+        for (int q = 0; q < nrhs; q++) {
+            double sr = 0, si = 0;
+            const double2 *x = xs + q * n;
+            for (int c = lane; c < n; c += 32) {
+                const double2 av = row[c], xx = x[c];
+                sr += av.x * xx.x - av.y * xx.y;
+                si += av.x * xx.y + av.y * xx.x;
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                sr += __shfl_down_sync(0xffffffffu, sr, o);
+                si += __shfl_down_sync(0xffffffffu, si, o);
+            }
+            if (lane == 0) {
+                const long long idx = ((long long)b * nrhs + q) * n + r;
+                const double2 bb = bv[idx];
+                const double2 res = make_double2(bb.x - sr, bb.y - si);
+                rv[idx] = res;
+                atomic_max_pos(&rn[b * nrhs + q], fmax(fabs(res.x), fabs(res.y)));
+                atomic_max_pos(&bn[b * nrhs + q], fmax(fabs(bb.x), fabs(bb.y)));
+            }
+        }
+    }
+}
+
+int pb_residual(pb_lu_engine *e, int n, int nb, int nrhs, const double2 *a, int ld, long stride,
+                const double2 *b, const double2 *x, double2 *r, double *rn, double *bn)
+{
+    PB_CUDA(cudaMemsetAsync(rn, 0, sizeof(double) * nb * nrhs, e->stream));
+    PB_CUDA(cudaMemsetAsync(bn, 0, sizeof(double) * nb * nrhs, e->stream));
+    const size_t smem = (size_t)nrhs * n * sizeof(double2);
+    static bool attr_set = false;
+    if (!attr_set) {
+        int dev = 0, cap = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&cap, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        PB_CUDA(cudaFuncSetAttribute(k_residual, cudaFuncAttributeMaxDynamicSharedMemorySize, cap));
+        attr_set = true;
+    }
+    const int rpb = 64;
+    dim3 g(ceil_div(n, rpb), nb);
+    k_residual<<<g, 256, smem, e->stream>>>(a, n, ld, stride, b, x, r, rn, bn, nrhs, rpb);
+    e->launches++;
+    PB_CHECK_LAUNCH();
+    return PB_OK;
+}

@@ -1,0 +1,47 @@
+// pb_lu.cuh — batched dense complex LU (partial pivoting) and triangular solves.
+#pragma once
+#include "pb_common.cuh"
+#include <cublas_v2.h>
+
+// Trailing-update engine of the LU.
+enum pb_gemm_kind {
+    PB_GEMM_FP64 = 0,   // complex FP64 GEMM
+    PB_GEMM_FP32 = 1,   // complex FP32 GEMM, SIMT
+    PB_GEMM_TC   = 2,   // complex FP32 inputs on the tensor cores (BF16x9 FP32 emulation,
+                        // TF32 if the emulation is unavailable), FP32 accumulation
+};
+
+struct pb_lu_engine {
+    cublasHandle_t blas = nullptr;
+    cudaStream_t stream = nullptr;
+    int gemm_kind = PB_GEMM_FP64;
+    int tc_compute = -1;       // resolved cublasComputeType_t for PB_GEMM_TC
+    long launches = 0;         // kernels launched (own kernels + library calls)
+};
+
+int pb_lu_engine_init(pb_lu_engine *e, cudaStream_t s);
+void pb_lu_engine_free(pb_lu_engine *e);
+
+// Factorise nb matrices (row-major, order n, leading dimension ld, batch stride
+// `stride` elements) in place. piv: [nb*n] device, info: [nb] device (-1 = regular,
+// else first zero-pivot row). T = float or double.
+template <typename T>
+int pb_lu_factor(pb_lu_engine *e, int n, int nb, typename cplx_t<T>::type *a, int ld,
+                 long stride, int *piv, int *info);
+
+// Row permutation perm[b*n + i] (row i of P*b comes from row perm[i]) from pivots.
+int pb_lu_perm(pb_lu_engine *e, int n, int nb, const int *piv, int *perm);
+
+// Solve A x = r for nb matrices x nrhs right-hand sides using the factors (type TF).
+// r, x: FP64 complex [nb][nrhs][n] device (may alias). Each RHS is scaled by its
+// max-norm before conversion to TF and scaled back afterwards.
+template <typename TF>
+int pb_lu_solve_batched(pb_lu_engine *e, int n, int nb, int nrhs,
+                        const typename cplx_t<TF>::type *lu, int ld, long stride,
+                        const int *perm, const double2 *r, double2 *x);
+
+// r = b - A x for nb FP64 matrices, nrhs vectors each; also writes per-vector
+// max|r| and max|b| into rn[nb*nrhs], bn[nb*nrhs].
+int pb_residual(pb_lu_engine *e, int n, int nb, int nrhs, const double2 *a, int ld,
+                long stride, const double2 *b, const double2 *x, double2 *r, double *rn,
+                double *bn);

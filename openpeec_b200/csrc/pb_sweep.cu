@@ -1,0 +1,490 @@
+// pb_sweep.cu — the frequency sweep (reference solve(), src/solve.c:171-430, dense path)
+// executed as batches of frequencies on the device.
+//
+// Two equivalent MNA formulations are built directly by the fill epilogues:
+//  * reduced (default when every matrix node is a charge cell and there are no lumped
+//    node elements): the node block j w C = j w P^-1 is eliminated exactly, leaving the
+//    branch-current system  (j w Zb + G^T P G) ib = G^T P b  of order nseg, with
+//    Zb = diag(zint) + j w Lp, G the node/segment incidence (mna.c:244-251). Node
+//    voltages follow from v = P (b - G ib) / (j w). No inverse of P is formed.
+//  * full: the reference's unknown vector [nodes | L | V | segments] (mna.c:81-84)
+//    augmented with cell charges q (P q - v = 0, KCL + j w q), which is algebraically
+//    identical to stamping j w P^-1 (mna.c:286-295) and is the reference's own compressed
+//    formulation (mna.c:86-107, 271-284).
+// Dense solve: batched LU of the whole batch; FP64 LU (plain path) or FP32 LU with
+// tensor-core trailing updates + FP64 iterative refinement against the FP64 matrix.
+#include "pb_ctx.cuh"
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+// ---------------------------------------------------------------- small kernels
+// rhs'[f][j][k] = (P b_j)[ca_k] - (P b_j)[cb_k],  b_j = e(pc1_j) - e(pc2_j)   (cells)
+__global__ void k_rhs_reduced(int nb, int np, int n, int nc, const double2 *P, long long pst,
+                              const int *ca, const int *cb, const int *pc, double2 *rhs)
+{
+    const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (idx >= (long long)nb * np * n) return;
+    const int k = (int)(idx % n);
+    const int j = (int)((idx / n) % np);
+    const int f = (int)(idx / ((long long)n * np));
+    const double2 *Pf = P + f * pst;
+    const int c1 = pc[2 * j], c2 = pc[2 * j + 1];
+    auto pb = [&](int c) -> double2 {
+        double2 v = make_double2(0, 0);
+        if (c < 0) return v;
+        if (c1 >= 0) { const double2 p = Pf[(long long)c * nc + c1]; v.x += p.x; v.y += p.y; }
+        if (c2 >= 0) { const double2 p = Pf[(long long)c * nc + c2]; v.x -= p.x; v.y -= p.y; }
+        return v;
+    };
+    const double2 a = pb(ca[k]), b = pb(cb[k]);
+    rhs[idx] = make_double2(a.x - b.x, a.y - b.y);
+}
+
+// Z[f][i][j] = (1/jw) sum_c (P[pc1_i][c] - P[pc2_i][c]) * (b_j - G ib_j)[c]
+__global__ void __launch_bounds__(256)
+k_z_reduced(int np, int n, int nc, const double2 *P, long long pst, const int *inc_off,
+            const int *inc_seg, const int *pc, const double2 *x, const double *freq, double2 *z)
+{
+    const int f = blockIdx.z, i = blockIdx.y, j = blockIdx.x;
+    const double2 *Pf = P + f * pst;
+    const double2 *ib = x + ((long long)f * np + j) * n;
+    const int a1 = pc[2 * i], a2 = pc[2 * i + 1], b1 = pc[2 * j], b2 = pc[2 * j + 1];
+    double sr = 0, si = 0;
+    for (int c = threadIdx.x; c < nc; c += blockDim.x) {
+        double yr = (c == b1 ? 1.0 : 0.0) - (c == b2 ? 1.0 : 0.0), yi = 0;
+        for (int e = inc_off[c]; e < inc_off[c + 1]; e++) {
+            const int s = inc_seg[e];
+            const int k = (s > 0 ? s : -s) - 1;
+            const double sg = s > 0 ? 1.0 : -1.0;
+            yr -= sg * ib[k].x;
+            yi -= sg * ib[k].y;
+        }
+        double wr = 0, wi = 0;
+        if (a1 >= 0) { const double2 p = Pf[(long long)a1 * nc + c]; wr += p.x; wi += p.y; }
+        if (a2 >= 0) { const double2 p = Pf[(long long)a2 * nc + c]; wr -= p.x; wi -= p.y; }
+        sr += wr * yr - wi * yi;
+        si += wr * yi + wi * yr;
+    }
+    __shared__ double rs[256], is_[256];
+    rs[threadIdx.x] = sr;
+    is_[threadIdx.x] = si;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) { rs[threadIdx.x] += rs[threadIdx.x + o]; is_[threadIdx.x] += is_[threadIdx.x + o]; }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const double om = 2 * PB_PI * freq[f];
+        // (sr + j si) / (j om) = (si - j sr) / om
+        z[((long long)f * np + i) * np + j] = make_double2(is_[0] / om, -rs[0] / om);
+    }
+}
+
+__global__ void k_rhs_full(int nb, int np, int n, const int *pm, double2 *rhs)
+{
+    const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (idx >= (long long)nb * np * n) return;
+    const int k = (int)(idx % n);
+    const int j = (int)((idx / n) % np);
+    double v = 0;
+    if (pm[2 * j] == k) v += 1;        // mna.c:367-376
+    if (pm[2 * j + 1] == k) v -= 1;
+    rhs[idx] = make_double2(v, 0);
+}
+
+__global__ void k_z_full(int nb, int np, int n, const int *pm, const double2 *x, double2 *z)
+{
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= nb * np * np) return;
+    const int j = idx % np, i = (idx / np) % np, f = idx / (np * np);
+    const double2 *xv = x + ((long long)f * np + j) * n;
+    const int a = pm[2 * i], b = pm[2 * i + 1];
+    double2 v = make_double2(0, 0);
+    if (a >= 0) { v.x += xv[a].x; v.y += xv[a].y; }
+    if (b >= 0) { v.x -= xv[b].x; v.y -= xv[b].y; }
+    z[idx] = v;
+}
+
+// full form: blocks of the augmented matrix (Lp block with -zint, P block)
+__global__ void k_full_blocks(int nb, int n, int ns, int nc, int offS, int offQ,
+                              const double2 *lp, long long lst, const double2 *P, long long pst,
+                              const double2 *zint, const double *freq, double2 *m, long long mst)
+{
+    const long long per = (long long)ns * ns + (long long)nc * nc;
+    const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (idx >= per * nb) return;
+    const int f = (int)(idx / per);
+    long long e = idx - f * per;
+    double2 *M = m + f * mst;
+    const double om = 2 * PB_PI * freq[f];
+    if (e < (long long)ns * ns) {
+        const int k = (int)(e / ns), q = (int)(e % ns);
+        const double2 l = lp[f * lst + e];
+        double2 v = make_double2(om * l.y, -om * l.x);   // -j w Lp (mna.c:263)
+        if (k == q) { const double2 zz = zint[(long long)f * ns + k]; v.x -= zz.x; v.y -= zz.y; }
+        M[(long long)(offS + k) * n + offS + q] = v;
+    } else {
+        e -= (long long)ns * ns;
+        const int c = (int)(e / nc), d = (int)(e % nc);
+        M[(long long)(offQ + c) * n + offQ + d] = P[f * pst + e];
+    }
+}
+
+__global__ void k_full_stamps(int nb, int n, int ne, const int *row, const int *col, const int *off,
+                              const pb_stamp *st, const double *freq, double2 *m, long long mst)
+{
+    const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (idx >= (long long)ne * nb) return;
+    const int f = (int)(idx / ne), e = (int)(idx % ne);
+    const double om = 2 * PB_PI * freq[f];
+    double vr = 0, vi = 0;
+    for (int q = off[e]; q < off[e + 1]; q++) {
+        const pb_stamp s = st[q];
+        if (s.kind == ST_CONST) vr += s.val;
+        else if (s.kind == ST_JW) vi += om * s.val;
+        else vi -= om * s.val;
+    }
+    double2 *p = &m[f * mst + (long long)row[e] * n + col[e]];
+    p->x += vr;
+    p->y += vi;
+}
+
+__global__ void k_to_f32(const double2 *a, float2 *b, long long n)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        b[i] = make_float2((float)a[i].x, (float)a[i].y);
+}
+
+__global__ void k_axpy(double2 *x, const double2 *d, long long n)
+{
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < n) { x[i].x += d[i].x; x[i].y += d[i].y; }
+}
+
+// ---------------------------------------------------------------- helpers
+struct DevBuf {
+    void *p = nullptr;
+    ~DevBuf() { if (p) cudaFree(p); }
+    int alloc(size_t bytes)
+    {
+        if (p) { cudaFree(p); p = nullptr; }
+        if (bytes == 0) bytes = 16;
+        cudaError_t e = cudaMalloc(&p, bytes);
+        if (e != cudaSuccess) { p = nullptr; return pb_cuda_fail(e, "cudaMalloc", __FILE__, __LINE__); }
+        return PB_OK;
+    }
+    template <typename T> T *as() const { return (T *)p; }
+};
+
+// Quadrature-level signature of a wavenumber: floor(kw * size) over the distinct cell
+// sizes that can be a pair's lmax (partial.c:166-173, 216-227). Equal signatures mean
+// every pair uses the same nsub, hence the same static part.
+static void level_signature(const pb_ctx *c, double kw, std::vector<long> &sig)
+{
+    sig.clear();
+    sig.push_back(kw > 0 ? 1 : 0);
+    if (kw <= 0) return;
+    auto add = [&](const std::vector<pb_cell_t> &v) {
+        for (const auto &s : v) {
+            sig.push_back((long)std::floor(kw * s.len));
+            sig.push_back((long)std::floor(kw * std::max(s.len, s.wid)));
+        }
+    };
+    add(c->seg);
+    add(c->chg);
+    std::sort(sig.begin() + 1, sig.end());
+    sig.erase(std::unique(sig.begin() + 1, sig.end()), sig.end());
+}
+
+struct PhaseTimer {
+    cudaEvent_t a = nullptr, b = nullptr;
+    double acc = 0;
+    PhaseTimer() { cudaEventCreate(&a); cudaEventCreate(&b); }
+    ~PhaseTimer() { cudaEventDestroy(a); cudaEventDestroy(b); }
+    void start(cudaStream_t s) { cudaEventRecord(a, s); }
+    void stop(cudaStream_t s)
+    {
+        cudaEventRecord(b, s);
+        cudaEventSynchronize(b);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, a, b);
+        acc += ms;
+    }
+};
+
+int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts *opts_in,
+                  double *zmat, double *segi, pb_sweep_stats *stats)
+{
+    pb_sweep_opts o;
+    if (opts_in) o = *opts_in;
+    else { o.fill_prec = PB_PREC_MIXED; o.lu = PB_LU_TC; o.form = PB_FORM_AUTO; o.batch = 0;
+           o.refine_tol = 0; o.refine_maxit = 0; o.verbose = 0; }
+    if (nfreq <= 0 || freq == nullptr) { pb_set_error("pb_sweep: no frequencies"); return PB_ERR_ARG; }
+    for (int i = 0; i < nfreq; i++)
+        if (!(freq[i] > 0)) { pb_set_error("pb_sweep: frequencies must be > 0"); return PB_ERR_ARG; }
+    int form = o.form;
+    if (form == PB_FORM_AUTO) form = c->reduced_ok ? PB_FORM_REDUCED : PB_FORM_FULL;
+    if (form == PB_FORM_REDUCED && !c->reduced_ok) {
+        pb_set_error("reduced formulation needs every matrix node to be a charge cell and no lumped node elements");
+        return PB_ERR_UNSUP;
+    }
+    const int mixed = (o.lu != PB_LU_FP64);
+    const int fill32 = (o.fill_prec == PB_PREC_MIXED);
+    const double tol = o.refine_tol > 0 ? o.refine_tol : 1e-12;
+    const int maxit = o.refine_maxit > 0 ? o.refine_maxit : 30;
+    c->lu.gemm_kind = (o.lu == PB_LU_TC) ? PB_GEMM_TC : (o.lu == PB_LU_FP32) ? PB_GEMM_FP32 : PB_GEMM_FP64;
+    const long launches0 = c->launches + c->lu.launches;
+
+    const int ns = (int)c->seg.size(), nc = c->ncell, np = (int)c->port.size();
+    const int n = (form == PB_FORM_REDUCED) ? ns : c->nfull;
+    const cudaStream_t st = c->stream;
+    if (n <= 0) { pb_set_error("pb_sweep: empty system"); return PB_ERR_ARG; }
+
+    // batch size from free memory
+    size_t fr = 0, tot = 0;
+    PB_CUDA(cudaMemGetInfo(&fr, &tot));
+    const double n2 = (double)n * n;
+    double perf = n2 * 16 + (mixed ? n2 * 8 : 0) + (double)nc * nc * 16 + (double)ns * 16
+                + (form == PB_FORM_FULL ? (double)ns * ns * 16 : 0) + 4.0 * np * n * 16 + 8.0 * n;
+    const double fixed = (double)ns * ns * 8 + (double)nc * nc * 8;
+    int B = o.batch;
+    if (B <= 0) {
+        const double avail = 0.80 * (double)fr - fixed - 256e6;
+        B = (int)std::max(1.0, std::floor(avail / perf));
+        B = std::min(B, 256);
+    }
+    B = std::max(1, std::min(B, nfreq));
+
+    DevBuf bM64, bM32, bP, bLp, bStLp, bStP, bZint, bPiv, bPerm, bInfo, bRhs, bX, bR, bD, bRn, bBn,
+        bFreq, bZ, bPC;
+    PB_TRY(bM64.alloc((size_t)B * n2 * 16));
+    if (mixed) PB_TRY(bM32.alloc((size_t)B * n2 * 8));
+    PB_TRY(bP.alloc((size_t)B * nc * nc * 16 + 16));
+    if (form == PB_FORM_FULL) PB_TRY(bLp.alloc((size_t)B * ns * ns * 16 + 16));
+    PB_TRY(bStLp.alloc((size_t)ns * ns * 8 + 16));
+    PB_TRY(bStP.alloc((size_t)nc * nc * 8 + 16));
+    PB_TRY(bZint.alloc((size_t)B * ns * 16 + 16));
+    PB_TRY(bPiv.alloc((size_t)B * n * 4));
+    PB_TRY(bPerm.alloc((size_t)B * n * 4));
+    PB_TRY(bInfo.alloc((size_t)B * 4));
+    const size_t vb = (size_t)B * np * n * 16;
+    PB_TRY(bRhs.alloc(vb));
+    PB_TRY(bX.alloc(vb));
+    PB_TRY(bR.alloc(vb));
+    PB_TRY(bD.alloc(vb));
+    PB_TRY(bRn.alloc((size_t)B * np * 8));
+    PB_TRY(bBn.alloc((size_t)B * np * 8));
+    PB_TRY(bFreq.alloc((size_t)B * 8));
+    PB_TRY(bZ.alloc((size_t)B * np * np * 16));
+    PB_TRY(bPC.alloc((size_t)2 * np * 4));
+
+    // port endpoints: cells (reduced) or matrix indices (full)
+    std::vector<int> pc(2 * np);
+    for (int j = 0; j < np; j++) {
+        if (form == PB_FORM_REDUCED) {
+            const int m1 = c->nodemap[c->port[j].n1], m2 = c->nodemap[c->port[j].n2];
+            pc[2 * j] = m1 >= 0 ? c->cell_of_node[c->port[j].n1] : -1;
+            pc[2 * j + 1] = m2 >= 0 ? c->cell_of_node[c->port[j].n2] : -1;
+        } else {
+            pc[2 * j] = c->nodemap[c->port[j].n1];
+            pc[2 * j + 1] = c->nodemap[c->port[j].n2];
+        }
+    }
+    PB_CUDA(cudaMemcpyAsync(bPC.p, pc.data(), sizeof(int) * 2 * np, cudaMemcpyHostToDevice, st));
+
+    PhaseTimer tStatic, tCorr, tAsm, tLu, tRef, tAll;
+    double samples = 0, luflops = 0, maxres = 0;
+    int maxits = 0, refreshes = 0;
+    std::vector<long> cur_sig, sig;
+    bool static_valid = false;
+    std::vector<double2> zh((size_t)B * np * np);
+    std::vector<double> rnh(B * np), bnh(B * np);
+    std::vector<int> infoh(B);
+    tAll.start(st);
+
+    for (int b0 = 0; b0 < nfreq; b0 += B) {
+        const int nb = std::min(B, nfreq - b0);
+        const double *fb = freq + b0;
+        PB_CUDA(cudaMemcpyAsync(bFreq.p, fb, sizeof(double) * nb, cudaMemcpyHostToDevice, st));
+        tAsm.start(st);
+        PB_TRY(pb_zint(c->g, c->skin, nb, bFreq.as<double>(), bZint.as<double2>(), st, &c->launches));
+        tAsm.stop(st);
+        // fill in chunks of <= 32 frequencies with one quadrature-level signature
+        int f = 0;
+        while (f < nb) {
+            const double kw0 = c->retardation ? 2 * PB_PI * fb[f] / PB_C0 : 0.0;
+            level_signature(c, kw0, sig);
+            int e = f + 1;
+            const int chunk_max = fill32 ? PB_FMAX : 1;        // plain path: one frequency at a time
+            if (c->retardation) {
+                std::vector<long> s2;
+                while (e < nb && e - f < chunk_max) {
+                    level_signature(c, 2 * PB_PI * fb[e] / PB_C0, s2);
+                    if (s2 != sig) break;
+                    e++;
+                }
+            } else {
+                e = std::min(nb, f + PB_FMAX);
+            }
+            const int nf = e - f;
+            // plain path re-evaluates the static part at every frequency, like the reference
+            if (!static_valid || sig != cur_sig || (!fill32 && c->retardation)) {
+                tStatic.start(st);
+                if (c->capacitance && nc > 0) PB_TRY(pb_pot_static(c->g, kw0, bStP.as<double>(), st, &c->launches));
+                PB_TRY(pb_lp_static(c->g, kw0, bStLp.as<double>(), st, &c->launches));
+                tStatic.stop(st);
+                cur_sig = sig;
+                static_valid = true;
+                refreshes++;
+            }
+            double kw[PB_FMAX];
+            for (int q = 0; q < nf; q++) kw[q] = c->retardation ? 2 * PB_PI * fb[f + q] / PB_C0 : 0.0;
+            tCorr.start(st);
+            if (c->capacitance && nc > 0)
+                PB_TRY(pb_pot_corr(c->g, nf, kw, fill32, bStP.as<double>(), bP.as<double2>() + (long long)f * nc * nc,
+                                   (long long)nc * nc, st, &c->launches, &samples));
+            pb_epi_args ea;
+            for (int q = 0; q < nf; q++) ea.omega[q] = 2 * PB_PI * fb[f + q];
+            if (form == PB_FORM_REDUCED) {
+                ea.m64 = bM64.as<double2>() + (long long)f * n * n;
+                ea.m32 = mixed ? bM32.as<float2>() + (long long)f * n * n : nullptr;
+                ea.m_stride = (long long)n * n;
+                ea.pm = bP.as<double2>() + (long long)f * nc * nc;
+                ea.pm_stride = (long long)nc * nc;
+                ea.zint = bZint.as<double2>() + (long long)f * ns;
+                PB_TRY(pb_lp_corr(c->g, nf, kw, fill32, bStLp.as<double>(), PB_EPI_REDUCED, ea, st,
+                                  &c->launches, &samples));
+            } else {
+                ea.out = bLp.as<double2>() + (long long)f * ns * ns;
+                ea.out_stride = (long long)ns * ns;
+                PB_TRY(pb_lp_corr(c->g, nf, kw, fill32, bStLp.as<double>(), PB_EPI_STORE, ea, st,
+                                  &c->launches, &samples));
+            }
+            tCorr.stop(st);
+            f = e;
+        }
+        if (form == PB_FORM_FULL) {
+            tAsm.start(st);
+            PB_CUDA(cudaMemsetAsync(bM64.p, 0, (size_t)nb * n2 * 16, st));
+            const int offQ = c->nunknown;
+            const long long per = (long long)ns * ns + (c->capacitance ? (long long)nc * nc : 0);
+            k_full_blocks<<<ceil_div(per * nb, 256), 256, 0, st>>>(
+                nb, n, ns, c->capacitance ? nc : 0, c->offS, offQ, bLp.as<double2>(), (long long)ns * ns,
+                bP.as<double2>(), (long long)nc * nc, bZint.as<double2>(), bFreq.as<double>(),
+                bM64.as<double2>(), (long long)n * n);
+            c->launches++;
+            PB_CHECK_LAUNCH();
+            const int ne = (int)c->fe_row.size();
+            if (ne > 0) {
+                k_full_stamps<<<ceil_div((long long)ne * nb, 256), 256, 0, st>>>(
+                    nb, n, ne, c->d_fe_row, c->d_fe_col, c->d_fe_off, c->d_fe_st, bFreq.as<double>(),
+                    bM64.as<double2>(), (long long)n * n);
+                c->launches++;
+                PB_CHECK_LAUNCH();
+            }
+            if (mixed) {
+                k_to_f32<<<1184, 256, 0, st>>>(bM64.as<double2>(), bM32.as<float2>(), (long long)nb * n * n);
+                c->launches++;
+                PB_CHECK_LAUNCH();
+            }
+            tAsm.stop(st);
+        }
+        // factorise the batch
+        tLu.start(st);
+        if (mixed) PB_TRY(pb_lu_factor<float>(&c->lu, n, nb, bM32.as<float2>(), n, (long)n * n, bPiv.as<int>(), bInfo.as<int>()));
+        else PB_TRY(pb_lu_factor<double>(&c->lu, n, nb, bM64.as<double2>(), n, (long)n * n, bPiv.as<int>(), bInfo.as<int>()));
+        PB_TRY(pb_lu_perm(&c->lu, n, nb, bPiv.as<int>(), bPerm.as<int>()));
+        tLu.stop(st);
+        luflops += 8.0 / 3.0 * (double)n * n * n * nb;
+        PB_CUDA(cudaMemcpyAsync(infoh.data(), bInfo.p, sizeof(int) * nb, cudaMemcpyDeviceToHost, st));
+        PB_CUDA(cudaStreamSynchronize(st));
+        for (int q = 0; q < nb; q++)
+            if (infoh[q] >= 0) {
+                pb_set_error("singular matrix at f = %.5e Hz (row %d : floating node or ideal voltage source loop?)",
+                             fb[q], infoh[q]);
+                return PB_ERR_SINGULAR;
+            }
+        // right-hand sides
+        tRef.start(st);
+        const long long nv = (long long)nb * np * n;
+        if (form == PB_FORM_REDUCED) {
+            k_rhs_reduced<<<ceil_div(nv, 256), 256, 0, st>>>(nb, np, n, nc, bP.as<double2>(), (long long)nc * nc,
+                                                             c->g.seg_ca, c->g.seg_cb, bPC.as<int>(), bRhs.as<double2>());
+        } else {
+            k_rhs_full<<<ceil_div(nv, 256), 256, 0, st>>>(nb, np, n, bPC.as<int>(), bRhs.as<double2>());
+        }
+        c->launches++;
+        PB_CHECK_LAUNCH();
+        if (!mixed) {
+            PB_TRY(pb_lu_solve_batched<double>(&c->lu, n, nb, np, bM64.as<double2>(), n, (long)n * n,
+                                               bPerm.as<int>(), bRhs.as<double2>(), bX.as<double2>()));
+        } else {
+            // iterative refinement: x_0 = LU^-1 b, r = b - A x (FP64), x += LU^-1 r
+            PB_TRY(pb_lu_solve_batched<float>(&c->lu, n, nb, np, bM32.as<float2>(), n, (long)n * n,
+                                              bPerm.as<int>(), bRhs.as<double2>(), bX.as<double2>()));
+            double prev = 1e300;
+            int it = 0;
+            for (it = 1; it <= maxit; it++) {
+                PB_TRY(pb_residual(&c->lu, n, nb, np, bM64.as<double2>(), n, (long)n * n, bRhs.as<double2>(),
+                                   bX.as<double2>(), bR.as<double2>(), bRn.as<double>(), bBn.as<double>()));
+                PB_CUDA(cudaMemcpyAsync(rnh.data(), bRn.p, sizeof(double) * nb * np, cudaMemcpyDeviceToHost, st));
+                PB_CUDA(cudaMemcpyAsync(bnh.data(), bBn.p, sizeof(double) * nb * np, cudaMemcpyDeviceToHost, st));
+                PB_CUDA(cudaStreamSynchronize(st));
+                double worst = 0;
+                for (int q = 0; q < nb * np; q++) worst = std::max(worst, bnh[q] > 0 ? rnh[q] / bnh[q] : 0.0);
+                if (worst <= tol || worst > 0.5 * prev) { maxres = std::max(maxres, worst); break; }
+                prev = worst;
+                PB_TRY(pb_lu_solve_batched<float>(&c->lu, n, nb, np, bM32.as<float2>(), n, (long)n * n,
+                                                  bPerm.as<int>(), bR.as<double2>(), bD.as<double2>()));
+                k_axpy<<<ceil_div(nv, 256), 256, 0, st>>>(bX.as<double2>(), bD.as<double2>(), nv);
+                c->launches++;
+                PB_CHECK_LAUNCH();
+            }
+            if (it > maxit) maxres = std::max(maxres, prev);
+            maxits = std::max(maxits, it);
+        }
+        // port voltages -> Z
+        if (form == PB_FORM_REDUCED) {
+            dim3 g(np, np, nb);
+            k_z_reduced<<<g, 256, 0, st>>>(np, n, nc, bP.as<double2>(), (long long)nc * nc, c->d_inc_off,
+                                           c->d_inc_seg, bPC.as<int>(), bX.as<double2>(), bFreq.as<double>(),
+                                           bZ.as<double2>());
+        } else {
+            k_z_full<<<ceil_div(nb * np * np, 128), 128, 0, st>>>(nb, np, n, bPC.as<int>(), bX.as<double2>(), bZ.as<double2>());
+        }
+        c->launches++;
+        PB_CHECK_LAUNCH();
+        tRef.stop(st);
+        if (zmat) PB_CUDA(cudaMemcpyAsync(zmat + 2 * (size_t)b0 * np * np, bZ.p, sizeof(double2) * nb * np * np,
+                                          cudaMemcpyDeviceToHost, st));
+        if (segi) {
+            const int off = (form == PB_FORM_REDUCED) ? 0 : c->offS;
+            for (int q = 0; q < nb; q++)
+                for (int j = 0; j < np; j++)
+                    PB_CUDA(cudaMemcpyAsync(segi + 2 * (((size_t)(b0 + q) * np + j) * ns),
+                                            bX.as<double2>() + ((long long)q * np + j) * n + off,
+                                            sizeof(double2) * ns, cudaMemcpyDeviceToHost, st));
+        }
+        PB_CUDA(cudaStreamSynchronize(st));
+    }
+    tAll.stop(st);
+    if (stats) {
+        stats->t_static_ms = tStatic.acc;
+        stats->t_corr_ms = tCorr.acc;
+        stats->t_assemble_ms = tAsm.acc;
+        stats->t_lu_ms = tLu.acc;
+        stats->t_refine_ms = tRef.acc;
+        stats->t_total_ms = tAll.acc;
+        stats->corr_samples = samples;
+        stats->lu_flops = luflops;
+        stats->max_resid = maxres;
+        stats->max_iters = maxits;
+        stats->form_used = form;
+        stats->n_system = n;
+        stats->static_refreshes = refreshes;
+        stats->kernel_launches = (int)(c->launches + c->lu.launches - launches0);
+    }
+    return PB_OK;
+}

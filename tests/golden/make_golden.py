@@ -1,0 +1,104 @@
+"""Write the golden fixtures of the parity tests from the reference implementation.
+
+Runs only where the reference checkout is available (it builds oracle/_ref from the
+reference's own sources with oracle/Makefile). For every case it stores:
+  * the discretised problem exactly as the reference's wire_build produced it,
+  * sampled partial-inductance / potential-coefficient entries from the reference's
+    lp_entry / pot_entry (src/partial.c:371-424, src/potential.c:124-150),
+  * the Z matrix of the reference's own sweep (solve(), src/solve.c:171-430) at the
+    listed frequencies.
+
+    python tests/golden/make_golden.py            # all small cases (about a minute)
+    python tests/golden/make_golden.py --cfg2     # + the full 64x32 plate at 2 frequencies
+"""
+import argparse
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from openpeec_b200 import configs  # noqa: E402
+from oracle.pyoracle import RefLib  # noqa: E402
+
+REF = os.environ.get("PEEC_REFERENCE", "/root/reference")
+C0 = 2.99792458e8
+
+
+def sample_pairs(n, count, rng):
+    if n == 0:
+        return np.zeros((0, 2), np.int32)
+    diag = np.arange(min(n, 16))
+    pairs = [np.stack([diag, diag], 1)]
+    near = rng.integers(0, n, count // 2)
+    pairs.append(np.stack([near, np.clip(near + rng.integers(-3, 4, len(near)), 0, n - 1)], 1))
+    pairs.append(rng.integers(0, n, (count // 2, 2)))
+    return np.concatenate(pairs).astype(np.int32)
+
+
+def make_case(name, peec_text, freqs, count=300, threads=8):
+    with tempfile.NamedTemporaryFile("w", suffix=".peec", delete=False) as f:
+        f.write(peec_text)
+        path = f.name
+    RefLib.set_threads(threads)
+    r = RefLib(path)
+    prob = r.problem()
+    rng = np.random.default_rng(1234)
+    kws = [0.0, 2 * np.pi * max(freqs) / C0]
+    lp = sample_pairs(r.nseg, count, rng)
+    lp_v = np.array([[r.lp_entry(int(i), int(j), kw) for (i, j) in lp] for kw in kws])
+    pp = sample_pairs(r.ncell, count // 2, rng) if r.ncell > 0 else np.zeros((0, 2), np.int32)
+    p_v = np.array([[r.pot_entry(int(i), int(j), kw) for (i, j) in pp] for kw in kws]) \
+        if len(pp) else np.zeros((2, 0), complex)
+    zs = []
+    for f in freqs:
+        r.set_freqs(f, f, 1, 0)
+        zs.append(r.solve()[0])
+    os.unlink(path)
+    out = os.path.join(HERE, name + ".npz")
+    tmp = os.path.join(HERE, name + "_prob.npz")
+    prob.save(tmp)
+    pz = dict(np.load(tmp))
+    os.unlink(tmp)
+    np.savez_compressed(out, **{"prob_" + k: v for k, v in pz.items()}, freqs=np.array(freqs),
+                        z=np.array(zs), kws=np.array(kws), lp_ij=lp, lp_v=lp_v, p_ij=pp, p_v=p_v,
+                        peec=np.array(peec_text))
+    print(name, "nseg", r.nseg, "ncell", r.ncell, "nunknown", r.nunknown, "->", out)
+
+
+def sample(fn):
+    with open(os.path.join(REF, "data", "sample", fn)) as f:
+        return f.read()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--cfg2", action="store_true")
+    a = ap.parse_args()
+    subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True,
+                   stdout=subprocess.DEVNULL)
+    f1 = [1e7 * (100.0 ** (i / 99.0)) for i in range(100)]
+    make_case("cfg1_dipole_qs", configs.CFG1, f1[::9] + [f1[-1]])
+    make_case("dipole_halfwave", sample("dipole_halfwave.peec"), [2.8e8, 2.93e8, 3.0e8, 6.0e8])
+    make_case("monopole_gp", sample("monopole_gp.peec"), [2.8e8, 2.93e8, 3.0e8, 6.0e8])
+    make_case("strip_dipole_ret", sample("strip_dipole_ret.peec"), [1e8, 2.8e8, 5e8])
+    make_case("plate_thick", sample("plate_thick.peec"), [1e6, 1e8])
+    make_case("quad_square", sample("quad_square.peec"), [1e6, 1e8])
+    make_case("disk_cap", sample("disk_cap.peec"), [1e7, 3e8])
+    make_case("plate_cap", sample("plate_cap.peec"), [1e7, 3e8])
+    make_case("rlc_series", sample("rlc_series.peec"), [1e5, 1e6, 1e7])
+    make_case("cfg2_small", configs.cfg2(16, 8, 512), [5e6, 3.2e8, 6.4e8, 1.28e9, 2.56e9])
+    for i in range(3):
+        make_case("cfg3_small_%d" % i, configs.cfg3_instance(0, i, 20, 80),
+                  [5e7, 3.3e8, 1.1e9, 3e9])
+    if a.cfg2:
+        make_case("cfg2_full", configs.CFG2, [5e6, 1.28e9], count=200, threads=os.cpu_count())
+
+
+if __name__ == "__main__":
+    main()

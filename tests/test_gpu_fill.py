@@ -1,0 +1,78 @@
+"""Parity of the CUDA partial-element fill (Lp, P) with the oracle and the reference.
+
+Tolerances (per entry, relative to |entry|):
+  FP64 path  (static + correction in FP64)            : 1e-11
+  mixed path (FP64 static, FP32 retardation correction): 1e-5  (the stated Lp/P bar)
+"""
+import numpy as np
+import pytest
+
+from conftest import golden_names, relerr
+from openpeec_b200 import abi, api
+from oracle.pyoracle import Oracle
+
+pytestmark = pytest.mark.gpu
+CASES = [n for n in golden_names() if n not in ("cfg2_full", "rlc_series")]
+C0 = 2.99792458e8
+
+
+def entry_err(got, ref):
+    """Relative error per entry, entries below 1e-9 of the matrix scale compared absolutely."""
+    scale = np.max(np.abs(ref)) if ref.size else 1.0
+    return relerr(got, ref, 1e-9 * scale)
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_lp_matches_oracle(name, golden):
+    prob, fx = golden(name)
+    o = Oracle(prob)
+    with api.Context(prob) as ctx:
+        for kw in fx["kws"]:
+            ref = o.lp_fill(kw)
+            assert entry_err(ctx.lp_fill(kw, abi.PREC_FP64), ref) <= 1e-11, (name, kw)
+            assert entry_err(ctx.lp_fill(kw, abi.PREC_MIXED), ref) <= 1e-5, (name, kw)
+
+
+@pytest.mark.parametrize("name", [n for n in CASES if n not in ("plate_thick", "quad_square")])
+def test_pot_matches_oracle(name, golden):
+    prob, fx = golden(name)
+    if not prob.capacitance:
+        pytest.skip("no capacitive cells")
+    o = Oracle(prob)
+    with api.Context(prob) as ctx:
+        for kw in fx["kws"]:
+            ref = o.pot_fill(kw)
+            assert entry_err(ctx.pot_fill(kw, abi.PREC_FP64), ref) <= 1e-11, (name, kw)
+            assert entry_err(ctx.pot_fill(kw, abi.PREC_MIXED), ref) <= 1e-5, (name, kw)
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_entries_match_reference_golden(name, golden):
+    prob, fx = golden(name)
+    with api.Context(prob) as ctx:
+        for ik, kw in enumerate(fx["kws"]):
+            lp = ctx.lp_fill(kw, abi.PREC_MIXED)
+            got = np.array([lp[i, j] for i, j in fx["lp_ij"]])
+            scale = np.max(np.abs(lp))
+            assert relerr(got, fx["lp_v"][ik], 1e-9 * scale) <= 1e-5, name
+            if prob.capacitance and len(fx["p_ij"]):
+                pm = ctx.pot_fill(kw, abi.PREC_MIXED)
+                got = np.array([pm[i, j] for i, j in fx["p_ij"]])
+                assert relerr(got, fx["p_v"][ik], 1e-9 * np.max(np.abs(pm))) <= 1e-5, name
+
+
+def test_fill_is_deterministic(golden):
+    prob, fx = golden("cfg2_small")
+    kw = fx["kws"][1]
+    with api.Context(prob) as ctx:
+        a = ctx.lp_fill(kw, abi.PREC_MIXED)
+        b = ctx.lp_fill(kw, abi.PREC_MIXED)
+    assert a.tobytes() == b.tobytes()
+
+
+def test_lp_symmetric_and_positive_self(golden):
+    prob, _ = golden("cfg2_small")
+    with api.Context(prob) as ctx:
+        lp = ctx.lp_fill(2 * np.pi * 1e9 / C0, abi.PREC_MIXED)
+    assert np.array_equal(lp, lp.T)
+    assert np.all(np.diag(lp).real > 0)

@@ -1,0 +1,106 @@
+"""Frequency sweeps on the GPU against the reference's Z matrices (golden fixtures).
+
+Tolerances on max_f |Z - Z_ref| / |Z_ref|:
+  plain FP64 path (FP64 fill, FP64 LU)                         : 1e-9
+  mixed path (FP32 correction, tensor-core LU, FP64 refinement): 1e-6
+"""
+import numpy as np
+import pytest
+
+from conftest import golden_names, relerr
+from openpeec_b200 import abi, api
+
+pytestmark = pytest.mark.gpu
+CASES = [n for n in golden_names() if n not in ("cfg2_full",)]
+
+
+def zerr(z, ref):
+    return relerr(z, ref, 1e-300)
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_plain_fp64_sweep(name, golden):
+    prob, fx = golden(name)
+    with api.Context(prob) as ctx:
+        z, st = ctx.sweep(fx["freqs"], fill_prec=abi.PREC_FP64, lu=abi.LU_FP64)
+    assert zerr(z, fx["z"]) <= 1e-9, (name, zerr(z, fx["z"]))
+
+
+@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("lu", [abi.LU_FP32, abi.LU_TC])
+def test_mixed_sweep(name, lu, golden):
+    prob, fx = golden(name)
+    with api.Context(prob) as ctx:
+        z, st = ctx.sweep(fx["freqs"], fill_prec=abi.PREC_MIXED, lu=lu)
+    assert zerr(z, fx["z"]) <= 1e-6, (name, zerr(z, fx["z"]), st)
+
+
+@pytest.mark.parametrize("name", ["cfg1_dipole_qs", "cfg2_small", "dipole_halfwave", "cfg3_small_1"])
+def test_full_and_reduced_forms_agree(name, golden):
+    prob, fx = golden(name)
+    with api.Context(prob) as ctx:
+        zr, sr = ctx.sweep(fx["freqs"], fill_prec=abi.PREC_FP64, lu=abi.LU_FP64, form=abi.FORM_REDUCED)
+        zf, sf = ctx.sweep(fx["freqs"], fill_prec=abi.PREC_FP64, lu=abi.LU_FP64, form=abi.FORM_FULL)
+    assert sr["form_used"] == abi.FORM_REDUCED and sf["form_used"] == abi.FORM_FULL
+    assert zerr(zr, zf) <= 1e-9
+
+
+def test_monopole_is_half_dipole(golden):
+    """Image theory: the quarter-wave monopole over ground is the half-wave dipole / 2
+    (reference check peec_check.sh:382-397, measured 3e-10 there)."""
+    pm, fm = golden("monopole_gp")
+    pd, fd = golden("dipole_halfwave")
+    assert np.array_equal(fm["freqs"], fd["freqs"])
+    with api.Context(pm) as a, api.Context(pd) as b:
+        zm, _ = a.sweep(fm["freqs"])
+        zd, _ = b.sweep(fd["freqs"])
+    assert relerr(zm, zd / 2, 1e-300) <= 1e-6
+
+
+def test_halfwave_dipole_resonance(golden):
+    """Rin near the first resonance of the half-wave dipole is ~73 ohm (Balanis)."""
+    prob, fx = golden("dipole_halfwave")
+    with api.Context(prob) as ctx:
+        z, _ = ctx.sweep(fx["freqs"])
+    assert 60 < z[1, 0, 0].real < 85
+
+
+def test_sweep_deterministic_and_batch_invariant(golden):
+    prob, fx = golden("cfg2_small")
+    with api.Context(prob) as ctx:
+        a, _ = ctx.sweep(fx["freqs"], batch=2)
+        b, _ = ctx.sweep(fx["freqs"], batch=2)
+        c, _ = ctx.sweep(fx["freqs"], batch=5)
+    assert a.tobytes() == b.tobytes()
+    assert zerr(a, c) <= 1e-9
+
+
+def test_segment_currents_reduced_vs_full(golden):
+    prob, fx = golden("cfg2_small")
+    with api.Context(prob) as ctx:
+        _, ir, _ = ctx.sweep(fx["freqs"][:2], fill_prec=abi.PREC_FP64, lu=abi.LU_FP64,
+                             form=abi.FORM_REDUCED, want_segi=True)
+        _, iff, _ = ctx.sweep(fx["freqs"][:2], fill_prec=abi.PREC_FP64, lu=abi.LU_FP64,
+                              form=abi.FORM_FULL, want_segi=True)
+    assert relerr(ir, iff, 1e-6 * np.max(np.abs(iff))) <= 1e-7
+
+
+def test_singular_structure_reports_error():
+    """A floating node: a wire whose second end carries no charge cell and no path
+    (capacitance off) makes the MNA matrix singular; the sweep must say so."""
+    from openpeec_b200 import geometry
+    txt = """OpenPEEC 1 0
+capacitance = 0
+wire = 0 0 0 0 0 0.1 1e-3 5.8e7 2
+wire = 0 0 0.2 0 0 0.3 1e-3 5.8e7 2
+node = 1 0 0 0
+node = 2 0 0 0.1
+port = 1 2 50
+frequency = 1e6 1e6 0
+end
+"""
+    prob = geometry.build(geometry.parse_peec(txt))
+    with api.Context(prob) as ctx:
+        with pytest.raises(api.PbError) as e:
+            ctx.sweep([1e6], fill_prec=abi.PREC_FP64, lu=abi.LU_FP64)
+    assert e.value.code == abi.PB_ERR_SINGULAR
