@@ -108,7 +108,8 @@ typedef struct pb_ctx pb_ctx;
 
 /* MNA formulation inside the sweep. */
 #define PB_FORM_AUTO    0    /* reduced when applicable, else full                       */
-#define PB_FORM_FULL    1    /* the reference's dense MNA with C = P^-1 (mna.c:175-297)   */
+#define PB_FORM_FULL    1    /* the reference's dense MNA (mna.c:175-297), node block jwP^-1
+                                written with explicit cell charges (mna.c:86-107), no inverse */
 #define PB_FORM_REDUCED 2    /* branch-current Schur form (requires every node = a cell) */
 
 typedef struct {
@@ -116,7 +117,7 @@ typedef struct {
     int    lu;              /* PB_LU_*                                                 */
     int    form;            /* PB_FORM_*                                               */
     int    batch;           /* frequencies per device batch (0 = automatic)            */
-    double refine_tol;      /* target relative FP64 residual (0 = 1e-12)               */
+    double refine_tol;      /* unused (refinement stops at FP64 backward-error level)  */
     int    refine_maxit;    /* max refinement / GMRES iterations (0 = 30)              */
     int    verbose;
 } pb_sweep_opts;
@@ -125,12 +126,14 @@ typedef struct {
     double t_static_ms, t_corr_ms, t_assemble_ms, t_lu_ms, t_refine_ms, t_total_ms;
     double corr_samples;    /* retardation-correction quadrature samples evaluated    */
     double lu_flops;        /* (8/3) n^3 per frequency, summed                       */
-    double max_resid;       /* largest final relative FP64 residual over the sweep   */
+    double max_resid;       /* largest final normwise backward error |r|/(|A||x|+|b|) */
     int    max_iters;       /* largest refinement iteration count                    */
     int    form_used;       /* PB_FORM_FULL or PB_FORM_REDUCED                       */
     int    n_system;        /* order of the factorised system                        */
     int    static_refreshes;/* how many times the cached static part was rebuilt     */
     int    kernel_launches; /* kernels launched by the last pb_sweep call            */
+    int    fp64_fallbacks;  /* frequencies whose mixed solve did not converge and were
+                               re-factorised in FP64 (reported, never silent)          */
 } pb_sweep_stats;
 
 const char *pb_last_error(void);
@@ -182,6 +185,12 @@ int  pb_lu_solve(int n, const double *a, const int *piv, double *b);
  * info[b] = -1 or the zero-pivot row of matrix b. Device pointers (cudaMalloc'd).
  */
 int  pb_lu_decomp_batched_dev(int n, int nb, double *a_dev, int *piv_dev, int *info_host);
+
+/* Measured FP32 FMA throughput of the current GPU in TFLOP/s (dependent FMA chains on
+ * every SM): the denominator of the fill kernels' roofline. */
+int  pb_fp32_peak(double *tflops);
+/* cudaDeviceSynchronize on the current device (timing brackets). */
+int  pb_device_sync(void);
 
 #ifdef __cplusplus
 }

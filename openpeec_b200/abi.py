@@ -67,7 +67,7 @@ class PbSweepStats(C.Structure):
         ("corr_samples", C.c_double), ("lu_flops", C.c_double),
         ("max_resid", C.c_double), ("max_iters", C.c_int), ("form_used", C.c_int),
         ("n_system", C.c_int), ("static_refreshes", C.c_int),
-        ("kernel_launches", C.c_int),
+        ("kernel_launches", C.c_int), ("fp64_fallbacks", C.c_int),
     ]
 
     def as_dict(self):
@@ -123,6 +123,8 @@ def lib():
     L.pb_lu_decomp.argtypes = [C.c_int, _vp, _vp]
     L.pb_lu_solve.argtypes = [C.c_int, _vp, _vp, _vp]
     L.pb_lu_decomp_batched_dev.argtypes = [C.c_int, C.c_int, _vp, _vp, _vp]
+    L.pb_fp32_peak.argtypes = [C.POINTER(C.c_double)]
+    L.pb_device_sync.restype = C.c_int
     _lib = L
     return L
 

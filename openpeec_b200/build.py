@@ -19,6 +19,10 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
          "-ccbin", "/usr/bin/g++"]
 SOURCES = ["pb_api.cu", "pb_fill.cu", "pb_lu.cu", "pb_sweep.cu"]
+# The fill keeps multiply and add separate (as the reference's CPU build does) so that the
+# quadrature-order decisions (e.g. rc/lmax > 2) and the cancellation-prone FP64 closed
+# forms round like the reference; the hot accumulations use explicit fma().
+PER_FILE = {"pb_fill.cu": ["--fmad=false"]}
 
 
 def _deps():
@@ -35,7 +39,7 @@ def build(force=False, verbose=False):
         o = os.path.join(OBJ, src.replace(".cu", ".o"))
         objs.append(o)
         if (force or not os.path.exists(o) or os.path.getmtime(o) < max(os.path.getmtime(s), dep_m)):
-            cmd = [NVCC] + ARCH + FLAGS + ["-c", s, "-o", o]
+            cmd = [NVCC] + ARCH + FLAGS + PER_FILE.get(src, []) + ["-c", s, "-o", o]
             if verbose:
                 cmd += ["-Xptxas", "-v"]
                 print(" ".join(cmd))
@@ -46,7 +50,8 @@ def build(force=False, verbose=False):
             if verbose:
                 sys.stderr.write(r.stderr)
     if force or not os.path.exists(OUT) or os.path.getmtime(OUT) < max(os.path.getmtime(o) for o in objs):
-        cmd = [NVCC] + ARCH + ["-shared", "-o", OUT] + objs + ["-lcublas", "-ccbin", "/usr/bin/g++"]
+        cmd = [NVCC] + ARCH + ["-shared", "-o", OUT] + objs + ["-lcublas", "-ccbin", "/usr/bin/g++",
+               "-Xlinker", "-rpath=/usr/local/cuda/lib64"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             sys.stderr.write(r.stdout + r.stderr)

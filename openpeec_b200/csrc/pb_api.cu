@@ -412,3 +412,55 @@ int pb_lu_solve(int n, const double *a, const int *piv, double *b)
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- FP32 SIMT peak
+// Dependent FMA chains, 8 independent per thread, enough warps to fill every SM: the
+// measured FP32 FMA throughput of this GPU, the denominator of the fill roofline.
+__global__ void __launch_bounds__(256) k_fma_peak(float *out, int iters, float a, float b)
+{
+    float x[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) x[k] = threadIdx.x * 1e-3f + k;
+    for (int i = 0; i < iters; i++) {
+#pragma unroll
+        for (int k = 0; k < 8; k++) x[k] = fmaf(x[k], a, b);
+    }
+    float s = 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) s += x[k];
+    if (s == 12345.f) out[0] = s;                 // keeps the chains live
+}
+
+extern "C" int pb_fp32_peak(double *tflops)
+{
+    if (!tflops) return PB_ERR_ARG;
+    PB_TRY(need_device());
+    int dev = 0, nsm = 0;
+    PB_CUDA(cudaGetDevice(&dev));
+    PB_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    float *out = nullptr;
+    PB_CUDA(cudaMalloc(&out, sizeof(float)));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const int blocks = nsm * 8, iters = 1 << 16;
+    k_fma_peak<<<blocks, 256>>>(out, 1024, 0.999f, 1e-3f);           // warm-up
+    cudaEventRecord(e0);
+    k_fma_peak<<<blocks, 256>>>(out, iters, 0.999f, 1e-3f);
+    cudaEventRecord(e1);
+    cudaError_t e = cudaEventSynchronize(e1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(out);
+    if (e != cudaSuccess) return pb_cuda_fail(e, "k_fma_peak", __FILE__, __LINE__);
+    *tflops = 2.0 * 8.0 * iters * (double)blocks * 256 / (ms * 1e-3) / 1e12;
+    return PB_OK;
+}
+
+extern "C" int pb_device_sync(void)
+{
+    PB_CUDA(cudaDeviceSynchronize());
+    return PB_OK;
+}

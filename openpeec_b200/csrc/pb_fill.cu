@@ -29,7 +29,30 @@ template <typename R> __device__ __forceinline__ R WG8(int i);
 template <> __device__ __forceinline__ float WG8<float>(int i) { return (float)cWG8[i]; }
 template <> __device__ __forceinline__ double WG8<double>(int i) { return cWG8[i]; }
 
-__device__ __forceinline__ void sc(float x, float *s, float *c) { sincosf(x, s, c); }
+// FP32 sine/cosine for the correction integrand, arguments 0 <= x < ~1e3.
+// Quadrant reduction x = q*pi/2 + r with pi/2 split in two floats (Cody-Waite), then
+// the Taylor series of sin (to r^9) and cos (to r^8) on |r| <= pi/4: truncation below
+// 2e-9 there, and relative accuracy is kept for small x (sin r ~ r), which the
+// imaginary part -sin(kR)/R of the integrand needs at low frequency.
+__device__ __forceinline__ void sc(float x, float *s, float *c)
+{
+    const float q = rintf(x * 0.636619772367581343f);               // 2/pi
+    float r = fmaf(-q, 1.57079625129699707f, x);                    // pi/2 high part
+    r = fmaf(-q, 7.54978995489188216e-8f, r);                       // pi/2 low part
+    const float r2 = r * r;
+    float ps = fmaf(r2, 2.75573192e-6f, -1.98412698e-4f);           // 1/9!, -1/7!
+    ps = fmaf(ps, r2, 8.33333333e-3f);                              // 1/5!
+    ps = fmaf(ps, r2, -1.66666667e-1f);                             // -1/3!
+    const float sn = fmaf(ps * r2, r, r);
+    float pc = fmaf(r2, 2.48015873e-5f, -1.38888889e-3f);           // 1/8!, -1/6!
+    pc = fmaf(pc, r2, 4.16666667e-2f);                              // 1/4!
+    pc = fmaf(pc, r2, -0.5f);
+    const float cs = fmaf(pc, r2, 1.0f);
+    const int iq = ((int)q) & 3;
+    const float ss = (iq & 1) ? cs : sn, cc = (iq & 1) ? sn : cs;
+    *s = (iq & 2) ? -ss : ss;
+    *c = ((iq + 1) & 2) ? -cc : cc;
+}
 __device__ __forceinline__ void sc(double x, double *s, double *c) { sincos(x, s, c); }
 
 struct KArg {
@@ -409,6 +432,80 @@ k_pot_corr(pb_fill_geom g, KArg k, const double *st, double2 *out, long long ost
     }
 }
 
+static int grid_for(long long work, int per_block, int blocks_per_sm = 8);
+// ---------------------------------------------------------------- sample counting
+__device__ __forceinline__ long long pair_samples(const Cell &s1, const Cell &s2, int same, double kw,
+                                                  const pb_dev_cells &set, int i1, int i2)
+{
+    if (same && s1.wid <= 0 && s1.npv <= 0) { const int n = corr_nsub(s1, s1, kw); return 64LL * n * n; }
+    const int ty = pair_type(s1, s2);
+    if (ty == PT_POLY)
+        return (long long)(set.qoff[i1 + 1] - set.qoff[i1]) * (set.qoff[i2 + 1] - set.qoff[i2]);
+    if (ty == PT_HL || ty == PT_RIBBON) { const int n = ribbon_nsub(s1, s2, kw); return 256LL * n * n; }
+    const int n = corr_nsub(s1, s2, kw);
+    return 64LL * n * n;
+}
+
+__global__ void k_count(pb_fill_geom g, double kw, unsigned long long *out)
+{
+    unsigned long long acc_lp = 0, acc_p = 0;
+    const int n = g.seg.n, nc = g.ncell;
+    const long long T1 = (long long)n * (n + 1) / 2, T2 = (long long)nc * (nc + 1) / 2;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < T1 + T2;
+         t += (long long)gridDim.x * blockDim.x) {
+        if (t < T1) {
+            int i, j;
+            tri_index(t, n, i, j);
+            Cell si, sj;
+            load_cell(si, g.seg.cell, g.pv, i, 0, g.gpz);
+            double t1[3], t2[3];
+            tangent(si, t1);
+            if (i == j) {
+                acc_lp += pair_samples(si, si, 1, kw, g.seg, i, i);
+                const double tdm = t1[0] * t1[0] + t1[1] * t1[1] - t1[2] * t1[2];
+                if (g.gp && tdm != 0) { load_cell(sj, g.seg.cell, g.pv, i, 1, g.gpz); acc_lp += pair_samples(si, sj, 0, kw, g.seg, i, i); }
+            } else {
+                load_cell(sj, g.seg.cell, g.pv, j, 0, g.gpz);
+                tangent(sj, t2);
+                const double tdot = dot3(t1, t2), tdm = t1[0] * t2[0] + t1[1] * t2[1] - t1[2] * t2[2];
+                if (tdot != 0) acc_lp += pair_samples(si, sj, 0, kw, g.seg, i, j);
+                if (g.gp && tdm != 0) { load_cell(sj, g.seg.cell, g.pv, j, 1, g.gpz); acc_lp += pair_samples(si, sj, 0, kw, g.seg, i, j); }
+            }
+        } else {
+            int ci, cj;
+            tri_index(t - T1, nc, ci, cj);
+            for (int e = g.csoff[ci]; e < g.csoff[ci + 1]; e++)
+                for (int q = g.csoff[cj]; q < g.csoff[cj + 1]; q++) {
+                    const int a = min(g.csidx[e], g.csidx[q]), b = max(g.csidx[e], g.csidx[q]);
+                    Cell sa, sb;
+                    load_cell(sa, g.chg.cell, g.pv, a, 0, g.gpz);
+                    load_cell(sb, g.chg.cell, g.pv, b, 0, g.gpz);
+                    acc_p += pair_samples(sa, sb, a == b, kw, g.chg, a, b);
+                    if (g.gp) { load_cell(sb, g.chg.cell, g.pv, b, 1, g.gpz); acc_p += pair_samples(sa, sb, 0, kw, g.chg, a, b); }
+                }
+        }
+    }
+    atomicAdd(&out[0], acc_lp);
+    atomicAdd(&out[1], acc_p);
+}
+
+int pb_count_samples(const pb_fill_geom &g, double kw, double *lp_samples, double *p_samples,
+                     cudaStream_t s)
+{
+    unsigned long long *d = nullptr, h[2] = {0, 0};
+    PB_CUDA(cudaMalloc(&d, 16));
+    PB_CUDA(cudaMemsetAsync(d, 0, 16, s));
+    const long long T = (long long)g.seg.n * (g.seg.n + 1) / 2 + (long long)g.ncell * (g.ncell + 1) / 2;
+    if (T > 0) k_count<<<grid_for(T, 256), 256, 0, s>>>(g, kw, d);
+    cudaError_t e = cudaMemcpyAsync(h, d, 16, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFree(d);
+    if (e != cudaSuccess) return pb_cuda_fail(e, "pb_count_samples", __FILE__, __LINE__);
+    *lp_samples = (double)h[0];
+    *p_samples = (double)h[1];
+    return PB_OK;
+}
+
 // ---------------------------------------------------------------- internal impedance
 __device__ double2 cdiv_d(double2 a, double2 b)                   // complex.h:40-45
 {
@@ -497,7 +594,7 @@ __global__ void k_zint(pb_fill_geom g, int skin, int nf, const double *freq, dou
 }
 
 // ---------------------------------------------------------------- host launchers
-static int grid_for(long long work, int per_block, int blocks_per_sm = 8)
+static int grid_for(long long work, int per_block, int blocks_per_sm)
 {
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
@@ -551,7 +648,7 @@ static int launch_pot_corr(const pb_fill_geom &g, const KArg &k, const double *s
     return PB_OK;
 }
 
-static int pick_f(int nf) { return nf <= 1 ? 1 : nf <= 8 ? 8 : nf <= 16 ? 16 : 32; }
+static int pick_f(int nf) { return nf <= 1 ? 1 : nf <= 8 ? 8 : 16; }
 
 int pb_lp_corr(const pb_fill_geom &g, int nf, const double *kw, int use_fp32, const double *stLp,
                int epi, const pb_epi_args &ea, cudaStream_t s, long *launches, double *samples)
@@ -566,13 +663,11 @@ int pb_lp_corr(const pb_fill_geom &g, int nf, const double *kw, int use_fp32, co
     if (use_fp32) {
         r = F == 1 ? launch_lp_corr<float, 1>(g, k, stLp, epi, ea, s)
           : F == 8 ? launch_lp_corr<float, 8>(g, k, stLp, epi, ea, s)
-          : F == 16 ? launch_lp_corr<float, 16>(g, k, stLp, epi, ea, s)
-                    : launch_lp_corr<float, 32>(g, k, stLp, epi, ea, s);
+          : launch_lp_corr<float, 16>(g, k, stLp, epi, ea, s);
     } else {
         r = F == 1 ? launch_lp_corr<double, 1>(g, k, stLp, epi, ea, s)
           : F == 8 ? launch_lp_corr<double, 8>(g, k, stLp, epi, ea, s)
-          : F == 16 ? launch_lp_corr<double, 16>(g, k, stLp, epi, ea, s)
-                    : launch_lp_corr<double, 32>(g, k, stLp, epi, ea, s);
+          : launch_lp_corr<double, 16>(g, k, stLp, epi, ea, s);
     }
     if (launches) (*launches)++;
     (void)samples;
@@ -592,13 +687,11 @@ int pb_pot_corr(const pb_fill_geom &g, int nf, const double *kw, int use_fp32, c
     if (use_fp32) {
         r = F == 1 ? launch_pot_corr<float, 1>(g, k, stP, pout, pstride, s)
           : F == 8 ? launch_pot_corr<float, 8>(g, k, stP, pout, pstride, s)
-          : F == 16 ? launch_pot_corr<float, 16>(g, k, stP, pout, pstride, s)
-                    : launch_pot_corr<float, 32>(g, k, stP, pout, pstride, s);
+          : launch_pot_corr<float, 16>(g, k, stP, pout, pstride, s);
     } else {
         r = F == 1 ? launch_pot_corr<double, 1>(g, k, stP, pout, pstride, s)
           : F == 8 ? launch_pot_corr<double, 8>(g, k, stP, pout, pstride, s)
-          : F == 16 ? launch_pot_corr<double, 16>(g, k, stP, pout, pstride, s)
-                    : launch_pot_corr<double, 32>(g, k, stP, pout, pstride, s);
+          : launch_pot_corr<double, 16>(g, k, stP, pout, pstride, s);
     }
     if (launches) (*launches)++;
     (void)samples;

@@ -24,7 +24,7 @@ struct pb_fill_geom {
     int *seg_ca = nullptr, *seg_cb = nullptr;  // [nseg]
 };
 
-#define PB_FMAX 32
+#define PB_FMAX 16
 
 // Epilogue of the Lp correction kernel.
 enum { PB_EPI_STORE = 0, PB_EPI_REDUCED = 1 };
@@ -57,6 +57,11 @@ int pb_lp_corr(const pb_fill_geom &g, int nf, const double *kw, int use_fp32,
 int pb_pot_corr(const pb_fill_geom &g, int nf, const double *kw, int use_fp32,
                 const double *stP, double2 *pout, long long pstride, cudaStream_t s,
                 long *launches, double *samples);
+
+// Exact number of correction quadrature samples of one Lp / P fill at wavenumber kw
+// (used for throughput and roofline accounting).
+int pb_count_samples(const pb_fill_geom &g, double kw, double *lp_samples, double *p_samples,
+                     cudaStream_t s);
 
 // Internal impedance per segment (skin.c:112-133, mna.c:128-138, mna.c:254-258).
 int pb_zint(const pb_fill_geom &g, int skin, int nf, const double *freq, double2 *zint,

@@ -540,7 +540,8 @@ __device__ __forceinline__ void atomic_max_pos(double *addr, double v)
 
 __global__ void __launch_bounds__(256)
 k_residual(const double2 *a, int n, int ld, long long stride, const double2 *bv,
-           const double2 *xv, double2 *rv, double *rn, double *bn, int nrhs, int rows_per_block)
+           const double2 *xv, double2 *rv, double *rn, double *bn, double *xn, double *an,
+           int nrhs, int rows_per_block)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     double2 *xs = reinterpret_cast<double2 *>(smraw);     // [nrhs][n]
@@ -548,10 +549,24 @@ k_residual(const double2 *a, int n, int ld, long long stride, const double2 *bv,
     a += (long long)b * stride;
     for (int e = tid; e < nrhs * n; e += blockDim.x) xs[e] = xv[(long long)b * nrhs * n + e];
     __syncthreads();
+    if (blockIdx.x == 0) {
+        for (int q = warp; q < nrhs; q += 8) {
+            double m = 0;
+            for (int c = lane; c < n; c += 32) m = fmax(m, fmax(fabs(xs[q * n + c].x), fabs(xs[q * n + c].y)));
+            for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+            if (lane == 0) xn[b * nrhs + q] = m;
+        }
+    }
     const int rbeg = blockIdx.x * rows_per_block;
     const int rend = min(n, rbeg + rows_per_block);
     for (int r = rbeg + warp; r < rend; r += 8) {
         const double2 *row = a + (long long)r * ld;
+        if (an) {
+            double sa = 0;
+            for (int c = lane; c < n; c += 32) sa += fabs(row[c].x) + fabs(row[c].y);
+            for (int o = 16; o > 0; o >>= 1) sa += __shfl_down_sync(0xffffffffu, sa, o);
+            if (lane == 0) atomic_max_pos(&an[b], sa);
+        }
         for (int q = 0; q < nrhs; q++) {
             double sr = 0, si = 0;
             const double2 *x = xs + q * n;
@@ -577,10 +592,12 @@ k_residual(const double2 *a, int n, int ld, long long stride, const double2 *bv,
 }
 
 int pb_residual(pb_lu_engine *e, int n, int nb, int nrhs, const double2 *a, int ld, long stride,
-                const double2 *b, const double2 *x, double2 *r, double *rn, double *bn)
+                const double2 *b, const double2 *x, double2 *r, double *rn, double *bn, double *xn,
+                double *an)
 {
     PB_CUDA(cudaMemsetAsync(rn, 0, sizeof(double) * nb * nrhs, e->stream));
     PB_CUDA(cudaMemsetAsync(bn, 0, sizeof(double) * nb * nrhs, e->stream));
+    if (an) PB_CUDA(cudaMemsetAsync(an, 0, sizeof(double) * nb, e->stream));
     const size_t smem = (size_t)nrhs * n * sizeof(double2);
     static bool attr_set = false;
     if (!attr_set) {
@@ -592,7 +609,7 @@ int pb_residual(pb_lu_engine *e, int n, int nb, int nrhs, const double2 *a, int 
     }
     const int rpb = 64;
     dim3 g(ceil_div(n, rpb), nb);
-    k_residual<<<g, 256, smem, e->stream>>>(a, n, ld, stride, b, x, r, rn, bn, nrhs, rpb);
+    k_residual<<<g, 256, smem, e->stream>>>(a, n, ld, stride, b, x, r, rn, bn, xn, an, nrhs, rpb);
     e->launches++;
     PB_CHECK_LAUNCH();
     return PB_OK;

@@ -40,8 +40,9 @@ int pb_lu_solve_batched(pb_lu_engine *e, int n, int nb, int nrhs,
                         const typename cplx_t<TF>::type *lu, int ld, long stride,
                         const int *perm, const double2 *r, double2 *x);
 
-// r = b - A x for nb FP64 matrices, nrhs vectors each; also writes per-vector
-// max|r| and max|b| into rn[nb*nrhs], bn[nb*nrhs].
+// r = b - A x for nb FP64 matrices, nrhs vectors each; also writes the infinity norms
+// (max |re|,|im| component) of r, b and x per vector into rn, bn, xn [nb*nrhs] and,
+// when an != nullptr, the infinity norm of each matrix (max row sum of |re|+|im|).
 int pb_residual(pb_lu_engine *e, int n, int nb, int nrhs, const double2 *a, int ld,
                 long stride, const double2 *b, const double2 *x, double2 *r, double *rn,
-                double *bn);
+                double *bn, double *xn, double *an);

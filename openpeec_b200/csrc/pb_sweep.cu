@@ -274,6 +274,9 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
     PB_TRY(bX.alloc(vb));
     PB_TRY(bR.alloc(vb));
     PB_TRY(bD.alloc(vb));
+    DevBuf bXn, bAn;
+    PB_TRY(bXn.alloc((size_t)B * np * 8));
+    PB_TRY(bAn.alloc((size_t)B * 8));
     PB_TRY(bRn.alloc((size_t)B * np * 8));
     PB_TRY(bBn.alloc((size_t)B * np * 8));
     PB_TRY(bFreq.alloc((size_t)B * 8));
@@ -300,7 +303,9 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
     std::vector<long> cur_sig, sig;
     bool static_valid = false;
     std::vector<double2> zh((size_t)B * np * np);
-    std::vector<double> rnh(B * np), bnh(B * np);
+    std::vector<double> rnh(B * np), bnh(B * np), xnh(B * np), anh(B);
+    int fallbacks = 0;
+    double lp_samp = 0, p_samp = 0;
     std::vector<int> infoh(B);
     tAll.start(st);
 
@@ -335,6 +340,8 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
                 if (c->capacitance && nc > 0) PB_TRY(pb_pot_static(c->g, kw0, bStP.as<double>(), st, &c->launches));
                 PB_TRY(pb_lp_static(c->g, kw0, bStLp.as<double>(), st, &c->launches));
                 tStatic.stop(st);
+                if (kw0 > 0) PB_TRY(pb_count_samples(c->g, kw0, &lp_samp, &p_samp, st));
+                else lp_samp = p_samp = 0;
                 cur_sig = sig;
                 static_valid = true;
                 refreshes++;
@@ -363,6 +370,7 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
                                   &c->launches, &samples));
             }
             tCorr.stop(st);
+            samples += (lp_samp + (c->capacitance ? p_samp : 0)) * nf;
             f = e;
         }
         if (form == PB_FORM_FULL) {
@@ -370,11 +378,11 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
             PB_CUDA(cudaMemsetAsync(bM64.p, 0, (size_t)nb * n2 * 16, st));
             const int offQ = c->nunknown;
             const long long per = (long long)ns * ns + (c->capacitance ? (long long)nc * nc : 0);
-            k_full_blocks<<<ceil_div(per * nb, 256), 256, 0, st>>>(
+            if (per > 0) k_full_blocks<<<ceil_div(per * nb, 256), 256, 0, st>>>(
                 nb, n, ns, c->capacitance ? nc : 0, c->offS, offQ, bLp.as<double2>(), (long long)ns * ns,
                 bP.as<double2>(), (long long)nc * nc, bZint.as<double2>(), bFreq.as<double>(),
                 bM64.as<double2>(), (long long)n * n);
-            c->launches++;
+            if (per > 0) c->launches++;
             PB_CHECK_LAUNCH();
             const int ne = (int)c->fe_row.size();
             if (ne > 0) {
@@ -421,29 +429,61 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
             PB_TRY(pb_lu_solve_batched<double>(&c->lu, n, nb, np, bM64.as<double2>(), n, (long)n * n,
                                                bPerm.as<int>(), bRhs.as<double2>(), bX.as<double2>()));
         } else {
-            // iterative refinement: x_0 = LU^-1 b, r = b - A x (FP64), x += LU^-1 r
+            // Iterative refinement in FP64 against the FP64 matrix:
+            //   x_0 = LU^-1 b,  r = b - A x,  x += LU^-1 r,
+            // until the normwise backward error eta = |r| / (|A| |x| + |b|) (infinity norms)
+            // reaches the level of an FP64 factorisation. A frequency whose iteration
+            // stalls above that is re-solved with an FP64 LU of its matrix (counted in
+            // stats->fp64_fallbacks).
             PB_TRY(pb_lu_solve_batched<float>(&c->lu, n, nb, np, bM32.as<float2>(), n, (long)n * n,
                                               bPerm.as<int>(), bRhs.as<double2>(), bX.as<double2>()));
-            double prev = 1e300;
+            const double eta_tol = std::max(1e-14, 8.0 * std::sqrt((double)n) * 1.1e-16);
+            std::vector<int> state(nb, 0);        // 0 active, 1 converged, 2 failed
+            std::vector<double> prev(nb, 1e300);
             int it = 0;
-            for (it = 1; it <= maxit; it++) {
+            for (it = 1; it <= maxit + 1; it++) {
                 PB_TRY(pb_residual(&c->lu, n, nb, np, bM64.as<double2>(), n, (long)n * n, bRhs.as<double2>(),
-                                   bX.as<double2>(), bR.as<double2>(), bRn.as<double>(), bBn.as<double>()));
+                                   bX.as<double2>(), bR.as<double2>(), bRn.as<double>(), bBn.as<double>(),
+                                   bXn.as<double>(), it == 1 ? bAn.as<double>() : nullptr));
                 PB_CUDA(cudaMemcpyAsync(rnh.data(), bRn.p, sizeof(double) * nb * np, cudaMemcpyDeviceToHost, st));
                 PB_CUDA(cudaMemcpyAsync(bnh.data(), bBn.p, sizeof(double) * nb * np, cudaMemcpyDeviceToHost, st));
+                PB_CUDA(cudaMemcpyAsync(xnh.data(), bXn.p, sizeof(double) * nb * np, cudaMemcpyDeviceToHost, st));
+                if (it == 1) PB_CUDA(cudaMemcpyAsync(anh.data(), bAn.p, sizeof(double) * nb, cudaMemcpyDeviceToHost, st));
                 PB_CUDA(cudaStreamSynchronize(st));
-                double worst = 0;
-                for (int q = 0; q < nb * np; q++) worst = std::max(worst, bnh[q] > 0 ? rnh[q] / bnh[q] : 0.0);
-                if (worst <= tol || worst > 0.5 * prev) { maxres = std::max(maxres, worst); break; }
-                prev = worst;
+                int active = 0;
+                for (int q = 0; q < nb; q++) {
+                    if (state[q] != 0) continue;
+                    double eta = 0;
+                    for (int j = 0; j < np; j++) {
+                        const int v = q * np + j;
+                        const double den = anh[q] * xnh[v] + bnh[v];
+                        eta = std::max(eta, den > 0 ? rnh[v] / den : 0.0);
+                    }
+                    if (eta <= eta_tol) { state[q] = 1; maxres = std::max(maxres, eta); }
+                    else if (eta > 0.5 * prev[q] || it > maxit) {
+                        if (eta <= 1e3 * eta_tol) { state[q] = 1; maxres = std::max(maxres, eta); }
+                        else state[q] = 2;
+                    } else { prev[q] = eta; active++; }
+                }
+                if (active == 0) break;
                 PB_TRY(pb_lu_solve_batched<float>(&c->lu, n, nb, np, bM32.as<float2>(), n, (long)n * n,
                                                   bPerm.as<int>(), bR.as<double2>(), bD.as<double2>()));
                 k_axpy<<<ceil_div(nv, 256), 256, 0, st>>>(bX.as<double2>(), bD.as<double2>(), nv);
                 c->launches++;
                 PB_CHECK_LAUNCH();
             }
-            if (it > maxit) maxres = std::max(maxres, prev);
             maxits = std::max(maxits, it);
+            for (int q = 0; q < nb; q++) {
+                if (state[q] != 2) continue;
+                fallbacks++;
+                double2 *mq = bM64.as<double2>() + (long long)q * n * n;
+                int *pq = bPiv.as<int>() + (long long)q * n, *permq = bPerm.as<int>() + (long long)q * n;
+                PB_TRY(pb_lu_factor<double>(&c->lu, n, 1, mq, n, (long)n * n, pq, bInfo.as<int>() + q));
+                PB_TRY(pb_lu_perm(&c->lu, n, 1, pq, permq));
+                PB_TRY(pb_lu_solve_batched<double>(&c->lu, n, 1, np, mq, n, (long)n * n, permq,
+                                                   bRhs.as<double2>() + (long long)q * np * n,
+                                                   bX.as<double2>() + (long long)q * np * n));
+            }
         }
         // port voltages -> Z
         if (form == PB_FORM_REDUCED) {
@@ -485,6 +525,7 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
         stats->n_system = n;
         stats->static_refreshes = refreshes;
         stats->kernel_launches = (int)(c->launches + c->lu.launches - launches0);
+        stats->fp64_fallbacks = fallbacks;
     }
     return PB_OK;
 }

@@ -1113,3 +1113,75 @@ int or_sweep(const or_prob *o, int nfreq, const double *freq, double *zmat, int 
     free(lp); free(pm); free(cm); free(a); free(b); free(piv);
     return ret;
 }
+
+/* ------------------------------------------------------------------ CPU timing
+ * Same bounded samples as the reference harness, on the restatement (used as the CPU
+ * baseline when the reference build is not available). */
+#include <time.h>
+static double or_now(void)
+{
+    struct timespec t;
+    clock_gettime(CLOCK_MONOTONIC, &t);
+    return t.tv_sec + 1e-9 * t.tv_nsec;
+}
+
+double or_time_entries(const or_prob *o, int which, int n, const int *ij, double kw)
+{
+    double sink = 0;
+    const double t0 = or_now();
+    int e;
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : sink)
+    for (e = 0; e < n; e++) {
+        double v[2];
+        if (which) or_pot_entry(o, ij[2 * e], ij[2 * e + 1], kw, v);
+        else or_lp_entry(o, ij[2 * e], ij[2 * e + 1], kw, v);
+        sink += v[0];
+    }
+    return (or_now() - t0) + 0 * sink;
+}
+
+double or_time_lu(int n, unsigned seed)
+{
+    double *a = (double *)malloc(sizeof(double) * 2 * (size_t)n * n);
+    int *piv = (int *)malloc(sizeof(int) * (size_t)n);
+    unsigned s = seed;
+    for (size_t i = 0; i < 2 * (size_t)n * n; i++) {
+        s = s * 1103515245u + 12345u;
+        a[i] = ((s >> 8) & 0xffff) / 65536.0 - 0.5;
+    }
+    const double t0 = or_now();
+    or_lu_decomp(n, a, piv);
+    const double t1 = or_now();
+    free(a);
+    free(piv);
+    return t1 - t0;
+}
+
+double or_time_solves(int n, int ncol)
+{
+    double *a = (double *)calloc(2 * (size_t)n * n, sizeof(double));
+    double *b = (double *)malloc(sizeof(double) * 2 * (size_t)n);
+    int *piv = (int *)malloc(sizeof(int) * (size_t)n);
+    for (size_t i = 0; i < (size_t)n * n; i++) a[2 * i] = (i % (n + 1)) == 0 ? n : 0.5 / (1 + i % 7);
+    for (int i = 0; i < n; i++) piv[i] = i;
+    const double t0 = or_now();
+    for (int j = 0; j < ncol; j++) {
+        memset(b, 0, sizeof(double) * 2 * n);
+        b[2 * (j % n)] = 1;
+        or_lu_solve(n, a, piv, b);
+    }
+    const double t1 = or_now();
+    free(a); free(b); free(piv);
+    return t1 - t0;
+}
+
+int or_set_threads(int n)
+{
+#ifdef _OPENMP
+    if (n > 0) omp_set_num_threads(n);
+    return omp_get_max_threads();
+#else
+    (void)n;
+    return 1;
+#endif
+}

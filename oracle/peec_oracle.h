@@ -39,4 +39,11 @@ void or_zint(const or_prob *o, int k, double f, double *out);
 /* Single-pair geometric integral (partial.c:256-317) between current cells. */
 void or_pair_k(const or_prob *o, int i, int j, int mirror_j, double kw, double *out);
 
+
+
+/* CPU-baseline timing helpers (bounded samples, all OpenMP threads). */
+double or_time_entries(const or_prob *o, int which, int n, const int *ij, double kw);
+double or_time_lu(int n, unsigned seed);
+double or_time_solves(int n, int ncol);
+int    or_set_threads(int n);
 #endif

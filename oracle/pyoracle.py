@@ -154,6 +154,8 @@ class RefLib:
             L = C.CDLL(REF_SO)
             L.rh_load.restype = _vp
             L.rh_load.argtypes = [C.c_char_p]
+            L.rh_load_light.restype = _vp
+            L.rh_load_light.argtypes = [C.c_char_p]
             L.rh_free.argtypes = [_vp]
             L.rh_info.argtypes = [_vp, _vp]
             L.rh_infod.argtypes = [_vp, _vp]
@@ -178,8 +180,8 @@ class RefLib:
             cls._L = L
         return cls._L
 
-    def __init__(self, path):
-        self.h = self.lib().rh_load(path.encode())
+    def __init__(self, path, light=False):
+        self.h = (self.lib().rh_load_light if light else self.lib().rh_load)(path.encode())
         if not self.h:
             raise RuntimeError("reference failed to load " + path)
         info = np.zeros(20, np.int32)

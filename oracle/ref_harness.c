@@ -47,6 +47,26 @@ void *rh_load(const char *path)
     return h;
 }
 
+/* Same as rh_load without the static setup fill (for timing samples): geometry,
+ * charge-cell grouping and MNA numbering only. */
+void *rh_load_light(const char *path)
+{
+    FILE *fp = fopen(path, "r");
+    if (fp == NULL) return NULL;
+    rh_t *h = (rh_t *)calloc(1, sizeof(rh_t));
+    h->log = open_log();
+    if (input_data(fp, &h->p)) {
+        fclose(fp);
+        free(h);
+        return NULL;
+    }
+    fclose(fp);
+    if (wire_build(&h->p, h->log)) return NULL;
+    if (h->p.capacitance && h->p.nchg > 0 && pot_cells(&h->p)) return NULL;
+    if (mna_numbering(&h->p, h->log)) return NULL;
+    return h;
+}
+
 void rh_free(void *hv)
 {
     rh_t *h = (rh_t *)hv;
@@ -258,4 +278,71 @@ int rh_set_threads(int n)
     (void)n;
     return 1;
 #endif
+}
+
+/* ------------------------------------------------------------------ CPU timing
+ * Bounded samples of the reference's per-frequency work, timed with all OpenMP
+ * threads: seconds to evaluate the listed Lp (which=0) or P (which=1) entries. */
+#include <time.h>
+static double rh_now(void)
+{
+    struct timespec t;
+    clock_gettime(CLOCK_MONOTONIC, &t);
+    return t.tv_sec + 1e-9 * t.tv_nsec;
+}
+
+double rh_time_entries(void *hv, int which, int n, const int *ij, double kw)
+{
+    const peec_t *p = &((rh_t *)hv)->p;
+    double sink = 0;
+    const double t0 = rh_now();
+    int e;
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : sink)
+    for (e = 0; e < n; e++) {
+        const d_complex_t v = which ? pot_entry(p, ij[2 * e], ij[2 * e + 1], kw)
+                                    : lp_entry(p, ij[2 * e], ij[2 * e + 1], kw);
+        sink += v.r;
+    }
+    const double t1 = rh_now();
+    return (t1 - t0) + 0 * sink;
+}
+
+/* Seconds of the reference's lu_decomp on a random diagonally weighted complex matrix. */
+double rh_time_lu(int n, unsigned seed)
+{
+    d_complex_t *a = (d_complex_t *)malloc((size_t)n * n * sizeof(d_complex_t));
+    int *piv = (int *)malloc((size_t)n * sizeof(int));
+    unsigned s = seed;
+    for (size_t i = 0; i < (size_t)n * n; i++) {
+        s = s * 1103515245u + 12345u;
+        a[i].r = ((s >> 8) & 0xffff) / 65536.0 - 0.5;
+        s = s * 1103515245u + 12345u;
+        a[i].i = ((s >> 8) & 0xffff) / 65536.0 - 0.5;
+    }
+    const double t0 = rh_now();
+    lu_decomp(n, a, piv);
+    const double t1 = rh_now();
+    free(a);
+    free(piv);
+    return t1 - t0;
+}
+
+/* Seconds of `ncol` of the reference's column solves of C = P^-1 (potential.c:274-281),
+ * on the already factorised order-n random matrix of rh_time_lu's kind. */
+double rh_time_solves(int n, int ncol)
+{
+    d_complex_t *a = (d_complex_t *)malloc((size_t)n * n * sizeof(d_complex_t));
+    d_complex_t *b = (d_complex_t *)malloc((size_t)n * sizeof(d_complex_t));
+    int *piv = (int *)malloc((size_t)n * sizeof(int));
+    for (size_t i = 0; i < (size_t)n * n; i++) { a[i].r = (i % (n + 1)) == 0 ? n : 0.5 / (1 + i % 7); a[i].i = 0; }
+    for (int i = 0; i < n; i++) piv[i] = i;
+    const double t0 = rh_now();
+    for (int j = 0; j < ncol; j++) {
+        memset(b, 0, (size_t)n * sizeof(d_complex_t));
+        b[j % n] = d_complex(1, 0);
+        lu_solve(n, a, piv, b);
+    }
+    const double t1 = rh_now();
+    free(a); free(b); free(piv);
+    return t1 - t0;
 }
