@@ -134,6 +134,9 @@ typedef struct {
     int    kernel_launches; /* kernels launched by the last pb_sweep call            */
     int    fp64_fallbacks;  /* frequencies whose mixed solve did not converge and were
                                re-factorised in FP64 (reported, never silent)          */
+    int    fp64_direct;     /* frequencies solved directly in FP64 because a lower or
+                               equal frequency of the same sweep needed the fallback   */
+    double fp64_max_hz;     /* highest frequency that needed FP64                     */
 } pb_sweep_stats;
 
 const char *pb_last_error(void);

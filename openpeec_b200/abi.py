@@ -68,6 +68,7 @@ class PbSweepStats(C.Structure):
         ("max_resid", C.c_double), ("max_iters", C.c_int), ("form_used", C.c_int),
         ("n_system", C.c_int), ("static_refreshes", C.c_int),
         ("kernel_launches", C.c_int), ("fp64_fallbacks", C.c_int),
+        ("fp64_direct", C.c_int), ("fp64_max_hz", C.c_double),
     ]
 
     def as_dict(self):

@@ -36,7 +36,9 @@ template <> __device__ __forceinline__ double WG8<double>(int i) { return cWG8[i
 // imaginary part -sin(kR)/R of the integrand needs at low frequency.
 __device__ __forceinline__ void sc(float x, float *s, float *c)
 {
-    const float q = rintf(x * 0.636619772367581343f);               // 2/pi
+    // q = nearest integer to x*2/pi via the 1.5*2^23 shifter (its low mantissa bits hold q)
+    const float tq = fmaf(x, 0.636619772367581343f, 12582912.0f);
+    const float q = tq - 12582912.0f;
     float r = fmaf(-q, 1.57079625129699707f, x);                    // pi/2 high part
     r = fmaf(-q, 7.54978995489188216e-8f, r);                       // pi/2 low part
     const float r2 = r * r;
@@ -48,7 +50,7 @@ __device__ __forceinline__ void sc(float x, float *s, float *c)
     pc = fmaf(pc, r2, 4.16666667e-2f);                              // 1/4!
     pc = fmaf(pc, r2, -0.5f);
     const float cs = fmaf(pc, r2, 1.0f);
-    const int iq = ((int)q) & 3;
+    const int iq = __float_as_int(tq) & 3;
     const float ss = (iq & 1) ? cs : sn, cc = (iq & 1) ? sn : cs;
     *s = (iq & 2) ? -ss : ss;
     *c = ((iq + 1) & 2) ? -cc : cc;

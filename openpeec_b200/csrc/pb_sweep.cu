@@ -304,7 +304,8 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
     bool static_valid = false;
     std::vector<double2> zh((size_t)B * np * np);
     std::vector<double> rnh(B * np), bnh(B * np), xnh(B * np), anh(B);
-    int fallbacks = 0;
+    int fallbacks = 0, fp64_direct = 0;
+    double fp64_hz = 0;                          // frequencies <= this are solved in FP64
     double lp_samp = 0, p_samp = 0;
     std::vector<int> infoh(B);
     tAll.start(st);
@@ -399,16 +400,24 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
             }
             tAsm.stop(st);
         }
-        // factorise the batch
+        // Precision per frequency. Frequencies at or below fp64_hz (the highest frequency
+        // whose mixed solve stalled earlier in this sweep) go straight to an FP64 LU; they
+        // form a prefix of the ascending batch. The rest are factorised in FP32 and refined.
+        int nd = 0;
+        if (mixed) while (nd < nb && fb[nd] <= fp64_hz) nd++;
+        else nd = nb;
+        const long long nn = (long long)n * n;
         tLu.start(st);
-        if (mixed) PB_TRY(pb_lu_factor<float>(&c->lu, n, nb, bM32.as<float2>(), n, (long)n * n, bPiv.as<int>(), bInfo.as<int>()));
-        else PB_TRY(pb_lu_factor<double>(&c->lu, n, nb, bM64.as<double2>(), n, (long)n * n, bPiv.as<int>(), bInfo.as<int>()));
+        if (nd > 0) PB_TRY(pb_lu_factor<double>(&c->lu, n, nd, bM64.as<double2>(), n, nn, bPiv.as<int>(), bInfo.as<int>()));
+        if (nb > nd)
+            PB_TRY(pb_lu_factor<float>(&c->lu, n, nb - nd, bM32.as<float2>() + nd * nn, n, nn,
+                                       bPiv.as<int>() + (long long)nd * n, bInfo.as<int>() + nd));
         PB_TRY(pb_lu_perm(&c->lu, n, nb, bPiv.as<int>(), bPerm.as<int>()));
         tLu.stop(st);
         luflops += 8.0 / 3.0 * (double)n * n * n * nb;
         PB_CUDA(cudaMemcpyAsync(infoh.data(), bInfo.p, sizeof(int) * nb, cudaMemcpyDeviceToHost, st));
         PB_CUDA(cudaStreamSynchronize(st));
-        for (int q = 0; q < nb; q++)
+        for (int q = 0; q < nd; q++)
             if (infoh[q] >= 0) {
                 pb_set_error("singular matrix at f = %.5e Hz (row %d : floating node or ideal voltage source loop?)",
                              fb[q], infoh[q]);
@@ -425,66 +434,100 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
         }
         c->launches++;
         PB_CHECK_LAUNCH();
-        if (!mixed) {
-            PB_TRY(pb_lu_solve_batched<double>(&c->lu, n, nb, np, bM64.as<double2>(), n, (long)n * n,
+        if (nd > 0)
+            PB_TRY(pb_lu_solve_batched<double>(&c->lu, n, nd, np, bM64.as<double2>(), n, nn,
                                                bPerm.as<int>(), bRhs.as<double2>(), bX.as<double2>()));
-        } else {
+        std::vector<int> state(nb, 1);            // 0 active, 1 converged / direct, 2 failed
+        if (nb > nd) {
             // Iterative refinement in FP64 against the FP64 matrix:
             //   x_0 = LU^-1 b,  r = b - A x,  x += LU^-1 r,
             // until the normwise backward error eta = |r| / (|A| |x| + |b|) (infinity norms)
             // reaches the level of an FP64 factorisation. A frequency whose iteration
-            // stalls above that is re-solved with an FP64 LU of its matrix (counted in
-            // stats->fp64_fallbacks).
-            PB_TRY(pb_lu_solve_batched<float>(&c->lu, n, nb, np, bM32.as<float2>(), n, (long)n * n,
-                                              bPerm.as<int>(), bRhs.as<double2>(), bX.as<double2>()));
+            // stalls above that is re-solved with an FP64 LU (stats->fp64_fallbacks).
+            const int mb = nb - nd;
+            const long long vo = (long long)nd * np * n;
+            double2 *m64 = bM64.as<double2>() + nd * nn;
+            float2 *m32 = bM32.as<float2>() + nd * nn;
+            int *perm = bPerm.as<int>() + (long long)nd * n;
+            for (int q = 0; q < mb; q++)
+                if (infoh[nd + q] >= 0) state[nd + q] = 2;          // zero FP32 pivot: go FP64
+            PB_TRY(pb_lu_solve_batched<float>(&c->lu, n, mb, np, m32, n, nn, perm, bRhs.as<double2>() + vo,
+                                              bX.as<double2>() + vo));
             const double eta_tol = std::max(1e-14, 8.0 * std::sqrt((double)n) * 1.1e-16);
-            std::vector<int> state(nb, 0);        // 0 active, 1 converged, 2 failed
             std::vector<double> prev(nb, 1e300);
+            for (int q = nd; q < nb; q++) if (state[q] == 1) state[q] = 0;
             int it = 0;
             for (it = 1; it <= maxit + 1; it++) {
-                PB_TRY(pb_residual(&c->lu, n, nb, np, bM64.as<double2>(), n, (long)n * n, bRhs.as<double2>(),
-                                   bX.as<double2>(), bR.as<double2>(), bRn.as<double>(), bBn.as<double>(),
-                                   bXn.as<double>(), it == 1 ? bAn.as<double>() : nullptr));
-                PB_CUDA(cudaMemcpyAsync(rnh.data(), bRn.p, sizeof(double) * nb * np, cudaMemcpyDeviceToHost, st));
-                PB_CUDA(cudaMemcpyAsync(bnh.data(), bBn.p, sizeof(double) * nb * np, cudaMemcpyDeviceToHost, st));
-                PB_CUDA(cudaMemcpyAsync(xnh.data(), bXn.p, sizeof(double) * nb * np, cudaMemcpyDeviceToHost, st));
-                if (it == 1) PB_CUDA(cudaMemcpyAsync(anh.data(), bAn.p, sizeof(double) * nb, cudaMemcpyDeviceToHost, st));
+                PB_TRY(pb_residual(&c->lu, n, mb, np, m64, n, nn, bRhs.as<double2>() + vo, bX.as<double2>() + vo,
+                                   bR.as<double2>() + vo, bRn.as<double>(), bBn.as<double>(), bXn.as<double>(),
+                                   it == 1 ? bAn.as<double>() : nullptr));
+                PB_CUDA(cudaMemcpyAsync(rnh.data(), bRn.p, sizeof(double) * mb * np, cudaMemcpyDeviceToHost, st));
+                PB_CUDA(cudaMemcpyAsync(bnh.data(), bBn.p, sizeof(double) * mb * np, cudaMemcpyDeviceToHost, st));
+                PB_CUDA(cudaMemcpyAsync(xnh.data(), bXn.p, sizeof(double) * mb * np, cudaMemcpyDeviceToHost, st));
+                if (it == 1) PB_CUDA(cudaMemcpyAsync(anh.data(), bAn.p, sizeof(double) * mb, cudaMemcpyDeviceToHost, st));
                 PB_CUDA(cudaStreamSynchronize(st));
                 int active = 0;
-                for (int q = 0; q < nb; q++) {
-                    if (state[q] != 0) continue;
+                for (int q = 0; q < mb; q++) {
+                    if (state[nd + q] != 0) continue;
                     double eta = 0;
                     for (int j = 0; j < np; j++) {
                         const int v = q * np + j;
                         const double den = anh[q] * xnh[v] + bnh[v];
                         eta = std::max(eta, den > 0 ? rnh[v] / den : 0.0);
                     }
-                    if (eta <= eta_tol) { state[q] = 1; maxres = std::max(maxres, eta); }
-                    else if (eta > 0.5 * prev[q] || it > maxit) {
-                        if (eta <= 1e3 * eta_tol) { state[q] = 1; maxres = std::max(maxres, eta); }
-                        else state[q] = 2;
-                    } else { prev[q] = eta; active++; }
+                    if (eta <= eta_tol) { state[nd + q] = 1; maxres = std::max(maxres, eta); }
+                    else if (eta > 0.5 * prev[nd + q] || it > maxit) state[nd + q] = 2;
+                    else { prev[nd + q] = eta; active++; }
                 }
                 if (active == 0) break;
-                PB_TRY(pb_lu_solve_batched<float>(&c->lu, n, nb, np, bM32.as<float2>(), n, (long)n * n,
-                                                  bPerm.as<int>(), bR.as<double2>(), bD.as<double2>()));
-                k_axpy<<<ceil_div(nv, 256), 256, 0, st>>>(bX.as<double2>(), bD.as<double2>(), nv);
+                PB_TRY(pb_lu_solve_batched<float>(&c->lu, n, mb, np, m32, n, nn, perm, bR.as<double2>() + vo,
+                                                  bD.as<double2>() + vo));
+                const long long mv = (long long)mb * np * n;
+                k_axpy<<<ceil_div(mv, 256), 256, 0, st>>>(bX.as<double2>() + vo, bD.as<double2>() + vo, mv);
                 c->launches++;
                 PB_CHECK_LAUNCH();
             }
             maxits = std::max(maxits, it);
-            for (int q = 0; q < nb; q++) {
-                if (state[q] != 2) continue;
-                fallbacks++;
-                double2 *mq = bM64.as<double2>() + (long long)q * n * n;
-                int *pq = bPiv.as<int>() + (long long)q * n, *permq = bPerm.as<int>() + (long long)q * n;
-                PB_TRY(pb_lu_factor<double>(&c->lu, n, 1, mq, n, (long)n * n, pq, bInfo.as<int>() + q));
-                PB_TRY(pb_lu_perm(&c->lu, n, 1, pq, permq));
-                PB_TRY(pb_lu_solve_batched<double>(&c->lu, n, 1, np, mq, n, (long)n * n, permq,
-                                                   bRhs.as<double2>() + (long long)q * np * n,
-                                                   bX.as<double2>() + (long long)q * np * n));
+            // FP64 fallback, batched: copy the stalled frequencies' FP64 matrices into the
+            // (no longer needed) FP32 factor storage, factorise and solve them together.
+            std::vector<int> failed;
+            for (int q = nd; q < nb; q++) if (state[q] == 2) failed.push_back(q);
+            const int cap = std::max(1, B / 2);
+            for (size_t g0 = 0; g0 < failed.size(); g0 += cap) {
+                const int ng = (int)std::min<size_t>(cap, failed.size() - g0);
+                double2 *scr = reinterpret_cast<double2 *>(bM32.p);
+                for (int t = 0; t < ng; t++) {
+                    const int q = failed[g0 + t];
+                    PB_CUDA(cudaMemcpyAsync(scr + t * nn, bM64.as<double2>() + q * nn, sizeof(double2) * nn,
+                                            cudaMemcpyDeviceToDevice, st));
+                    PB_CUDA(cudaMemcpyAsync(bR.as<double2>() + (long long)t * np * n,
+                                            bRhs.as<double2>() + (long long)q * np * n, sizeof(double2) * np * n,
+                                            cudaMemcpyDeviceToDevice, st));
+                }
+                PB_TRY(pb_lu_factor<double>(&c->lu, n, ng, scr, n, nn, bPiv.as<int>(), bInfo.as<int>()));
+                PB_TRY(pb_lu_perm(&c->lu, n, ng, bPiv.as<int>(), bPerm.as<int>()));
+                PB_TRY(pb_lu_solve_batched<double>(&c->lu, n, ng, np, scr, n, nn, bPerm.as<int>(), bR.as<double2>(),
+                                                   bD.as<double2>()));
+                PB_CUDA(cudaMemcpyAsync(infoh.data(), bInfo.p, sizeof(int) * ng, cudaMemcpyDeviceToHost, st));
+                for (int t = 0; t < ng; t++) {
+                    const int q = failed[g0 + t];
+                    PB_CUDA(cudaMemcpyAsync(bX.as<double2>() + (long long)q * np * n, bD.as<double2>() + (long long)t * np * n,
+                                            sizeof(double2) * np * n, cudaMemcpyDeviceToDevice, st));
+                }
+                PB_CUDA(cudaStreamSynchronize(st));
+                for (int t = 0; t < ng; t++)
+                    if (infoh[t] >= 0) {
+                        pb_set_error("singular matrix at f = %.5e Hz (row %d : floating node or ideal voltage source loop?)",
+                                     fb[failed[g0 + t]], infoh[t]);
+                        return PB_ERR_SINGULAR;
+                    }
+                fallbacks += ng;
+                fp64_hz = std::max(fp64_hz, fb[failed[g0 + ng - 1]]);
+                if (o.verbose)
+                    for (int t = 0; t < ng; t++) fprintf(stderr, "pb_sweep: FP64 fallback at f = %.6e Hz\n", fb[failed[g0 + t]]);
             }
         }
+        fp64_direct += nd;
         // port voltages -> Z
         if (form == PB_FORM_REDUCED) {
             dim3 g(np, np, nb);
@@ -526,6 +569,8 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
         stats->static_refreshes = refreshes;
         stats->kernel_launches = (int)(c->launches + c->lu.launches - launches0);
         stats->fp64_fallbacks = fallbacks;
+        stats->fp64_direct = fp64_direct;
+        stats->fp64_max_hz = fp64_hz;
     }
     return PB_OK;
 }
