@@ -120,6 +120,8 @@ typedef struct {
     double refine_tol;      /* unused (refinement stops at FP64 backward-error level)  */
     int    refine_maxit;    /* max refinement / GMRES iterations (0 = 30)              */
     int    verbose;
+    int    corr_freqs;      /* frequencies per retardation-correction launch, 1..16
+                               (0 = automatic); a tuning knob, results do not depend on it */
 } pb_sweep_opts;
 
 typedef struct {

@@ -56,6 +56,7 @@ class PbSweepOpts(C.Structure):
     _fields_ = [
         ("fill_prec", C.c_int), ("lu", C.c_int), ("form", C.c_int), ("batch", C.c_int),
         ("refine_tol", C.c_double), ("refine_maxit", C.c_int), ("verbose", C.c_int),
+        ("corr_freqs", C.c_int),
     ]
 
 

@@ -29,190 +29,299 @@ template <typename R> __device__ __forceinline__ R WG8(int i);
 template <> __device__ __forceinline__ float WG8<float>(int i) { return (float)cWG8[i]; }
 template <> __device__ __forceinline__ double WG8<double>(int i) { return cWG8[i]; }
 
-// FP32 sine/cosine for the correction integrand, arguments 0 <= x < ~1e3.
-// Quadrant reduction x = q*pi/2 + r with pi/2 split in two floats (Cody-Waite), then
-// the Taylor series of sin (to r^9) and cos (to r^8) on |r| <= pi/4: truncation below
-// 2e-9 there, and relative accuracy is kept for small x (sin r ~ r), which the
-// imaginary part -sin(kR)/R of the integrand needs at low frequency.
-__device__ __forceinline__ void sc(float x, float *s, float *c)
+// Wavenumbers of one launch. kh[f] = k_f / 2 (the integrand is written in kR/2).
+// eq = 1 when the k_f are equally spaced (linear sweeps): then the FP32 path advances
+// sin/cos(k_f R/2) from frequency to frequency by angle addition instead of evaluating
+// them anew, re-seeding every 8 frequencies.
+struct KArg {
+    double kw[PB_FMAX];
+    double kh[PB_FMAX];
+    double dkh;
+    int nf, eq;
+};
+
+// sin/cos(kh * r) for the FP32 path with the argument formed and reduced in FP64:
+// the product kh*r and the quadrant reduction carry no FP32 rounding (their absolute
+// error would grow with kR); only the reduced angle |t| <= pi/4 goes to the FP32 series.
+__device__ __forceinline__ void seed_sc(double kh, float r, float *s, float *c)
 {
-    // q = nearest integer to x*2/pi via the 1.5*2^23 shifter (its low mantissa bits hold q)
-    const float tq = fmaf(x, 0.636619772367581343f, 12582912.0f);
-    const float q = tq - 12582912.0f;
-    float r = fmaf(-q, 1.57079625129699707f, x);                    // pi/2 high part
-    r = fmaf(-q, 7.54978995489188216e-8f, r);                       // pi/2 low part
-    const float r2 = r * r;
-    float ps = fmaf(r2, 2.75573192e-6f, -1.98412698e-4f);           // 1/9!, -1/7!
-    ps = fmaf(ps, r2, 8.33333333e-3f);                              // 1/5!
-    ps = fmaf(ps, r2, -1.66666667e-1f);                             // -1/3!
-    const float sn = fmaf(ps * r2, r, r);
-    float pc = fmaf(r2, 2.48015873e-5f, -1.38888889e-3f);           // 1/8!, -1/6!
-    pc = fmaf(pc, r2, 4.16666667e-2f);                              // 1/4!
+    const double x = kh * (double)r;
+    const double tq = fma(x, 0.63661977236758134308, 6755399441055744.0);  // 1.5*2^52 shifter
+    const double q = tq - 6755399441055744.0;
+    double t = fma(-q, 1.5707963267948966, x);                               // pi/2 high
+    t = fma(-q, 6.123233995736766e-17, t);                                    // pi/2 low
+    const float rr = (float)t, r2 = rr * rr;
+    float ps = fmaf(r2, 2.75573192e-6f, -1.98412698e-4f);
+    ps = fmaf(ps, r2, 8.33333333e-3f);
+    ps = fmaf(ps, r2, -1.66666667e-1f);
+    const float sn = fmaf(ps * r2, rr, rr);
+    float pc = fmaf(r2, 2.48015873e-5f, -1.38888889e-3f);
+    pc = fmaf(pc, r2, 4.16666667e-2f);
     pc = fmaf(pc, r2, -0.5f);
     const float cs = fmaf(pc, r2, 1.0f);
-    const int iq = __float_as_int(tq) & 3;
+    const int iq = __double2loint(tq) & 3;
     const float ss = (iq & 1) ? cs : sn, cc = (iq & 1) ? sn : cs;
     *s = (iq & 2) ? -ss : ss;
     *c = ((iq + 1) & 2) ? -cc : cc;
 }
-__device__ __forceinline__ void sc(double x, double *s, double *c) { sincos(x, s, c); }
 
-struct KArg {
-    double kw[PB_FMAX];
-    int nf;
-};
-
-template <typename R, int F> struct Acc {
-    R re[F], im[F];
-};
-
-// Accumulate one sample at distance r with weight w for every wavenumber.
-template <typename R, int F>
-__device__ __forceinline__ void accum(Acc<R, F> &a, const R *kh, int nf, R r, R w)
-{
-    if (r > (R)0) {
-        const R q = (R)-2 * w / r;
+// Accumulators of one lane for F wavenumbers. FP32 path: FP32 partial sums, flushed
+// into FP64 totals every 8 samples (bounded FP32 summation error). FP64 path: FP64.
+// Accumulators of one lane for F wavenumbers.
+// FP32 path: FP32 partial sums in registers, flushed every 8 samples into this lane's FP64
+// totals kept in shared memory (tot[(2f + c) * 32], conflict-free across lanes), which
+// bounds the FP32 summation error without holding 2F doubles in registers.
+// FP64 path: FP64 sums in registers.
+template <typename R, int F> struct Acc;
+template <int F> struct Acc<float, F> {
+    float pr[F], pi[F];
+    double *tot;
+    int cnt;
+    __device__ __forceinline__ void init(double *slot)
+    {
+        tot = slot;
+#pragma unroll
+        for (int f = 0; f < F; f++) { pr[f] = pi[f] = 0.f; tot[(2 * f) * 32] = 0.0; tot[(2 * f + 1) * 32] = 0.0; }
+        cnt = 0;
+    }
+    __device__ __forceinline__ void flush()
+    {
 #pragma unroll
         for (int f = 0; f < F; f++) {
-            if (f < nf) {
-                R s, c;
-                sc(kh[f] * r, &s, &c);
-                const R t = q * s;
-                a.re[f] = fma(t, s, a.re[f]);
-                a.im[f] = fma(t, c, a.im[f]);
+            tot[(2 * f) * 32] += (double)pr[f];
+            tot[(2 * f + 1) * 32] += (double)pi[f];
+            pr[f] = pi[f] = 0.f;
+        }
+        cnt = 0;
+    }
+    __device__ __forceinline__ double re(int f) const { return tot[(2 * f) * 32]; }
+    __device__ __forceinline__ double im(int f) const { return tot[(2 * f + 1) * 32]; }
+};
+template <int F> struct Acc<double, F> {
+    double tr[F], ti[F];
+    __device__ __forceinline__ void init(double *)
+    {
+#pragma unroll
+        for (int f = 0; f < F; f++) tr[f] = ti[f] = 0.0;
+    }
+    __device__ __forceinline__ void flush() {}
+    __device__ __forceinline__ double re(int f) const { return tr[f]; }
+    __device__ __forceinline__ double im(int f) const { return ti[f]; }
+};
+
+// Accumulate one sample at distance r with weight w for every wavenumber:
+//   (e^{-jkR}-1)/R = -(2 sin(kR/2)/R) (sin(kR/2) + j cos(kR/2)),  R -> 0 limit -jk.
+template <int F, int EQ>
+__device__ __forceinline__ void accum(Acc<float, F> &a, const KArg &k, float r, float w)
+{
+    if (r > 0.f) {
+        const float q = -2.f * w * __frcp_rn(r);
+        if (EQ) {
+            float sd, cd;
+            seed_sc(k.dkh, r, &sd, &cd);
+#pragma unroll
+            for (int g = 0; g < F; g += 8) {
+                float s, c;
+                seed_sc(k.kh[g], r, &s, &c);
+#pragma unroll
+                for (int u = 0; u < 8; u++) {
+                    const int f = g + u;
+                    if (f < F && f < k.nf) {
+                        const float t = q * s;
+                        a.pr[f] = fmaf(t, s, a.pr[f]);
+                        a.pi[f] = fmaf(t, c, a.pi[f]);
+                        const float s2 = fmaf(s, cd, c * sd);
+                        c = fmaf(c, cd, -(s * sd));
+                        s = s2;
+                    }
+                }
+            }
+        } else {
+#pragma unroll
+            for (int f = 0; f < F; f++) {
+                if (f < k.nf) {
+                    float s, c;
+                    seed_sc(k.kh[f], r, &s, &c);
+                    const float t = q * s;
+                    a.pr[f] = fmaf(t, s, a.pr[f]);
+                    a.pi[f] = fmaf(t, c, a.pi[f]);
+                }
             }
         }
     } else {
-        // R -> 0 limit of (e^{-jkR}-1)/R is -jk (surface.c:164-166)
 #pragma unroll
         for (int f = 0; f < F; f++)
-            if (f < nf) a.im[f] -= (R)2 * w * kh[f];
+            if (f < k.nf) a.pi[f] -= 2.f * w * (float)k.kh[f];
     }
+    if (++a.cnt == 8) a.flush();
 }
 
-// ribbon_corr (surface.c:134-178): 4^4 * nsub^2 samples; HL pairs use it too.
-template <typename R, int F>
-__device__ void corr_ribbon(const Cell &s1, const Cell &s2, int nsub, double scale,
-                            const R *kh, int nf, Acc<R, F> &a, int lane)
+template <int F, int EQ>
+__device__ __forceinline__ void accum(Acc<double, F> &a, const KArg &k, double r, double w)
 {
-    double t1d[3], w1d[3], n1d[3], c1d[3], t2d[3], w2d[3], n2d[3], c2d[3];
-    frame(s1, t1d, w1d, n1d, c1d);
-    frame(s2, t2d, w2d, n2d, c2d);
-    R t1[3], w1[3], t2[3], w2[3], cd[3];
+    if (r > 0) {
+        const double q = -2 * w / r;
 #pragma unroll
-    for (int c = 0; c < 3; c++) {
-        t1[c] = (R)t1d[c]; w1[c] = (R)w1d[c]; t2[c] = (R)t2d[c]; w2[c] = (R)w2d[c];
-        cd[c] = (R)(c2d[c] - c1d[c]);
-    }
-    const R L1 = (R)s1.len, W1 = (R)s1.wid, L2 = (R)s2.len, W2 = (R)s2.wid;
-    const R sc_ = (R)(scale * s1.len * s2.len / (16.0 * nsub * nsub));
-    const R rn = (R)nsub;
-    const int S = 256 * nsub * nsub;
-    for (int s = lane; s < S; s += 32) {
-        const int q = s & 3, m = (s >> 2) & 3, j = (s >> 4) & 3, i = (s >> 6) & 3;
-        const int rest = s >> 8, ja = rest % nsub, ia = rest / nsub;
-        const R a1 = L1 * ((ia + (R)0.5 * (1 + XG4<R>(i))) / rn - (R)0.5);
-        const R b1 = W1 * ((R)0.5 * (1 + XG4<R>(j)) - (R)0.5);
-        const R a2 = L2 * ((ja + (R)0.5 * (1 + XG4<R>(m))) / rn - (R)0.5);
-        const R b2 = W2 * ((R)0.5 * (1 + XG4<R>(q)) - (R)0.5);
-        R d2 = 0;
-#pragma unroll
-        for (int c = 0; c < 3; c++) {
-            const R p1 = a1 * t1[c] + b1 * w1[c];
-            const R p2 = a2 * t2[c] + b2 * w2[c];
-            const R d = (cd[c] + p2) - p1;
-            d2 += d * d;
+        for (int f = 0; f < F; f++) {
+            if (f < k.nf) {
+                double s, c;
+                sincos(k.kh[f] * r, &s, &c);
+                const double t = q * s;
+                a.tr[f] = fma(t, s, a.tr[f]);
+                a.ti[f] = fma(t, c, a.ti[f]);
+            }
         }
-        const R w = WG4<R>(i) * WG4<R>(j) * WG4<R>(m) * WG4<R>(q) * sc_;
-        accum<R, F>(a, kh, nf, sqrt(d2), w);
-    }
-}
-
-// gauss_kernel mode 1 (partial.c:61-99): 8x8 Gauss on nsub x nsub sub-squares.
-template <typename R, int F>
-__device__ void corr_wire(const Cell &s1, const Cell &s2, double aeff, int nsub, double scale,
-                          const R *kh, int nf, Acc<R, F> &a, int lane)
-{
-    R e1[3], e2[3], d0[3];
-#pragma unroll
-    for (int c = 0; c < 3; c++) {
-        e1[c] = (R)(s1.x2[c] - s1.x1[c]);
-        e2[c] = (R)(s2.x2[c] - s2.x1[c]);
-        d0[c] = (R)(s2.x1[c] - s1.x1[c]);
-    }
-    const R a2 = (R)(aeff * aeff);
-    const R sc_ = (R)(scale * s1.len * s2.len * 0.25 / ((double)nsub * nsub));
-    const R rn = (R)nsub;
-    const int S = 64 * nsub * nsub;
-    for (int s = lane; s < S; s += 32) {
-        const int j = s & 7, i = (s >> 3) & 7, rest = s >> 6, i2 = rest % nsub, i1 = rest / nsub;
-        const R u = (i1 + (R)0.5 * (1 + XG8<R>(i))) / rn;
-        const R v = (i2 + (R)0.5 * (1 + XG8<R>(j))) / rn;
-        R d2 = a2;
-#pragma unroll
-        for (int c = 0; c < 3; c++) {
-            const R d = (d0[c] + e2[c] * v) - e1[c] * u;
-            d2 += d * d;
-        }
-        accum<R, F>(a, kh, nf, sqrt(d2), WG8<R>(i) * WG8<R>(j) * sc_);
-    }
-}
-
-// poly_corr (polygon.c:305-334): 3-point triangle rules on both cells.
-template <typename R, int F>
-__device__ void corr_poly(const Cell &s1, const Cell &s2, const double4 *q1, int n1,
-                          const double4 *q2, int n2, double scale, const R *kh, int nf,
-                          Acc<R, F> &a, int lane)
-{
-    R cd[3];
-    const R zs = s2.mirror ? (R)-1 : (R)1;
-#pragma unroll
-    for (int c = 0; c < 3; c++)
-        cd[c] = (R)(0.5 * (s2.x1[c] + s2.x2[c]) - 0.5 * (s1.x1[c] + s1.x2[c]));
-    const double w1 = (s1.wid > 0) ? s1.wid : 1, w2 = (s2.wid > 0) ? s2.wid : 1;
-    const R sc_ = (R)(scale / (w1 * w2));
-    const int S = n1 * n2;
-    for (int s = lane; s < S; s += 32) {
-        const int k1 = s / n2, k2 = s - k1 * n2;
-        const double4 o1 = q1[k1], o2 = q2[k2];
-        const R dx = (cd[0] + (R)o2.x) - (R)o1.x;
-        const R dy = (cd[1] + (R)o2.y) - (R)o1.y;
-        const R dz = (cd[2] + zs * (R)o2.z) - (R)o1.z;
-        accum<R, F>(a, kh, nf, sqrt(dx * dx + dy * dy + dz * dz), (R)(o1.w * o2.w) * sc_);
-    }
-}
-
-// Correction of neumann_pair_k / neumann_self_k for one (possibly mirrored) pair.
-template <typename R, int F>
-__device__ void corr_pair(const Cell &s1, const Cell &s2, int same, double a1, double a2,
-                          double scale, double kw0, const pb_dev_cells &set, int i1, int i2,
-                          const R *kh, int nf, Acc<R, F> &a, int lane)
-{
-    if (same && s1.wid <= 0 && s1.npv <= 0) {          // partial.c:320-328 (wire self)
-        corr_wire<R, F>(s1, s1, a1, corr_nsub(s1, s1, kw0), scale, kh, nf, a, lane);
-        return;
-    }
-    const int ty = pair_type(s1, s2);
-    if (ty == PT_POLY) {
-        corr_poly<R, F>(s1, s2, set.qpt + set.qoff[i1], set.qoff[i1 + 1] - set.qoff[i1],
-                        set.qpt + set.qoff[i2], set.qoff[i2 + 1] - set.qoff[i2], scale, kh, nf, a, lane);
-    } else if (ty == PT_HL || ty == PT_RIBBON) {
-        corr_ribbon<R, F>(s1, s2, ribbon_nsub(s1, s2, kw0), scale, kh, nf, a, lane);
     } else {
-        corr_wire<R, F>(s1, s2, 0.5 * (a1 + a2), corr_nsub(s1, s2, kw0), scale, kh, nf, a, lane);
+#pragma unroll
+        for (int f = 0; f < F; f++)
+            if (f < k.nf) a.ti[f] -= 2 * w * k.kh[f];
     }
 }
 
-template <typename R, int F>
-__device__ __forceinline__ void warp_allreduce(Acc<R, F> &a)
+// One (possibly mirrored) pair term reduced to what its sample loop needs, in the
+// precision of that loop. Built from the FP64 cells just before the loop so that the
+// cells are not live during it.
+enum { TT_RIBBON = 0, TT_WIRE = 1, TT_POLY = 2 };
+template <typename R> struct Term {
+    int ty, nsub, n1, n2;
+    R cd[3], u1[3], v1[3], u2[3], v2[3];
+    R L1, W1, L2, W2, sc, a2, zs;
+    const double4 *q1, *q2;
+};
+
+// Quadrature choice and geometry of neumann_pair_k's retardation term
+// (partial.c:256-317, neumann_self_k partial.c:320-328).
+template <typename R>
+__device__ void make_term(Term<R> &T, const Cell &s1, const Cell &s2, int same, double a1, double a2,
+                          double scale, double kw0, const pb_dev_cells &set, int i1, int i2)
 {
+    int ty;
+    const bool wire_self = same && s1.wid <= 0 && s1.npv <= 0;
+    if (wire_self) ty = PT_WIRE;
+    else ty = pair_type(s1, s2);
+    if (ty == PT_POLY) {                                   // poly_corr, polygon.c:305-334
+        T.ty = TT_POLY;
+        T.q1 = set.qpt + set.qoff[i1];
+        T.n1 = set.qoff[i1 + 1] - set.qoff[i1];
+        T.q2 = set.qpt + set.qoff[i2];
+        T.n2 = set.qoff[i2 + 1] - set.qoff[i2];
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+            T.cd[c] = (R)(0.5 * (s2.x1[c] + s2.x2[c]) - 0.5 * (s1.x1[c] + s1.x2[c]));
+        T.zs = s2.mirror ? (R)-1 : (R)1;
+        const double w1 = (s1.wid > 0) ? s1.wid : 1, w2 = (s2.wid > 0) ? s2.wid : 1;
+        T.sc = (R)(scale / (w1 * w2));
+        T.nsub = 1;
+    } else if (ty == PT_HL || ty == PT_RIBBON) {           // ribbon_corr, surface.c:134-178
+        T.ty = TT_RIBBON;
+        const int nsub = ribbon_nsub(s1, s2, kw0);
+        double t1d[3], w1d[3], n1d[3], c1d[3], t2d[3], w2d[3], n2d[3], c2d[3];
+        frame(s1, t1d, w1d, n1d, c1d);
+        frame(s2, t2d, w2d, n2d, c2d);
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            T.u1[c] = (R)t1d[c]; T.v1[c] = (R)w1d[c]; T.u2[c] = (R)t2d[c]; T.v2[c] = (R)w2d[c];
+            T.cd[c] = (R)(c2d[c] - c1d[c]);
+        }
+        T.L1 = (R)s1.len; T.W1 = (R)s1.wid; T.L2 = (R)s2.len; T.W2 = (R)s2.wid;
+        T.sc = (R)(scale * s1.len * s2.len / (16.0 * nsub * nsub));
+        T.nsub = nsub;
+    } else {                                               // gauss_kernel mode 1, partial.c:61-99
+        T.ty = TT_WIRE;
+        const Cell &b = wire_self ? s1 : s2;
+        const double aeff = wire_self ? a1 : 0.5 * (a1 + a2);
+        const int nsub = corr_nsub(s1, b, kw0);
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            T.u1[c] = (R)(s1.x2[c] - s1.x1[c]);
+            T.u2[c] = (R)(b.x2[c] - b.x1[c]);
+            T.cd[c] = (R)(b.x1[c] - s1.x1[c]);
+        }
+        T.a2 = (R)(aeff * aeff);
+        T.sc = (R)(scale * s1.len * b.len * 0.25 / ((double)nsub * nsub));
+        T.nsub = nsub;
+    }
+}
+
+template <typename R, int F, int EQ>
+__device__ void run_term(const Term<R> &T, const KArg &k, Acc<R, F> &a, int lane)
+{
+    const int nsub = T.nsub;
+    const R rn = (R)nsub;
+    if (T.ty == TT_RIBBON) {
+        for (int sq = 0; sq < nsub * nsub; sq++) {
+            const int ia = sq / nsub, ja = sq - ia * nsub;
+            for (int s = lane; s < 256; s += 32) {
+                const int q = s & 3, m = (s >> 2) & 3, j = (s >> 4) & 3, i = (s >> 6) & 3;
+                const R a1 = T.L1 * ((ia + (R)0.5 * (1 + XG4<R>(i))) / rn - (R)0.5);
+                const R b1 = T.W1 * ((R)0.5 * (1 + XG4<R>(j)) - (R)0.5);
+                const R a2 = T.L2 * ((ja + (R)0.5 * (1 + XG4<R>(m))) / rn - (R)0.5);
+                const R b2 = T.W2 * ((R)0.5 * (1 + XG4<R>(q)) - (R)0.5);
+                R d2 = 0;
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    const R p1 = a1 * T.u1[c] + b1 * T.v1[c];
+                    const R p2 = a2 * T.u2[c] + b2 * T.v2[c];
+                    const R d = (T.cd[c] + p2) - p1;
+                    d2 += d * d;
+                }
+                accum<F, EQ>(a, k, sqrt(d2), WG4<R>(i) * WG4<R>(j) * WG4<R>(m) * WG4<R>(q) * T.sc);
+            }
+        }
+    } else if (T.ty == TT_WIRE) {
+        for (int sq = 0; sq < nsub * nsub; sq++) {
+            const int i1 = sq / nsub, i2 = sq - i1 * nsub;
+            for (int s = lane; s < 64; s += 32) {
+                const int j = s & 7, i = (s >> 3) & 7;
+                const R u = (i1 + (R)0.5 * (1 + XG8<R>(i))) / rn;
+                const R v = (i2 + (R)0.5 * (1 + XG8<R>(j))) / rn;
+                R d2 = T.a2;
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    const R d = (T.cd[c] + T.u2[c] * v) - T.u1[c] * u;
+                    d2 += d * d;
+                }
+                accum<F, EQ>(a, k, sqrt(d2), WG8<R>(i) * WG8<R>(j) * T.sc);
+            }
+        }
+    } else {
+        const int S = T.n1 * T.n2;
+        for (int s = lane; s < S; s += 32) {
+            const int k1 = s / T.n2, k2 = s - k1 * T.n2;
+            const double4 o1 = T.q1[k1], o2 = T.q2[k2];
+            const R dx = (T.cd[0] + (R)o2.x) - (R)o1.x;
+            const R dy = (T.cd[1] + (R)o2.y) - (R)o1.y;
+            const R dz = (T.cd[2] + T.zs * (R)o2.z) - (R)o1.z;
+            accum<F, EQ>(a, k, sqrt(dx * dx + dy * dy + dz * dz), (R)(o1.w * o2.w) * T.sc);
+        }
+    }
+}
+
+template <typename R, int F, int EQ>
+__device__ __forceinline__ void corr_term(const Cell &s1, const Cell &s2, int same, double a1, double a2,
+                                          double scale, double kw0, const pb_dev_cells &set, int i1,
+                                          int i2, const KArg &k, Acc<R, F> &acc, int lane)
+{
+    Term<R> T;
+    make_term<R>(T, s1, s2, same, a1, a2, scale, kw0, set, i1, i2);
+    run_term<R, F, EQ>(T, k, acc, lane);
+}
+
+// Warp sum of every frequency's accumulator; lane f receives frequency f (no divergence).
+template <typename R, int F>
+__device__ __forceinline__ void reduce_select(Acc<R, F> &a, int lane, double &cr, double &ci)
+{
+    a.flush();
+    cr = ci = 0;
 #pragma unroll
     for (int f = 0; f < F; f++) {
+        double x = a.re(f), y = a.im(f);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
-            a.re[f] += __shfl_xor_sync(0xffffffffu, a.re[f], o);
-            a.im[f] += __shfl_xor_sync(0xffffffffu, a.im[f], o);
+            x += __shfl_xor_sync(0xffffffffu, x, o);
+            y += __shfl_xor_sync(0xffffffffu, y, o);
         }
+        if (f == lane) { cr = x; ci = y; }
     }
 }
 
@@ -292,144 +401,131 @@ k_pot_static(pb_fill_geom g, double kw, double *st)
 }
 
 // ---------------------------------------------------------------- correction kernels
-template <typename R, int F, int EPI>
-__global__ void __launch_bounds__(256)
+#define PB_CORR_WARPS 4
+#ifndef PB_CORR_MINB
+#define PB_CORR_MINB 4      // resident blocks per SM the register budget is sized for
+#endif
+
+template <typename R, int F, int EPI, int EQ>
+__global__ void __launch_bounds__(32 * PB_CORR_WARPS, PB_CORR_MINB)
 k_lp_corr(pb_fill_geom g, KArg k, const double *st, pb_epi_args ea)
 {
+    __shared__ double tot[PB_CORR_WARPS][2 * F][32];
     const int n = g.seg.n;
     const long long T = (long long)n * (n + 1) / 2;
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const double coef = PB_MU0 / (4 * PB_PI);
     const double kw0 = k.kw[0];
     const int nf = k.nf;
-    R kh[F];
-#pragma unroll
-    for (int f = 0; f < F; f++) kh[f] = (R)(0.5 * (f < nf ? k.kw[f] : 0.0));
-    const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
-    for (long long t = blockIdx.x * (long long)(blockDim.x >> 5) + (threadIdx.x >> 5); t < T; t += nwarps) {
+    const long long nwarps = (long long)gridDim.x * PB_CORR_WARPS;
+    for (long long t = blockIdx.x * (long long)PB_CORR_WARPS + wib; t < T; t += nwarps) {
         int i, j;
         tri_index(t, n, i, j);
         Acc<R, F> acc;
-#pragma unroll
-        for (int f = 0; f < F; f++) { acc.re[f] = 0; acc.im[f] = 0; }
+        acc.init(&tot[wib][0][lane]);
         if (kw0 > 0) {
-            Cell si, sj;
-            load_cell(si, g.seg.cell, g.pv, i, 0, g.gpz);
-            const double ai = g.seg.cell[i].aL, aj = g.seg.cell[j].aL;
-            double t1[3], t2[3];
-            tangent(si, t1);
-            if (i == j) {
-                corr_pair<R, F>(si, si, 1, ai, ai, coef, kw0, g.seg, i, i, kh, nf, acc, lane);
-                if (g.gp) {
-                    load_cell(sj, g.seg.cell, g.pv, i, 1, g.gpz);
-                    const double tdm = t1[0] * t1[0] + t1[1] * t1[1] - t1[2] * t1[2];
-                    if (tdm != 0)
-                        corr_pair<R, F>(si, sj, 0, ai, ai, -tdm * coef, kw0, g.seg, i, i, kh, nf, acc, lane);
-                }
-            } else {
-                load_cell(sj, g.seg.cell, g.pv, j, 0, g.gpz);
-                tangent(sj, t2);
-                const double tdot = dot3(t1, t2);
-                const double tdm = t1[0] * t2[0] + t1[1] * t2[1] - t1[2] * t2[2];
-                if (tdot != 0)
-                    corr_pair<R, F>(si, sj, 0, ai, aj, tdot * coef, kw0, g.seg, i, j, kh, nf, acc, lane);
-                if (g.gp && tdm != 0) {
-                    load_cell(sj, g.seg.cell, g.pv, j, 1, g.gpz);
-                    corr_pair<R, F>(si, sj, 0, ai, aj, -tdm * coef, kw0, g.seg, i, j, kh, nf, acc, lane);
-                }
-            }
-            warp_allreduce<R, F>(acc);
-        }
-        const double s0 = st[(long long)i * n + j];
-#pragma unroll
-        for (int f = 0; f < F; f++) {
-            if (f == lane && f < nf) {
-                const double lr = s0 + (double)acc.re[f], li = (double)acc.im[f];
-                if (EPI == PB_EPI_STORE) {
-                    double2 *o = ea.out + f * ea.out_stride;
-                    o[(long long)i * n + j] = make_double2(lr, li);
-                    o[(long long)j * n + i] = make_double2(lr, li);
+            // term 1: direct pair (self for i == j); term 2: ground-plane image
+            // (partial.c:392-423). Each term rebuilds its cells so they are dead in the loops.
+            for (int term = 0; term < 2; term++) {
+                Cell si, sj;
+                load_cell(si, g.seg.cell, g.pv, i, 0, g.gpz);
+                load_cell(sj, g.seg.cell, g.pv, j, term, g.gpz);
+                double t1[3], t2[3];
+                tangent(si, t1);
+                double wgt;
+                if (i == j) {
+                    wgt = term == 0 ? 1.0 : -(t1[0] * t1[0] + t1[1] * t1[1] - t1[2] * t1[2]);
                 } else {
-                    const double om = ea.omega[f];
-                    double vr = -om * om * lr, vi = -om * om * li;
-                    if (i == j) {
-                        const double2 z = ea.zint[f * (long long)n + i];
-                        vr -= om * z.y;
-                        vi += om * z.x;
-                    }
-                    const int nc = g.ncell;
-                    const double2 *P = ea.pm + f * ea.pm_stride;
-                    const int ca = g.seg_ca[i], cb = g.seg_cb[i], da = g.seg_ca[j], db = g.seg_cb[j];
-                    if (ca >= 0 && da >= 0) { const double2 p = P[(long long)ca * nc + da]; vr += p.x; vi += p.y; }
-                    if (ca >= 0 && db >= 0) { const double2 p = P[(long long)ca * nc + db]; vr -= p.x; vi -= p.y; }
-                    if (cb >= 0 && da >= 0) { const double2 p = P[(long long)cb * nc + da]; vr -= p.x; vi -= p.y; }
-                    if (cb >= 0 && db >= 0) { const double2 p = P[(long long)cb * nc + db]; vr += p.x; vi += p.y; }
-                    double2 *m = ea.m64 + f * ea.m_stride;
-                    m[(long long)i * n + j] = make_double2(vr, vi);
-                    m[(long long)j * n + i] = make_double2(vr, vi);
-                    if (ea.m32) {
-                        float2 *m2 = ea.m32 + f * ea.m_stride;
-                        m2[(long long)i * n + j] = make_float2((float)vr, (float)vi);
-                        m2[(long long)j * n + i] = make_float2((float)vr, (float)vi);
-                    }
+                    Cell u;
+                    load_cell(u, g.seg.cell, g.pv, j, 0, g.gpz);
+                    tangent(u, t2);
+                    wgt = term == 0 ? dot3(t1, t2) : -(t1[0] * t2[0] + t1[1] * t2[1] - t1[2] * t2[2]);
+                }
+                if (wgt == 0 || (term == 1 && !g.gp)) continue;
+                corr_term<R, F, EQ>(si, sj, (i == j && term == 0), g.seg.cell[i].aL, g.seg.cell[j].aL,
+                                    wgt * coef, kw0, g.seg, i, j, k, acc, lane);
+            }
+        }
+        double cr, cim;
+        reduce_select<R, F>(acc, lane, cr, cim);
+        const double s0 = st[(long long)i * n + j];
+        const int f = lane;
+        if (f < nf) {
+            const double lr = s0 + cr, li = cim;
+            if (EPI == PB_EPI_STORE) {
+                double2 *o = ea.out + f * ea.out_stride;
+                o[(long long)i * n + j] = make_double2(lr, li);
+                o[(long long)j * n + i] = make_double2(lr, li);
+            } else {
+                const double om = ea.omega[f];
+                double vr = -om * om * lr, vi = -om * om * li;
+                if (i == j) {
+                    const double2 z = ea.zint[f * (long long)n + i];
+                    vr -= om * z.y;
+                    vi += om * z.x;
+                }
+                const int nc = g.ncell;
+                const double2 *P = ea.pm + f * ea.pm_stride;
+                const int ca = g.seg_ca[i], cb = g.seg_cb[i], da = g.seg_ca[j], db = g.seg_cb[j];
+                if (ca >= 0 && da >= 0) { const double2 p = P[(long long)ca * nc + da]; vr += p.x; vi += p.y; }
+                if (ca >= 0 && db >= 0) { const double2 p = P[(long long)ca * nc + db]; vr -= p.x; vi -= p.y; }
+                if (cb >= 0 && da >= 0) { const double2 p = P[(long long)cb * nc + da]; vr -= p.x; vi -= p.y; }
+                if (cb >= 0 && db >= 0) { const double2 p = P[(long long)cb * nc + db]; vr += p.x; vi += p.y; }
+                double2 *m = ea.m64 + f * ea.m_stride;
+                m[(long long)i * n + j] = make_double2(vr, vi);
+                m[(long long)j * n + i] = make_double2(vr, vi);
+                if (ea.m32) {
+                    float2 *m2 = ea.m32 + f * ea.m_stride;
+                    m2[(long long)i * n + j] = make_float2((float)vr, (float)vi);
+                    m2[(long long)j * n + i] = make_float2((float)vr, (float)vi);
                 }
             }
         }
     }
 }
 
-template <typename R, int F>
-__global__ void __launch_bounds__(256)
+template <typename R, int F, int EQ>
+__global__ void __launch_bounds__(32 * PB_CORR_WARPS, PB_CORR_MINB)
 k_pot_corr(pb_fill_geom g, KArg k, const double *st, double2 *out, long long ostride)
 {
+    __shared__ double tot[PB_CORR_WARPS][2 * F][32];
     const int nc = g.ncell;
     const long long T = (long long)nc * (nc + 1) / 2;
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const double kw0 = k.kw[0];
     const int nf = k.nf;
-    R kh[F];
-#pragma unroll
-    for (int f = 0; f < F; f++) kh[f] = (R)(0.5 * (f < nf ? k.kw[f] : 0.0));
-    const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
-    for (long long t = blockIdx.x * (long long)(blockDim.x >> 5) + (threadIdx.x >> 5); t < T; t += nwarps) {
+    const long long nwarps = (long long)gridDim.x * PB_CORR_WARPS;
+    for (long long t = blockIdx.x * (long long)PB_CORR_WARPS + wib; t < T; t += nwarps) {
         int ci, cj;
         tri_index(t, nc, ci, cj);
         Acc<R, F> acc;
-#pragma unroll
-        for (int f = 0; f < F; f++) { acc.re[f] = 0; acc.im[f] = 0; }
+        acc.init(&tot[wib][0][lane]);
         const double scale = 1.0 / (4 * PB_PI * PB_EPS0 * g.carea[ci] * g.carea[cj]);
-        if (kw0 > 0) {
+        if (kw0 > 0) {                                    // potential.c:124-150
             for (int e = g.csoff[ci]; e < g.csoff[ci + 1]; e++) {
                 const int h1 = g.csidx[e];
                 for (int q = g.csoff[cj]; q < g.csoff[cj + 1]; q++) {
                     const int h2 = g.csidx[q];
                     const int a = min(h1, h2), b = max(h1, h2);
-                    Cell sa, sb;
-                    load_cell(sa, g.chg.cell, g.pv, a, 0, g.gpz);
-                    const double aa = g.chg.cell[a].aP, ab = g.chg.cell[b].aP;
-                    if (a == b) {
-                        corr_pair<R, F>(sa, sa, 1, aa, aa, scale, kw0, g.chg, a, a, kh, nf, acc, lane);
-                    } else {
-                        load_cell(sb, g.chg.cell, g.pv, b, 0, g.gpz);
-                        corr_pair<R, F>(sa, sb, 0, aa, ab, scale, kw0, g.chg, a, b, kh, nf, acc, lane);
-                    }
-                    if (g.gp) {
-                        load_cell(sb, g.chg.cell, g.pv, b, 1, g.gpz);
-                        corr_pair<R, F>(sa, sb, 0, aa, ab, -scale, kw0, g.chg, a, b, kh, nf, acc, lane);
+                    for (int term = 0; term < (g.gp ? 2 : 1); term++) {
+                        Cell sa, sb;
+                        load_cell(sa, g.chg.cell, g.pv, a, 0, g.gpz);
+                        load_cell(sb, g.chg.cell, g.pv, b, term, g.gpz);
+                        corr_term<R, F, EQ>(sa, sb, (a == b && term == 0), g.chg.cell[a].aP, g.chg.cell[b].aP,
+                                            term == 0 ? scale : -scale, kw0, g.chg, a, b, k, acc, lane);
                     }
                 }
             }
-            warp_allreduce<R, F>(acc);
         }
+        double cr, cim;
+        reduce_select<R, F>(acc, lane, cr, cim);
         const double s0 = st[(long long)ci * nc + cj];
-#pragma unroll
-        for (int f = 0; f < F; f++) {
-            if (f == lane && f < nf) {
-                double2 *o = out + f * ostride;
-                const double2 v = make_double2(s0 + (double)acc.re[f], (double)acc.im[f]);
-                o[(long long)ci * nc + cj] = v;
-                o[(long long)cj * nc + ci] = v;
-            }
+        const int f = lane;
+        if (f < nf) {
+            double2 *o = out + f * ostride;
+            const double2 v = make_double2(s0 + cr, cim);
+            o[(long long)ci * nc + cj] = v;
+            o[(long long)cj * nc + ci] = v;
         }
     }
 }
@@ -633,9 +729,15 @@ static int launch_lp_corr(const pb_fill_geom &g, const KArg &k, const double *st
                           const pb_epi_args &ea, cudaStream_t s)
 {
     const long long T = (long long)g.seg.n * (g.seg.n + 1) / 2;
-    const int grid = grid_for(T, 8, 8);
-    if (epi == PB_EPI_STORE) k_lp_corr<R, F, PB_EPI_STORE><<<grid, 256, 0, s>>>(g, k, st, ea);
-    else k_lp_corr<R, F, PB_EPI_REDUCED><<<grid, 256, 0, s>>>(g, k, st, ea);
+    const int grid = grid_for(T, PB_CORR_WARPS, 16);
+    const bool eq = k.eq && sizeof(R) == 4;
+    if (epi == PB_EPI_STORE) {
+        if (eq) k_lp_corr<R, F, PB_EPI_STORE, 1><<<grid, 32 * PB_CORR_WARPS, 0, s>>>(g, k, st, ea);
+        else k_lp_corr<R, F, PB_EPI_STORE, 0><<<grid, 32 * PB_CORR_WARPS, 0, s>>>(g, k, st, ea);
+    } else {
+        if (eq) k_lp_corr<R, F, PB_EPI_REDUCED, 1><<<grid, 32 * PB_CORR_WARPS, 0, s>>>(g, k, st, ea);
+        else k_lp_corr<R, F, PB_EPI_REDUCED, 0><<<grid, 32 * PB_CORR_WARPS, 0, s>>>(g, k, st, ea);
+    }
     PB_CHECK_LAUNCH();
     return PB_OK;
 }
@@ -645,9 +747,25 @@ static int launch_pot_corr(const pb_fill_geom &g, const KArg &k, const double *s
                            long long ostride, cudaStream_t s)
 {
     const long long T = (long long)g.ncell * (g.ncell + 1) / 2;
-    k_pot_corr<R, F><<<grid_for(T, 8, 8), 256, 0, s>>>(g, k, st, out, ostride);
+    if (k.eq && sizeof(R) == 4) k_pot_corr<R, F, 1><<<grid_for(T, PB_CORR_WARPS, 16), 32 * PB_CORR_WARPS, 0, s>>>(g, k, st, out, ostride);
+    else k_pot_corr<R, F, 0><<<grid_for(T, PB_CORR_WARPS, 16), 32 * PB_CORR_WARPS, 0, s>>>(g, k, st, out, ostride);
     PB_CHECK_LAUNCH();
     return PB_OK;
+}
+
+// wavenumber set of a launch; equally spaced sets (linear sweeps) use the recurrence
+static void make_karg(KArg &k, int nf, const double *kw)
+{
+    for (int f = 0; f < PB_FMAX; f++) {
+        k.kw[f] = f < nf ? kw[f] : 0.0;
+        k.kh[f] = 0.5 * k.kw[f];
+    }
+    k.nf = nf;
+    k.dkh = nf > 1 ? 0.5 * (kw[1] - kw[0]) : 0.0;
+    k.eq = nf > 1;
+    for (int f = 1; f < nf && k.eq; f++)
+        if (fabs(kw[f] - kw[0] - f * (kw[1] - kw[0])) > 1e-9 * fabs(kw[nf - 1])) k.eq = 0;
+    if (k.dkh <= 0) k.eq = 0;
 }
 
 static int pick_f(int nf) { return nf <= 1 ? 1 : nf <= 8 ? 8 : 16; }
@@ -658,8 +776,7 @@ int pb_lp_corr(const pb_fill_geom &g, int nf, const double *kw, int use_fp32, co
     if (g.seg.n == 0) return PB_OK;
     if (nf < 1 || nf > PB_FMAX) { pb_set_error("pb_lp_corr: bad frequency count %d", nf); return PB_ERR_ARG; }
     KArg k;
-    for (int f = 0; f < PB_FMAX; f++) k.kw[f] = f < nf ? kw[f] : 0.0;
-    k.nf = nf;
+    make_karg(k, nf, kw);
     const int F = pick_f(nf);
     int r;
     if (use_fp32) {
@@ -682,8 +799,7 @@ int pb_pot_corr(const pb_fill_geom &g, int nf, const double *kw, int use_fp32, c
     if (g.ncell == 0) return PB_OK;
     if (nf < 1 || nf > PB_FMAX) { pb_set_error("pb_pot_corr: bad frequency count %d", nf); return PB_ERR_ARG; }
     KArg k;
-    for (int f = 0; f < PB_FMAX; f++) k.kw[f] = f < nf ? kw[f] : 0.0;
-    k.nf = nf;
+    make_karg(k, nf, kw);
     const int F = pick_f(nf);
     int r;
     if (use_fp32) {

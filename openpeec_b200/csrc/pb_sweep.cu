@@ -220,7 +220,7 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
     pb_sweep_opts o;
     if (opts_in) o = *opts_in;
     else { o.fill_prec = PB_PREC_MIXED; o.lu = PB_LU_TC; o.form = PB_FORM_AUTO; o.batch = 0;
-           o.refine_tol = 0; o.refine_maxit = 0; o.verbose = 0; }
+           o.refine_tol = 0; o.refine_maxit = 0; o.verbose = 0; o.corr_freqs = 0; }
     if (nfreq <= 0 || freq == nullptr) { pb_set_error("pb_sweep: no frequencies"); return PB_ERR_ARG; }
     for (int i = 0; i < nfreq; i++)
         if (!(freq[i] > 0)) { pb_set_error("pb_sweep: frequencies must be > 0"); return PB_ERR_ARG; }
@@ -323,7 +323,8 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
             const double kw0 = c->retardation ? 2 * PB_PI * fb[f] / PB_C0 : 0.0;
             level_signature(c, kw0, sig);
             int e = f + 1;
-            const int chunk_max = fill32 ? PB_FMAX : 1;        // plain path: one frequency at a time
+            // plain path: one frequency at a time (static part re-evaluated each time)
+            const int chunk_max = !fill32 ? 1 : (o.corr_freqs > 0 ? std::min(o.corr_freqs, PB_FMAX) : PB_FMAX);
             if (c->retardation) {
                 std::vector<long> s2;
                 while (e < nb && e - f < chunk_max) {
@@ -332,7 +333,7 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
                     e++;
                 }
             } else {
-                e = std::min(nb, f + PB_FMAX);
+                e = std::min(nb, f + chunk_max);
             }
             const int nf = e - f;
             // plain path re-evaluates the static part at every frequency, like the reference
