@@ -323,8 +323,13 @@ int pb_pot_fill(pb_ctx *c, double kw, int prec, double *p_host)
     PB_CUDA(cudaMalloc(&st, sizeof(double) * (size_t)n * n));
     cudaError_t e = cudaMalloc(&out, sizeof(double2) * (size_t)n * n);
     if (e != cudaSuccess) { cudaFree(st); return pb_cuda_fail(e, "cudaMalloc", __FILE__, __LINE__); }
+    double2 *ig = nullptr;
+    if (kw > 0) {
+        e = cudaMalloc(&ig, sizeof(double2) * (size_t)c->chg.size() * c->chg.size());
+        if (e != cudaSuccess) { cudaFree(st); cudaFree(out); return pb_cuda_fail(e, "cudaMalloc", __FILE__, __LINE__); }
+    }
     int r = pb_pot_static(c->g, kw, st, c->stream, &c->launches);
-    if (r == PB_OK) r = pb_pot_corr(c->g, 1, &kw, prec == PB_PREC_MIXED, st, out, (long long)n * n, c->stream, &c->launches, nullptr);
+    if (r == PB_OK) r = pb_pot_corr(c->g, 1, &kw, prec == PB_PREC_MIXED, st, out, (long long)n * n, ig, c->stream, &c->launches, nullptr);
     if (r == PB_OK) {
         e = cudaMemcpyAsync(p_host, out, sizeof(double2) * (size_t)n * n, cudaMemcpyDeviceToHost, c->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
@@ -332,6 +337,7 @@ int pb_pot_fill(pb_ctx *c, double kw, int prec, double *p_host)
     }
     cudaFree(st);
     cudaFree(out);
+    if (ig) cudaFree(ig);
     return r;
 }
 

@@ -43,9 +43,9 @@ struct KArg {
 // sin/cos(kh * r) for the FP32 path with the argument formed and reduced in FP64:
 // the product kh*r and the quadrant reduction carry no FP32 rounding (their absolute
 // error would grow with kR); only the reduced angle |t| <= pi/4 goes to the FP32 series.
-__device__ __forceinline__ void seed_sc(double kh, float r, float *s, float *c)
+__device__ __forceinline__ void seed_sc(double kh, double r, float *s, float *c)
 {
-    const double x = kh * (double)r;
+    const double x = kh * r;
     const double tq = fma(x, 0.63661977236758134308, 6755399441055744.0);  // 1.5*2^52 shifter
     const double q = tq - 6755399441055744.0;
     double t = fma(-q, 1.5707963267948966, x);                               // pi/2 high
@@ -112,17 +112,18 @@ template <int F> struct Acc<double, F> {
 // Accumulate one sample at distance r with weight w for every wavenumber:
 //   (e^{-jkR}-1)/R = -(2 sin(kR/2)/R) (sin(kR/2) + j cos(kR/2)),  R -> 0 limit -jk.
 template <int F, int EQ>
-__device__ __forceinline__ void accum(Acc<float, F> &a, const KArg &k, float r, float w)
+__device__ __forceinline__ void accum(Acc<float, F> &a, const KArg &k, double rd, float w)
 {
-    if (r > 0.f) {
+    const float r = (float)rd;
+    if (rd > 0) {
         const float q = -2.f * w * __frcp_rn(r);
         if (EQ) {
             float sd, cd;
-            seed_sc(k.dkh, r, &sd, &cd);
+            seed_sc(k.dkh, rd, &sd, &cd);
 #pragma unroll
             for (int g = 0; g < F; g += 8) {
                 float s, c;
-                seed_sc(k.kh[g], r, &s, &c);
+                seed_sc(k.kh[g], rd, &s, &c);
 #pragma unroll
                 for (int u = 0; u < 8; u++) {
                     const int f = g + u;
@@ -141,7 +142,7 @@ __device__ __forceinline__ void accum(Acc<float, F> &a, const KArg &k, float r, 
             for (int f = 0; f < F; f++) {
                 if (f < k.nf) {
                     float s, c;
-                    seed_sc(k.kh[f], r, &s, &c);
+                    seed_sc(k.kh[f], rd, &s, &c);
                     const float t = q * s;
                     a.pr[f] = fmaf(t, s, a.pr[f]);
                     a.pi[f] = fmaf(t, c, a.pi[f]);
@@ -184,8 +185,10 @@ __device__ __forceinline__ void accum(Acc<double, F> &a, const KArg &k, double r
 enum { TT_RIBBON = 0, TT_WIRE = 1, TT_POLY = 2 };
 template <typename R> struct Term {
     int ty, nsub, n1, n2;
-    R cd[3], u1[3], v1[3], u2[3], v2[3];
-    R L1, W1, L2, W2, sc, a2, zs;
+    double cd[3];                 // centre (or start-point) offset, kept in FP64
+    double a2;                    // equivalent radius squared (wire kernel)
+    R u1[3], v1[3], u2[3], v2[3];
+    R L1, W1, L2, W2, sc, zs;
     const double4 *q1, *q2;
 };
 
@@ -199,6 +202,7 @@ __device__ void make_term(Term<R> &T, const Cell &s1, const Cell &s2, int same, 
     const bool wire_self = same && s1.wid <= 0 && s1.npv <= 0;
     if (wire_self) ty = PT_WIRE;
     else ty = pair_type(s1, s2);
+    T.a2 = 0;
     if (ty == PT_POLY) {                                   // poly_corr, polygon.c:305-334
         T.ty = TT_POLY;
         T.q1 = set.qpt + set.qoff[i1];
@@ -206,8 +210,7 @@ __device__ void make_term(Term<R> &T, const Cell &s1, const Cell &s2, int same, 
         T.q2 = set.qpt + set.qoff[i2];
         T.n2 = set.qoff[i2 + 1] - set.qoff[i2];
 #pragma unroll
-        for (int c = 0; c < 3; c++)
-            T.cd[c] = (R)(0.5 * (s2.x1[c] + s2.x2[c]) - 0.5 * (s1.x1[c] + s1.x2[c]));
+        for (int c = 0; c < 3; c++) T.cd[c] = 0.5 * (s2.x1[c] + s2.x2[c]) - 0.5 * (s1.x1[c] + s1.x2[c]);
         T.zs = s2.mirror ? (R)-1 : (R)1;
         const double w1 = (s1.wid > 0) ? s1.wid : 1, w2 = (s2.wid > 0) ? s2.wid : 1;
         T.sc = (R)(scale / (w1 * w2));
@@ -221,7 +224,7 @@ __device__ void make_term(Term<R> &T, const Cell &s1, const Cell &s2, int same, 
 #pragma unroll
         for (int c = 0; c < 3; c++) {
             T.u1[c] = (R)t1d[c]; T.v1[c] = (R)w1d[c]; T.u2[c] = (R)t2d[c]; T.v2[c] = (R)w2d[c];
-            T.cd[c] = (R)(c2d[c] - c1d[c]);
+            T.cd[c] = c2d[c] - c1d[c];
         }
         T.L1 = (R)s1.len; T.W1 = (R)s1.wid; T.L2 = (R)s2.len; T.W2 = (R)s2.wid;
         T.sc = (R)(scale * s1.len * s2.len / (16.0 * nsub * nsub));
@@ -235,12 +238,30 @@ __device__ void make_term(Term<R> &T, const Cell &s1, const Cell &s2, int same, 
         for (int c = 0; c < 3; c++) {
             T.u1[c] = (R)(s1.x2[c] - s1.x1[c]);
             T.u2[c] = (R)(b.x2[c] - b.x1[c]);
-            T.cd[c] = (R)(b.x1[c] - s1.x1[c]);
+            T.cd[c] = b.x1[c] - s1.x1[c];
         }
-        T.a2 = (R)(aeff * aeff);
+        T.a2 = aeff * aeff;
         T.sc = (R)(scale * s1.len * b.len * 0.25 / ((double)nsub * nsub));
         T.nsub = nsub;
     }
+}
+
+// Distance of one sample: the large centre offset cd is added in FP64 to the small
+// in-cell offset p (FP32 on the mixed path), and R is formed in FP64 (rsqrt seed + one
+// Newton step), so the phase k*R/2 carries no error growing with the distance.
+__device__ __forceinline__ double dist64(const double *cd, const float *p, double a2)
+{
+    const double dx = cd[0] + (double)p[0], dy = cd[1] + (double)p[1], dz = cd[2] + (double)p[2];
+    const double d2 = fma(dx, dx, fma(dy, dy, fma(dz, dz, a2)));
+    if (d2 <= 0) return 0.0;
+    double y = (double)rsqrtf((float)d2);
+    y = y * fma(-0.5 * d2 * y, y, 1.5);
+    return d2 * y;
+}
+__device__ __forceinline__ double dist64(const double *cd, const double *p, double a2)
+{
+    const double dx = cd[0] + p[0], dy = cd[1] + p[1], dz = cd[2] + p[2];
+    return sqrt(dx * dx + dy * dy + dz * dz + a2);
 }
 
 template <typename R, int F, int EQ>
@@ -257,15 +278,10 @@ __device__ void run_term(const Term<R> &T, const KArg &k, Acc<R, F> &a, int lane
                 const R b1 = T.W1 * ((R)0.5 * (1 + XG4<R>(j)) - (R)0.5);
                 const R a2 = T.L2 * ((ja + (R)0.5 * (1 + XG4<R>(m))) / rn - (R)0.5);
                 const R b2 = T.W2 * ((R)0.5 * (1 + XG4<R>(q)) - (R)0.5);
-                R d2 = 0;
+                R p[3];
 #pragma unroll
-                for (int c = 0; c < 3; c++) {
-                    const R p1 = a1 * T.u1[c] + b1 * T.v1[c];
-                    const R p2 = a2 * T.u2[c] + b2 * T.v2[c];
-                    const R d = (T.cd[c] + p2) - p1;
-                    d2 += d * d;
-                }
-                accum<F, EQ>(a, k, sqrt(d2), WG4<R>(i) * WG4<R>(j) * WG4<R>(m) * WG4<R>(q) * T.sc);
+                for (int c = 0; c < 3; c++) p[c] = (a2 * T.u2[c] + b2 * T.v2[c]) - (a1 * T.u1[c] + b1 * T.v1[c]);
+                accum<F, EQ>(a, k, dist64(T.cd, p, 0.0), WG4<R>(i) * WG4<R>(j) * WG4<R>(m) * WG4<R>(q) * T.sc);
             }
         }
     } else if (T.ty == TT_WIRE) {
@@ -275,13 +291,10 @@ __device__ void run_term(const Term<R> &T, const KArg &k, Acc<R, F> &a, int lane
                 const int j = s & 7, i = (s >> 3) & 7;
                 const R u = (i1 + (R)0.5 * (1 + XG8<R>(i))) / rn;
                 const R v = (i2 + (R)0.5 * (1 + XG8<R>(j))) / rn;
-                R d2 = T.a2;
+                R p[3];
 #pragma unroll
-                for (int c = 0; c < 3; c++) {
-                    const R d = (T.cd[c] + T.u2[c] * v) - T.u1[c] * u;
-                    d2 += d * d;
-                }
-                accum<F, EQ>(a, k, sqrt(d2), WG8<R>(i) * WG8<R>(j) * T.sc);
+                for (int c = 0; c < 3; c++) p[c] = T.u2[c] * v - T.u1[c] * u;
+                accum<F, EQ>(a, k, dist64(T.cd, p, T.a2), WG8<R>(i) * WG8<R>(j) * T.sc);
             }
         }
     } else {
@@ -289,22 +302,13 @@ __device__ void run_term(const Term<R> &T, const KArg &k, Acc<R, F> &a, int lane
         for (int s = lane; s < S; s += 32) {
             const int k1 = s / T.n2, k2 = s - k1 * T.n2;
             const double4 o1 = T.q1[k1], o2 = T.q2[k2];
-            const R dx = (T.cd[0] + (R)o2.x) - (R)o1.x;
-            const R dy = (T.cd[1] + (R)o2.y) - (R)o1.y;
-            const R dz = (T.cd[2] + T.zs * (R)o2.z) - (R)o1.z;
-            accum<F, EQ>(a, k, sqrt(dx * dx + dy * dy + dz * dz), (R)(o1.w * o2.w) * T.sc);
+            R p[3];
+            p[0] = (R)o2.x - (R)o1.x;
+            p[1] = (R)o2.y - (R)o1.y;
+            p[2] = T.zs * (R)o2.z - (R)o1.z;
+            accum<F, EQ>(a, k, dist64(T.cd, p, 0.0), (R)(o1.w * o2.w) * T.sc);
         }
     }
-}
-
-template <typename R, int F, int EQ>
-__device__ __forceinline__ void corr_term(const Cell &s1, const Cell &s2, int same, double a1, double a2,
-                                          double scale, double kw0, const pb_dev_cells &set, int i1,
-                                          int i2, const KArg &k, Acc<R, F> &acc, int lane)
-{
-    Term<R> T;
-    make_term<R>(T, s1, s2, same, a1, a2, scale, kw0, set, i1, i2);
-    run_term<R, F, EQ>(T, k, acc, lane);
 }
 
 // Warp sum of every frequency's accumulator; lane f receives frequency f (no divergence).
@@ -401,57 +405,107 @@ k_pot_static(pb_fill_geom g, double kw, double *st)
 }
 
 // ---------------------------------------------------------------- correction kernels
+// One warp owns a group of 32 consecutive upper-triangle pairs. Set-up: lane l builds the
+// (at most two) term descriptors of pair l of the group - the FP64 dispatch, frames and
+// quadrature choice - into shared memory. Then the whole warp sweeps the samples of the
+// 32 pairs one after the other (lanes split the samples), so the FP64 set-up costs one
+// lane-evaluation per pair instead of 32.
 #define PB_CORR_WARPS 4
 #ifndef PB_CORR_MINB
 #define PB_CORR_MINB 4      // resident blocks per SM the register budget is sized for
 #endif
+#define PB_GROUP 32
 
-template <typename R, int F, int EPI, int EQ>
-__global__ void __launch_bounds__(32 * PB_CORR_WARPS, PB_CORR_MINB)
-k_lp_corr(pb_fill_geom g, KArg k, const double *st, pb_epi_args ea)
+enum { PB_SET_LP = 0, PB_SET_IG = 1 };
+
+struct TaskHdr { int i, j, nterm, pad; };
+
+template <typename R, int F>
+constexpr size_t corr_smem_bytes()
 {
-    __shared__ double tot[PB_CORR_WARPS][2 * F][32];
-    const int n = g.seg.n;
-    const long long T = (long long)n * (n + 1) / 2;
+    return (size_t)PB_CORR_WARPS * (2 * PB_GROUP * sizeof(Term<R>) + PB_GROUP * sizeof(TaskHdr) +
+                                     (sizeof(R) == 4 ? 2 * F * 32 * sizeof(double) : 0));
+}
+
+template <typename R, int F, int SET, int EPI, int EQ>
+__global__ void __launch_bounds__(32 * PB_CORR_WARPS, PB_CORR_MINB)
+k_corr(pb_fill_geom g, KArg k, const double *st, pb_epi_args ea, double2 *ig, long long igs)
+{
+    extern __shared__ __align__(16) unsigned char smraw[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    Term<R> *terms = reinterpret_cast<Term<R> *>(smraw) + (size_t)wib * 2 * PB_GROUP;
+    TaskHdr *hdr = reinterpret_cast<TaskHdr *>(smraw + (size_t)PB_CORR_WARPS * 2 * PB_GROUP * sizeof(Term<R>))
+                   + wib * PB_GROUP;
+    double *tot = reinterpret_cast<double *>(smraw + (size_t)PB_CORR_WARPS * (2 * PB_GROUP * sizeof(Term<R>) +
+                                                                            PB_GROUP * sizeof(TaskHdr)))
+                  + (size_t)wib * 2 * F * 32;
+    const pb_dev_cells &set = SET == PB_SET_LP ? g.seg : g.chg;
+    const int n = set.n;
+    const long long T = (long long)n * (n + 1) / 2;
     const double coef = PB_MU0 / (4 * PB_PI);
     const double kw0 = k.kw[0];
     const int nf = k.nf;
-    const long long nwarps = (long long)gridDim.x * PB_CORR_WARPS;
-    for (long long t = blockIdx.x * (long long)PB_CORR_WARPS + wib; t < T; t += nwarps) {
-        int i, j;
-        tri_index(t, n, i, j);
-        Acc<R, F> acc;
-        acc.init(&tot[wib][0][lane]);
-        if (kw0 > 0) {
-            // term 1: direct pair (self for i == j); term 2: ground-plane image
-            // (partial.c:392-423). Each term rebuilds its cells so they are dead in the loops.
-            for (int term = 0; term < 2; term++) {
-                Cell si, sj;
-                load_cell(si, g.seg.cell, g.pv, i, 0, g.gpz);
-                load_cell(sj, g.seg.cell, g.pv, j, term, g.gpz);
-                double t1[3], t2[3];
-                tangent(si, t1);
-                double wgt;
-                if (i == j) {
-                    wgt = term == 0 ? 1.0 : -(t1[0] * t1[0] + t1[1] * t1[1] - t1[2] * t1[2]);
-                } else {
-                    Cell u;
-                    load_cell(u, g.seg.cell, g.pv, j, 0, g.gpz);
-                    tangent(u, t2);
-                    wgt = term == 0 ? dot3(t1, t2) : -(t1[0] * t2[0] + t1[1] * t2[1] - t1[2] * t2[2]);
+    const long long stride = (long long)gridDim.x * PB_CORR_WARPS * PB_GROUP;
+    for (long long g0 = ((long long)blockIdx.x * PB_CORR_WARPS + wib) * PB_GROUP; g0 < T; g0 += stride) {
+        // ---- set-up: lane -> pair g0 + lane
+        const long long t = g0 + lane;
+        if (t < T) {
+            int i, j;
+            tri_index(t, n, i, j);
+            int nt = 0;
+            if (kw0 > 0) {
+                for (int term = 0; term < 2; term++) {
+                    if (term == 1 && !g.gp) break;
+                    Cell si, sj;
+                    load_cell(si, set.cell, g.pv, i, 0, g.gpz);
+                    load_cell(sj, set.cell, g.pv, j, term, g.gpz);
+                    double wgt, a1, a2;
+                    if (SET == PB_SET_LP) {                 // partial.c:392-423
+                        double t1[3], t2[3];
+                        tangent(si, t1);
+                        if (i == j) {
+                            wgt = term == 0 ? 1.0 : -(t1[0] * t1[0] + t1[1] * t1[1] - t1[2] * t1[2]);
+                        } else {
+                            Cell u;
+                            load_cell(u, set.cell, g.pv, j, 0, g.gpz);
+                            tangent(u, t2);
+                            wgt = term == 0 ? dot3(t1, t2) : -(t1[0] * t2[0] + t1[1] * t2[1] - t1[2] * t2[2]);
+                        }
+                        wgt *= coef;
+                        a1 = set.cell[i].aL;
+                        a2 = set.cell[j].aL;
+                    } else {                                // potential.c:219-236
+                        wgt = term == 0 ? 1.0 : -1.0;
+                        a1 = set.cell[i].aP;
+                        a2 = set.cell[j].aP;
+                    }
+                    if (wgt == 0) continue;
+                    make_term<R>(terms[2 * lane + nt], si, sj, (i == j && term == 0), a1, a2, wgt, kw0, set, i, j);
+                    nt++;
                 }
-                if (wgt == 0 || (term == 1 && !g.gp)) continue;
-                corr_term<R, F, EQ>(si, sj, (i == j && term == 0), g.seg.cell[i].aL, g.seg.cell[j].aL,
-                                    wgt * coef, kw0, g.seg, i, j, k, acc, lane);
             }
+            hdr[lane] = TaskHdr{i, j, nt, 0};
         }
-        double cr, cim;
-        reduce_select<R, F>(acc, lane, cr, cim);
-        const double s0 = st[(long long)i * n + j];
-        const int f = lane;
-        if (f < nf) {
-            const double lr = s0 + cr, li = cim;
+        __syncwarp();
+        // ---- samples of the 32 pairs, one after the other
+        for (int tk = 0; tk < PB_GROUP; tk++) {
+            if (g0 + tk >= T) break;
+            const TaskHdr h = hdr[tk];
+            Acc<R, F> acc;
+            acc.init(tot + lane);
+            for (int q = 0; q < h.nterm; q++) {
+                const Term<R> tm = terms[2 * tk + q];
+                run_term<R, F, EQ>(tm, k, acc, lane);
+            }
+            double cr, cim;
+            reduce_select<R, F>(acc, lane, cr, cim);
+            const int f = lane, i = h.i, j = h.j;
+            if (f >= nf) continue;
+            if (SET == PB_SET_IG) {
+                ig[f * igs + (long long)i * n + j] = make_double2(cr, cim);
+                continue;
+            }
+            const double lr = st[(long long)i * n + j] + cr, li = cim;
             if (EPI == PB_EPI_STORE) {
                 double2 *o = ea.out + f * ea.out_stride;
                 o[(long long)i * n + j] = make_double2(lr, li);
@@ -467,10 +521,10 @@ k_lp_corr(pb_fill_geom g, KArg k, const double *st, pb_epi_args ea)
                 const int nc = g.ncell;
                 const double2 *P = ea.pm + f * ea.pm_stride;
                 const int ca = g.seg_ca[i], cb = g.seg_cb[i], da = g.seg_ca[j], db = g.seg_cb[j];
-                if (ca >= 0 && da >= 0) { const double2 p = P[(long long)ca * nc + da]; vr += p.x; vi += p.y; }
-                if (ca >= 0 && db >= 0) { const double2 p = P[(long long)ca * nc + db]; vr -= p.x; vi -= p.y; }
-                if (cb >= 0 && da >= 0) { const double2 p = P[(long long)cb * nc + da]; vr -= p.x; vi -= p.y; }
-                if (cb >= 0 && db >= 0) { const double2 p = P[(long long)cb * nc + db]; vr += p.x; vi += p.y; }
+                if (ca >= 0 && da >= 0) { const double2 pp = P[(long long)ca * nc + da]; vr += pp.x; vi += pp.y; }
+                if (ca >= 0 && db >= 0) { const double2 pp = P[(long long)ca * nc + db]; vr -= pp.x; vi -= pp.y; }
+                if (cb >= 0 && da >= 0) { const double2 pp = P[(long long)cb * nc + da]; vr -= pp.x; vi -= pp.y; }
+                if (cb >= 0 && db >= 0) { const double2 pp = P[(long long)cb * nc + db]; vr += pp.x; vi += pp.y; }
                 double2 *m = ea.m64 + f * ea.m_stride;
                 m[(long long)i * n + j] = make_double2(vr, vi);
                 m[(long long)j * n + i] = make_double2(vr, vi);
@@ -481,53 +535,40 @@ k_lp_corr(pb_fill_geom g, KArg k, const double *st, pb_epi_args ea)
                 }
             }
         }
+        __syncwarp();
     }
 }
 
-template <typename R, int F, int EQ>
-__global__ void __launch_bounds__(32 * PB_CORR_WARPS, PB_CORR_MINB)
-k_pot_corr(pb_fill_geom g, KArg k, const double *st, double2 *out, long long ostride)
+// P(f)[ci][cj] = static + 1/(4 pi eps0 Ai Aj) * sum over sub-cell pairs of the correction
+// (potential.c:124-150 ordering of the sub-pairs); thread per (f, ci <= cj).
+__global__ void k_pot_aggr(pb_fill_geom g, int nf, const double *st, const double2 *ig, long long igs,
+                           double2 *out, long long ostride)
 {
-    __shared__ double tot[PB_CORR_WARPS][2 * F][32];
-    const int nc = g.ncell;
+    const int nc = g.ncell, nh = g.chg.n;
     const long long T = (long long)nc * (nc + 1) / 2;
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const double kw0 = k.kw[0];
-    const int nf = k.nf;
-    const long long nwarps = (long long)gridDim.x * PB_CORR_WARPS;
-    for (long long t = blockIdx.x * (long long)PB_CORR_WARPS + wib; t < T; t += nwarps) {
-        int ci, cj;
-        tri_index(t, nc, ci, cj);
-        Acc<R, F> acc;
-        acc.init(&tot[wib][0][lane]);
-        const double scale = 1.0 / (4 * PB_PI * PB_EPS0 * g.carea[ci] * g.carea[cj]);
-        if (kw0 > 0) {                                    // potential.c:124-150
-            for (int e = g.csoff[ci]; e < g.csoff[ci + 1]; e++) {
-                const int h1 = g.csidx[e];
-                for (int q = g.csoff[cj]; q < g.csoff[cj + 1]; q++) {
-                    const int h2 = g.csidx[q];
-                    const int a = min(h1, h2), b = max(h1, h2);
-                    for (int term = 0; term < (g.gp ? 2 : 1); term++) {
-                        Cell sa, sb;
-                        load_cell(sa, g.chg.cell, g.pv, a, 0, g.gpz);
-                        load_cell(sb, g.chg.cell, g.pv, b, term, g.gpz);
-                        corr_term<R, F, EQ>(sa, sb, (a == b && term == 0), g.chg.cell[a].aP, g.chg.cell[b].aP,
-                                            term == 0 ? scale : -scale, kw0, g.chg, a, b, k, acc, lane);
-                    }
-                }
+    const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (idx >= T * nf) return;
+    const int f = (int)(idx / T);
+    int ci, cj;
+    tri_index(idx - f * T, nc, ci, cj);
+    double sr = 0, si = 0;
+    if (ig) {
+        const double2 *I = ig + f * igs;
+        for (int e = g.csoff[ci]; e < g.csoff[ci + 1]; e++) {
+            const int h1 = g.csidx[e];
+            for (int q = g.csoff[cj]; q < g.csoff[cj + 1]; q++) {
+                const int h2 = g.csidx[q];
+                const double2 v = I[(long long)min(h1, h2) * nh + max(h1, h2)];
+                sr += v.x;
+                si += v.y;
             }
         }
-        double cr, cim;
-        reduce_select<R, F>(acc, lane, cr, cim);
-        const double s0 = st[(long long)ci * nc + cj];
-        const int f = lane;
-        if (f < nf) {
-            double2 *o = out + f * ostride;
-            const double2 v = make_double2(s0 + cr, cim);
-            o[(long long)ci * nc + cj] = v;
-            o[(long long)cj * nc + ci] = v;
-        }
     }
+    const double sc = 1.0 / (4 * PB_PI * PB_EPS0 * g.carea[ci] * g.carea[cj]);
+    const double2 v = make_double2(st[(long long)ci * nc + cj] + sc * sr, sc * si);
+    double2 *o = out + f * ostride;
+    o[(long long)ci * nc + cj] = v;
+    o[(long long)cj * nc + ci] = v;
 }
 
 static int grid_for(long long work, int per_block, int blocks_per_sm = 8);
@@ -724,33 +765,45 @@ int pb_pot_static(const pb_fill_geom &g, double kw, double *stP, cudaStream_t s,
     return PB_OK;
 }
 
-template <typename R, int F>
-static int launch_lp_corr(const pb_fill_geom &g, const KArg &k, const double *st, int epi,
-                          const pb_epi_args &ea, cudaStream_t s)
+template <typename R, int F, int SET, int EPI, int EQ>
+static int launch_corr(const pb_fill_geom &g, const KArg &k, const double *st, const pb_epi_args &ea,
+                       double2 *ig, long long igs, cudaStream_t s)
 {
-    const long long T = (long long)g.seg.n * (g.seg.n + 1) / 2;
-    const int grid = grid_for(T, PB_CORR_WARPS, 16);
-    const bool eq = k.eq && sizeof(R) == 4;
-    if (epi == PB_EPI_STORE) {
-        if (eq) k_lp_corr<R, F, PB_EPI_STORE, 1><<<grid, 32 * PB_CORR_WARPS, 0, s>>>(g, k, st, ea);
-        else k_lp_corr<R, F, PB_EPI_STORE, 0><<<grid, 32 * PB_CORR_WARPS, 0, s>>>(g, k, st, ea);
-    } else {
-        if (eq) k_lp_corr<R, F, PB_EPI_REDUCED, 1><<<grid, 32 * PB_CORR_WARPS, 0, s>>>(g, k, st, ea);
-        else k_lp_corr<R, F, PB_EPI_REDUCED, 0><<<grid, 32 * PB_CORR_WARPS, 0, s>>>(g, k, st, ea);
+    const int n = SET == PB_SET_LP ? g.seg.n : g.chg.n;
+    const long long T = (long long)n * (n + 1) / 2;
+    constexpr size_t smem = corr_smem_bytes<R, F>();
+    static bool attr_set = false;
+    if (!attr_set) {
+        PB_CUDA(cudaFuncSetAttribute(k_corr<R, F, SET, EPI, EQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr_set = true;
     }
+    const int grid = grid_for((T + PB_GROUP - 1) / PB_GROUP, PB_CORR_WARPS, PB_CORR_MINB);
+    k_corr<R, F, SET, EPI, EQ><<<grid, 32 * PB_CORR_WARPS, smem, s>>>(g, k, st, ea, ig, igs);
     PB_CHECK_LAUNCH();
     return PB_OK;
 }
 
-template <typename R, int F>
-static int launch_pot_corr(const pb_fill_geom &g, const KArg &k, const double *st, double2 *out,
-                           long long ostride, cudaStream_t s)
+template <typename R, int F, int SET, int EPI>
+static int launch_corr_eq(const pb_fill_geom &g, const KArg &k, const double *st, const pb_epi_args &ea,
+                          double2 *ig, long long igs, cudaStream_t s)
 {
-    const long long T = (long long)g.ncell * (g.ncell + 1) / 2;
-    if (k.eq && sizeof(R) == 4) k_pot_corr<R, F, 1><<<grid_for(T, PB_CORR_WARPS, 16), 32 * PB_CORR_WARPS, 0, s>>>(g, k, st, out, ostride);
-    else k_pot_corr<R, F, 0><<<grid_for(T, PB_CORR_WARPS, 16), 32 * PB_CORR_WARPS, 0, s>>>(g, k, st, out, ostride);
-    PB_CHECK_LAUNCH();
-    return PB_OK;
+    if (k.eq && sizeof(R) == 4) return launch_corr<R, F, SET, EPI, 1>(g, k, st, ea, ig, igs, s);
+    return launch_corr<R, F, SET, EPI, 0>(g, k, st, ea, ig, igs, s);
+}
+
+template <int SET, int EPI>
+static int launch_corr_any(const pb_fill_geom &g, const KArg &k, int use_fp32, const double *st,
+                           const pb_epi_args &ea, double2 *ig, long long igs, cudaStream_t s)
+{
+    const int F = k.nf <= 1 ? 1 : k.nf <= 8 ? 8 : 16;
+    if (use_fp32) {
+        if (F == 1) return launch_corr_eq<float, 1, SET, EPI>(g, k, st, ea, ig, igs, s);
+        if (F == 8) return launch_corr_eq<float, 8, SET, EPI>(g, k, st, ea, ig, igs, s);
+        return launch_corr_eq<float, 16, SET, EPI>(g, k, st, ea, ig, igs, s);
+    }
+    if (F == 1) return launch_corr_eq<double, 1, SET, EPI>(g, k, st, ea, ig, igs, s);
+    if (F == 8) return launch_corr_eq<double, 8, SET, EPI>(g, k, st, ea, ig, igs, s);
+    return launch_corr_eq<double, 16, SET, EPI>(g, k, st, ea, ig, igs, s);
 }
 
 // wavenumber set of a launch; equally spaced sets (linear sweeps) use the recurrence
@@ -768,8 +821,6 @@ static void make_karg(KArg &k, int nf, const double *kw)
     if (k.dkh <= 0) k.eq = 0;
 }
 
-static int pick_f(int nf) { return nf <= 1 ? 1 : nf <= 8 ? 8 : 16; }
-
 int pb_lp_corr(const pb_fill_geom &g, int nf, const double *kw, int use_fp32, const double *stLp,
                int epi, const pb_epi_args &ea, cudaStream_t s, long *launches, double *samples)
 {
@@ -777,43 +828,37 @@ int pb_lp_corr(const pb_fill_geom &g, int nf, const double *kw, int use_fp32, co
     if (nf < 1 || nf > PB_FMAX) { pb_set_error("pb_lp_corr: bad frequency count %d", nf); return PB_ERR_ARG; }
     KArg k;
     make_karg(k, nf, kw);
-    const int F = pick_f(nf);
-    int r;
-    if (use_fp32) {
-        r = F == 1 ? launch_lp_corr<float, 1>(g, k, stLp, epi, ea, s)
-          : F == 8 ? launch_lp_corr<float, 8>(g, k, stLp, epi, ea, s)
-          : launch_lp_corr<float, 16>(g, k, stLp, epi, ea, s);
-    } else {
-        r = F == 1 ? launch_lp_corr<double, 1>(g, k, stLp, epi, ea, s)
-          : F == 8 ? launch_lp_corr<double, 8>(g, k, stLp, epi, ea, s)
-          : launch_lp_corr<double, 16>(g, k, stLp, epi, ea, s);
-    }
+    const int r = epi == PB_EPI_STORE
+        ? launch_corr_any<PB_SET_LP, PB_EPI_STORE>(g, k, use_fp32, stLp, ea, nullptr, 0, s)
+        : launch_corr_any<PB_SET_LP, PB_EPI_REDUCED>(g, k, use_fp32, stLp, ea, nullptr, 0, s);
     if (launches) (*launches)++;
     (void)samples;
     return r;
 }
 
 int pb_pot_corr(const pb_fill_geom &g, int nf, const double *kw, int use_fp32, const double *stP,
-                double2 *pout, long long pstride, cudaStream_t s, long *launches, double *samples)
+                double2 *pout, long long pstride, double2 *igbuf, cudaStream_t s, long *launches,
+                double *samples)
 {
     if (g.ncell == 0) return PB_OK;
     if (nf < 1 || nf > PB_FMAX) { pb_set_error("pb_pot_corr: bad frequency count %d", nf); return PB_ERR_ARG; }
     KArg k;
     make_karg(k, nf, kw);
-    const int F = pick_f(nf);
-    int r;
-    if (use_fp32) {
-        r = F == 1 ? launch_pot_corr<float, 1>(g, k, stP, pout, pstride, s)
-          : F == 8 ? launch_pot_corr<float, 8>(g, k, stP, pout, pstride, s)
-          : launch_pot_corr<float, 16>(g, k, stP, pout, pstride, s);
-    } else {
-        r = F == 1 ? launch_pot_corr<double, 1>(g, k, stP, pout, pstride, s)
-          : F == 8 ? launch_pot_corr<double, 8>(g, k, stP, pout, pstride, s)
-          : launch_pot_corr<double, 16>(g, k, stP, pout, pstride, s);
+    const long long igs = (long long)g.chg.n * g.chg.n;
+    const bool corr = kw[0] > 0;
+    if (corr) {
+        if (!igbuf) { pb_set_error("pb_pot_corr: missing sub-cell buffer"); return PB_ERR_ARG; }
+        pb_epi_args ea;
+        const int r = launch_corr_any<PB_SET_IG, PB_EPI_STORE>(g, k, use_fp32, nullptr, ea, igbuf, igs, s);
+        if (r != PB_OK) return r;
+        if (launches) (*launches)++;
     }
+    const long long T = (long long)g.ncell * (g.ncell + 1) / 2 * nf;
+    k_pot_aggr<<<ceil_div(T, 256), 256, 0, s>>>(g, nf, stP, corr ? igbuf : nullptr, igs, pout, pstride);
     if (launches) (*launches)++;
+    PB_CHECK_LAUNCH();
     (void)samples;
-    return r;
+    return PB_OK;
 }
 
 int pb_zint(const pb_fill_geom &g, int skin, int nf, const double *freq, double2 *zint,

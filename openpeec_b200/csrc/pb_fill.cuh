@@ -54,9 +54,11 @@ int pb_pot_static(const pb_fill_geom &g, double kw, double *stP, cudaStream_t s,
 int pb_lp_corr(const pb_fill_geom &g, int nf, const double *kw, int use_fp32,
                const double *stLp, int epi, const pb_epi_args &ea, cudaStream_t s,
                long *launches, double *samples);
+// P correction: sub-cell pair corrections go to igbuf [nf][nchg*nchg] (upper triangle,
+// needed only when kw > 0) and are aggregated to cells with the static part into pout.
 int pb_pot_corr(const pb_fill_geom &g, int nf, const double *kw, int use_fp32,
-                const double *stP, double2 *pout, long long pstride, cudaStream_t s,
-                long *launches, double *samples);
+                const double *stP, double2 *pout, long long pstride, double2 *igbuf,
+                cudaStream_t s, long *launches, double *samples);
 
 // Exact number of correction quadrature samples of one Lp / P fill at wavenumber kw
 // (used for throughput and roofline accounting).

@@ -248,7 +248,8 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
     const double n2 = (double)n * n;
     double perf = n2 * 16 + (mixed ? n2 * 8 : 0) + (double)nc * nc * 16 + (double)ns * 16
                 + (form == PB_FORM_FULL ? (double)ns * ns * 16 : 0) + 4.0 * np * n * 16 + 8.0 * n;
-    const double fixed = (double)ns * ns * 8 + (double)nc * nc * 8;
+    const double fixed = (double)ns * ns * 8 + (double)nc * nc * 8 +
+                         (c->retardation ? (double)PB_FMAX * c->chg.size() * c->chg.size() * 16 : 0.0);
     int B = o.batch;
     if (B <= 0) {
         const double avail = 0.80 * (double)fr - fixed - 256e6;
@@ -262,6 +263,9 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
     PB_TRY(bM64.alloc((size_t)B * n2 * 16));
     if (mixed) PB_TRY(bM32.alloc((size_t)B * n2 * 8));
     PB_TRY(bP.alloc((size_t)B * nc * nc * 16 + 16));
+    DevBuf bIg;                                  // sub-cell P corrections of one fill chunk
+    if (c->capacitance && nc > 0 && c->retardation)
+        PB_TRY(bIg.alloc((size_t)PB_FMAX * c->chg.size() * c->chg.size() * 16));
     if (form == PB_FORM_FULL) PB_TRY(bLp.alloc((size_t)B * ns * ns * 16 + 16));
     PB_TRY(bStLp.alloc((size_t)ns * ns * 8 + 16));
     PB_TRY(bStP.alloc((size_t)nc * nc * 8 + 16));
@@ -353,7 +357,7 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
             tCorr.start(st);
             if (c->capacitance && nc > 0)
                 PB_TRY(pb_pot_corr(c->g, nf, kw, fill32, bStP.as<double>(), bP.as<double2>() + (long long)f * nc * nc,
-                                   (long long)nc * nc, st, &c->launches, &samples));
+                                   (long long)nc * nc, bIg.as<double2>(), st, &c->launches, &samples));
             pb_epi_args ea;
             for (int q = 0; q < nf; q++) ea.omega[q] = 2 * PB_PI * fb[f + q];
             if (form == PB_FORM_REDUCED) {
