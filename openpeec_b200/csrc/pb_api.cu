@@ -1,6 +1,7 @@
 // pb_api.cu — C entry points of the batched core (include/peec_b200.h).
 #include "pb_ctx.cuh"
 #include <algorithm>
+#include <cmath>
 #include <cstdarg>
 #include <cstring>
 #include <map>
@@ -233,6 +234,21 @@ int pb_create(const pb_problem_t *prob, pb_ctx **out)
     auto fail = [&](int rr) { pb_destroy(c); return rr; };
     pb_fill_geom &g = c->g;
     g.gp = c->gp; g.gpz = c->gpz; g.ncell = c->ncell;
+    {
+        // bounding box of every cell point (and its ground-plane image) -> distance bound
+        double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+        auto add = [&](const double *x) {
+            for (int q = 0; q < 3; q++) { lo[q] = std::min(lo[q], x[q]); hi[q] = std::max(hi[q], x[q]); }
+            if (c->gp) { lo[2] = std::min(lo[2], 2 * c->gpz - x[2]); hi[2] = std::max(hi[2], 2 * c->gpz - x[2]); }
+        };
+        double wmax = 0;
+        for (auto *v : {&c->seg, &c->chg})
+            for (auto &x : *v) { add(x.x1); add(x.x2); wmax = std::max(wmax, std::max(x.wid, x.len)); }
+        for (size_t q = 0; q + 2 < c->pv.size(); q += 3) add(&c->pv[q]);
+        double d2 = 0;
+        for (int q = 0; q < 3; q++) if (hi[q] >= lo[q]) d2 += (hi[q] - lo[q]) * (hi[q] - lo[q]);
+        g.rmax = std::sqrt(d2) + 2 * wmax;
+    }
     g.seg.n = (int)c->seg.size();
     g.chg.n = (int)c->chg.size();
     if ((r = upload(&g.seg.cell, c->seg.data(), c->seg.size(), s))) return fail(r);

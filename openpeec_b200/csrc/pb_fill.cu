@@ -38,6 +38,7 @@ struct KArg {
     double kh[PB_FMAX];
     double dkh;
     int nf, eq;
+    int small_step;      // dkh * (largest distance) < pi/4: the step angle needs no reduction
 };
 
 // sin/cos(kh * r) for the FP32 path with the argument formed and reduced in FP64:
@@ -68,7 +69,7 @@ __device__ __forceinline__ void seed_sc(double kh, double r, float *s, float *c)
 // Accumulators of one lane for F wavenumbers. FP32 path: FP32 partial sums, flushed
 // into FP64 totals every 8 samples (bounded FP32 summation error). FP64 path: FP64.
 // Accumulators of one lane for F wavenumbers.
-// FP32 path: FP32 partial sums in registers, flushed every 8 samples into this lane's FP64
+// FP32 path: FP32 partial sums in registers, flushed every 16 samples into this lane's FP64
 // totals kept in shared memory (tot[(2f + c) * 32], conflict-free across lanes), which
 // bounds the FP32 summation error without holding 2F doubles in registers.
 // FP64 path: FP64 sums in registers.
@@ -112,14 +113,26 @@ template <int F> struct Acc<double, F> {
 // Accumulate one sample at distance r with weight w for every wavenumber:
 //   (e^{-jkR}-1)/R = -(2 sin(kR/2)/R) (sin(kR/2) + j cos(kR/2)),  R -> 0 limit -jk.
 template <int F, int EQ>
-__device__ __forceinline__ void accum(Acc<float, F> &a, const KArg &k, double rd, float w)
+__device__ __forceinline__ void accum(Acc<float, F> &a, const KArg &k, double rd, double rinv, double wd)
 {
-    const float r = (float)rd;
+    const float w = (float)wd;
     if (rd > 0) {
-        const float q = -2.f * w * __frcp_rn(r);
+        const float q = (float)(-2.0 * wd * rinv);
         if (EQ) {
             float sd, cd;
-            seed_sc(k.dkh, rd, &sd, &cd);
+            if (k.small_step) {
+                const float x = (float)(k.dkh * rd), x2 = x * x;
+                float ps = fmaf(x2, 2.75573192e-6f, -1.98412698e-4f);
+                ps = fmaf(ps, x2, 8.33333333e-3f);
+                ps = fmaf(ps, x2, -1.66666667e-1f);
+                sd = fmaf(ps * x2, x, x);
+                float pc = fmaf(x2, 2.48015873e-5f, -1.38888889e-3f);
+                pc = fmaf(pc, x2, 4.16666667e-2f);
+                pc = fmaf(pc, x2, -0.5f);
+                cd = fmaf(pc, x2, 1.0f);
+            } else {
+                seed_sc(k.dkh, rd, &sd, &cd);
+            }
 #pragma unroll
             for (int g = 0; g < F; g += 8) {
                 float s, c;
@@ -154,12 +167,13 @@ __device__ __forceinline__ void accum(Acc<float, F> &a, const KArg &k, double rd
         for (int f = 0; f < F; f++)
             if (f < k.nf) a.pi[f] -= 2.f * w * (float)k.kh[f];
     }
-    if (++a.cnt == 8) a.flush();
+    if (++a.cnt == 16) a.flush();
 }
 
 template <int F, int EQ>
-__device__ __forceinline__ void accum(Acc<double, F> &a, const KArg &k, double r, double w)
+__device__ __forceinline__ void accum(Acc<double, F> &a, const KArg &k, double r, double rinv, double w)
 {
+    (void)rinv;
     if (r > 0) {
         const double q = -2 * w / r;
 #pragma unroll
@@ -187,8 +201,9 @@ template <typename R> struct Term {
     int ty, nsub, n1, n2;
     double cd[3];                 // centre (or start-point) offset, kept in FP64
     double a2;                    // equivalent radius squared (wire kernel)
+    double sc;                    // folded scale (term weight x quadrature Jacobian)
     R u1[3], v1[3], u2[3], v2[3];
-    R L1, W1, L2, W2, sc, zs;
+    R L1, W1, L2, W2, zs;
     const double4 *q1, *q2;
 };
 
@@ -213,7 +228,7 @@ __device__ void make_term(Term<R> &T, const Cell &s1, const Cell &s2, int same, 
         for (int c = 0; c < 3; c++) T.cd[c] = 0.5 * (s2.x1[c] + s2.x2[c]) - 0.5 * (s1.x1[c] + s1.x2[c]);
         T.zs = s2.mirror ? (R)-1 : (R)1;
         const double w1 = (s1.wid > 0) ? s1.wid : 1, w2 = (s2.wid > 0) ? s2.wid : 1;
-        T.sc = (R)(scale / (w1 * w2));
+        T.sc = scale / (w1 * w2);
         T.nsub = 1;
     } else if (ty == PT_HL || ty == PT_RIBBON) {           // ribbon_corr, surface.c:134-178
         T.ty = TT_RIBBON;
@@ -227,7 +242,7 @@ __device__ void make_term(Term<R> &T, const Cell &s1, const Cell &s2, int same, 
             T.cd[c] = c2d[c] - c1d[c];
         }
         T.L1 = (R)s1.len; T.W1 = (R)s1.wid; T.L2 = (R)s2.len; T.W2 = (R)s2.wid;
-        T.sc = (R)(scale * s1.len * s2.len / (16.0 * nsub * nsub));
+        T.sc = scale * s1.len * s2.len / (16.0 * nsub * nsub);
         T.nsub = nsub;
     } else {                                               // gauss_kernel mode 1, partial.c:61-99
         T.ty = TT_WIRE;
@@ -241,7 +256,7 @@ __device__ void make_term(Term<R> &T, const Cell &s1, const Cell &s2, int same, 
             T.cd[c] = b.x1[c] - s1.x1[c];
         }
         T.a2 = aeff * aeff;
-        T.sc = (R)(scale * s1.len * b.len * 0.25 / ((double)nsub * nsub));
+        T.sc = scale * s1.len * b.len * 0.25 / ((double)nsub * nsub);
         T.nsub = nsub;
     }
 }
@@ -249,18 +264,20 @@ __device__ void make_term(Term<R> &T, const Cell &s1, const Cell &s2, int same, 
 // Distance of one sample: the large centre offset cd is added in FP64 to the small
 // in-cell offset p (FP32 on the mixed path), and R is formed in FP64 (rsqrt seed + one
 // Newton step), so the phase k*R/2 carries no error growing with the distance.
-__device__ __forceinline__ double dist64(const double *cd, const float *p, double a2)
+__device__ __forceinline__ double dist64(const double *cd, const float *p, double a2, double &rinv)
 {
     const double dx = cd[0] + (double)p[0], dy = cd[1] + (double)p[1], dz = cd[2] + (double)p[2];
     const double d2 = fma(dx, dx, fma(dy, dy, fma(dz, dz, a2)));
-    if (d2 <= 0) return 0.0;
+    if (d2 <= 0) { rinv = 0; return 0.0; }
     double y = (double)rsqrtf((float)d2);
     y = y * fma(-0.5 * d2 * y, y, 1.5);
+    rinv = y;
     return d2 * y;
 }
-__device__ __forceinline__ double dist64(const double *cd, const double *p, double a2)
+__device__ __forceinline__ double dist64(const double *cd, const double *p, double a2, double &rinv)
 {
     const double dx = cd[0] + p[0], dy = cd[1] + p[1], dz = cd[2] + p[2];
+    rinv = 0;
     return sqrt(dx * dx + dy * dy + dz * dz + a2);
 }
 
@@ -281,7 +298,9 @@ __device__ void run_term(const Term<R> &T, const KArg &k, Acc<R, F> &a, int lane
                 R p[3];
 #pragma unroll
                 for (int c = 0; c < 3; c++) p[c] = (a2 * T.u2[c] + b2 * T.v2[c]) - (a1 * T.u1[c] + b1 * T.v1[c]);
-                accum<F, EQ>(a, k, dist64(T.cd, p, 0.0), WG4<R>(i) * WG4<R>(j) * WG4<R>(m) * WG4<R>(q) * T.sc);
+                double ri;
+                const double rd = dist64(T.cd, p, 0.0, ri);
+                accum<F, EQ>(a, k, rd, ri, cWG4[i] * cWG4[j] * cWG4[m] * cWG4[q] * T.sc);
             }
         }
     } else if (T.ty == TT_WIRE) {
@@ -294,7 +313,9 @@ __device__ void run_term(const Term<R> &T, const KArg &k, Acc<R, F> &a, int lane
                 R p[3];
 #pragma unroll
                 for (int c = 0; c < 3; c++) p[c] = T.u2[c] * v - T.u1[c] * u;
-                accum<F, EQ>(a, k, dist64(T.cd, p, T.a2), WG8<R>(i) * WG8<R>(j) * T.sc);
+                double ri;
+                const double rd = dist64(T.cd, p, T.a2, ri);
+                accum<F, EQ>(a, k, rd, ri, cWG8[i] * cWG8[j] * T.sc);
             }
         }
     } else {
@@ -306,16 +327,35 @@ __device__ void run_term(const Term<R> &T, const KArg &k, Acc<R, F> &a, int lane
             p[0] = (R)o2.x - (R)o1.x;
             p[1] = (R)o2.y - (R)o1.y;
             p[2] = T.zs * (R)o2.z - (R)o1.z;
-            accum<F, EQ>(a, k, dist64(T.cd, p, 0.0), (R)(o1.w * o2.w) * T.sc);
+            double ri;
+            const double rd = dist64(T.cd, p, 0.0, ri);
+            accum<F, EQ>(a, k, rd, ri, o1.w * o2.w * T.sc);
         }
     }
 }
 
-// Warp sum of every frequency's accumulator; lane f receives frequency f (no divergence).
-template <typename R, int F>
-__device__ __forceinline__ void reduce_select(Acc<R, F> &a, int lane, double &cr, double &ci)
+// Warp sum of every frequency's accumulator; lane f receives frequency f.
+// FP32 path: the per-lane FP64 totals already sit in shared memory (tot[(2f+c)*32 + lane]),
+// so lane f adds up its frequency's 32 entries directly (no shuffles).
+template <int F>
+__device__ __forceinline__ void reduce_select(Acc<float, F> &a, int lane, double &cr, double &ci)
 {
     a.flush();
+    __syncwarp();
+    cr = ci = 0;
+    if (lane < F) {
+        const double *base = a.tot - lane;            // this warp's tot array
+#pragma unroll 8
+        for (int l = 0; l < 32; l++) {
+            cr += base[(2 * lane) * 32 + l];
+            ci += base[(2 * lane + 1) * 32 + l];
+        }
+    }
+    __syncwarp();
+}
+template <int F>
+__device__ __forceinline__ void reduce_select(Acc<double, F> &a, int lane, double &cr, double &ci)
+{
     cr = ci = 0;
 #pragma unroll
     for (int f = 0; f < F; f++) {
@@ -414,7 +454,7 @@ k_pot_static(pb_fill_geom g, double kw, double *st)
 #ifndef PB_CORR_MINB
 #define PB_CORR_MINB 4      // resident blocks per SM the register budget is sized for
 #endif
-#define PB_GROUP 32
+#define PB_GROUP 16
 
 enum { PB_SET_LP = 0, PB_SET_IG = 1 };
 
@@ -449,7 +489,7 @@ k_corr(pb_fill_geom g, KArg k, const double *st, pb_epi_args ea, double2 *ig, lo
     for (long long g0 = ((long long)blockIdx.x * PB_CORR_WARPS + wib) * PB_GROUP; g0 < T; g0 += stride) {
         // ---- set-up: lane -> pair g0 + lane
         const long long t = g0 + lane;
-        if (t < T) {
+        if (lane < PB_GROUP && t < T) {
             int i, j;
             tri_index(t, n, i, j);
             int nt = 0;
@@ -498,7 +538,7 @@ k_corr(pb_fill_geom g, KArg k, const double *st, pb_epi_args ea, double2 *ig, lo
                 run_term<R, F, EQ>(tm, k, acc, lane);
             }
             double cr, cim;
-            reduce_select<R, F>(acc, lane, cr, cim);
+            reduce_select<F>(acc, lane, cr, cim);
             const int f = lane, i = h.i, j = h.j;
             if (f >= nf) continue;
             if (SET == PB_SET_IG) {
@@ -807,7 +847,7 @@ static int launch_corr_any(const pb_fill_geom &g, const KArg &k, int use_fp32, c
 }
 
 // wavenumber set of a launch; equally spaced sets (linear sweeps) use the recurrence
-static void make_karg(KArg &k, int nf, const double *kw)
+static void make_karg(KArg &k, int nf, const double *kw, double rmax)
 {
     for (int f = 0; f < PB_FMAX; f++) {
         k.kw[f] = f < nf ? kw[f] : 0.0;
@@ -819,6 +859,7 @@ static void make_karg(KArg &k, int nf, const double *kw)
     for (int f = 1; f < nf && k.eq; f++)
         if (fabs(kw[f] - kw[0] - f * (kw[1] - kw[0])) > 1e-9 * fabs(kw[nf - 1])) k.eq = 0;
     if (k.dkh <= 0) k.eq = 0;
+    k.small_step = k.eq && k.dkh * rmax < 0.78;
 }
 
 int pb_lp_corr(const pb_fill_geom &g, int nf, const double *kw, int use_fp32, const double *stLp,
@@ -827,7 +868,7 @@ int pb_lp_corr(const pb_fill_geom &g, int nf, const double *kw, int use_fp32, co
     if (g.seg.n == 0) return PB_OK;
     if (nf < 1 || nf > PB_FMAX) { pb_set_error("pb_lp_corr: bad frequency count %d", nf); return PB_ERR_ARG; }
     KArg k;
-    make_karg(k, nf, kw);
+    make_karg(k, nf, kw, g.rmax);
     const int r = epi == PB_EPI_STORE
         ? launch_corr_any<PB_SET_LP, PB_EPI_STORE>(g, k, use_fp32, stLp, ea, nullptr, 0, s)
         : launch_corr_any<PB_SET_LP, PB_EPI_REDUCED>(g, k, use_fp32, stLp, ea, nullptr, 0, s);
@@ -843,7 +884,7 @@ int pb_pot_corr(const pb_fill_geom &g, int nf, const double *kw, int use_fp32, c
     if (g.ncell == 0) return PB_OK;
     if (nf < 1 || nf > PB_FMAX) { pb_set_error("pb_pot_corr: bad frequency count %d", nf); return PB_ERR_ARG; }
     KArg k;
-    make_karg(k, nf, kw);
+    make_karg(k, nf, kw, g.rmax);
     const long long igs = (long long)g.chg.n * g.chg.n;
     const bool corr = kw[0] > 0;
     if (corr) {
