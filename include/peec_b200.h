@@ -191,6 +191,20 @@ int  pb_lu_solve(int n, const double *a, const int *piv, double *b);
  */
 int  pb_lu_decomp_batched_dev(int n, int nb, double *a_dev, int *piv_dev, int *info_host);
 
+/*
+ * Partial-inductance fill that allocates nothing. It has no counterpart in the reference
+ * (whose lp_fill mallocs p->lp itself, src/partial.c:428-435); it exists for host programs
+ * that own all device memory through their own pool and may not call cudaMalloc/cudaFree.
+ * Same matrix as pb_lp_fill: seg_dev = nseg cells in device memory (no polygon cells),
+ * lp_dev = caller-allocated device output [nseg*nseg] complex, both triangles.
+ * Limit: nseg <= 512. The only scratch is a fixed 2 MiB array in the library that every
+ * GPU loading it holds until exit; the first call on a device looks its address up.
+ * Calls share that scratch and run on the default stream: calls that overlap on the GPU
+ * (e.g. from several host threads) race, so serialise them.
+ */
+int  pb_lp_fill_noalloc(int nseg, const pb_cell_t *seg_dev, int gp, double gpz, double kw,
+                        int prec, double *lp_dev);
+
 /* Measured FP32 FMA throughput of the current GPU in TFLOP/s (dependent FMA chains on
  * every SM): the denominator of the fill kernels' roofline. */
 int  pb_fp32_peak(double *tflops);

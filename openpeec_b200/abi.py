@@ -126,6 +126,7 @@ def lib():
     L.pb_lu_solve.argtypes = [C.c_int, _vp, _vp, _vp]
     L.pb_lu_decomp_batched_dev.argtypes = [C.c_int, C.c_int, _vp, _vp, _vp]
     L.pb_fp32_peak.argtypes = [C.POINTER(C.c_double)]
+    L.pb_lp_fill_noalloc.argtypes = [C.c_int, _vp, C.c_int, C.c_double, C.c_double, C.c_int, _vp]
     L.pb_device_sync.restype = C.c_int
     _lib = L
     return L
