@@ -194,11 +194,14 @@ int  pb_lu_decomp_batched_dev(int n, int nb, double *a_dev, int *piv_dev, int *i
 /*
  * Partial-inductance fill that allocates nothing. It has no counterpart in the reference
  * (whose lp_fill mallocs p->lp itself, src/partial.c:428-435); it exists for host programs
- * that own all device memory through their own pool and may not call cudaMalloc/cudaFree.
+ * that own all device memory through their own pool and may not call cudaMalloc/cudaFree
+ * (which may synchronise the whole device and would bypass the host's memory budget).
  * Same matrix as pb_lp_fill: seg_dev = nseg cells in device memory (no polygon cells),
  * lp_dev = caller-allocated device output [nseg*nseg] complex, both triangles.
  * Limit: nseg <= 512. The only scratch is a fixed 2 MiB array in the library that every
- * GPU loading it holds until exit; the first call on a device looks its address up.
+ * GPU loading it holds until exit. The first call on each device does a one-time set-up
+ * (it looks the array's device address up with cudaGetSymbolAddress), so make that first
+ * call before any stream capture.
  * Calls share that scratch and run on the default stream: calls that overlap on the GPU
  * (e.g. from several host threads) race, so serialise them.
  */

@@ -8,7 +8,10 @@
 // pb_lp_fill_noalloc computes the same matrix with the same kernels, but takes every
 // input and output as caller-owned device memory and keeps its only scratch buffer (the
 // FP64 static table) in the file-scope array below, which every GPU that loads this
-// library holds until the process exits.
+// library holds until the process exits. The first call on each device looks the array's
+// device address up (cudaGetSymbolAddress, with that device current); make that first
+// call before any stream capture. Every call reuses the same array and the same input
+// flag, so calls that overlap on the GPU race: serialise them.
 #include <mutex>
 #include "pb_ctx.cuh"
 
