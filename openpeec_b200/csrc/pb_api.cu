@@ -235,19 +235,26 @@ int pb_create(const pb_problem_t *prob, pb_ctx **out)
     pb_fill_geom &g = c->g;
     g.gp = c->gp; g.gpz = c->gpz; g.ncell = c->ncell;
     {
-        // bounding box of every cell point (and its ground-plane image) -> distance bound
-        double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-        auto add = [&](const double *x) {
-            for (int q = 0; q < 3; q++) { lo[q] = std::min(lo[q], x[q]); hi[q] = std::max(hi[q], x[q]); }
-            if (c->gp) { lo[2] = std::min(lo[2], 2 * c->gpz - x[2]); hi[2] = std::max(hi[2], 2 * c->gpz - x[2]); }
-        };
-        double wmax = 0;
+        // largest cell extent -> bound on |R - D| = |p| <= extent(cell 1) + extent(cell 2)
+        // of the correction samples (offsets p within the two cells of a term)
+        double ext = 0;
         for (auto *v : {&c->seg, &c->chg})
-            for (auto &x : *v) { add(x.x1); add(x.x2); wmax = std::max(wmax, std::max(x.wid, x.len)); }
-        for (size_t q = 0; q + 2 < c->pv.size(); q += 3) add(&c->pv[q]);
-        double d2 = 0;
-        for (int q = 0; q < 3; q++) if (hi[q] >= lo[q]) d2 += (hi[q] - lo[q]) * (hi[q] - lo[q]);
-        g.rmax = std::sqrt(d2) + 2 * wmax;
+            for (auto &x : *v) {
+                double e = x.len + x.wid + x.thick + 2 * x.radius;
+                if (x.npv > 0) {
+                    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+                    for (int q = 0; q < x.npv; q++)
+                        for (int d = 0; d < 3; d++) {
+                            lo[d] = std::min(lo[d], c->pv[3 * (x.pvoff + q) + d]);
+                            hi[d] = std::max(hi[d], c->pv[3 * (x.pvoff + q) + d]);
+                        }
+                    double d2 = 0;
+                    for (int d = 0; d < 3; d++) d2 += (hi[d] - lo[d]) * (hi[d] - lo[d]);
+                    e = std::max(e, std::sqrt(d2));
+                }
+                ext = std::max(ext, e);
+            }
+        g.pmax = 2 * ext;
     }
     g.seg.n = (int)c->seg.size();
     g.chg.n = (int)c->chg.size();

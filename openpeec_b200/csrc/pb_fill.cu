@@ -5,12 +5,17 @@
 // * Static part: FP64, one thread per entry (k_lp_static / k_pot_static), evaluated
 //   once per quadrature level and cached across the frequency sweep.
 // * Retardation correction: one warp per entry; the 32 lanes split the quadrature
-//   samples; each sample's R is computed once and reused for up to 32 wavenumbers of
+//   samples; each sample's R is computed once and reused for up to 16 wavenumbers of
 //   the sweep (per-lane accumulators, one per frequency). FP32 in the mixed path, FP64
 //   in the plain path. The integrand is evaluated as
 //       (e^{-jkR} - 1)/R = -(2 sin(kR/2)/R) * (sin(kR/2) + j cos(kR/2)),
 //   which has no cancellation (the reference's cos(kR)-1, partial.c:168, would lose all
 //   digits in FP32 for small kR).
+// * FP32 phase: R = D + delta with D = |centre offset| of the term (FP64, once per term)
+//   and delta = (R^2 - D^2) / (R + D) formed in FP32 from the small in-cell offset p, so
+//   the error of delta scales with the cell size, not with the distance. sin/cos(kD/2)
+//   come from FP64 once per term and frequency group; each sample only rotates them by
+//   the small angle k delta / 2. The sample loop has no FP64 arithmetic.
 // * Epilogue: store Lp / P, or assemble the reduced MNA matrix directly.
 #include "pb_fill.cuh"
 #include "pb_geom.cuh"
@@ -37,42 +42,55 @@ struct KArg {
     double kw[PB_FMAX];
     double kh[PB_FMAX];
     double dkh;
+    float khf[PB_FMAX];
+    float dkhf;
     int nf, eq;
-    int small_step;      // dkh * (largest distance) < pi/4: the step angle needs no reduction
-};
+    int reduce;          // kh * (bound on |delta|) may exceed pi/4: reduce the FP32 angles
+    int step_tiny;       // |dkh| * (bound on |delta|) < 0.01: two-term step sine/cosine
+};                       // (selects the RED instance of the FP32 kernels)
 
-// sin/cos(kh * r) for the FP32 path with the argument formed and reduced in FP64:
-// the product kh*r and the quadrant reduction carry no FP32 rounding (their absolute
-// error would grow with kR); only the reduced angle |t| <= pi/4 goes to the FP32 series.
-__device__ __forceinline__ void seed_sc(double kh, double r, float *s, float *c)
+// FP32 copies of the 4- and 8-point Gauss-Legendre nodes and weights (the FP64 tables
+// cXG4/cWG4/cXG8/cWG8 rounded to nearest), for uniform loads in the FP32 sample loops.
+__constant__ float cXG4f[4] = {-0.8611363115940526f, -0.3399810435848563f, 0.3399810435848563f, 0.8611363115940526f};
+__constant__ float cWG4f[4] = {0.3478548451374538f, 0.6521451548625461f, 0.6521451548625461f, 0.3478548451374538f};
+// cWG4 - cWG4f: the weights' FP32 rounding is the same for every sample of every term and
+// would bias the quadrature (~2e-8 relative), so products carry the tail explicitly.
+__constant__ float cWG4lo[4] = {-7.538937474e-09f, 7.538937474e-09f, 7.538937474e-09f, -7.538937474e-09f};
+
+// sin and cos of an FP32 angle: optional Cody-Waite reduction by pi/2 (pi/2 split into
+// an FP32 head and tail, so q * head is exact inside the FMA), then the Taylor series of
+// sin to x^9 and cos to x^8 on |t| <= pi/4 (truncation below 2e-9).
+template <int RED>
+__device__ __forceinline__ void sincos_f32(float x, float &s, float &c)
 {
-    const double x = kh * r;
-    const double tq = fma(x, 0.63661977236758134308, 6755399441055744.0);  // 1.5*2^52 shifter
-    const double q = tq - 6755399441055744.0;
-    double t = fma(-q, 1.5707963267948966, x);                               // pi/2 high
-    t = fma(-q, 6.123233995736766e-17, t);                                    // pi/2 low
-    const float rr = (float)t, r2 = rr * rr;
+    float t = x;
+    int iq = 0;
+    if (RED) {
+        const float q = rintf(x * 0.636619772f);
+        t = fmaf(-q, 1.57079637f, x);
+        t = fmaf(-q, -4.37113883e-8f, t);
+        iq = (int)q;
+    }
+    const float r2 = t * t;
     float ps = fmaf(r2, 2.75573192e-6f, -1.98412698e-4f);
     ps = fmaf(ps, r2, 8.33333333e-3f);
     ps = fmaf(ps, r2, -1.66666667e-1f);
-    const float sn = fmaf(ps * r2, rr, rr);
+    const float sn = fmaf(ps * r2, t, t);
     float pc = fmaf(r2, 2.48015873e-5f, -1.38888889e-3f);
     pc = fmaf(pc, r2, 4.16666667e-2f);
     pc = fmaf(pc, r2, -0.5f);
     const float cs = fmaf(pc, r2, 1.0f);
-    const int iq = __double2loint(tq) & 3;
     const float ss = (iq & 1) ? cs : sn, cc = (iq & 1) ? sn : cs;
-    *s = (iq & 2) ? -ss : ss;
-    *c = ((iq + 1) & 2) ? -cc : cc;
+    s = (iq & 2) ? -ss : ss;
+    c = ((iq + 1) & 2) ? -cc : cc;
 }
 
-// Accumulators of one lane for F wavenumbers. FP32 path: FP32 partial sums, flushed
-// into FP64 totals every 8 samples (bounded FP32 summation error). FP64 path: FP64.
 // Accumulators of one lane for F wavenumbers.
-// FP32 path: FP32 partial sums in registers, flushed every 16 samples into this lane's FP64
-// totals kept in shared memory (tot[(2f + c) * 32], conflict-free across lanes), which
+// FP32 path: FP32 partial sums in registers, flushed every PB_FLUSH samples into this lane's
+// FP64 totals kept in shared memory (tot[(2f + c) * 32], conflict-free across lanes), which
 // bounds the FP32 summation error without holding 2F doubles in registers.
 // FP64 path: FP64 sums in registers.
+#define PB_FLUSH 16
 template <typename R, int F> struct Acc;
 template <int F> struct Acc<float, F> {
     float pr[F], pi[F];
@@ -110,37 +128,51 @@ template <int F> struct Acc<double, F> {
     __device__ __forceinline__ double im(int f) const { return ti[f]; }
 };
 
-// Accumulate one sample at distance r with weight w for every wavenumber:
-//   (e^{-jkR}-1)/R = -(2 sin(kR/2)/R) (sin(kR/2) + j cos(kR/2)),  R -> 0 limit -jk.
-template <int F, int EQ>
-__device__ __forceinline__ void accum(Acc<float, F> &a, const KArg &k, double rd, double rinv, double wd)
+// Per-term phase bases of the FP32 path (shared memory of the warp): EQ launches hold
+// sin/cos(kh[8g] D) for the groups g < F/8 and sin/cos(dkh D) after them; other launches
+// hold sin/cos(kh[f] D) for every f < F. Each base is an FP32 head + tail pair
+// (sin_hi, cos_hi, sin_lo, cos_lo): its rounding would otherwise be the same for every
+// sample of the term and not average out.
+template <int F, int EQ> constexpr int nbase() { return EQ ? (F + 7) / 8 + 1 : F; }
+
+// sin/cos(A + B) from the head+tail base b = sin/cos(A) and FP32 sB, cB of a small B.
+__device__ __forceinline__ void rot_base(const float4 b, float sB, float cB, float &s, float &c)
 {
-    const float w = (float)wd;
-    if (rd > 0) {
-        const float q = (float)(-2.0 * wd * rinv);
+    s = fmaf(b.x, cB, fmaf(b.y, sB, fmaf(b.w, sB, b.z)));
+    c = fmaf(b.y, cB, fmaf(-b.x, sB, fmaf(-b.z, sB, b.w)));
+}
+
+// Accumulate one FP32 sample for every wavenumber: distance R = D + dl with weight
+// factor qw = -2 w (w = quadrature weight x term scale), q = qw / R:
+//   (e^{-jkR}-1)/R = q sin(kR/2) (sin(kR/2) + j cos(kR/2)),  R -> 0 limit -jk.
+template <int F, int EQ, int RED>
+__device__ __forceinline__ void accum32(Acc<float, F> &a, const KArg &k, const float4 *base,
+                                        float r2, float rinv, float dl, float qw)
+{
+    if (r2 > 0) {
+        const float q = qw * rinv;
         if (EQ) {
-            float sd, cd;
-            if (k.small_step) {
-                const float x = (float)(k.dkh * rd), x2 = x * x;
-                float ps = fmaf(x2, 2.75573192e-6f, -1.98412698e-4f);
-                ps = fmaf(ps, x2, 8.33333333e-3f);
-                ps = fmaf(ps, x2, -1.66666667e-1f);
-                sd = fmaf(ps * x2, x, x);
-                float pc = fmaf(x2, 2.48015873e-5f, -1.38888889e-3f);
-                pc = fmaf(pc, x2, 4.16666667e-2f);
-                pc = fmaf(pc, x2, -0.5f);
-                cd = fmaf(pc, x2, 1.0f);
+            constexpr int NG = (F + 7) / 8;
+            float ss, cs;
+            if (k.step_tiny) {                     // |x| < 0.01: x^5/120 and x^4/24 < 1e-11
+                const float x = k.dkhf * dl, x2 = x * x;
+                ss = fmaf(x2 * x, -0.166666667f, x);
+                cs = fmaf(x2, -0.5f, 1.f);
             } else {
-                seed_sc(k.dkh, rd, &sd, &cd);
+                sincos_f32<RED>(k.dkhf * dl, ss, cs);
             }
+            float sd, cd;
+            rot_base(base[NG], ss, cs, sd, cd);
 #pragma unroll
-            for (int g = 0; g < F; g += 8) {
+            for (int g = 0; g < NG; g++) {
+                float ts, tc;
+                sincos_f32<RED>(k.khf[8 * g] * dl, ts, tc);
                 float s, c;
-                seed_sc(k.kh[g], rd, &s, &c);
+                rot_base(base[g], ts, tc, s, c);
 #pragma unroll
                 for (int u = 0; u < 8; u++) {
-                    const int f = g + u;
-                    if (f < F && f < k.nf) {
+                    const int f = 8 * g + u;
+                    if (f < F) {
                         const float t = q * s;
                         a.pr[f] = fmaf(t, s, a.pr[f]);
                         a.pi[f] = fmaf(t, c, a.pi[f]);
@@ -153,21 +185,42 @@ __device__ __forceinline__ void accum(Acc<float, F> &a, const KArg &k, double rd
         } else {
 #pragma unroll
             for (int f = 0; f < F; f++) {
-                if (f < k.nf) {
-                    float s, c;
-                    seed_sc(k.kh[f], rd, &s, &c);
-                    const float t = q * s;
-                    a.pr[f] = fmaf(t, s, a.pr[f]);
-                    a.pi[f] = fmaf(t, c, a.pi[f]);
-                }
+                float ts, tc;
+                sincos_f32<RED>(k.khf[f] * dl, ts, tc);
+                float s, c;
+                rot_base(base[f], ts, tc, s, c);
+                const float t = q * s;
+                a.pr[f] = fmaf(t, s, a.pr[f]);
+                a.pi[f] = fmaf(t, c, a.pi[f]);
             }
         }
     } else {
 #pragma unroll
-        for (int f = 0; f < F; f++)
-            if (f < k.nf) a.pi[f] -= 2.f * w * (float)k.kh[f];
+        for (int f = 0; f < F; f++) a.pi[f] = fmaf(qw, k.khf[f], a.pi[f]);
     }
-    if (++a.cnt == 16) a.flush();
+    if (++a.cnt == PB_FLUSH) a.flush();
+}
+
+// One sample of the FP32 path from its in-cell offset p (R = |cd + p|, plus the wire
+// kernel's a^2): dl = R - D = p.(p + 2 cd) / (R + D) with R + D from R^2 in FP32
+// (v = cd + p), then R = D + dl with D as FP32 head + tail, so that 1/R carries no
+// rounding shared by all samples of the term. Where D + dl cancels (a sample next to
+// the other cell of an adjacent pair) the direct FP32 R is taken instead.
+template <int F, int EQ, int RED>
+__device__ __forceinline__ void sample32(Acc<float, F> &a, const KArg &k, const float4 *base,
+                                         const float *cd, float a2, float D, float Dlo, float px,
+                                         float py, float pz, float qw)
+{
+    const float vx = cd[0] + px, vy = cd[1] + py, vz = cd[2] + pz;
+    const float r2 = fmaf(vx, vx, fmaf(vy, vy, fmaf(vz, vz, a2)));
+    const float e = fmaf(px, fmaf(2.f, cd[0], px), fmaf(py, fmaf(2.f, cd[1], py), pz * fmaf(2.f, cd[2], pz)));
+    const float ra = r2 * rsqrtf(r2);
+    const float dl = __fdividef(e, ra + D);
+    const float rd = D + (dl + Dlo);
+    const float r = rd > 0.5f * ra ? rd : ra;
+    float rinv = __fdividef(1.f, r);
+    rinv = fmaf(rinv, fmaf(-r, rinv, 1.f), rinv);
+    accum32<F, EQ, RED>(a, k, base, r2, rinv, dl, qw);
 }
 
 template <int F, int EQ>
@@ -197,10 +250,18 @@ __device__ __forceinline__ void accum(Acc<double, F> &a, const KArg &k, double r
 // precision of that loop. Built from the FP64 cells just before the loop so that the
 // cells are not live during it.
 enum { TT_RIBBON = 0, TT_WIRE = 1, TT_POLY = 2 };
-template <typename R> struct Term {
-    int ty, nsub, n1, n2;
-    double cd[3];                 // centre (or start-point) offset, kept in FP64
+// Centre offset of a term in the form its sample loop reads it.
+template <typename R> struct TermOffset;
+template <> struct TermOffset<double> {
+    double cd[3];                 // centre (or start-point) offset
     double a2;                    // equivalent radius squared (wire kernel)
+};
+template <> struct TermOffset<float> {
+    double D;                     // sqrt(|cd|^2 + a2), FP64: the term's phase kh * D
+    float cdf[3], a2f, Df, Dlo, inv_rn;   // D = Df + Dlo
+};
+template <typename R> struct Term : TermOffset<R> {
+    int ty, nsub, n1, n2;
     double sc;                    // folded scale (term weight x quadrature Jacobian)
     R u1[3], v1[3], u2[3], v2[3];
     R L1, W1, L2, W2, zs;
@@ -217,7 +278,7 @@ __device__ void make_term(Term<R> &T, const Cell &s1, const Cell &s2, int same, 
     const bool wire_self = same && s1.wid <= 0 && s1.npv <= 0;
     if (wire_self) ty = PT_WIRE;
     else ty = pair_type(s1, s2);
-    T.a2 = 0;
+    double cdl[3], a2l = 0;
     if (ty == PT_POLY) {                                   // poly_corr, polygon.c:305-334
         T.ty = TT_POLY;
         T.q1 = set.qpt + set.qoff[i1];
@@ -225,7 +286,7 @@ __device__ void make_term(Term<R> &T, const Cell &s1, const Cell &s2, int same, 
         T.q2 = set.qpt + set.qoff[i2];
         T.n2 = set.qoff[i2 + 1] - set.qoff[i2];
 #pragma unroll
-        for (int c = 0; c < 3; c++) T.cd[c] = 0.5 * (s2.x1[c] + s2.x2[c]) - 0.5 * (s1.x1[c] + s1.x2[c]);
+        for (int c = 0; c < 3; c++) cdl[c] = 0.5 * (s2.x1[c] + s2.x2[c]) - 0.5 * (s1.x1[c] + s1.x2[c]);
         T.zs = s2.mirror ? (R)-1 : (R)1;
         const double w1 = (s1.wid > 0) ? s1.wid : 1, w2 = (s2.wid > 0) ? s2.wid : 1;
         T.sc = scale / (w1 * w2);
@@ -239,7 +300,7 @@ __device__ void make_term(Term<R> &T, const Cell &s1, const Cell &s2, int same, 
 #pragma unroll
         for (int c = 0; c < 3; c++) {
             T.u1[c] = (R)t1d[c]; T.v1[c] = (R)w1d[c]; T.u2[c] = (R)t2d[c]; T.v2[c] = (R)w2d[c];
-            T.cd[c] = c2d[c] - c1d[c];
+            cdl[c] = c2d[c] - c1d[c];
         }
         T.L1 = (R)s1.len; T.W1 = (R)s1.wid; T.L2 = (R)s2.len; T.W2 = (R)s2.wid;
         T.sc = scale * s1.len * s2.len / (16.0 * nsub * nsub);
@@ -253,27 +314,28 @@ __device__ void make_term(Term<R> &T, const Cell &s1, const Cell &s2, int same, 
         for (int c = 0; c < 3; c++) {
             T.u1[c] = (R)(s1.x2[c] - s1.x1[c]);
             T.u2[c] = (R)(b.x2[c] - b.x1[c]);
-            T.cd[c] = b.x1[c] - s1.x1[c];
+            cdl[c] = b.x1[c] - s1.x1[c];
         }
-        T.a2 = aeff * aeff;
+        a2l = aeff * aeff;
         T.sc = scale * s1.len * b.len * 0.25 / ((double)nsub * nsub);
         T.nsub = nsub;
     }
+    if constexpr (sizeof(R) == 4) {
+        T.D = sqrt(cdl[0] * cdl[0] + cdl[1] * cdl[1] + cdl[2] * cdl[2] + a2l);
+#pragma unroll
+        for (int c = 0; c < 3; c++) T.cdf[c] = (float)cdl[c];
+        T.a2f = (float)a2l;
+        T.Df = (float)T.D;
+        T.Dlo = (float)(T.D - (double)T.Df);
+        T.inv_rn = 1.0f / (float)T.nsub;
+    } else {
+#pragma unroll
+        for (int c = 0; c < 3; c++) T.cd[c] = cdl[c];
+        T.a2 = a2l;
+    }
 }
 
-// Distance of one sample: the large centre offset cd is added in FP64 to the small
-// in-cell offset p (FP32 on the mixed path), and R is formed in FP64 (rsqrt seed + one
-// Newton step), so the phase k*R/2 carries no error growing with the distance.
-__device__ __forceinline__ double dist64(const double *cd, const float *p, double a2, double &rinv)
-{
-    const double dx = cd[0] + (double)p[0], dy = cd[1] + (double)p[1], dz = cd[2] + (double)p[2];
-    const double d2 = fma(dx, dx, fma(dy, dy, fma(dz, dz, a2)));
-    if (d2 <= 0) { rinv = 0; return 0.0; }
-    double y = (double)rsqrtf((float)d2);
-    y = y * fma(-0.5 * d2 * y, y, 1.5);
-    rinv = y;
-    return d2 * y;
-}
+// Distance of one sample of the FP64 path.
 __device__ __forceinline__ double dist64(const double *cd, const double *p, double a2, double &rinv)
 {
     const double dx = cd[0] + p[0], dy = cd[1] + p[1], dz = cd[2] + p[2];
@@ -330,6 +392,104 @@ __device__ void run_term(const Term<R> &T, const KArg &k, Acc<R, F> &a, int lane
             double ri;
             const double rd = dist64(T.cd, p, 0.0, ri);
             accum<F, EQ>(a, k, rd, ri, o1.w * o2.w * T.sc);
+        }
+    }
+}
+
+// Samples of one term on the FP32 path. Lane l takes the same quadrature points as the
+// FP64 path (sample s = l + 32 t of each sub-square), but with the lane-fixed parts of the
+// point (and of its weight) hoisted out of the loops; the phase bases sin/cos(kh D) of the
+// term are computed in FP64 by the first lanes into the warp's `base` slots.
+template <int F, int EQ, int RED>
+__device__ void run_term32(const Term<float> &T, const KArg &k, Acc<float, F> &a, int lane,
+                           float4 *base)
+{
+    constexpr int NB = nbase<F, EQ>();
+    __syncwarp();                                   // previous term's bases no longer read
+    if (lane < NB) {
+        const double kh = EQ ? (lane < NB - 1 ? k.kh[8 * lane] : k.dkh) : k.kh[lane];
+        double sn, cs;
+        sincos(kh * T.D, &sn, &cs);
+        const float sh = (float)sn, ch = (float)cs;
+        base[lane] = make_float4(sh, ch, (float)(sn - (double)sh), (float)(cs - (double)ch));
+    }
+    __syncwarp();
+    const float cd[3] = {T.cdf[0], T.cdf[1], T.cdf[2]};
+    const float D = T.Df, Dlo = T.Dlo, irn = T.inv_rn;
+    const int nsub = T.nsub;
+    if (T.ty == TT_RIBBON) {                        // ribbon_corr, surface.c:134-178
+        // sample s = lane + 32 t: q = lane&3, m = (lane>>2)&3, j = (lane>>4) + 2 (t&1), i = t>>1
+        const int lq = lane & 3, lm = (lane >> 2) & 3, lj = lane >> 4;
+        const float b2 = T.W2 * 0.5f * cXG4f[lq];
+        const float hm = 0.5f * (1.f + cXG4f[lm]);
+        const float b10 = T.W1 * 0.5f * cXG4f[lj], b11 = T.W1 * 0.5f * cXG4f[lj + 2];
+        const double wqm = cWG4[lq] * cWG4[lm] * (-2.0 * T.sc);
+        const double wl0d = cWG4[lj] * wqm, wl1d = cWG4[lj + 2] * wqm;
+        const float wl0 = (float)wl0d, wl1 = (float)wl1d;             // head + tail
+        const float wl0t = (float)(wl0d - (double)wl0), wl1t = (float)(wl1d - (double)wl1);
+        float B2[3], B10[3], B11[3], U1[3], U2[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            B2[c] = b2 * T.v2[c];
+            B10[c] = b10 * T.v1[c];
+            B11[c] = b11 * T.v1[c];
+            U1[c] = T.u1[c];
+            U2[c] = T.u2[c];
+        }
+        const float L1 = T.L1, L2 = T.L2;
+        for (int ja = 0; ja < nsub; ja++) {
+            const float a2c = L2 * fmaf((float)ja + hm, irn, -0.5f);
+            float Q0[3], Q1[3];
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                const float P2 = fmaf(a2c, U2[c], B2[c]);
+                Q0[c] = P2 - B10[c];
+                Q1[c] = P2 - B11[c];
+            }
+            for (int ia = 0; ia < nsub; ia++) {
+#pragma unroll 1
+                for (int i = 0; i < 4; i++) {
+                    const float a1 = L1 * fmaf((float)ia + 0.5f * (1.f + cXG4f[i]), irn, -0.5f);
+                    const float wi = cWG4f[i], wit = cWG4lo[i];
+                    // full weight W_i W_j W_m W_q (-2 sc) rounded once (head*head + cross terms)
+                    const float w0 = fmaf(wl0, wi, fmaf(wl0, wit, wl0t * wi));
+                    const float w1 = fmaf(wl1, wi, fmaf(wl1, wit, wl1t * wi));
+                    sample32<F, EQ, RED>(a, k, base, cd, 0.f, D, Dlo, fmaf(-a1, U1[0], Q0[0]),
+                                         fmaf(-a1, U1[1], Q0[1]), fmaf(-a1, U1[2], Q0[2]), w0);
+                    sample32<F, EQ, RED>(a, k, base, cd, 0.f, D, Dlo, fmaf(-a1, U1[0], Q1[0]),
+                                         fmaf(-a1, U1[1], Q1[1]), fmaf(-a1, U1[2], Q1[2]), w1);
+                }
+            }
+        }
+    } else if (T.ty == TT_WIRE) {                   // gauss_kernel mode 1, partial.c:61-99
+        const int lj = lane & 7, li = lane >> 3;
+        const float hj = 0.5f * (1.f + (float)cXG8[lj]);
+        const float hi0 = 0.5f * (1.f + (float)cXG8[li]), hi1 = 0.5f * (1.f + (float)cXG8[li + 4]);
+        const double wj = cWG8[lj] * (-2.0 * T.sc);
+        const float w0 = (float)(cWG8[li] * wj), w1 = (float)(cWG8[li + 4] * wj);
+        const float a2 = T.a2f;
+        float U1[3], U2[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) { U1[c] = T.u1[c]; U2[c] = T.u2[c]; }
+        for (int i1 = 0; i1 < nsub; i1++) {
+            const float ua = ((float)i1 + hi0) * irn, ub = ((float)i1 + hi1) * irn;
+            for (int i2 = 0; i2 < nsub; i2++) {
+                const float v = ((float)i2 + hj) * irn;
+                const float P0 = U2[0] * v, P1 = U2[1] * v, P2 = U2[2] * v;
+                sample32<F, EQ, RED>(a, k, base, cd, a2, D, Dlo, fmaf(-U1[0], ua, P0), fmaf(-U1[1], ua, P1),
+                                fmaf(-U1[2], ua, P2), w0);
+                sample32<F, EQ, RED>(a, k, base, cd, a2, D, Dlo, fmaf(-U1[0], ub, P0), fmaf(-U1[1], ub, P1),
+                                fmaf(-U1[2], ub, P2), w1);
+            }
+        }
+    } else {                                        // poly_corr, polygon.c:305-334
+        const int S = T.n1 * T.n2;
+        const double msc = -2.0 * T.sc;
+        for (int s = lane; s < S; s += 32) {
+            const int k1 = s / T.n2, k2 = s - k1 * T.n2;
+            const double4 o1 = T.q1[k1], o2 = T.q2[k2];
+            sample32<F, EQ, RED>(a, k, base, cd, 0.f, D, Dlo, (float)o2.x - (float)o1.x, (float)o2.y - (float)o1.y,
+                            T.zs * (float)o2.z - (float)o1.z, (float)(o1.w * o2.w * msc));
         }
     }
 }
@@ -460,14 +620,19 @@ enum { PB_SET_LP = 0, PB_SET_IG = 1 };
 
 struct TaskHdr { int i, j, nterm, pad; };
 
+__device__ __forceinline__ void prefetch_l1(const void *p)
+{
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
+
 template <typename R, int F>
 constexpr size_t corr_smem_bytes()
 {
     return (size_t)PB_CORR_WARPS * (2 * PB_GROUP * sizeof(Term<R>) + PB_GROUP * sizeof(TaskHdr) +
-                                     (sizeof(R) == 4 ? 2 * F * 32 * sizeof(double) : 0));
+                                     (sizeof(R) == 4 ? 2 * F * 32 * sizeof(double) + (PB_FMAX + 1) * sizeof(float4) : 0));
 }
 
-template <typename R, int F, int SET, int EPI, int EQ>
+template <typename R, int F, int SET, int EPI, int EQ, int RED>
 __global__ void __launch_bounds__(32 * PB_CORR_WARPS, PB_CORR_MINB)
 k_corr(pb_fill_geom g, KArg k, const double *st, pb_epi_args ea, double2 *ig, long long igs)
 {
@@ -479,6 +644,10 @@ k_corr(pb_fill_geom g, KArg k, const double *st, pb_epi_args ea, double2 *ig, lo
     double *tot = reinterpret_cast<double *>(smraw + (size_t)PB_CORR_WARPS * (2 * PB_GROUP * sizeof(Term<R>) +
                                                                             PB_GROUP * sizeof(TaskHdr)))
                   + (size_t)wib * 2 * F * 32;
+    float4 *bases = reinterpret_cast<float4 *>(smraw + (size_t)PB_CORR_WARPS * (2 * PB_GROUP * sizeof(Term<R>) +
+                                                                              PB_GROUP * sizeof(TaskHdr) +
+                                                                              2 * F * 32 * sizeof(double)))
+                    + (size_t)wib * (PB_FMAX + 1);
     const pb_dev_cells &set = SET == PB_SET_LP ? g.seg : g.chg;
     const int n = set.n;
     const long long T = (long long)n * (n + 1) / 2;
@@ -531,11 +700,26 @@ k_corr(pb_fill_geom g, KArg k, const double *st, pb_epi_args ea, double2 *ig, lo
         for (int tk = 0; tk < PB_GROUP; tk++) {
             if (g0 + tk >= T) break;
             const TaskHdr h = hdr[tk];
+            if (EPI == PB_EPI_REDUCED && SET == PB_SET_LP && lane < nf) {
+                // the epilogue's scattered P(f) reads: start them into L1 now, so that they
+                // arrive while the samples run instead of stalling the warp afterwards
+                const int ca = g.seg_ca[h.i], cb = g.seg_cb[h.i], da = g.seg_ca[h.j], db = g.seg_cb[h.j];
+                const double2 *P = ea.pm + lane * ea.pm_stride;
+                const int nc = g.ncell;
+                if (ca >= 0 && da >= 0) prefetch_l1(P + (long long)ca * nc + da);
+                if (ca >= 0 && db >= 0) prefetch_l1(P + (long long)ca * nc + db);
+                if (cb >= 0 && da >= 0) prefetch_l1(P + (long long)cb * nc + da);
+                if (cb >= 0 && db >= 0) prefetch_l1(P + (long long)cb * nc + db);
+            }
             Acc<R, F> acc;
             acc.init(tot + lane);
             for (int q = 0; q < h.nterm; q++) {
-                const Term<R> tm = terms[2 * tk + q];
-                run_term<R, F, EQ>(tm, k, acc, lane);
+                if constexpr (sizeof(R) == 4) {
+                    run_term32<F, EQ, RED>(terms[2 * tk + q], k, acc, lane, bases);
+                } else {
+                    const Term<R> tm = terms[2 * tk + q];
+                    run_term<R, F, EQ>(tm, k, acc, lane);
+                }
             }
             double cr, cim;
             reduce_select<F>(acc, lane, cr, cim);
@@ -805,7 +989,7 @@ int pb_pot_static(const pb_fill_geom &g, double kw, double *stP, cudaStream_t s,
     return PB_OK;
 }
 
-template <typename R, int F, int SET, int EPI, int EQ>
+template <typename R, int F, int SET, int EPI, int EQ, int RED>
 static int launch_corr(const pb_fill_geom &g, const KArg &k, const double *st, const pb_epi_args &ea,
                        double2 *ig, long long igs, cudaStream_t s)
 {
@@ -814,11 +998,11 @@ static int launch_corr(const pb_fill_geom &g, const KArg &k, const double *st, c
     constexpr size_t smem = corr_smem_bytes<R, F>();
     static bool attr_set = false;
     if (!attr_set) {
-        PB_CUDA(cudaFuncSetAttribute(k_corr<R, F, SET, EPI, EQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        PB_CUDA(cudaFuncSetAttribute(k_corr<R, F, SET, EPI, EQ, RED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         attr_set = true;
     }
     const int grid = grid_for((T + PB_GROUP - 1) / PB_GROUP, PB_CORR_WARPS, PB_CORR_MINB);
-    k_corr<R, F, SET, EPI, EQ><<<grid, 32 * PB_CORR_WARPS, smem, s>>>(g, k, st, ea, ig, igs);
+    k_corr<R, F, SET, EPI, EQ, RED><<<grid, 32 * PB_CORR_WARPS, smem, s>>>(g, k, st, ea, ig, igs);
     PB_CHECK_LAUNCH();
     return PB_OK;
 }
@@ -827,8 +1011,13 @@ template <typename R, int F, int SET, int EPI>
 static int launch_corr_eq(const pb_fill_geom &g, const KArg &k, const double *st, const pb_epi_args &ea,
                           double2 *ig, long long igs, cudaStream_t s)
 {
-    if (k.eq && sizeof(R) == 4) return launch_corr<R, F, SET, EPI, 1>(g, k, st, ea, ig, igs, s);
-    return launch_corr<R, F, SET, EPI, 0>(g, k, st, ea, ig, igs, s);
+    if (sizeof(R) == 8) return launch_corr<R, F, SET, EPI, 0, 0>(g, k, st, ea, ig, igs, s);
+    if (k.eq) {
+        if (k.reduce) return launch_corr<R, F, SET, EPI, 1, 1>(g, k, st, ea, ig, igs, s);
+        return launch_corr<R, F, SET, EPI, 1, 0>(g, k, st, ea, ig, igs, s);
+    }
+    if (k.reduce) return launch_corr<R, F, SET, EPI, 0, 1>(g, k, st, ea, ig, igs, s);
+    return launch_corr<R, F, SET, EPI, 0, 0>(g, k, st, ea, ig, igs, s);
 }
 
 template <int SET, int EPI>
@@ -846,12 +1035,17 @@ static int launch_corr_any(const pb_fill_geom &g, const KArg &k, int use_fp32, c
     return launch_corr_eq<double, 16, SET, EPI>(g, k, st, ea, ig, igs, s);
 }
 
-// wavenumber set of a launch; equally spaced sets (linear sweeps) use the recurrence
-static void make_karg(KArg &k, int nf, const double *kw, double rmax)
+// wavenumber set of a launch; equally spaced sets (linear sweeps) use the recurrence.
+// pmax bounds |R - D| of every sample (0 = unknown): angles kh * pmax below pi/4 need no
+// reduction in the FP32 path.
+static void make_karg(KArg &k, int nf, const double *kw, double pmax)
 {
+    double khmax = 0;
     for (int f = 0; f < PB_FMAX; f++) {
         k.kw[f] = f < nf ? kw[f] : 0.0;
         k.kh[f] = 0.5 * k.kw[f];
+        k.khf[f] = (float)k.kh[f];
+        khmax = fmax(khmax, k.kh[f]);
     }
     k.nf = nf;
     k.dkh = nf > 1 ? 0.5 * (kw[1] - kw[0]) : 0.0;
@@ -859,7 +1053,9 @@ static void make_karg(KArg &k, int nf, const double *kw, double rmax)
     for (int f = 1; f < nf && k.eq; f++)
         if (fabs(kw[f] - kw[0] - f * (kw[1] - kw[0])) > 1e-9 * fabs(kw[nf - 1])) k.eq = 0;
     if (k.dkh <= 0) k.eq = 0;
-    k.small_step = k.eq && k.dkh * rmax < 0.78;
+    k.dkhf = (float)k.dkh;
+    k.reduce = !(pmax > 0 && khmax * pmax < 0.78);      // |dkh| <= khmax: covers the step too
+    k.step_tiny = pmax > 0 && fabs(k.dkh) * pmax < 0.01;
 }
 
 int pb_lp_corr(const pb_fill_geom &g, int nf, const double *kw, int use_fp32, const double *stLp,
@@ -868,7 +1064,7 @@ int pb_lp_corr(const pb_fill_geom &g, int nf, const double *kw, int use_fp32, co
     if (g.seg.n == 0) return PB_OK;
     if (nf < 1 || nf > PB_FMAX) { pb_set_error("pb_lp_corr: bad frequency count %d", nf); return PB_ERR_ARG; }
     KArg k;
-    make_karg(k, nf, kw, g.rmax);
+    make_karg(k, nf, kw, g.pmax);
     const int r = epi == PB_EPI_STORE
         ? launch_corr_any<PB_SET_LP, PB_EPI_STORE>(g, k, use_fp32, stLp, ea, nullptr, 0, s)
         : launch_corr_any<PB_SET_LP, PB_EPI_REDUCED>(g, k, use_fp32, stLp, ea, nullptr, 0, s);
@@ -884,7 +1080,7 @@ int pb_pot_corr(const pb_fill_geom &g, int nf, const double *kw, int use_fp32, c
     if (g.ncell == 0) return PB_OK;
     if (nf < 1 || nf > PB_FMAX) { pb_set_error("pb_pot_corr: bad frequency count %d", nf); return PB_ERR_ARG; }
     KArg k;
-    make_karg(k, nf, kw, g.rmax);
+    make_karg(k, nf, kw, g.pmax);
     const long long igs = (long long)g.chg.n * g.chg.n;
     const bool corr = kw[0] > 0;
     if (corr) {

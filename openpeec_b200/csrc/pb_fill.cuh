@@ -15,7 +15,7 @@ struct pb_fill_geom {
     double *pv = nullptr;           // shared polygon vertex pool [3*npv]
     int gp = 0;
     double gpz = 0;
-    double rmax = 0;                // bound on any sample distance (incl. images)
+    double pmax = 0;                // bound on |R - D| of any correction sample (0 = unknown)
     int any_poly = 0;
     // charge cells grouped by node (potential.c:29-114)
     int ncell = 0;

@@ -223,23 +223,64 @@ int gemm_sub<double>(pb_lu_engine *e, int m, int nc, int k, const double2 *A, in
     return PB_OK;
 }
 
+// Right operand B (k x nc complex, row-major, leading dimension ldb, batch stride sb)
+// to the real 2k x 2nc row-major matrix with the 2x2 block [[br, bi], [-bi, br]] in
+// place of each entry b = br + j bi. With A and C read as real matrices (interleaved
+// re/im = 2 real columns per complex column), C_real -= A_real * B_emb is exactly the
+// complex update: C[i][2j] -= sum_l ar br - ai bi, C[i][2j+1] -= sum_l ar bi + ai br.
+__global__ void k_embed_right(const float2 *__restrict__ b, int k, int nc, int ldb, long long sb,
+                              float *__restrict__ be)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int l = blockIdx.y;
+    const long long z = blockIdx.z;
+    if (j >= nc) return;
+    const float2 v = b[z * sb + (long long)l * ldb + j];
+    float2 *r0 = reinterpret_cast<float2 *>(be + z * 4LL * k * nc + (2LL * l) * (2LL * nc) + 2LL * j);
+    float2 *r1 = r0 + nc;                       // next real row: 2nc floats = nc float2
+    *r0 = make_float2(v.x, v.y);
+    *r1 = make_float2(-v.y, v.x);
+}
+
+// Thin updates stay on the SIMT complex GEMM: below 128 in any dimension the BF16x9
+// real form was measured slower on B200 (launch and split overheads dominate).
+static const int kTcMinDim = 128;
+
 template <>
 int gemm_sub<float>(pb_lu_engine *e, int m, int nc, int k, const float2 *A, int lda,
                     const float2 *B, int ldb, float2 *Cm, int ldc, long long stride, int nb)
 {
     if (m <= 0 || nc <= 0 || k <= 0) return PB_OK;
-    const cuComplex alpha = make_cuComplex(-1, 0), beta = make_cuComplex(1, 0);
     cublasStatus_t s;
-    if (e->gemm_kind == PB_GEMM_TC) {
+    const size_t need = (size_t)nb * 4 * (size_t)k * nc * sizeof(float);
+    if (e->gemm_kind == PB_GEMM_TC && !e->tc_disabled && e->emb && need <= e->emb_cap &&
+        m >= kTcMinDim && nc >= kTcMinDim && k >= kTcMinDim) {
+        k_embed_right<<<dim3(ceil_div(nc, 128), k, nb), 128, 0, e->stream>>>(B, k, nc, ldb, stride, e->emb);
+        PB_CHECK_LAUNCH();
+        e->launches++;
+        const float ra = -1.0f, rb = 1.0f;
+        cublasSetMathMode(e->blas, CUBLAS_DEFAULT_MATH);
+        cublasSetEmulationStrategy(e->blas, CUBLAS_EMULATION_STRATEGY_EAGER);
+        // row-major real C (m x 2nc) -= A (m x 2k) * Bemb (2k x 2nc); cuBLAS is
+        // column-major, so it computes the transpose: C^T = Bemb^T A^T.
         s = cublasGemmStridedBatchedEx(
-            e->blas, CUBLAS_OP_N, CUBLAS_OP_N, nc, m, k, &alpha, B, CUDA_C_32F, ldb, stride,
-            A, CUDA_C_32F, lda, stride, &beta, Cm, CUDA_C_32F, ldc, stride, nb,
-            (cublasComputeType_t)e->tc_compute, CUBLAS_GEMM_DEFAULT);
-    } else {
-        s = cublasCgemmStridedBatched(
-            e->blas, CUBLAS_OP_N, CUBLAS_OP_N, nc, m, k, &alpha, (const cuComplex *)B, ldb,
-            stride, (const cuComplex *)A, lda, stride, &beta, (cuComplex *)Cm, ldc, stride, nb);
+            e->blas, CUBLAS_OP_N, CUBLAS_OP_N, 2 * nc, m, 2 * k, &ra, e->emb, CUDA_R_32F, 2 * nc,
+            4LL * k * nc, A, CUDA_R_32F, 2 * lda, 2 * stride, &rb, Cm, CUDA_R_32F, 2 * ldc, 2 * stride, nb,
+            CUBLAS_COMPUTE_32F_EMULATED_16BFX9, CUBLAS_GEMM_DEFAULT);
+        cublasSetEmulationStrategy(e->blas, CUBLAS_EMULATION_STRATEGY_DEFAULT);
+        cublasSetMathMode(e->blas, CUBLAS_PEDANTIC_MATH);
+        e->launches++;
+        if (s == CUBLAS_STATUS_SUCCESS) return PB_OK;
+        if (s != CUBLAS_STATUS_NOT_SUPPORTED) {
+            pb_set_error("BF16x9 real GEMM failed (%d)", (int)s);
+            return PB_ERR_CUDA;
+        }
+        e->tc_disabled = 1;                     // library without the emulation: SIMT from now on
     }
+    const cuComplex alpha = make_cuComplex(-1, 0), beta = make_cuComplex(1, 0);
+    s = cublasCgemmStridedBatched(
+        e->blas, CUBLAS_OP_N, CUBLAS_OP_N, nc, m, k, &alpha, (const cuComplex *)B, ldb,
+        stride, (const cuComplex *)A, lda, stride, &beta, (cuComplex *)Cm, ldc, stride, nb);
     e->launches++;
     if (s != CUBLAS_STATUS_SUCCESS) { pb_set_error("complex FP32 GEMM failed (%d)", (int)s); return PB_ERR_CUDA; }
     return PB_OK;
@@ -254,7 +295,6 @@ int pb_lu_engine_init(pb_lu_engine *e, cudaStream_t s)
     }
     cublasSetStream(e->blas, s);
     cublasSetMathMode(e->blas, CUBLAS_PEDANTIC_MATH);
-    e->tc_compute = (int)CUBLAS_COMPUTE_32F_EMULATED_16BFX9;
     return PB_OK;
 }
 

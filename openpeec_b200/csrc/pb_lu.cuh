@@ -7,16 +7,23 @@
 enum pb_gemm_kind {
     PB_GEMM_FP64 = 0,   // complex FP64 GEMM
     PB_GEMM_FP32 = 1,   // complex FP32 GEMM, SIMT
-    PB_GEMM_TC   = 2,   // complex FP32 inputs on the tensor cores (BF16x9 FP32 emulation,
-                        // TF32 if the emulation is unavailable), FP32 accumulation
+    PB_GEMM_TC   = 2,   // complex FP32 GEMM as one real FP32 GEMM on the tensor cores
+                        // (BF16x9 FP32 emulation: each FP32 operand split into 3 BF16
+                        // terms, FP32 accumulation); SIMT for thin updates
 };
 
 struct pb_lu_engine {
     cublasHandle_t blas = nullptr;
     cudaStream_t stream = nullptr;
     int gemm_kind = PB_GEMM_FP64;
-    int tc_compute = -1;       // resolved cublasComputeType_t for PB_GEMM_TC
     long launches = 0;         // kernels launched (own kernels + library calls)
+    // Scratch for PB_GEMM_TC: the k x nc complex right operand expanded to the real
+    // 2k x 2nc matrix [[re, im], [-im, re]] per entry, nb of them (4*k*nc floats each).
+    // Owned by the caller (the sweep sizes it at 4*n*n bytes per matrix); without it, or
+    // when an update needs more, the update runs as a SIMT complex GEMM.
+    float *emb = nullptr;
+    size_t emb_cap = 0;        // bytes
+    int tc_disabled = 0;       // set if the library rejects the emulated compute type
 };
 
 int pb_lu_engine_init(pb_lu_engine *e, cudaStream_t s);

@@ -246,7 +246,8 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
     size_t fr = 0, tot = 0;
     PB_CUDA(cudaMemGetInfo(&fr, &tot));
     const double n2 = (double)n * n;
-    double perf = n2 * 16 + (mixed ? n2 * 8 : 0) + (double)nc * nc * 16 + (double)ns * 16
+    const int tc = (o.lu == PB_LU_TC);
+    double perf = n2 * 16 + (mixed ? n2 * 8 : 0) + (tc ? n2 * 4 : 0) + (double)nc * nc * 16 + (double)ns * 16
                 + (form == PB_FORM_FULL ? (double)ns * ns * 16 : 0) + 4.0 * np * n * 16 + 8.0 * n;
     const double fixed = (double)ns * ns * 8 + (double)nc * nc * 8 +
                          (c->retardation ? (double)PB_FMAX * c->chg.size() * c->chg.size() * 16 : 0.0);
@@ -262,6 +263,18 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
         bFreq, bZ, bPC;
     PB_TRY(bM64.alloc((size_t)B * n2 * 16));
     if (mixed) PB_TRY(bM32.alloc((size_t)B * n2 * 8));
+    // real-embedded right operands of the tensor-core trailing updates: the largest is
+    // k x nc complex with k + nc = n, i.e. at most n^2/4 entries -> 4 * n^2/4 floats
+    DevBuf bEmb;
+    struct EmbGuard {
+        pb_lu_engine *e;
+        ~EmbGuard() { e->emb = nullptr; e->emb_cap = 0; }
+    } emb_guard{&c->lu};
+    if (tc) {
+        PB_TRY(bEmb.alloc((size_t)B * n2 * 4));
+        c->lu.emb = bEmb.as<float>();
+        c->lu.emb_cap = (size_t)B * n2 * 4;
+    }
     PB_TRY(bP.alloc((size_t)B * nc * nc * 16 + 16));
     DevBuf bIg;                                  // sub-cell P corrections of one fill chunk
     if (c->capacitance && nc > 0 && c->retardation)

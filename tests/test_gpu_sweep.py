@@ -140,3 +140,29 @@ end
         with pytest.raises(api.PbError) as e:
             ctx.sweep([1e6], fill_prec=abi.PREC_FP64, lu=abi.LU_FP64)
     assert e.value.code == abi.PB_ERR_SINGULAR
+
+
+def test_full_size_plate_against_reference(golden):
+    """The 4196-cell plate + wire (the benchmark structure) at 5 MHz and 1.28 GHz. At this
+    order the trailing updates of the LU (m, n, k >= 128) run as real BF16x9 tensor-core
+    GEMMs; after FP64 refinement Z must match the reference's within 1e-6."""
+    prob, fx = golden("cfg2_full")
+    with api.Context(prob) as ctx:
+        z, st = ctx.sweep(fx["freqs"], fill_prec=abi.PREC_MIXED, lu=abi.LU_TC)
+    assert zerr(z, fx["z"]) <= 1e-6, (zerr(z, fx["z"]), st)
+
+
+def test_tensor_core_lu_matches_plain_path():
+    """Mid-size plate (32 x 16 grid, 1076 current cells) over 150-900 MHz: the mixed sweep
+    (FP32 fill correction, BF16x9 trailing updates, FP64 refinement) against the plain
+    FP64 path within 1e-6, with the SIMT FP32 LU as a second check of the same answer."""
+    from openpeec_b200 import configs, geometry
+    prob = geometry.build(geometry.parse_peec(configs.cfg2(32, 16, 6, 1.5e8, 1.5e8)))
+    f = prob.freqs()
+    with api.Context(prob) as ctx:
+        zp, _ = ctx.sweep(f, fill_prec=abi.PREC_FP64, lu=abi.LU_FP64)
+        zt, st = ctx.sweep(f, fill_prec=abi.PREC_MIXED, lu=abi.LU_TC)
+        zs, _ = ctx.sweep(f, fill_prec=abi.PREC_MIXED, lu=abi.LU_FP32)
+    assert st["n_system"] >= 1000
+    assert zerr(zt, zp) <= 1e-6, (zerr(zt, zp), st)
+    assert zerr(zs, zp) <= 1e-6
