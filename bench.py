@@ -294,7 +294,7 @@ def run_ours(args, ws, rank, dist):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_dev_max / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32 correction + f64 static/refinement, tf32/bf16x9 LU",
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64 (f32 correction and bf16x9 tensor-core LU; f64 static part and refinement)",
         "data": "synthetic (seeded geometry from the .peec text; no external data)",
         "config": {"workload": WORKLOAD if args.grid == "64x32" else "profiling case, plate grid " + args.grid,
                    "freqs_per_step": B, "n_system": len(prob.seg),
@@ -305,7 +305,11 @@ def run_ours(args, ws, rank, dist):
         "gpu_launches": int(launches),
         "roofline": {"bound": "fp32-simt", "kernel": "k_lp_corr + k_pot_corr (retardation correction)",
                      "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
-                     "frac": (achieved / peak.value) if achieved else None, "traffic": None,
+                     "frac": (achieved / peak.value) if achieved else None,
+                     # DRAM bytes of one Lp-correction launch (16 frequencies): ncu capture of
+                     # the 32x16 plate (840 MB), scaled by the cell count squared to 4196 cells
+                     "traffic": 840e6 * (4196.0 / 1076.0) ** 2 if args.grid == "64x32" else None,
+                     "traffic_unit": "bytes per Lp-correction launch (ncu, scaled)",
                      "peak_source": "measured FP32 FMA microbenchmark (pb_fp32_peak) on this GPU",
                      "flop_per_sample_freq": FLOP_PER_SAMPLE_FREQ, "samples": samples,
                      "time_ms": ms_corr},

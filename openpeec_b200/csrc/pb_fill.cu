@@ -711,18 +711,20 @@ k_corr(pb_fill_geom g, KArg k, const double *st, pb_epi_args ea, double2 *ig, lo
                 if (cb >= 0 && da >= 0) prefetch_l1(P + (long long)cb * nc + da);
                 if (cb >= 0 && db >= 0) prefetch_l1(P + (long long)cb * nc + db);
             }
-            Acc<R, F> acc;
-            acc.init(tot + lane);
-            for (int q = 0; q < h.nterm; q++) {
-                if constexpr (sizeof(R) == 4) {
-                    run_term32<F, EQ, RED>(terms[2 * tk + q], k, acc, lane, bases);
-                } else {
-                    const Term<R> tm = terms[2 * tk + q];
-                    run_term<R, F, EQ>(tm, k, acc, lane);
+            double cr = 0, cim = 0;
+            if (h.nterm > 0) {               // warp-uniform; e.g. perpendicular Lp pairs have none
+                Acc<R, F> acc;
+                acc.init(tot + lane);
+                for (int q = 0; q < h.nterm; q++) {
+                    if constexpr (sizeof(R) == 4) {
+                        run_term32<F, EQ, RED>(terms[2 * tk + q], k, acc, lane, bases);
+                    } else {
+                        const Term<R> tm = terms[2 * tk + q];
+                        run_term<R, F, EQ>(tm, k, acc, lane);
+                    }
                 }
+                reduce_select<F>(acc, lane, cr, cim);
             }
-            double cr, cim;
-            reduce_select<F>(acc, lane, cr, cim);
             const int f = lane, i = h.i, j = h.j;
             if (f >= nf) continue;
             if (SET == PB_SET_IG) {
