@@ -222,7 +222,7 @@ def run_ours(args, ws, rank, dist):
     ctx = api.Context(prob)
     peak = ctypes.c_double()
     abi.lib().pb_fp32_peak(ctypes.byref(peak))
-    opts = dict(fill_prec=abi.PREC_MIXED, lu=abi.LU_TC, batch=B)
+    opts = dict(fill_prec=abi.PREC_MIXED, lu=abi.LU_TC, batch=B, accel=args.accel)
     for w in range(args.warmup):
         ctx.sweep(step_freqs(freqs, w, B, rank, ws), **opts)
     clocks = Clocks() if rank == 0 else None
@@ -298,7 +298,9 @@ def run_ours(args, ws, rank, dist):
         "data": "synthetic (seeded geometry from the .peec text; no external data)",
         "config": {"workload": WORKLOAD if args.grid == "64x32" else "profiling case, plate grid " + args.grid,
                    "freqs_per_step": B, "n_system": len(prob.seg),
-                   "form": "reduced branch-current MNA", "parallelism": "frequency batches per rank" if ws > 1 else "1 GPU",
+                   "form": "reduced branch-current MNA",
+                   "solve": ("FP32 LU every %d frequencies + FP64 GMRES(60)" % args.accel) if args.accel >= 2
+                            else "FP32 LU per frequency + FP64 refinement", "parallelism": "frequency batches per rank" if ws > 1 else "1 GPU",
                    "l2": "inputs larger than L2 (282 MB FP64 system matrix per frequency)"},
         "e2e": {"value": total_points / e2e_t, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
@@ -359,6 +361,8 @@ def main():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--grid", default="64x32", help="plate grid; not 64x32 only for profiling captures")
+    ap.add_argument("--accel", type=int, default=0,
+                    help="LU reuse: one FP32 factorisation per ACCEL frequencies, GMRES for the rest (0 = every frequency)")
     args = ap.parse_args()
     ws, rank = dist_env()
     if args.impl == "reference":

@@ -1,19 +1,14 @@
 /*
  * peec_b200.h — C ABI of the B200 frequency-sweep library (libpeec_b200.so).
  *
- * Two layers are exported from the same shared library:
- *
- *   1. The batched core ("pb_*"): plain C structs, pointers and sizes. The caller hands
- *      over the discretised geometry once (current cells, charge cells, nodes, ports)
- *      and then asks for partial-element matrices or a whole frequency sweep. All device
- *      memory is owned by an opaque context; every call is synchronous on return.
- *
- *   2. The reference-compatible entry points (lp_fill, pot_fill, solve, lu_decomp, ...):
- *      declared in peec_abi.h with the reference's own prototypes, implemented on top of
- *      layer 1. A program built from the reference's host files (parser, geometry,
- *      outputs, main) links against this library instead of the reference's
- *      partial.c / potential.c / surface.c / volume.c / polygon.c / skin.c / mna.c /
- *      lu.c / solve.c.
+ * The library exports one layer, the batched core ("pb_*"): plain C structs, pointers and
+ * sizes. The caller hands over the discretised geometry once (current cells, charge
+ * cells, nodes, ports) and then asks for partial-element matrices or a whole frequency
+ * sweep. All device memory is owned by an opaque context; every call is synchronous on
+ * return. A program built from the reference's host files (parser, geometry, outputs,
+ * main) uses it through a small replacement of the reference's solve() that converts its
+ * seg_t / chg arrays to pb_cell_t and calls pb_create + pb_sweep; that shim is written in
+ * the reference's own C and is not compiled into this library.
  *
  * Return convention of the core: 0 = success, non-zero = error; pb_last_error() returns a
  * message for the calling thread's last failure. There is no host fallback: if no CUDA
@@ -122,6 +117,13 @@ typedef struct {
     int    verbose;
     int    corr_freqs;      /* frequencies per retardation-correction launch, 1..16
                                (0 = automatic); a tuning knob, results do not depend on it */
+    int    accel;           /* LU reuse, the reference's acceleration = 1 (solve.c:47-64):
+                               0 or 1 = one factorisation per frequency;
+                               S >= 2 = one FP32 factorisation per S consecutive
+                               frequencies of the mixed path, the others solved by FP64
+                               right-preconditioned GMRES(60) with the nearest factored
+                               frequency's LU (gmres_solve, iterative.c:230-252); systems
+                               that do not converge are refactorised (FP64) */
 } pb_sweep_opts;
 
 typedef struct {
@@ -139,6 +141,11 @@ typedef struct {
     int    fp64_direct;     /* frequencies solved directly in FP64 because a lower or
                                equal frequency of the same sweep needed the fallback   */
     double fp64_max_hz;     /* highest frequency that needed FP64                     */
+    int    lu_count;        /* factorisations done (all precisions)                   */
+    int    gmres_solves;    /* systems solved by preconditioned GMRES (accel >= 2)    */
+    int    gmres_its_max;   /* largest GMRES iteration count of one system            */
+    int    gmres_refactored;/* systems refactorised at their own frequency (FP32)     */
+    double gmres_its_avg;   /* mean GMRES iterations per GMRES-solved system          */
 } pb_sweep_stats;
 
 const char *pb_last_error(void);

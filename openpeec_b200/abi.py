@@ -56,7 +56,7 @@ class PbSweepOpts(C.Structure):
     _fields_ = [
         ("fill_prec", C.c_int), ("lu", C.c_int), ("form", C.c_int), ("batch", C.c_int),
         ("refine_tol", C.c_double), ("refine_maxit", C.c_int), ("verbose", C.c_int),
-        ("corr_freqs", C.c_int),
+        ("corr_freqs", C.c_int), ("accel", C.c_int),
     ]
 
 
@@ -70,6 +70,8 @@ class PbSweepStats(C.Structure):
         ("n_system", C.c_int), ("static_refreshes", C.c_int),
         ("kernel_launches", C.c_int), ("fp64_fallbacks", C.c_int),
         ("fp64_direct", C.c_int), ("fp64_max_hz", C.c_double),
+        ("lu_count", C.c_int), ("gmres_solves", C.c_int), ("gmres_its_max", C.c_int),
+        ("gmres_refactored", C.c_int), ("gmres_its_avg", C.c_double),
     ]
 
     def as_dict(self):

@@ -447,7 +447,7 @@ int pb_lu_perm(pb_lu_engine *e, int n, int nb, const int *piv, int *perm)
 template <typename TF>
 __global__ void __launch_bounds__(1024)
 k_lu_solve(const T2_t<TF> *lu, int n, int ld, long long stride, const int *perm,
-           const double2 *r, double2 *x, int nrhs)
+           const double2 *r, double2 *x, int nrhs, const int *sys, const int *lu_of)
 {
     typedef T2_t<TF> T2;
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -455,10 +455,12 @@ k_lu_solve(const T2_t<TF> *lu, int n, int ld, long long stride, const int *perm,
     __shared__ T2 diag[32][33];
     __shared__ T2 tmp[32];
     __shared__ double red[33];
-    const int rhs = blockIdx.x, b = blockIdx.y, tid = threadIdx.x;
+    const int rhs = blockIdx.x, tid = threadIdx.x;
+    const int b = sys ? sys[blockIdx.y] : blockIdx.y;         // system (vector slot)
+    const int fm = lu_of ? lu_of[b] : b;                      // its factors
     const int lane = tid & 31, warp = tid >> 5;
-    lu += (long long)b * stride;
-    perm += (long long)b * n;
+    lu += (long long)fm * stride;
+    perm += (long long)fm * n;
     const double2 *rv = r + ((long long)b * nrhs + rhs) * n;
     double2 *xv = x + ((long long)b * nrhs + rhs) * n;
 
@@ -552,6 +554,15 @@ template <typename TF>
 int pb_lu_solve_batched(pb_lu_engine *e, int n, int nb, int nrhs, const T2_t<TF> *lu, int ld,
                         long stride, const int *perm, const double2 *r, double2 *x)
 {
+    return pb_lu_solve_mapped<TF>(e, n, nb, nrhs, lu, ld, stride, perm, r, x, nullptr, nullptr);
+}
+
+template <typename TF>
+int pb_lu_solve_mapped(pb_lu_engine *e, int n, int nb, int nrhs, const T2_t<TF> *lu, int ld,
+                       long stride, const int *perm, const double2 *r, double2 *x, const int *sys,
+                       const int *lu_of)
+{
+    if (nb <= 0) return PB_OK;
     const size_t smem = (size_t)n * sizeof(T2_t<TF>);
     static bool attr_set = false;
     if (!attr_set) {
@@ -562,11 +573,13 @@ int pb_lu_solve_batched(pb_lu_engine *e, int n, int nb, int nrhs, const T2_t<TF>
         attr_set = true;
     }
     dim3 g(nrhs, nb);
-    k_lu_solve<TF><<<g, 1024, smem, e->stream>>>(lu, n, ld, stride, perm, r, x, nrhs);
+    k_lu_solve<TF><<<g, 1024, smem, e->stream>>>(lu, n, ld, stride, perm, r, x, nrhs, sys, lu_of);
     e->launches++;
     PB_CHECK_LAUNCH();
     return PB_OK;
 }
+template int pb_lu_solve_mapped<float>(pb_lu_engine *, int, int, int, const float2 *, int, long, const int *, const double2 *, double2 *, const int *, const int *);
+template int pb_lu_solve_mapped<double>(pb_lu_engine *, int, int, int, const double2 *, int, long, const int *, const double2 *, double2 *, const int *, const int *);
 template int pb_lu_solve_batched<float>(pb_lu_engine *, int, int, int, const float2 *, int, long, const int *, const double2 *, double2 *);
 template int pb_lu_solve_batched<double>(pb_lu_engine *, int, int, int, const double2 *, int, long, const int *, const double2 *, double2 *);
 
@@ -581,15 +594,15 @@ __device__ __forceinline__ void atomic_max_pos(double *addr, double v)
 __global__ void __launch_bounds__(256)
 k_residual(const double2 *a, int n, int ld, long long stride, const double2 *bv,
            const double2 *xv, double2 *rv, double *rn, double *bn, double *xn, double *an,
-           int nrhs, int rows_per_block)
+           int nrhs, int rows_per_block, const int *sys)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     double2 *xs = reinterpret_cast<double2 *>(smraw);     // [nrhs][n]
-    const int b = blockIdx.y, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int b = sys ? sys[blockIdx.y] : blockIdx.y, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     a += (long long)b * stride;
     for (int e = tid; e < nrhs * n; e += blockDim.x) xs[e] = xv[(long long)b * nrhs * n + e];
     __syncthreads();
-    if (blockIdx.x == 0) {
+    if (blockIdx.x == 0 && xn) {
         for (int q = warp; q < nrhs; q += 8) {
             double m = 0;
             for (int c = lane; c < n; c += 32) m = fmax(m, fmax(fabs(xs[q * n + c].x), fabs(xs[q * n + c].y)));
@@ -621,11 +634,15 @@ k_residual(const double2 *a, int n, int ld, long long stride, const double2 *bv,
             }
             if (lane == 0) {
                 const long long idx = ((long long)b * nrhs + q) * n + r;
-                const double2 bb = bv[idx];
-                const double2 res = make_double2(bb.x - sr, bb.y - si);
-                rv[idx] = res;
-                atomic_max_pos(&rn[b * nrhs + q], fmax(fabs(res.x), fabs(res.y)));
-                atomic_max_pos(&bn[b * nrhs + q], fmax(fabs(bb.x), fabs(bb.y)));
+                if (bv) {
+                    const double2 bb = bv[idx];
+                    const double2 res = make_double2(bb.x - sr, bb.y - si);
+                    rv[idx] = res;
+                    atomic_max_pos(&rn[b * nrhs + q], fmax(fabs(res.x), fabs(res.y)));
+                    atomic_max_pos(&bn[b * nrhs + q], fmax(fabs(bb.x), fabs(bb.y)));
+                } else {
+                    rv[idx] = make_double2(sr, si);          // product only: r = A x
+                }
             }
         }
     }
@@ -649,7 +666,54 @@ int pb_residual(pb_lu_engine *e, int n, int nb, int nrhs, const double2 *a, int 
     }
     const int rpb = 64;
     dim3 g(ceil_div(n, rpb), nb);
-    k_residual<<<g, 256, smem, e->stream>>>(a, n, ld, stride, b, x, r, rn, bn, xn, an, nrhs, rpb);
+    k_residual<<<g, 256, smem, e->stream>>>(a, n, ld, stride, b, x, r, rn, bn, xn, an, nrhs, rpb, nullptr);
+    e->launches++;
+    PB_CHECK_LAUNCH();
+    return PB_OK;
+}
+
+int pb_residual_mapped(pb_lu_engine *e, int n, int nb, int nrhs, const double2 *a, int ld, long stride,
+                       const double2 *b, const double2 *x, double2 *r, double *rn, double *bn, double *xn,
+                       double *an, int nall, const int *sys)
+{
+    PB_CUDA(cudaMemsetAsync(rn, 0, sizeof(double) * nall * nrhs, e->stream));
+    PB_CUDA(cudaMemsetAsync(bn, 0, sizeof(double) * nall * nrhs, e->stream));
+    if (an) PB_CUDA(cudaMemsetAsync(an, 0, sizeof(double) * nall, e->stream));
+    if (nb <= 0) return PB_OK;
+    const size_t smem = (size_t)nrhs * n * sizeof(double2);
+    static bool attr_set = false;
+    if (!attr_set) {
+        int dev = 0, cap = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&cap, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        PB_CUDA(cudaFuncSetAttribute(k_residual, cudaFuncAttributeMaxDynamicSharedMemorySize, cap));
+        attr_set = true;
+    }
+    const int rpb = 64;
+    dim3 g(ceil_div(n, rpb), nb);
+    k_residual<<<g, 256, smem, e->stream>>>(a, n, ld, stride, b, x, r, rn, bn, xn, an, nrhs, rpb, sys);
+    e->launches++;
+    PB_CHECK_LAUNCH();
+    return PB_OK;
+}
+
+int pb_matvec_mapped(pb_lu_engine *e, int n, int nb, int nrhs, const double2 *a, int ld, long stride,
+                     const double2 *x, double2 *y, const int *sys)
+{
+    if (nb <= 0) return PB_OK;
+    const size_t smem = (size_t)nrhs * n * sizeof(double2);
+    static bool attr_set = false;
+    if (!attr_set) {
+        int dev = 0, cap = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&cap, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        PB_CUDA(cudaFuncSetAttribute(k_residual, cudaFuncAttributeMaxDynamicSharedMemorySize, cap));
+        attr_set = true;
+    }
+    const int rpb = 64;
+    dim3 g(ceil_div(n, rpb), nb);
+    k_residual<<<g, 256, smem, e->stream>>>(a, n, ld, stride, nullptr, x, y, nullptr, nullptr, nullptr,
+                                            nullptr, nrhs, rpb, sys);
     e->launches++;
     PB_CHECK_LAUNCH();
     return PB_OK;

@@ -47,6 +47,24 @@ int pb_lu_solve_batched(pb_lu_engine *e, int n, int nb, int nrhs,
                         const typename cplx_t<TF>::type *lu, int ld, long stride,
                         const int *perm, const double2 *r, double2 *x);
 
+// Same with an indirection: CTA row y solves system sys[y] (vector slot, nullptr = y)
+// with the factors of matrix lu_of[system] (nullptr = the system itself).
+template <typename TF>
+int pb_lu_solve_mapped(pb_lu_engine *e, int n, int nb, int nrhs,
+                       const typename cplx_t<TF>::type *lu, int ld, long stride,
+                       const int *perm, const double2 *r, double2 *x, const int *sys,
+                       const int *lu_of);
+
+// pb_residual for the nb systems sys[0..nb) of a batch of nall; the norms of the other
+// systems are left at 0.
+int pb_residual_mapped(pb_lu_engine *e, int n, int nb, int nrhs, const double2 *a, int ld, long stride,
+                       const double2 *b, const double2 *x, double2 *r, double *rn, double *bn, double *xn,
+                       double *an, int nall, const int *sys);
+
+// y = A x for the nb systems sys[0..nb) (nullptr = 0..nb), nrhs vectors each.
+int pb_matvec_mapped(pb_lu_engine *e, int n, int nb, int nrhs, const double2 *a, int ld, long stride,
+                     const double2 *x, double2 *y, const int *sys);
+
 // r = b - A x for nb FP64 matrices, nrhs vectors each; also writes the infinity norms
 // (max |re|,|im| component) of r, b and x per vector into rn, bn, xn [nb*nrhs] and,
 // when an != nullptr, the infinity norm of each matrix (max row sum of |re|+|im|).

@@ -14,6 +14,7 @@
 // Dense solve: batched LU of the whole batch; FP64 LU (plain path) or FP32 LU with
 // tensor-core trailing updates + FP64 iterative refinement against the FP64 matrix.
 #include "pb_ctx.cuh"
+#include "pb_gmres.cuh"
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -220,7 +221,7 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
     pb_sweep_opts o;
     if (opts_in) o = *opts_in;
     else { o.fill_prec = PB_PREC_MIXED; o.lu = PB_LU_TC; o.form = PB_FORM_AUTO; o.batch = 0;
-           o.refine_tol = 0; o.refine_maxit = 0; o.verbose = 0; o.corr_freqs = 0; }
+           o.refine_tol = 0; o.refine_maxit = 0; o.verbose = 0; o.corr_freqs = 0; o.accel = 0; }
     if (nfreq <= 0 || freq == nullptr) { pb_set_error("pb_sweep: no frequencies"); return PB_ERR_ARG; }
     for (int i = 0; i < nfreq; i++)
         if (!(freq[i] > 0)) { pb_set_error("pb_sweep: frequencies must be > 0"); return PB_ERR_ARG; }
@@ -321,7 +322,8 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
     bool static_valid = false;
     std::vector<double2> zh((size_t)B * np * np);
     std::vector<double> rnh(B * np), bnh(B * np), xnh(B * np), anh(B);
-    int fallbacks = 0, fp64_direct = 0;
+    int fallbacks = 0, fp64_direct = 0, lu_count = 0, gm_solves = 0, gm_max = 0, refactored = 0;
+    long gm_its = 0;
     double fp64_hz = 0;                          // frequencies <= this are solved in FP64
     double lp_samp = 0, p_samp = 0;
     std::vector<int> infoh(B);
@@ -425,14 +427,25 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
         if (mixed) while (nd < nb && fb[nd] <= fp64_hz) nd++;
         else nd = nb;
         const long long nn = (long long)n * n;
+        // LU reuse (accel >= 2): factor every S-th frequency of the mixed part (the anchors,
+        // centred in their groups); the others are solved by GMRES preconditioned with the
+        // nearest anchor's factors.
+        const int mb = nb - nd;
+        const int S = (mixed && o.accel >= 2 && mb >= 2) ? o.accel : 0;
+        const int aoff = S ? std::min(S / 2, mb - 1) : 0;
+        const int nanch = S ? (mb - 1 - aoff) / S + 1 : mb;
+        std::vector<int> lu_of(std::max(mb, 1));
+        for (int q = 0; q < mb; q++)
+            lu_of[q] = S ? std::min(nanch - 1, std::max(0, (int)std::floor((q - aoff) / (double)S + 0.5))) : q;
         tLu.start(st);
         if (nd > 0) PB_TRY(pb_lu_factor<double>(&c->lu, n, nd, bM64.as<double2>(), n, nn, bPiv.as<int>(), bInfo.as<int>()));
-        if (nb > nd)
-            PB_TRY(pb_lu_factor<float>(&c->lu, n, nb - nd, bM32.as<float2>() + nd * nn, n, nn,
+        if (mb > 0)
+            PB_TRY(pb_lu_factor<float>(&c->lu, n, nanch, bM32.as<float2>() + (nd + aoff) * nn, n, S ? S * nn : nn,
                                        bPiv.as<int>() + (long long)nd * n, bInfo.as<int>() + nd));
-        PB_TRY(pb_lu_perm(&c->lu, n, nb, bPiv.as<int>(), bPerm.as<int>()));
+        PB_TRY(pb_lu_perm(&c->lu, n, nd + (mb > 0 ? nanch : 0), bPiv.as<int>(), bPerm.as<int>()));
         tLu.stop(st);
-        luflops += 8.0 / 3.0 * (double)n * n * n * nb;
+        luflops += 8.0 / 3.0 * (double)n * n * n * (nd + (mb > 0 ? nanch : 0));
+        lu_count += nd + (mb > 0 ? nanch : 0);
         PB_CUDA(cudaMemcpyAsync(infoh.data(), bInfo.p, sizeof(int) * nb, cudaMemcpyDeviceToHost, st));
         PB_CUDA(cudaStreamSynchronize(st));
         for (int q = 0; q < nd; q++)
@@ -456,7 +469,75 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
             PB_TRY(pb_lu_solve_batched<double>(&c->lu, n, nd, np, bM64.as<double2>(), n, nn,
                                                bPerm.as<int>(), bRhs.as<double2>(), bX.as<double2>()));
         std::vector<int> state(nb, 1);            // 0 active, 1 converged / direct, 2 failed
-        if (nb > nd) {
+        if (nb > nd && S) {
+            // GMRES with the anchors' FP32 factors (anchors themselves converge in a few
+            // steps, like the refinement below)
+            const long long vo = (long long)nd * np * n;
+            std::vector<int> gst(mb, 0);
+            for (int q = 0; q < mb; q++)
+                if (infoh[nd + lu_of[q]] >= 0) gst[q] = 2;            // zero FP32 pivot: go FP64
+            pb_gmres_args ga;
+            ga.eng = &c->lu;
+            ga.n = n;
+            ga.nsys = mb;
+            ga.nrhs = np;
+            ga.A = bM64.as<double2>() + nd * nn;
+            ga.A_stride = nn;
+            ga.lu = bM32.as<float2>() + (nd + aoff) * nn;
+            ga.lu_stride = S * nn;
+            ga.perm = bPerm.as<int>() + (long long)nd * n;
+            ga.lu_of = lu_of.data();
+            ga.b = bRhs.as<double2>() + vo;
+            ga.x = bX.as<double2>() + vo;
+            ga.eta = std::max(1e-14, 8.0 * std::sqrt((double)n) * 1.1e-16);
+            ga.m = PB_GMRES_MAXM;
+            ga.max_cycles = 2;
+            pb_gmres_result gr;
+            PB_TRY(pb_gmres_batched(ga, gst, &gr));
+            gm_solves += gr.solved;
+            gm_its += gr.iters_total;
+            gm_max = std::max(gm_max, gr.iters_max);
+            maxits = std::max(maxits, gr.iters_max);
+            // Systems the stale factors could not bring to the target are refactorised at
+            // their own frequency (accel_rhs, solve.c:52-60), in FP32, and solved again. Their
+            // FP32 copies are intact (only the anchors were factorised in place); they are
+            // compacted to the front of the FP32 storage, whose anchor factors are no longer
+            // needed, and factorised together.
+            std::vector<int> redo;
+            for (int q = 0; q < mb; q++)
+                if (gst[q] == 2 && infoh[nd + lu_of[q]] < 0) redo.push_back(q);
+            if (!redo.empty()) {
+                const int nr = (int)redo.size();
+                float2 *m32 = bM32.as<float2>() + nd * nn;
+                for (int t = 0; t < nr; t++)
+                    if (redo[t] != t)
+                        PB_CUDA(cudaMemcpyAsync(m32 + t * nn, m32 + redo[t] * nn, sizeof(float2) * nn,
+                                                cudaMemcpyDeviceToDevice, st));
+                tLu.start(st);
+                PB_TRY(pb_lu_factor<float>(&c->lu, n, nr, m32, n, nn, bPiv.as<int>() + (long long)nd * n,
+                                           bInfo.as<int>() + nd));
+                PB_TRY(pb_lu_perm(&c->lu, n, nr, bPiv.as<int>() + (long long)nd * n, bPerm.as<int>() + (long long)nd * n));
+                tLu.stop(st);
+                luflops += 8.0 / 3.0 * (double)n * n * n * nr;
+                lu_count += nr;
+                std::vector<int> rinfo(nr);
+                PB_CUDA(cudaMemcpyAsync(rinfo.data(), bInfo.as<int>() + nd, sizeof(int) * nr, cudaMemcpyDeviceToHost, st));
+                PB_CUDA(cudaStreamSynchronize(st));
+                std::vector<int> gst2(mb, 1);
+                for (int t = 0; t < nr; t++) {
+                    lu_of[redo[t]] = t;
+                    gst2[redo[t]] = rinfo[t] >= 0 ? 2 : 0;
+                }
+                ga.lu = m32;
+                ga.lu_stride = nn;
+                PB_TRY(pb_gmres_batched(ga, gst2, &gr));
+                for (int q = 0; q < mb; q++) if (gst[q] == 2) gst[q] = gst2[q];
+                gm_its += gr.iters_total;
+                gm_max = std::max(gm_max, gr.iters_max);
+                refactored += nr;
+            }
+            for (int q = 0; q < mb; q++) state[nd + q] = gst[q];
+        } else if (nb > nd) {
             // Iterative refinement in FP64 against the FP64 matrix:
             //   x_0 = LU^-1 b,  r = b - A x,  x += LU^-1 r,
             // until the normwise backward error eta = |r| / (|A| |x| + |b|) (infinity norms)
@@ -506,6 +587,8 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
                 PB_CHECK_LAUNCH();
             }
             maxits = std::max(maxits, it);
+        }
+        if (nb > nd) {
             // FP64 fallback, batched: copy the stalled frequencies' FP64 matrices into the
             // (no longer needed) FP32 factor storage, factorise and solve them together.
             std::vector<int> failed;
@@ -523,6 +606,7 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
                                             cudaMemcpyDeviceToDevice, st));
                 }
                 PB_TRY(pb_lu_factor<double>(&c->lu, n, ng, scr, n, nn, bPiv.as<int>(), bInfo.as<int>()));
+                lu_count += ng;
                 PB_TRY(pb_lu_perm(&c->lu, n, ng, bPiv.as<int>(), bPerm.as<int>()));
                 PB_TRY(pb_lu_solve_batched<double>(&c->lu, n, ng, np, scr, n, nn, bPerm.as<int>(), bR.as<double2>(),
                                                    bD.as<double2>()));
@@ -589,6 +673,11 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
         stats->fp64_fallbacks = fallbacks;
         stats->fp64_direct = fp64_direct;
         stats->fp64_max_hz = fp64_hz;
+        stats->lu_count = lu_count;
+        stats->gmres_solves = gm_solves;
+        stats->gmres_its_max = gm_max;
+        stats->gmres_refactored = refactored;
+        stats->gmres_its_avg = gm_solves > 0 ? (double)gm_its / gm_solves : 0.0;
     }
     return PB_OK;
 }

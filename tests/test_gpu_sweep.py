@@ -166,3 +166,31 @@ def test_tensor_core_lu_matches_plain_path():
     assert st["n_system"] >= 1000
     assert zerr(zt, zp) <= 1e-6, (zerr(zt, zp), st)
     assert zerr(zs, zp) <= 1e-6
+
+
+@pytest.mark.parametrize("name", ["cfg2_small", "dipole_halfwave", "strip_dipole_ret", "cfg3_small_0", "rlc_series"])
+def test_accel_gmres_matches_reference(name, golden):
+    """LU reuse (the reference's acceleration = 1): one FP32 LU per 2 frequencies, GMRES
+    with the stale factors for the other; Z as the reference's dense solve, within the same
+    bound as the fresh-LU mixed path."""
+    prob, fx = golden(name)
+    with api.Context(prob) as ctx:
+        z, st = ctx.sweep(fx["freqs"], fill_prec=abi.PREC_MIXED, lu=abi.LU_TC, accel=2)
+    err = np.abs(z - fx["z"]).reshape(len(z), -1).max(1) / np.abs(fx["z"]).reshape(len(z), -1).max(1)
+    tol = cond_tolerance(prob, fx["freqs"])
+    assert np.all(err <= tol), (name, err, tol, st)
+
+
+def test_accel_gmres_sweep_uses_fewer_factorisations():
+    """Mid-size plate over 24 frequencies 200-315 MHz: with one LU per 8 frequencies the
+    GMRES path factorises 3 matrices instead of 24, solves the rest by GMRES, and its Z
+    equals the plain FP64 path's within 1e-6."""
+    from openpeec_b200 import configs, geometry
+    prob = geometry.build(geometry.parse_peec(configs.cfg2(32, 16, 24, 2.0e8, 5e6)))
+    f = prob.freqs()
+    with api.Context(prob) as ctx:
+        zp, _ = ctx.sweep(f, fill_prec=abi.PREC_FP64, lu=abi.LU_FP64)
+        za, st = ctx.sweep(f, fill_prec=abi.PREC_MIXED, lu=abi.LU_TC, accel=8)
+    assert st["lu_count"] == 3 and st["fp64_fallbacks"] == 0, st
+    assert st["gmres_solves"] == 24 and st["gmres_its_max"] <= 60, st
+    assert zerr(za, zp) <= 1e-6, (zerr(za, zp), st)
