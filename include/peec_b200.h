@@ -180,6 +180,29 @@ int  pb_sweep(pb_ctx *ctx, int nfreq, const double *freq, const pb_sweep_opts *o
               double *zmat, double *segi, pb_sweep_stats *stats);
 
 /*
+ * Plane-wave incidence (the reference's planewave key, src/input_data.c:501-519):
+ * arrival direction (theta, phi) in degrees (propagation is the opposite direction),
+ * polarisation 1 = theta-hat, 2 = phi-hat, amplitude [V/m] and phase [deg]. Over a
+ * ground plane the PEC reflection is added (mna_rhs_planewave, src/mna.c:434-468).
+ */
+typedef struct {
+    double theta_deg, phi_deg;
+    int    pol;
+    int    pad_;
+    double amp, phase_deg;
+} pb_planewave_t;
+
+/*
+ * Plane-wave sweep (solve.c:372-389): the same fill and solve as pb_sweep with the
+ * induced EMF -integral(E_inc . dl) of every current cell as the excitation and the ports
+ * left open. voc [nport*nfreq] complex receives the open-circuit port voltages
+ * V(n1) - V(n2) in the reference's layout (voc[i*nfreq + ifreq], include/peec.h:229);
+ * segipw [nfreq*nseg] complex (may be NULL) the induced segment currents.
+ */
+int  pb_planewave(pb_ctx *ctx, int nfreq, const double *freq, const pb_sweep_opts *opts,
+                  const pb_planewave_t *pw, double *voc, double *segipw, pb_sweep_stats *stats);
+
+/*
  * Dense complex LU with partial pivoting on a host matrix, executed on the GPU
  * (reference lu_decomp, src/lu.c:16-66): row-major a[n*n] complex is replaced by L\U,
  * piv[k] = row swapped with row k at step k. Returns -1 on success or the 0-based row of

@@ -78,6 +78,11 @@ class PbSweepStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class PbPlanewave(C.Structure):
+    _fields_ = [("theta_deg", C.c_double), ("phi_deg", C.c_double), ("pol", C.c_int),
+                ("pad_", C.c_int), ("amp", C.c_double), ("phase_deg", C.c_double)]
+
+
 def ptr(a):
     """Address of a contiguous numpy array (None for None / empty)."""
     if a is None or a.size == 0:
@@ -124,6 +129,8 @@ def lib():
     L.pb_pot_fill.argtypes = [_vp, C.c_double, C.c_int, _vp]
     L.pb_sweep.argtypes = [_vp, C.c_int, _vp, C.POINTER(PbSweepOpts), _vp, _vp,
                            C.POINTER(PbSweepStats)]
+    L.pb_planewave.argtypes = [_vp, C.c_int, _vp, C.POINTER(PbSweepOpts), C.POINTER(PbPlanewave),
+                               _vp, _vp, C.POINTER(PbSweepStats)]
     L.pb_lu_decomp.argtypes = [C.c_int, _vp, _vp]
     L.pb_lu_solve.argtypes = [C.c_int, _vp, _vp, _vp]
     L.pb_lu_decomp_batched_dev.argtypes = [C.c_int, C.c_int, _vp, _vp, _vp]

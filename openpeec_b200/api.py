@@ -81,6 +81,27 @@ class Context:
         return z, st.as_dict()
 
 
+    def planewave(self, freqs, pw, fill_prec=abi.PREC_MIXED, lu=abi.LU_TC, form=abi.FORM_AUTO,
+                  batch=0, accel=0, want_segi=False):
+        """Plane-wave incidence (pb_planewave): pw = (theta_deg, phi_deg, pol, amp,
+        phase_deg). Returns voc [nport, nfreq] (open-circuit port voltages), the induced
+        segment currents [nfreq, nseg] when want_segi, and the stats."""
+        freqs = np.ascontiguousarray(freqs, np.float64)
+        npt = len(self.prob.port)
+        voc = np.zeros((npt, len(freqs)), np.complex128)
+        seg = np.zeros((len(freqs), self.nseg), np.complex128) if want_segi else None
+        o = abi.PbSweepOpts(int(fill_prec), int(lu), int(form), int(batch), 0.0, 0, 0, 0, int(accel))
+        w = abi.PbPlanewave(float(pw[0]), float(pw[1]), int(pw[2]), 0, float(pw[3]),
+                            float(pw[4]) if len(pw) > 4 else 0.0)
+        st = abi.PbSweepStats()
+        _check(abi.lib().pb_planewave(self.h, len(freqs), freqs.ctypes.data, C.byref(o), C.byref(w),
+                                      voc.ctypes.data, None if seg is None else seg.ctypes.data,
+                                      C.byref(st)))
+        if want_segi:
+            return voc, seg, st.as_dict()
+        return voc, st.as_dict()
+
+
 def lu_decomp(a):
     """GPU LU with the reference's contract (src/lu.c:16-66): returns (info, LU, piv)."""
     a = np.ascontiguousarray(a, np.complex128).copy()

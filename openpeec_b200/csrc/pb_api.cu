@@ -26,7 +26,8 @@ int pb_cuda_fail(cudaError_t e, const char *what, const char *file, int line)
 }
 
 int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts *opts,
-                  double *zmat, double *segi, pb_sweep_stats *stats);
+                  double *zmat, double *segi, pb_sweep_stats *stats,
+                  const pb_planewave_t *pw, double *voc, double *segipw);
 
 extern "C" const char *pb_last_error(void) { return g_err.c_str(); }
 
@@ -369,7 +370,17 @@ int pb_sweep(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts *opts
 {
     if (!c) { pb_set_error("pb_sweep: null context"); return PB_ERR_ARG; }
     PB_CUDA(cudaSetDevice(c->dev));
-    return pb_sweep_impl(c, nfreq, freq, opts, zmat, segi, stats);
+    return pb_sweep_impl(c, nfreq, freq, opts, zmat, segi, stats, nullptr, nullptr, nullptr);
+}
+
+int pb_planewave(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts *opts,
+                 const pb_planewave_t *pw, double *voc, double *segipw, pb_sweep_stats *stats)
+{
+    if (!c) { pb_set_error("pb_planewave: null context"); return PB_ERR_ARG; }
+    if (!pw) { pb_set_error("pb_planewave: null plane wave"); return PB_ERR_ARG; }
+    if (!(pw->amp > 0)) { pb_set_error("pb_planewave: amplitude must be > 0"); return PB_ERR_ARG; }
+    PB_CUDA(cudaSetDevice(c->dev));
+    return pb_sweep_impl(c, nfreq, freq, opts, nullptr, nullptr, stats, pw, voc, segipw);
 }
 
 // ---------------------------------------------------------------- dense LU entry points

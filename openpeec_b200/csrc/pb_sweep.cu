@@ -42,15 +42,17 @@ __global__ void k_rhs_reduced(int nb, int np, int n, int nc, const double2 *P, l
     rhs[idx] = make_double2(a.x - b.x, a.y - b.y);
 }
 
-// Z[f][i][j] = (1/jw) sum_c (P[pc1_i][c] - P[pc2_i][c]) * (b_j - G ib_j)[c]
+// Z[f][i][j] = (1/jw) sum_c (P[pc1_i][c] - P[pc2_i][c]) * (b_j - G ib_j)[c]: the voltage of
+// port i for excitation j, which injects +1 A / -1 A at cells pcx[2j] / pcx[2j+1] (-1 = none).
 __global__ void __launch_bounds__(256)
-k_z_reduced(int np, int n, int nc, const double2 *P, long long pst, const int *inc_off,
-            const int *inc_seg, const int *pc, const double2 *x, const double *freq, double2 *z)
+k_z_reduced(int np, int nx, int n, int nc, const double2 *P, long long pst, const int *inc_off,
+            const int *inc_seg, const int *pc, const int *pcx, const double2 *x, const double *freq,
+            double2 *z)
 {
     const int f = blockIdx.z, i = blockIdx.y, j = blockIdx.x;
     const double2 *Pf = P + f * pst;
-    const double2 *ib = x + ((long long)f * np + j) * n;
-    const int a1 = pc[2 * i], a2 = pc[2 * i + 1], b1 = pc[2 * j], b2 = pc[2 * j + 1];
+    const double2 *ib = x + ((long long)f * nx + j) * n;
+    const int a1 = pc[2 * i], a2 = pc[2 * i + 1], b1 = pcx[2 * j], b2 = pcx[2 * j + 1];
     double sr = 0, si = 0;
     for (int c = threadIdx.x; c < nc; c += blockDim.x) {
         double yr = (c == b1 ? 1.0 : 0.0) - (c == b2 ? 1.0 : 0.0), yi = 0;
@@ -78,8 +80,70 @@ k_z_reduced(int np, int n, int nc, const double2 *P, long long pst, const int *i
     if (threadIdx.x == 0) {
         const double om = 2 * PB_PI * freq[f];
         // (sr + j si) / (j om) = (si - j sr) / om
-        z[((long long)f * np + i) * np + j] = make_double2(is_[0] / om, -rs[0] / om);
+        z[((long long)f * np + i) * nx + j] = make_double2(is_[0] / om, -rs[0] / om);
     }
+}
+
+// Plane-wave excitation (mna_rhs_planewave, src/mna.c:434-468).
+struct PwArgs {
+    double rh[3];        // arrival direction
+    double ev[3];        // polarisation unit vector
+    double2 e0;          // amplitude x e^{j phase}
+};
+
+__device__ __forceinline__ double pw_sinc(double x) { return fabs(x) < 1e-8 ? 1.0 : sin(x) / x; }
+
+// EMF integral(E . dl) of one wave over a straight cell (pw_emf, src/mna.c:408-432):
+// (E0 e.t) len e^{j k r.rc} sinc(k len (r.t)/2), times the width average for ribbons / bars.
+__device__ double2 pw_emf(const pb_cell_t &s, const double *rh, const double *ev, double2 e0, double kw)
+{
+    double tv[3], rc[3];
+    for (int q = 0; q < 3; q++) {
+        tv[q] = (s.x2[q] - s.x1[q]) / s.len;
+        rc[q] = 0.5 * (s.x1[q] + s.x2[q]);
+    }
+    const double et = ev[0] * tv[0] + ev[1] * tv[1] + ev[2] * tv[2];
+    const double rt = rh[0] * tv[0] + rh[1] * tv[1] + rh[2] * tv[2];
+    const double rr = rh[0] * rc[0] + rh[1] * rc[1] + rh[2] * rc[2];
+    double amp = et * s.len * pw_sinc(0.5 * kw * s.len * rt);
+    const double wl = sqrt(s.wv[0] * s.wv[0] + s.wv[1] * s.wv[1] + s.wv[2] * s.wv[2]);
+    if (s.wid > 0 && wl > 0) {
+        const double rw = (rh[0] * s.wv[0] + rh[1] * s.wv[1] + rh[2] * s.wv[2]) / wl;
+        amp *= pw_sinc(0.5 * kw * s.wid * rw);
+    }
+    double sn, cs;
+    sincos(kw * rr, &sn, &cs);
+    return make_double2(amp * (e0.x * cs - e0.y * sn), amp * (e0.x * sn + e0.y * cs));
+}
+
+// Right-hand side of the plane-wave excitation. Full form: -EMF on the branch rows
+// offS + k (mna.c:464). Reduced form: the branch equation Zb i = G^T v + EMF times jw,
+// with no node injection: rhs = jw EMF.
+__global__ void k_rhs_planewave(int nb, int n, int ns, int reduced, int offS, const pb_cell_t *seg,
+                                const double *freq, int gp, double gpz, PwArgs a, double2 *rhs)
+{
+    const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (idx >= (long long)nb * n) return;
+    const int f = (int)(idx / n), r = (int)(idx % n);
+    const int k = reduced ? r : r - offS;
+    double2 v = make_double2(0, 0);
+    if (k >= 0 && k < ns) {
+        const double om = 2 * PB_PI * freq[f];
+        const double kw = om / PB_C0;
+        double2 emf = pw_emf(seg[k], a.rh, a.ev, a.e0, kw);
+        if (gp) {       // PEC reflection: mirrored arrival, horizontal polarisation flipped
+            const double rh2[3] = {a.rh[0], a.rh[1], -a.rh[2]};
+            const double ev2[3] = {-a.ev[0], -a.ev[1], a.ev[2]};
+            double sn, cs;
+            sincos(2 * kw * a.rh[2] * gpz, &sn, &cs);
+            const double2 e0r = make_double2(a.e0.x * cs - a.e0.y * sn, a.e0.x * sn + a.e0.y * cs);
+            const double2 r2 = pw_emf(seg[k], rh2, ev2, e0r, kw);
+            emf.x += r2.x;
+            emf.y += r2.y;
+        }
+        v = reduced ? make_double2(-om * emf.y, om * emf.x) : make_double2(-emf.x, -emf.y);
+    }
+    rhs[idx] = v;
 }
 
 __global__ void k_rhs_full(int nb, int np, int n, const int *pm, double2 *rhs)
@@ -94,12 +158,12 @@ __global__ void k_rhs_full(int nb, int np, int n, const int *pm, double2 *rhs)
     rhs[idx] = make_double2(v, 0);
 }
 
-__global__ void k_z_full(int nb, int np, int n, const int *pm, const double2 *x, double2 *z)
+__global__ void k_z_full(int nb, int np, int nx, int n, const int *pm, const double2 *x, double2 *z)
 {
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= nb * np * np) return;
-    const int j = idx % np, i = (idx / np) % np, f = idx / (np * np);
-    const double2 *xv = x + ((long long)f * np + j) * n;
+    if (idx >= nb * np * nx) return;
+    const int j = idx % nx, i = (idx / nx) % np, f = idx / (np * nx);
+    const double2 *xv = x + ((long long)f * nx + j) * n;
     const int a = pm[2 * i], b = pm[2 * i + 1];
     double2 v = make_double2(0, 0);
     if (a >= 0) { v.x += xv[a].x; v.y += xv[a].y; }
@@ -216,7 +280,8 @@ struct PhaseTimer {
 };
 
 int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts *opts_in,
-                  double *zmat, double *segi, pb_sweep_stats *stats)
+                  double *zmat, double *segi, pb_sweep_stats *stats,
+                  const pb_planewave_t *pw, double *voc, double *segipw)
 {
     pb_sweep_opts o;
     if (opts_in) o = *opts_in;
@@ -239,6 +304,7 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
     const long launches0 = c->launches + c->lu.launches;
 
     const int ns = (int)c->seg.size(), nc = c->ncell, np = (int)c->port.size();
+    const int nr = pw ? 1 : np;                  // right-hand sides per frequency
     const int n = (form == PB_FORM_REDUCED) ? ns : c->nfull;
     const cudaStream_t st = c->stream;
     if (n <= 0) { pb_set_error("pb_sweep: empty system"); return PB_ERR_ARG; }
@@ -249,7 +315,7 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
     const double n2 = (double)n * n;
     const int tc = (o.lu == PB_LU_TC);
     double perf = n2 * 16 + (mixed ? n2 * 8 : 0) + (tc ? n2 * 4 : 0) + (double)nc * nc * 16 + (double)ns * 16
-                + (form == PB_FORM_FULL ? (double)ns * ns * 16 : 0) + 4.0 * np * n * 16 + 8.0 * n;
+                + (form == PB_FORM_FULL ? (double)ns * ns * 16 : 0) + 4.0 * nr * n * 16 + 8.0 * n;
     const double fixed = (double)ns * ns * 8 + (double)nc * nc * 8 +
                          (c->retardation ? (double)PB_FMAX * c->chg.size() * c->chg.size() * 16 : 0.0);
     int B = o.batch;
@@ -287,19 +353,19 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
     PB_TRY(bPiv.alloc((size_t)B * n * 4));
     PB_TRY(bPerm.alloc((size_t)B * n * 4));
     PB_TRY(bInfo.alloc((size_t)B * 4));
-    const size_t vb = (size_t)B * np * n * 16;
+    const size_t vb = (size_t)B * nr * n * 16;
     PB_TRY(bRhs.alloc(vb));
     PB_TRY(bX.alloc(vb));
     PB_TRY(bR.alloc(vb));
     PB_TRY(bD.alloc(vb));
     DevBuf bXn, bAn;
-    PB_TRY(bXn.alloc((size_t)B * np * 8));
+    PB_TRY(bXn.alloc((size_t)B * nr * 8));
     PB_TRY(bAn.alloc((size_t)B * 8));
-    PB_TRY(bRn.alloc((size_t)B * np * 8));
-    PB_TRY(bBn.alloc((size_t)B * np * 8));
+    PB_TRY(bRn.alloc((size_t)B * nr * 8));
+    PB_TRY(bBn.alloc((size_t)B * nr * 8));
     PB_TRY(bFreq.alloc((size_t)B * 8));
-    PB_TRY(bZ.alloc((size_t)B * np * np * 16));
-    PB_TRY(bPC.alloc((size_t)2 * np * 4));
+    PB_TRY(bZ.alloc((size_t)B * np * nr * 16 + 16));
+    PB_TRY(bPC.alloc((size_t)2 * (np + 1) * 4));
 
     // port endpoints: cells (reduced) or matrix indices (full)
     std::vector<int> pc(2 * np);
@@ -313,7 +379,24 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
             pc[2 * j + 1] = c->nodemap[c->port[j].n2];
         }
     }
-    PB_CUDA(cudaMemcpyAsync(bPC.p, pc.data(), sizeof(int) * 2 * np, cudaMemcpyHostToDevice, st));
+    pc.push_back(-1);                            // plane wave: no current injection
+    pc.push_back(-1);
+    PB_CUDA(cudaMemcpyAsync(bPC.p, pc.data(), sizeof(int) * 2 * (np + 1), cudaMemcpyHostToDevice, st));
+    PwArgs pwa;
+    if (pw) {
+        if (pw->pol != 1 && pw->pol != 2) { pb_set_error("pb_planewave: polarisation must be 1 or 2"); return PB_ERR_ARG; }
+        const double th = pw->theta_deg * PB_PI / 180, ph = pw->phi_deg * PB_PI / 180;
+        const double sth = sin(th), cth = cos(th), cph = cos(ph), sph = sin(ph);
+        const double rh[3] = {sth * cph, sth * sph, cth};
+        const double thh[3] = {cth * cph, cth * sph, -sth};
+        const double phh[3] = {-sph, cph, 0};
+        for (int q = 0; q < 3; q++) {
+            pwa.rh[q] = rh[q];
+            pwa.ev[q] = (pw->pol == 2) ? phh[q] : thh[q];
+        }
+        const double pr = pw->phase_deg * PB_PI / 180;
+        pwa.e0 = make_double2(pw->amp * cos(pr), pw->amp * sin(pr));
+    }
 
     PhaseTimer tStatic, tCorr, tAsm, tLu, tRef, tAll;
     double samples = 0, luflops = 0, maxres = 0;
@@ -321,7 +404,7 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
     std::vector<long> cur_sig, sig;
     bool static_valid = false;
     std::vector<double2> zh((size_t)B * np * np);
-    std::vector<double> rnh(B * np), bnh(B * np), xnh(B * np), anh(B);
+    std::vector<double> rnh(B * nr), bnh(B * nr), xnh(B * nr), anh(B);
     int fallbacks = 0, fp64_direct = 0, lu_count = 0, gm_solves = 0, gm_max = 0, refactored = 0;
     long gm_its = 0;
     double fp64_hz = 0;                          // frequencies <= this are solved in FP64
@@ -456,23 +539,27 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
             }
         // right-hand sides
         tRef.start(st);
-        const long long nv = (long long)nb * np * n;
-        if (form == PB_FORM_REDUCED) {
-            k_rhs_reduced<<<ceil_div(nv, 256), 256, 0, st>>>(nb, np, n, nc, bP.as<double2>(), (long long)nc * nc,
+        const long long nv = (long long)nb * nr * n;
+        if (pw) {
+            k_rhs_planewave<<<ceil_div(nv, 256), 256, 0, st>>>(nb, n, ns, form == PB_FORM_REDUCED, c->offS,
+                                                               c->g.seg.cell, bFreq.as<double>(), c->gp, c->gpz,
+                                                               pwa, bRhs.as<double2>());
+        } else if (form == PB_FORM_REDUCED) {
+            k_rhs_reduced<<<ceil_div(nv, 256), 256, 0, st>>>(nb, nr, n, nc, bP.as<double2>(), (long long)nc * nc,
                                                              c->g.seg_ca, c->g.seg_cb, bPC.as<int>(), bRhs.as<double2>());
         } else {
-            k_rhs_full<<<ceil_div(nv, 256), 256, 0, st>>>(nb, np, n, bPC.as<int>(), bRhs.as<double2>());
+            k_rhs_full<<<ceil_div(nv, 256), 256, 0, st>>>(nb, nr, n, bPC.as<int>(), bRhs.as<double2>());
         }
         c->launches++;
         PB_CHECK_LAUNCH();
         if (nd > 0)
-            PB_TRY(pb_lu_solve_batched<double>(&c->lu, n, nd, np, bM64.as<double2>(), n, nn,
+            PB_TRY(pb_lu_solve_batched<double>(&c->lu, n, nd, nr, bM64.as<double2>(), n, nn,
                                                bPerm.as<int>(), bRhs.as<double2>(), bX.as<double2>()));
         std::vector<int> state(nb, 1);            // 0 active, 1 converged / direct, 2 failed
         if (nb > nd && S) {
             // GMRES with the anchors' FP32 factors (anchors themselves converge in a few
             // steps, like the refinement below)
-            const long long vo = (long long)nd * np * n;
+            const long long vo = (long long)nd * nr * n;
             std::vector<int> gst(mb, 0);
             for (int q = 0; q < mb; q++)
                 if (infoh[nd + lu_of[q]] >= 0) gst[q] = 2;            // zero FP32 pivot: go FP64
@@ -480,7 +567,7 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
             ga.eng = &c->lu;
             ga.n = n;
             ga.nsys = mb;
-            ga.nrhs = np;
+            ga.nrhs = nr;
             ga.A = bM64.as<double2>() + nd * nn;
             ga.A_stride = nn;
             ga.lu = bM32.as<float2>() + (nd + aoff) * nn;
@@ -544,33 +631,33 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
             // reaches the level of an FP64 factorisation. A frequency whose iteration
             // stalls above that is re-solved with an FP64 LU (stats->fp64_fallbacks).
             const int mb = nb - nd;
-            const long long vo = (long long)nd * np * n;
+            const long long vo = (long long)nd * nr * n;
             double2 *m64 = bM64.as<double2>() + nd * nn;
             float2 *m32 = bM32.as<float2>() + nd * nn;
             int *perm = bPerm.as<int>() + (long long)nd * n;
             for (int q = 0; q < mb; q++)
                 if (infoh[nd + q] >= 0) state[nd + q] = 2;          // zero FP32 pivot: go FP64
-            PB_TRY(pb_lu_solve_batched<float>(&c->lu, n, mb, np, m32, n, nn, perm, bRhs.as<double2>() + vo,
+            PB_TRY(pb_lu_solve_batched<float>(&c->lu, n, mb, nr, m32, n, nn, perm, bRhs.as<double2>() + vo,
                                               bX.as<double2>() + vo));
             const double eta_tol = std::max(1e-14, 8.0 * std::sqrt((double)n) * 1.1e-16);
             std::vector<double> prev(nb, 1e300);
             for (int q = nd; q < nb; q++) if (state[q] == 1) state[q] = 0;
             int it = 0;
             for (it = 1; it <= maxit + 1; it++) {
-                PB_TRY(pb_residual(&c->lu, n, mb, np, m64, n, nn, bRhs.as<double2>() + vo, bX.as<double2>() + vo,
+                PB_TRY(pb_residual(&c->lu, n, mb, nr, m64, n, nn, bRhs.as<double2>() + vo, bX.as<double2>() + vo,
                                    bR.as<double2>() + vo, bRn.as<double>(), bBn.as<double>(), bXn.as<double>(),
                                    it == 1 ? bAn.as<double>() : nullptr));
-                PB_CUDA(cudaMemcpyAsync(rnh.data(), bRn.p, sizeof(double) * mb * np, cudaMemcpyDeviceToHost, st));
-                PB_CUDA(cudaMemcpyAsync(bnh.data(), bBn.p, sizeof(double) * mb * np, cudaMemcpyDeviceToHost, st));
-                PB_CUDA(cudaMemcpyAsync(xnh.data(), bXn.p, sizeof(double) * mb * np, cudaMemcpyDeviceToHost, st));
+                PB_CUDA(cudaMemcpyAsync(rnh.data(), bRn.p, sizeof(double) * mb * nr, cudaMemcpyDeviceToHost, st));
+                PB_CUDA(cudaMemcpyAsync(bnh.data(), bBn.p, sizeof(double) * mb * nr, cudaMemcpyDeviceToHost, st));
+                PB_CUDA(cudaMemcpyAsync(xnh.data(), bXn.p, sizeof(double) * mb * nr, cudaMemcpyDeviceToHost, st));
                 if (it == 1) PB_CUDA(cudaMemcpyAsync(anh.data(), bAn.p, sizeof(double) * mb, cudaMemcpyDeviceToHost, st));
                 PB_CUDA(cudaStreamSynchronize(st));
                 int active = 0;
                 for (int q = 0; q < mb; q++) {
                     if (state[nd + q] != 0) continue;
                     double eta = 0;
-                    for (int j = 0; j < np; j++) {
-                        const int v = q * np + j;
+                    for (int j = 0; j < nr; j++) {
+                        const int v = q * nr + j;
                         const double den = anh[q] * xnh[v] + bnh[v];
                         eta = std::max(eta, den > 0 ? rnh[v] / den : 0.0);
                     }
@@ -579,9 +666,9 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
                     else { prev[nd + q] = eta; active++; }
                 }
                 if (active == 0) break;
-                PB_TRY(pb_lu_solve_batched<float>(&c->lu, n, mb, np, m32, n, nn, perm, bR.as<double2>() + vo,
+                PB_TRY(pb_lu_solve_batched<float>(&c->lu, n, mb, nr, m32, n, nn, perm, bR.as<double2>() + vo,
                                                   bD.as<double2>() + vo));
-                const long long mv = (long long)mb * np * n;
+                const long long mv = (long long)mb * nr * n;
                 k_axpy<<<ceil_div(mv, 256), 256, 0, st>>>(bX.as<double2>() + vo, bD.as<double2>() + vo, mv);
                 c->launches++;
                 PB_CHECK_LAUNCH();
@@ -601,20 +688,20 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
                     const int q = failed[g0 + t];
                     PB_CUDA(cudaMemcpyAsync(scr + t * nn, bM64.as<double2>() + q * nn, sizeof(double2) * nn,
                                             cudaMemcpyDeviceToDevice, st));
-                    PB_CUDA(cudaMemcpyAsync(bR.as<double2>() + (long long)t * np * n,
-                                            bRhs.as<double2>() + (long long)q * np * n, sizeof(double2) * np * n,
+                    PB_CUDA(cudaMemcpyAsync(bR.as<double2>() + (long long)t * nr * n,
+                                            bRhs.as<double2>() + (long long)q * nr * n, sizeof(double2) * nr * n,
                                             cudaMemcpyDeviceToDevice, st));
                 }
                 PB_TRY(pb_lu_factor<double>(&c->lu, n, ng, scr, n, nn, bPiv.as<int>(), bInfo.as<int>()));
                 lu_count += ng;
                 PB_TRY(pb_lu_perm(&c->lu, n, ng, bPiv.as<int>(), bPerm.as<int>()));
-                PB_TRY(pb_lu_solve_batched<double>(&c->lu, n, ng, np, scr, n, nn, bPerm.as<int>(), bR.as<double2>(),
+                PB_TRY(pb_lu_solve_batched<double>(&c->lu, n, ng, nr, scr, n, nn, bPerm.as<int>(), bR.as<double2>(),
                                                    bD.as<double2>()));
                 PB_CUDA(cudaMemcpyAsync(infoh.data(), bInfo.p, sizeof(int) * ng, cudaMemcpyDeviceToHost, st));
                 for (int t = 0; t < ng; t++) {
                     const int q = failed[g0 + t];
-                    PB_CUDA(cudaMemcpyAsync(bX.as<double2>() + (long long)q * np * n, bD.as<double2>() + (long long)t * np * n,
-                                            sizeof(double2) * np * n, cudaMemcpyDeviceToDevice, st));
+                    PB_CUDA(cudaMemcpyAsync(bX.as<double2>() + (long long)q * nr * n, bD.as<double2>() + (long long)t * nr * n,
+                                            sizeof(double2) * nr * n, cudaMemcpyDeviceToDevice, st));
                 }
                 PB_CUDA(cudaStreamSynchronize(st));
                 for (int t = 0; t < ng; t++)
@@ -631,20 +718,39 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
         }
         fp64_direct += nd;
         // port voltages -> Z
+        // port voltages per excitation: Z columns (1 A at port j) or the open-circuit
+        // voltages of the plane-wave excitation (no injection: excitation cells -1)
+        const int *pcx = pw ? bPC.as<int>() + 2 * np : bPC.as<int>();
         if (form == PB_FORM_REDUCED) {
-            dim3 g(np, np, nb);
-            k_z_reduced<<<g, 256, 0, st>>>(np, n, nc, bP.as<double2>(), (long long)nc * nc, c->d_inc_off,
-                                           c->d_inc_seg, bPC.as<int>(), bX.as<double2>(), bFreq.as<double>(),
+            dim3 g(nr, np, nb);
+            k_z_reduced<<<g, 256, 0, st>>>(np, nr, n, nc, bP.as<double2>(), (long long)nc * nc, c->d_inc_off,
+                                           c->d_inc_seg, bPC.as<int>(), pcx, bX.as<double2>(), bFreq.as<double>(),
                                            bZ.as<double2>());
         } else {
-            k_z_full<<<ceil_div(nb * np * np, 128), 128, 0, st>>>(nb, np, n, bPC.as<int>(), bX.as<double2>(), bZ.as<double2>());
+            k_z_full<<<ceil_div(nb * np * nr, 128), 128, 0, st>>>(nb, np, nr, n, bPC.as<int>(), bX.as<double2>(),
+                                                                  bZ.as<double2>());
         }
         c->launches++;
         PB_CHECK_LAUNCH();
         tRef.stop(st);
-        if (zmat) PB_CUDA(cudaMemcpyAsync(zmat + 2 * (size_t)b0 * np * np, bZ.p, sizeof(double2) * nb * np * np,
-                                          cudaMemcpyDeviceToHost, st));
-        if (segi) {
+        if (zmat && !pw) PB_CUDA(cudaMemcpyAsync(zmat + 2 * (size_t)b0 * np * np, bZ.p, sizeof(double2) * nb * np * np,
+                                                 cudaMemcpyDeviceToHost, st));
+        if (voc && pw) {
+            PB_CUDA(cudaMemcpyAsync(zh.data(), bZ.p, sizeof(double2) * nb * np, cudaMemcpyDeviceToHost, st));
+            PB_CUDA(cudaStreamSynchronize(st));
+            for (int q = 0; q < nb; q++)
+                for (int i = 0; i < np; i++) {
+                    voc[2 * ((size_t)i * nfreq + b0 + q)] = zh[(size_t)q * np + i].x;
+                    voc[2 * ((size_t)i * nfreq + b0 + q) + 1] = zh[(size_t)q * np + i].y;
+                }
+        }
+        if (segipw && pw) {
+            const int off = (form == PB_FORM_REDUCED) ? 0 : c->offS;
+            for (int q = 0; q < nb; q++)
+                PB_CUDA(cudaMemcpyAsync(segipw + 2 * ((size_t)(b0 + q) * ns), bX.as<double2>() + (long long)q * n + off,
+                                        sizeof(double2) * ns, cudaMemcpyDeviceToHost, st));
+        }
+        if (segi && !pw) {
             const int off = (form == PB_FORM_REDUCED) ? 0 : c->offS;
             for (int q = 0; q < nb; q++)
                 for (int j = 0; j < np; j++)

@@ -39,6 +39,7 @@ class PeecInput:
         self.gpz = 0.0
         self.gmin = 0.0
         self.maxid = 0
+        self.planewave = None    # (theta_deg, phi_deg, pol, amp, phase_deg)
         self.unsupported = []
 
 
@@ -115,7 +116,12 @@ def parse_peec(text):
             p.gmin = float(a[0])
         elif key == "grading":
             p.grading = int(a[0])
-        elif key in ("quad", "disk", "dielectric", "planewave", "mutual", "isource",
+        elif key == "planewave":           # planewave = theta phi pol amp [phase] (input_data.c:501-519)
+            pol, amp = int(a[2]), float(a[3])
+            if pol not in (1, 2) or amp <= 0:
+                raise ValueError("planewave: polarisation 1/2 and amplitude > 0")
+            p.planewave = (float(a[0]), float(a[1]), pol, amp, float(a[4]) if len(a) > 4 else 0.0)
+        elif key in ("quad", "disk", "dielectric", "mutual", "isource",
                      "compression", "acceleration"):
             p.unsupported.append(key)
     return p
@@ -307,7 +313,7 @@ def build(p: PeecInput) -> Problem:
                    np.array(chgnode, dtype=np.int32), np.zeros(0), maxid, port, lump,
                    capacitance=p.capacitance, retardation=p.retardation, skin=p.skin,
                    gp=p.gp, gpz=p.gpz, gmin=p.gmin, f0=p.f0, f1=p.f1, nfreq=p.nfreq,
-                   flog=p.flog, title=p.title)
+                   flog=p.flog, title=p.title, planewave=p.planewave)
 
 
 def load_peec(path) -> Problem:

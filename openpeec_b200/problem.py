@@ -18,7 +18,7 @@ PI = 4.0 * math.atan(1.0)
 class Problem:
     def __init__(self, seg, chg, chgnode, pv, maxid, port, lump=None, mut=None,
                  capacitance=0, retardation=0, skin=0, gp=0, gpz=0.0, gmin=0.0,
-                 f0=0.0, f1=0.0, nfreq=1, flog=0, title=""):
+                 f0=0.0, f1=0.0, nfreq=1, flog=0, title="", planewave=None):
         self.seg = np.ascontiguousarray(seg, dtype=CELL_DTYPE)
         self.chg = np.ascontiguousarray(chg, dtype=CELL_DTYPE)
         self.chgnode = np.ascontiguousarray(chgnode, dtype=np.int32)
@@ -34,6 +34,7 @@ class Problem:
         self.gpz, self.gmin = float(gpz), float(gmin)
         self.f0, self.f1, self.nfreq, self.flog = float(f0), float(f1), int(nfreq), int(flog)
         self.title = title
+        self.planewave = tuple(planewave) if planewave is not None else None
 
     # include/peec.h:241-248
     def freq_at(self, i):

@@ -1114,6 +1114,109 @@ int or_sweep(const or_prob *o, int nfreq, const double *freq, double *zmat, int 
     return ret;
 }
 
+/* ------------------------------------------------------------------ plane wave
+ * mna_rhs_planewave / pw_emf (src/mna.c:408-468) and the plane-wave branch of solve()
+ * (src/solve.c:372-389), on the same dense MNA system as or_sweep. */
+static double pw_sinc(double x) { return (fabs(x) < 1e-8) ? 1.0 : (sin(x) / x); }
+
+static void pw_emf(const pb_cell_t *s, const double *rh, const double *ev, const double *e0,
+                   double kw, double *out)
+{
+    double tv[3], rc[3];
+    for (int c = 0; c < 3; c++) {
+        tv[c] = (s->x2[c] - s->x1[c]) / s->len;
+        rc[c] = 0.5 * (s->x1[c] + s->x2[c]);
+    }
+    const double et = ev[0] * tv[0] + ev[1] * tv[1] + ev[2] * tv[2];
+    const double rt = rh[0] * tv[0] + rh[1] * tv[1] + rh[2] * tv[2];
+    const double rr = rh[0] * rc[0] + rh[1] * rc[1] + rh[2] * rc[2];
+    double amp = et * s->len * pw_sinc(0.5 * kw * s->len * rt);
+    const double wl = sqrt(s->wv[0] * s->wv[0] + s->wv[1] * s->wv[1] + s->wv[2] * s->wv[2]);
+    if (s->wid > 0 && wl > 0) {
+        const double rw = (rh[0] * s->wv[0] + rh[1] * s->wv[1] + rh[2] * s->wv[2]) / wl;
+        amp *= pw_sinc(0.5 * kw * s->wid * rw);
+    }
+    const double c = cos(kw * rr), sn = sin(kw * rr);
+    out[0] = amp * (e0[0] * c - e0[1] * sn);
+    out[1] = amp * (e0[0] * sn + e0[1] * c);
+}
+
+/* pwp = {theta_deg, phi_deg, pol, amp, phase_deg}; voc [2*nport*nfreq] (voc[i*nfreq+f]);
+ * segipw [2*nfreq*nseg] or NULL. */
+int or_planewave(const or_prob *o, int nfreq, const double *freq, const double *pwp,
+                 double *voc, double *segipw)
+{
+    const int n = o->nunknown, ns = o->nseg, nc = o->ncell, np = o->nport;
+    double *lp = (double *)malloc(sizeof(double) * 2 * (size_t)(ns > 0 ? ns : 1) * (ns > 0 ? ns : 1));
+    double *pm = (double *)malloc(sizeof(double) * 2 * (size_t)(nc > 0 ? nc : 1) * (nc > 0 ? nc : 1));
+    double *cm = (double *)malloc(sizeof(double) * 2 * (size_t)(nc > 0 ? nc : 1) * (nc > 0 ? nc : 1));
+    double *a = (double *)malloc(sizeof(double) * 2 * (size_t)n * n);
+    double *b = (double *)malloc(sizeof(double) * 2 * (size_t)(n > nc ? n : nc));
+    int *piv = (int *)malloc(sizeof(int) * (size_t)(n > nc ? n : nc));
+    const int usecap = o->capacitance && nc > 0;
+    const double th = pwp[0] * O_PI / 180, ph = pwp[1] * O_PI / 180;
+    const double st = sin(th), ct = cos(th), cp = cos(ph), sp = sin(ph);
+    const double rh[3] = {st * cp, st * sp, ct};
+    const double thh[3] = {ct * cp, ct * sp, -st};
+    const double phh[3] = {-sp, cp, 0};
+    double ev[3];
+    for (int c = 0; c < 3; c++) ev[c] = ((int)pwp[2] == 2) ? phh[c] : thh[c];
+    const double e0[2] = {pwp[3] * cos(pwp[4] * O_PI / 180), pwp[3] * sin(pwp[4] * O_PI / 180)};
+    const double rh2[3] = {rh[0], rh[1], -rh[2]};
+    const double ev2[3] = {-ev[0], -ev[1], ev[2]};
+    int ret = 0;
+    for (int ifr = 0; ifr < nfreq; ifr++) {
+        const double f = freq[ifr];
+        const double kw = o->retardation ? 2 * O_PI * f / O_C0 : 0;
+        const double kwp = 2 * O_PI * f / O_C0;          /* the wave's own k (mna.c:437) */
+        if (ifr == 0 || o->retardation) {
+            or_lp_fill(o, kw, lp);
+            if (usecap) {
+                or_pot_fill(o, kw, pm);
+                if (or_lu_decomp(nc, pm, piv) >= 0) { ret = PB_ERR_SINGULAR; break; }
+                for (int j = 0; j < nc; j++) {
+                    memset(b, 0, sizeof(double) * 2 * nc);
+                    b[2 * j] = 1;
+                    or_lu_solve(nc, pm, piv, b);
+                    for (int i = 0; i < nc; i++) {
+                        cm[2 * ((size_t)i * nc + j)] = b[2 * i];
+                        cm[2 * ((size_t)i * nc + j) + 1] = b[2 * i + 1];
+                    }
+                }
+            }
+        }
+        or_mna_assemble(o, f, lp, usecap ? cm : NULL, a);
+        if (or_lu_decomp(n, a, piv) >= 0) { ret = PB_ERR_SINGULAR; break; }
+        memset(b, 0, sizeof(double) * 2 * n);
+        const double psi = 2 * kwp * rh[2] * o->gpz;
+        const double e0r[2] = {e0[0] * cos(psi) - e0[1] * sin(psi), e0[0] * sin(psi) + e0[1] * cos(psi)};
+        for (int k = 0; k < ns; k++) {
+            double emf[2], r2[2];
+            pw_emf(&o->seg[k], rh, ev, e0, kwp, emf);
+            if (o->gp) {
+                pw_emf(&o->seg[k], rh2, ev2, e0r, kwp, r2);
+                emf[0] += r2[0];
+                emf[1] += r2[1];
+            }
+            b[2 * (o->offS + k)] = -emf[0];
+            b[2 * (o->offS + k) + 1] = -emf[1];
+        }
+        or_lu_solve(n, a, piv, b);
+        for (int i = 0; i < np; i++) {
+            const int k1 = o->nodemap[o->port[i].n1], k2 = o->nodemap[o->port[i].n2];
+            voc[2 * ((size_t)i * nfreq + ifr)] = (k1 < 0 ? 0 : b[2 * k1]) - (k2 < 0 ? 0 : b[2 * k2]);
+            voc[2 * ((size_t)i * nfreq + ifr) + 1] = (k1 < 0 ? 0 : b[2 * k1 + 1]) - (k2 < 0 ? 0 : b[2 * k2 + 1]);
+        }
+        if (segipw)
+            for (int m = 0; m < ns; m++) {
+                segipw[2 * ((size_t)ifr * ns + m)] = b[2 * (o->offS + m)];
+                segipw[2 * ((size_t)ifr * ns + m) + 1] = b[2 * (o->offS + m) + 1];
+            }
+    }
+    free(lp); free(pm); free(cm); free(a); free(b); free(piv);
+    return ret;
+}
+
 /* ------------------------------------------------------------------ CPU timing
  * Same bounded samples as the reference harness, on the restatement (used as the CPU
  * baseline when the reference build is not available). */

@@ -34,6 +34,9 @@ int  or_lu_decomp(int n, double *a, int *piv);
 void or_lu_solve(int n, const double *a, const int *piv, double *b);
 /* Dense sweep of the reference solve() (solve.c:239-370); zmat [nfreq*nport*nport]. */
 int  or_sweep(const or_prob *o, int nfreq, const double *freq, double *zmat, int nthreads);
+/* plane-wave sweep: pwp = {theta_deg, phi_deg, pol, amp, phase_deg}; voc[i*nfreq+f] */
+int  or_planewave(const or_prob *o, int nfreq, const double *freq, const double *pwp,
+                  double *voc, double *segipw);
 /* Internal impedance of current cell k at f (skin.c:112-133 / mna.c:128-138). */
 void or_zint(const or_prob *o, int k, double f, double *out);
 /* Single-pair geometric integral (partial.c:256-317) between current cells. */

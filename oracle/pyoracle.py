@@ -61,6 +61,8 @@ class Oracle:
             L.or_lu_solve.argtypes = [C.c_int, _vp, _vp, _vp]
             L.or_sweep.argtypes = [_vp, C.c_int, _vp, _vp, C.c_int]
             L.or_sweep.restype = C.c_int
+            L.or_planewave.argtypes = [_vp, C.c_int, _vp, _vp, _vp, _vp]
+            L.or_planewave.restype = C.c_int
             L.or_zint.argtypes = [_vp, C.c_int, C.c_double, _vp]
             cls._L = L
         return cls._L
@@ -134,6 +136,19 @@ class Oracle:
             raise RuntimeError("oracle sweep failed (%d)" % r)
         return z
 
+    def planewave(self, freqs, pw):
+        """Plane-wave sweep (mna.c:434-468, solve.c:372-389): pw = (theta_deg, phi_deg,
+        pol, amp, phase_deg). Returns (voc [nport, nfreq], segipw [nfreq, nseg])."""
+        freqs = np.ascontiguousarray(freqs, np.float64)
+        pwp = np.array(pw, np.float64)
+        voc = np.zeros((len(self.prob.port), len(freqs)), np.complex128)
+        segipw = np.zeros((len(freqs), len(self.prob.seg)), np.complex128)
+        r = self.lib().or_planewave(self.h, len(freqs), freqs.ctypes.data, pwp.ctypes.data,
+                                    voc.ctypes.data, segipw.ctypes.data)
+        if r != 0:
+            raise RuntimeError("oracle plane-wave sweep failed (%d)" % r)
+        return voc, segipw
+
     @classmethod
     def lu_decomp(cls, a):
         a = np.ascontiguousarray(a, np.complex128).copy()
@@ -173,6 +188,8 @@ class RefLib:
             L.rh_nodemap.argtypes = [_vp, _vp]
             L.rh_mna_assemble.argtypes = [_vp, C.c_double, _vp]
             L.rh_solve.argtypes = [_vp, _vp]
+            L.rh_voc.argtypes = [_vp, _vp, _vp, _vp]
+            L.rh_voc.restype = C.c_int
             L.rh_set_freqs.argtypes = [_vp, C.c_double, C.c_double, C.c_int, C.c_int]
             L.rh_lu_decomp.argtypes = [C.c_int, _vp, _vp]
             L.rh_lu_solve.argtypes = [C.c_int, _vp, _vp, _vp]
@@ -272,6 +289,17 @@ class RefLib:
         if self.lib().rh_solve(self.h, z.ctypes.data) != 0:
             raise RuntimeError("reference solve failed")
         return z
+
+    def voc(self):
+        """Plane-wave results of the last solve(): (voc [nport, nfreq], segipw [nfreq, nseg]
+        or None, pw parameters) or None when the input has no plane wave."""
+        voc = np.zeros((self.nport, self.nfreq), np.complex128)
+        seg = np.zeros((self.nfreq, self.nseg), np.complex128)
+        pwp = np.zeros(5)
+        r = self.lib().rh_voc(self.h, voc.ctypes.data, seg.ctypes.data, pwp.ctypes.data)
+        if r == 0:
+            return None
+        return voc, (seg if r == 2 else None), pwp
 
     @classmethod
     def set_threads(cls, n):

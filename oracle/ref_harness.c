@@ -247,6 +247,21 @@ int rh_solve(void *hv, double *zmat)
     return r;
 }
 
+/* Plane-wave results of the last rh_solve: voc [2*nport*nfreq] (voc[i*nfreq+f]), segipw
+ * [2*nfreq*nseg] (when distribution = 1), and the wave's parameters pwp[5]. Returns 0 when
+ * the input has no plane wave. */
+int rh_voc(void *hv, double *voc, double *segipw, double *pwp)
+{
+    const peec_t *p = &((rh_t *)hv)->p;
+    if (!p->pw || p->voc == NULL) return 0;
+    if (voc) memcpy(voc, p->voc, (size_t)p->nport * p->nfreq * sizeof(d_complex_t));
+    if (segipw && p->segipw) memcpy(segipw, p->segipw, (size_t)p->nfreq * p->nseg * sizeof(d_complex_t));
+    if (pwp) {
+        pwp[0] = p->pwth; pwp[1] = p->pwph; pwp[2] = p->pwpol; pwp[3] = p->pwamp; pwp[4] = p->pwphase;
+    }
+    return 1 + (p->segipw != NULL);
+}
+
 /* Restrict the sweep to [ifreq0, ifreq0+count) of the parsed list (for timing samples). */
 void rh_set_freqs(void *hv, double f0, double f1, int nfreq, int flog)
 {

@@ -20,9 +20,10 @@ def golden_names():
     return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz")))
 
 
-def load_golden(name):
-    """(Problem, fixture dict) of a golden case written by tests/golden/make_golden.py."""
-    z = dict(np.load(os.path.join(GOLDEN, name + ".npz")))
+def load_golden(name, sub=""):
+    """(Problem, fixture dict) of a golden case written by tests/golden/make_golden.py
+    (plane-wave cases live in the sub-directory "pw")."""
+    z = dict(np.load(os.path.join(GOLDEN, sub, name + ".npz")))
     pz = {k[5:]: v for k, v in z.items() if k.startswith("prob_")}
     tmp = os.path.join(GOLDEN, ".__tmp_%d.npz" % os.getpid())
     np.savez(tmp, **pz)

@@ -10,6 +10,7 @@ reference's own sources with oracle/Makefile). For every case it stores:
 
     python tests/golden/make_golden.py            # all small cases (about a minute)
     python tests/golden/make_golden.py --cfg2     # + the full 64x32 plate at 2 frequencies
+    python tests/golden/make_golden.py --pw-only  # only the plane-wave cases (tests/golden/pw)
 """
 import argparse
 import os
@@ -71,6 +72,47 @@ def make_case(name, peec_text, freqs, count=300, threads=8):
     print(name, "nseg", r.nseg, "ncell", r.ncell, "nunknown", r.nunknown, "->", out)
 
 
+def make_pw_case(name, peec_text, freqs, threads=8):
+    """Plane-wave case: the reference's open-circuit port voltages (p->voc) and, when the
+    input asks for distributions, the induced segment currents (p->segipw), one solve per
+    frequency (solve.c:372-389). Written to tests/golden/pw/."""
+    with tempfile.NamedTemporaryFile("w", suffix=".peec", delete=False) as f:
+        f.write(peec_text)
+        path = f.name
+    RefLib.set_threads(threads)
+    r = RefLib(path)
+    prob = r.problem()
+    vocs, segs, pwp = [], [], None
+    for fr in freqs:
+        r.set_freqs(fr, fr, 1, 0)
+        r.solve()
+        voc, seg, pwp = r.voc()
+        vocs.append(voc[:, 0])
+        segs.append(seg[0] if seg is not None else np.zeros(r.nseg, complex))
+    os.unlink(path)
+    os.makedirs(os.path.join(HERE, "pw"), exist_ok=True)
+    out = os.path.join(HERE, "pw", name + ".npz")
+    tmp = os.path.join(HERE, name + "_prob.npz")
+    prob.save(tmp)
+    pz = dict(np.load(tmp))
+    os.unlink(tmp)
+    np.savez_compressed(out, **{"prob_" + k: v for k, v in pz.items()}, freqs=np.array(freqs),
+                        voc=np.array(vocs).T, segipw=np.array(segs), pw=pwp,
+                        has_segi=np.array(seg is not None), peec=np.array(peec_text))
+    print(name, "nseg", r.nseg, "voc", np.array(vocs).T.ravel()[:2], "->", out)
+
+
+def pw_cases():
+    loop_load = sample("loop_pw.peec").replace("planewave = 90 0 2 1.0",
+                                               "planewave = 90 0 2 1.0\ndistribution = 1\nresistor = 1 5 50")
+    mono = sample("monopole_gp.peec").replace("groundplane = 0", "groundplane = 0\nplanewave = 60 0 1 1.0")
+    make_pw_case("dipole_pw", sample("dipole_pw.peec"), [1.4376e8, 3.0e8])
+    make_pw_case("bent_pw", sample("bent_pw.peec"), [1.5e8])
+    make_pw_case("loop_pw", sample("loop_pw.peec"), [1e7])
+    make_pw_case("loop_pw_load", loop_load, [1e7, 1e8])
+    make_pw_case("mono_pw", mono, [1.3e8, 1.45e8, 1.6e8])
+
+
 def sample(fn):
     with open(os.path.join(REF, "data", "sample", fn)) as f:
         return f.read()
@@ -79,9 +121,13 @@ def sample(fn):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--cfg2", action="store_true")
+    ap.add_argument("--pw-only", action="store_true", help="only the plane-wave cases")
     a = ap.parse_args()
     subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True,
                    stdout=subprocess.DEVNULL)
+    pw_cases()
+    if a.pw_only:
+        return
     f1 = [1e7 * (100.0 ** (i / 99.0)) for i in range(100)]
     make_case("cfg1_dipole_qs", configs.CFG1, f1[::9] + [f1[-1]])
     make_case("dipole_halfwave", sample("dipole_halfwave.peec"), [2.8e8, 2.93e8, 3.0e8, 6.0e8])
