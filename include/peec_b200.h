@@ -124,6 +124,13 @@ typedef struct {
                                right-preconditioned GMRES(60) with the nearest factored
                                frequency's LU (gmres_solve, iterative.c:230-252); systems
                                that do not converge are refactorised (FP64) */
+    int    compress;        /* 1 = the reference's compression = 1 path (solve.c:251-294):
+                               H-matrix (ACA) of the Lp block, leaf-block + circuit-Schur
+                               preconditioner, matrix-free GMRES(60) per port to the relative
+                               residual refine_tol (0 = 1e-10, ACCEL_TOL); full MNA form,
+                               capacitance = 0 only */
+    int    pad_;
+    double ctol;            /* ACA relative tolerance (0 = 1e-6, the reference's default) */
 } pb_sweep_opts;
 
 typedef struct {
@@ -146,6 +153,9 @@ typedef struct {
     int    gmres_its_max;   /* largest GMRES iteration count of one system            */
     int    gmres_refactored;/* systems refactorised at their own frequency (FP32)     */
     double gmres_its_avg;   /* mean GMRES iterations per GMRES-solved system          */
+    int    hmat_far, hmat_near;        /* compressed path: far (low-rank) and near blocks */
+    int    hmat_max_rank, hmat_dense_far; /* largest ACA rank; far blocks kept dense      */
+    double hmat_mb, hmat_dense_mb;     /* H-matrix storage vs the dense Lp block [MiB]  */
 } pb_sweep_stats;
 
 const char *pb_last_error(void);

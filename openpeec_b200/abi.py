@@ -56,7 +56,8 @@ class PbSweepOpts(C.Structure):
     _fields_ = [
         ("fill_prec", C.c_int), ("lu", C.c_int), ("form", C.c_int), ("batch", C.c_int),
         ("refine_tol", C.c_double), ("refine_maxit", C.c_int), ("verbose", C.c_int),
-        ("corr_freqs", C.c_int), ("accel", C.c_int),
+        ("corr_freqs", C.c_int), ("accel", C.c_int), ("compress", C.c_int), ("pad_", C.c_int),
+        ("ctol", C.c_double),
     ]
 
 
@@ -72,6 +73,8 @@ class PbSweepStats(C.Structure):
         ("fp64_direct", C.c_int), ("fp64_max_hz", C.c_double),
         ("lu_count", C.c_int), ("gmres_solves", C.c_int), ("gmres_its_max", C.c_int),
         ("gmres_refactored", C.c_int), ("gmres_its_avg", C.c_double),
+        ("hmat_far", C.c_int), ("hmat_near", C.c_int), ("hmat_max_rank", C.c_int),
+        ("hmat_dense_far", C.c_int), ("hmat_mb", C.c_double), ("hmat_dense_mb", C.c_double),
     ]
 
     def as_dict(self):

@@ -65,13 +65,14 @@ class Context:
 
     def sweep(self, freqs, fill_prec=abi.PREC_MIXED, lu=abi.LU_TC, form=abi.FORM_AUTO,
               batch=0, refine_tol=0.0, refine_maxit=0, want_segi=False, zmat_out=None,
-              corr_freqs=0, verbose=0, accel=0):
+              corr_freqs=0, verbose=0, accel=0, compress=0, ctol=0.0):
         freqs = np.ascontiguousarray(freqs, np.float64)
         npt = len(self.prob.port)
         z = zmat_out if zmat_out is not None else np.zeros((len(freqs), npt, npt), np.complex128)
         segi = np.zeros((len(freqs), npt, self.nseg), np.complex128) if want_segi else None
         o = abi.PbSweepOpts(int(fill_prec), int(lu), int(form), int(batch), float(refine_tol),
-                            int(refine_maxit), int(verbose), int(corr_freqs), int(accel))
+                            int(refine_maxit), int(verbose), int(corr_freqs), int(accel),
+                            int(compress), 0, float(ctol))
         st = abi.PbSweepStats()
         _check(abi.lib().pb_sweep(self.h, len(freqs), freqs.ctypes.data, C.byref(o),
                                   z.ctypes.data, None if segi is None else segi.ctypes.data,
@@ -90,7 +91,7 @@ class Context:
         npt = len(self.prob.port)
         voc = np.zeros((npt, len(freqs)), np.complex128)
         seg = np.zeros((len(freqs), self.nseg), np.complex128) if want_segi else None
-        o = abi.PbSweepOpts(int(fill_prec), int(lu), int(form), int(batch), 0.0, 0, 0, 0, int(accel))
+        o = abi.PbSweepOpts(int(fill_prec), int(lu), int(form), int(batch), 0.0, 0, 0, 0, int(accel), 0, 0, 0.0)
         w = abi.PbPlanewave(float(pw[0]), float(pw[1]), int(pw[2]), 0, float(pw[3]),
                             float(pw[4]) if len(pw) > 4 else 0.0)
         st = abi.PbSweepStats()

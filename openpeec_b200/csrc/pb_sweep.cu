@@ -15,6 +15,7 @@
 // tensor-core trailing updates + FP64 iterative refinement against the FP64 matrix.
 #include "pb_ctx.cuh"
 #include "pb_gmres.cuh"
+#include "pb_hmat.cuh"
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -286,7 +287,15 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
     pb_sweep_opts o;
     if (opts_in) o = *opts_in;
     else { o.fill_prec = PB_PREC_MIXED; o.lu = PB_LU_TC; o.form = PB_FORM_AUTO; o.batch = 0;
-           o.refine_tol = 0; o.refine_maxit = 0; o.verbose = 0; o.corr_freqs = 0; o.accel = 0; }
+           o.refine_tol = 0; o.refine_maxit = 0; o.verbose = 0; o.corr_freqs = 0; o.accel = 0;
+           o.compress = 0; o.pad_ = 0; o.ctol = 0; }
+    if (o.compress) {
+        if (pw) { pb_set_error("plane-wave excitation is not built for the compressed path"); return PB_ERR_UNSUP; }
+        if (nfreq <= 0 || freq == nullptr) { pb_set_error("pb_sweep: no frequencies"); return PB_ERR_ARG; }
+        pb_hstats hs;
+        return pb_sweep_compressed(c, nfreq, freq, o, o.ctol > 0 ? o.ctol : 1e-6,
+                                   o.refine_tol > 0 ? o.refine_tol : 1e-10, zmat, stats, &hs);
+    }
     if (nfreq <= 0 || freq == nullptr) { pb_set_error("pb_sweep: no frequencies"); return PB_ERR_ARG; }
     for (int i = 0; i < nfreq; i++)
         if (!(freq[i] > 0)) { pb_set_error("pb_sweep: frequencies must be > 0"); return PB_ERR_ARG; }

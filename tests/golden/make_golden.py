@@ -11,6 +11,7 @@ reference's own sources with oracle/Makefile). For every case it stores:
     python tests/golden/make_golden.py            # all small cases (about a minute)
     python tests/golden/make_golden.py --cfg2     # + the full 64x32 plate at 2 frequencies
     python tests/golden/make_golden.py --pw-only  # only the plane-wave cases (tests/golden/pw)
+    python tests/golden/make_golden.py --comp-only  # only the compressed-path cases (tests/golden/comp)
 """
 import argparse
 import os
@@ -102,6 +103,55 @@ def make_pw_case(name, peec_text, freqs, threads=8):
     print(name, "nseg", r.nseg, "voc", np.array(vocs).T.ravel()[:2], "->", out)
 
 
+def make_comp_case(name, peec_text, freqs, threads=16):
+    """Compressed-path case: Z of the reference's compression = 1 solve (H-matrix + ACA,
+    leaf-Schur preconditioner, GMRES) and Z of its dense solve of the same input with the
+    compression key removed. Written to tests/golden/comp/."""
+    dense_text = "\n".join(l for l in peec_text.splitlines() if not l.startswith("compression"))
+    zs = {}
+    prob = None
+    for tag, text in (("z", peec_text), ("z_dense", dense_text)):
+        with tempfile.NamedTemporaryFile("w", suffix=".peec", delete=False) as f:
+            f.write(text + "\n")
+            path = f.name
+        RefLib.set_threads(threads)
+        r = RefLib(path)
+        if prob is None:
+            prob = r.problem()
+        out = []
+        for fr in freqs:
+            r.set_freqs(fr, fr, 1, 0)
+            out.append(r.solve()[0])
+        zs[tag] = np.array(out)
+        os.unlink(path)
+    os.makedirs(os.path.join(HERE, "comp"), exist_ok=True)
+    out = os.path.join(HERE, "comp", name + ".npz")
+    tmp = os.path.join(HERE, name + "_prob.npz")
+    prob.save(tmp)
+    pz = dict(np.load(tmp))
+    os.unlink(tmp)
+    np.savez_compressed(out, **{"prob_" + k: v for k, v in pz.items()}, freqs=np.array(freqs),
+                        peec=np.array(peec_text), **zs)
+    print(name, "nseg", len(prob.seg), "z", zs["z"].ravel()[:1], "dense", zs["z_dense"].ravel()[:1], "->", out)
+
+
+def comp_cases():
+    make_comp_case("compress_wire", sample("compress_wire.peec"), [1e6])
+    make_comp_case("compress_plate", sample("compress_plate.peec"), [1e8])
+    bars = """OpenPEEC 1 0
+title = volume-cell bar stack (reduced)
+compression = 1 1e-6
+retardation = 1
+plate = 0 0 0  0.04 0 0  0 0.04 0  2e-4 5.8e7 12 12 4
+node = 1 0 0 0
+node = 2 0.04 0.04 0
+port = 1 2 50
+frequency = 1e6 2e9 1 log
+end
+"""
+    make_comp_case("bars_small", bars, [1e6, 2e9])
+
+
 def pw_cases():
     loop_load = sample("loop_pw.peec").replace("planewave = 90 0 2 1.0",
                                                "planewave = 90 0 2 1.0\ndistribution = 1\nresistor = 1 5 50")
@@ -122,11 +172,14 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--cfg2", action="store_true")
     ap.add_argument("--pw-only", action="store_true", help="only the plane-wave cases")
+    ap.add_argument("--comp-only", action="store_true", help="only the compressed-path cases")
     a = ap.parse_args()
     subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True,
                    stdout=subprocess.DEVNULL)
-    pw_cases()
-    if a.pw_only:
+    if not a.comp_only:
+        pw_cases()
+    comp_cases()
+    if a.pw_only or a.comp_only:
         return
     f1 = [1e7 * (100.0 ** (i / 99.0)) for i in range(100)]
     make_case("cfg1_dipole_qs", configs.CFG1, f1[::9] + [f1[-1]])
