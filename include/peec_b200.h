@@ -128,7 +128,7 @@ typedef struct {
                                H-matrix (ACA) of the Lp block, leaf-block + circuit-Schur
                                preconditioner, matrix-free GMRES(60) per port to the relative
                                residual refine_tol (0 = 1e-10, ACCEL_TOL); full MNA form,
-                               capacitance = 0 only */
+                               with capacitance the charge block P is compressed too */
     int    pad_;
     double ctol;            /* ACA relative tolerance (0 = 1e-6, the reference's default) */
 } pb_sweep_opts;

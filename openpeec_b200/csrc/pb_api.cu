@@ -296,6 +296,7 @@ void pb_destroy(pb_ctx *c)
                     c->g.seg_cb, c->d_inc_off, c->d_inc_seg, c->d_fe_row, c->d_fe_col, c->d_fe_off,
                     c->d_fe_st, c->d_cellnode};
     for (void *p : ptrs) if (p) cudaFree(p);
+    for (auto &slot : c->cache) if (slot.p) cudaFree(slot.p);
     pb_lu_engine_free(&c->lu);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;

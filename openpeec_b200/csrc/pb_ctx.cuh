@@ -5,6 +5,11 @@
 #include "pb_fill.cuh"
 #include "pb_lu.cuh"
 
+// Device storage a context keeps across sweep calls (grow-only, freed by pb_destroy), so
+// repeated sweeps of one structure do not reallocate their batch buffers.
+struct pb_cache_slot { void *p = nullptr; size_t cap = 0; };
+#define PB_CACHE_SLOTS 32
+
 // One additive contribution to an MNA entry whose value scales as val * {1, jw, -jw}.
 enum { ST_CONST = 0, ST_JW = 1, ST_MJW = 2 };
 struct pb_stamp { int kind; double val; };
@@ -50,6 +55,8 @@ struct pb_ctx {
     int *d_fe_row = nullptr, *d_fe_col = nullptr, *d_fe_off = nullptr;
     pb_stamp *d_fe_st = nullptr;
     int *d_cellnode = nullptr;                 // [ncell] matrix index of the cell's node (-1 = ref)
+
+    pb_cache_slot cache[PB_CACHE_SLOTS];
 
     long launches = 0;
 };

@@ -1,8 +1,9 @@
 // pb_hmat.cu — compressed (matrix-free) sweep for large structures, compression = 1:
 //   * cluster tree + block partition on the host (hmatrix.c:91-227, same deterministic
 //     splits as the reference, so the same blocks),
-//   * the kernel block Lp(f) is filled densely on the device (it fits in HBM: 74k cells is
-//     89 GB in FP64) and its far blocks are compressed by partially pivoted ACA with the
+//   * the kernel blocks Lp(f) (and, with capacitance, P(f) over the node cells) are filled
+//     densely on the device (74k cells is 89 GB in FP64, within HBM) and their far blocks
+//     are compressed by partially pivoted ACA with the
 //     reference's restarts from unrepresented rows (aca_block, hmatrix.c:265-395), one CTA
 //     per block, entries read from the dense fill; near blocks (and far blocks that do not
 //     compress) are copied out dense,
@@ -512,101 +513,282 @@ void host_lu_solve(int n, const zc *a, const int *piv, zc *b)
 
 // ================================================================ the compressed sweep
 namespace {
-struct HDev {                                   // device side of one H-matrix build
-    Dev perm, aca, rank, U, V, rused, urep, dblk, D, fblk, t, leaf_of, dn_off, dn_idx, fr_off, fr_idx;
-    int nf = 0, nd = 0, nfr = 0;
-    long long ftlen = 0;
+// One compressed kernel block of the augmented system (hblock_t, include/peec.h:328-338):
+// unknowns [off, off+n), kernel matrix K (dense on the device), scale (Lp: -jw, P: 1).
+struct KBlock {
+    int off = 0, n = 0;
+    double2 scale = make_double2(1, 0);
+    pb_htree T;
+    int nl = 0;
+    std::vector<int> leaf_of, leaf_lo, leaf_hi;
+    std::vector<AcaBlk> ab;
+    long long uo = 0, vo = 0, so = 0;
+    Dev perm, aca, rank, U, V, rused, urep, leaf_of_d;
+    // per build
+    std::vector<DBlk> db;
+    std::vector<FBlk> fb;
+    long long toff = 0;
+    Dev dblk, D, fblk, t, dn_off, dn_idx, fr_off, fr_idx, hy;
+    // preconditioner
+    std::vector<int> lof, lidx, dpiv, sleaf, spos;
+    std::vector<long long> dof;
+    std::vector<zc> dlu;
+    std::vector<int> bri, bci, cri, cci;
+    std::vector<zc> bval, cval;
+    Dev lof_d, lidx_d, dof_d, dlu_d, dpiv_d, bro, bcol, bv, cro, ccol, cv, wb, ub;
 };
 
-struct PcDev {                                  // preconditioner on the device
-    Dev lof, lidx, dof, dlu, dpiv, bro, bcol, bval, cro, ccol, cval, slu, spiv, sperm, sinfo;
-    int nleaf = 0, n1 = 0;
-};
+// tree, leaves and ACA workspace of a block (hmat_build_gen, hmatrix.c:403-421)
+int kb_setup(KBlock &kb, const double *pts, cudaStream_t st)
+{
+    pb_htree_build(kb.T, kb.n, pts);
+    kb.nl = (int)kb.T.leafid.size();
+    kb.leaf_of.assign(kb.n, 0);
+    kb.leaf_lo.assign(kb.nl, 0);
+    kb.leaf_hi.assign(kb.nl, 0);
+    for (int r = 0; r < kb.nl; r++) {
+        kb.leaf_lo[r] = kb.T.lo[kb.T.leafid[r]];
+        kb.leaf_hi[r] = kb.T.hi[kb.T.leafid[r]];
+        for (int i = kb.leaf_lo[r]; i < kb.leaf_hi[r]; i++) kb.leaf_of[i] = r;
+        if (kb.leaf_hi[r] - kb.leaf_lo[r] > PB_PC_MAXM) {
+            pb_set_error("compressed sweep: leaf of %d cells exceeds %d (coincident cells?)",
+                         kb.leaf_hi[r] - kb.leaf_lo[r], PB_PC_MAXM);
+            return PB_ERR_UNSUP;
+        }
+    }
+    const int nfar = (int)kb.T.fr.size();
+    kb.ab.resize(nfar);
+    kb.uo = kb.vo = kb.so = 0;
+    for (int b = 0; b < nfar; b++) {
+        AcaBlk &B = kb.ab[b];
+        B.r0 = kb.T.lo[kb.T.fr[b]];
+        B.m = kb.T.hi[kb.T.fr[b]] - B.r0;
+        B.c0 = kb.T.lo[kb.T.fc[b]];
+        B.nn = kb.T.hi[kb.T.fc[b]] - B.c0;
+        B.lim = std::min(std::min(B.m, B.nn), PB_HM_MAXIT);
+        B.uoff = kb.uo;
+        B.voff = kb.vo;
+        B.soff = kb.so;
+        B.pad = 0;
+        kb.uo += (long long)B.lim * B.m;
+        kb.vo += (long long)B.lim * B.nn;
+        kb.so += B.m;
+    }
+    PB_TRY(upload(kb.perm, kb.T.perm, st));
+    PB_TRY(upload(kb.aca, kb.ab, st));
+    PB_TRY(kb.rank.alloc(sizeof(int) * std::max(1, nfar)));
+    PB_TRY(kb.U.alloc(sizeof(double2) * (size_t)std::max(1LL, kb.uo)));
+    PB_TRY(kb.V.alloc(sizeof(double2) * (size_t)std::max(1LL, kb.vo)));
+    PB_TRY(kb.rused.alloc(sizeof(int) * (size_t)std::max(1LL, kb.so)));
+    PB_TRY(kb.urep.alloc(sizeof(double) * (size_t)std::max(1LL, kb.so)));
+    PB_TRY(upload(kb.leaf_of_d, kb.leaf_of, st));
+    PB_TRY(kb.hy.alloc(sizeof(double2) * (size_t)kb.n));
+    PB_TRY(kb.wb.alloc(sizeof(double2) * (size_t)kb.n));
+    PB_TRY(kb.ub.alloc(sizeof(double2) * (size_t)kb.n));
+    return PB_OK;
+}
+
+// H-matrix of scale * K: ACA on the far blocks, dense copies of the rest, per-leaf lists,
+// and the scaled leaf-diagonal blocks for the preconditioner (dlu, host)
+int kb_compress(KBlock &kb, const double2 *K, double ctol, pb_ctx *c, pb_hstats *hs)
+{
+    const cudaStream_t st = c->stream;
+    const int nfar = (int)kb.T.fr.size(), nnear = (int)kb.T.nr.size();
+    if (nfar > 0) {
+        k_aca<<<nfar, 256, 0, st>>>(K, kb.n, kb.perm.as<int>(), kb.aca.as<AcaBlk>(), kb.U.as<double2>(),
+                                    kb.V.as<double2>(), kb.rused.as<int>(), kb.urep.as<double>(), ctol,
+                                    kb.rank.as<int>());
+        c->launches++;
+        PB_CHECK_LAUNCH();
+    }
+    std::vector<int> rank(std::max(1, nfar));
+    if (nfar > 0) PB_CUDA(cudaMemcpyAsync(rank.data(), kb.rank.p, sizeof(int) * nfar, cudaMemcpyDeviceToHost, st));
+    PB_CUDA(cudaStreamSynchronize(st));
+    kb.db.clear();
+    kb.fb.clear();
+    long long doff = 0;
+    kb.toff = 0;
+    size_t nz = 0;
+    for (int q = 0; q < nnear; q++) {
+        const pb_htree &T = kb.T;
+        DBlk B{T.lo[T.nr[q]], T.hi[T.nr[q]] - T.lo[T.nr[q]], T.lo[T.nc[q]], T.hi[T.nc[q]] - T.lo[T.nc[q]], doff};
+        doff += (long long)B.m * B.nn;
+        kb.db.push_back(B);
+    }
+    for (int b = 0; b < nfar; b++) {
+        const AcaBlk &A = kb.ab[b];
+        if (rank[b] <= 0) {
+            kb.db.push_back(DBlk{A.r0, A.m, A.c0, A.nn, doff});
+            doff += (long long)A.m * A.nn;
+            hs->ndense_far++;
+        } else {
+            kb.fb.push_back(FBlk{A.r0, A.m, A.c0, A.nn, A.uoff, A.voff, rank[b], (int)kb.toff});
+            kb.toff += rank[b];
+            hs->max_rank = std::max(hs->max_rank, rank[b]);
+            nz += (size_t)rank[b] * (A.m + A.nn);
+        }
+    }
+    nz += (size_t)doff;
+    hs->nfar += nfar;
+    hs->nnear += nnear;
+    hs->mem_mb += (double)nz * 16 / (1024.0 * 1024.0);
+    hs->dense_mb += (double)kb.n * kb.n * 16 / (1024.0 * 1024.0);
+    // per-leaf block lists in registration order (hmatrix.c:490-590)
+    const int nl = kb.nl;
+    std::vector<int> dn_off(nl + 1, 0), fr_off(nl + 1, 0), dn_idx, fr_idx;
+    {
+        std::vector<std::vector<int>> dl(nl), fl(nl);
+        for (size_t q = 0; q < kb.db.size(); q++)
+            for (int r = kb.leaf_of[kb.db[q].r0]; r < nl && kb.leaf_lo[r] < kb.db[q].r0 + kb.db[q].m; r++)
+                dl[r].push_back((int)q);
+        for (size_t q = 0; q < kb.fb.size(); q++)
+            for (int r = kb.leaf_of[kb.fb[q].r0]; r < nl && kb.leaf_lo[r] < kb.fb[q].r0 + kb.fb[q].m; r++)
+                fl[r].push_back((int)q);
+        for (int r = 0; r < nl; r++) {
+            dn_off[r + 1] = dn_off[r] + (int)dl[r].size();
+            fr_off[r + 1] = fr_off[r] + (int)fl[r].size();
+            dn_idx.insert(dn_idx.end(), dl[r].begin(), dl[r].end());
+            fr_idx.insert(fr_idx.end(), fl[r].begin(), fl[r].end());
+        }
+    }
+    PB_TRY(upload(kb.dblk, kb.db, st));
+    PB_TRY(kb.D.alloc(sizeof(double2) * (size_t)std::max(1LL, doff)));
+    if (!kb.db.empty()) {
+        k_gather<<<(unsigned)kb.db.size(), 256, 0, st>>>(K, kb.n, kb.perm.as<int>(), kb.dblk.as<DBlk>(), kb.scale,
+                                                         kb.D.as<double2>());
+        c->launches++;
+        PB_CHECK_LAUNCH();
+    }
+    // the low-rank factors carry the scale: U <- scale U
+    const double2 sm1 = make_double2(kb.scale.x - 1.0, kb.scale.y);
+    for (const FBlk &B : kb.fb) {
+        const long long cnt = (long long)B.rank * B.m;
+        k_axpy_c<<<ceil_div(cnt, 256), 256, 0, st>>>((int)cnt, sm1, kb.U.as<double2>() + B.uoff,
+                                                     kb.U.as<double2>() + B.uoff);
+        c->launches++;
+    }
+    PB_CHECK_LAUNCH();
+    PB_TRY(upload(kb.fblk, kb.fb, st));
+    PB_TRY(kb.t.alloc(sizeof(double2) * (size_t)std::max(1LL, kb.toff)));
+    PB_TRY(upload(kb.dn_off, dn_off, st));
+    PB_TRY(upload(kb.dn_idx, dn_idx, st));
+    PB_TRY(upload(kb.fr_off, fr_off, st));
+    PB_TRY(upload(kb.fr_idx, fr_idx, st));
+    // leaf diagonal blocks of scale * K (blk_leaves, precond.c:91-136)
+    kb.lof.assign(nl + 1, 0);
+    kb.dof.assign(nl + 1, 0);
+    kb.lidx.assign(kb.n, 0);
+    kb.dpiv.assign(kb.n, 0);
+    kb.sleaf.assign(kb.n, 0);
+    kb.spos.assign(kb.n, 0);
+    for (int r = 0; r < nl; r++) {
+        const int mm = kb.leaf_hi[r] - kb.leaf_lo[r];
+        kb.lof[r + 1] = kb.lof[r] + mm;
+        kb.dof[r + 1] = kb.dof[r] + (long long)mm * mm;
+        for (int a = 0; a < mm; a++) {
+            const int cell = kb.T.perm[kb.leaf_lo[r] + a];
+            kb.lidx[kb.lof[r] + a] = cell;
+            kb.sleaf[cell] = r;
+            kb.spos[cell] = a;
+        }
+    }
+    kb.dlu.assign(std::max<long long>(1, kb.dof[nl]), zc(0, 0));
+    std::vector<DBlk> lb(nl);
+    for (int r = 0; r < nl; r++) {
+        const int mm = kb.leaf_hi[r] - kb.leaf_lo[r];
+        lb[r] = DBlk{kb.leaf_lo[r], mm, kb.leaf_lo[r], mm, kb.dof[r]};
+    }
+    Dev bLb, bLd;
+    PB_TRY(upload(bLb, lb, st));
+    PB_TRY(bLd.alloc(sizeof(double2) * (size_t)std::max<long long>(1, kb.dof[nl])));
+    k_gather<<<nl, 256, 0, st>>>(K, kb.n, kb.perm.as<int>(), bLb.as<DBlk>(), kb.scale, bLd.as<double2>());
+    c->launches++;
+    PB_CHECK_LAUNCH();
+    PB_CUDA(cudaMemcpyAsync(kb.dlu.data(), bLd.p, sizeof(double2) * kb.dof[nl], cudaMemcpyDeviceToHost, st));
+    PB_CUDA(cudaStreamSynchronize(st));
+    return PB_OK;
+}
+
+// y[off..off+n) += scale H x[off..off+n)  (two phases, deterministic)
+int kb_apply(KBlock &kb, const double2 *x, double2 *y, pb_ctx *c)
+{
+    const cudaStream_t st = c->stream;
+    if (!kb.fb.empty())
+        k_hmv_t<<<(unsigned)kb.fb.size(), 128, 0, st>>>(kb.fblk.as<FBlk>(), kb.V.as<double2>(), kb.perm.as<int>(),
+                                                        x + kb.off, kb.t.as<double2>());
+    k_hmv_y<<<ceil_div((long long)kb.n * 32, 256), 256, 0, st>>>(
+        kb.n, kb.perm.as<int>(), kb.leaf_of_d.as<int>(), kb.dn_off.as<int>(), kb.dn_idx.as<int>(), kb.dblk.as<DBlk>(),
+        kb.D.as<double2>(), kb.fr_off.as<int>(), kb.fr_idx.as<int>(), kb.fblk.as<FBlk>(), kb.U.as<double2>(),
+        kb.t.as<double2>(), x + kb.off, kb.hy.as<double2>());
+    k_axpy_c<<<ceil_div(kb.n, 256), 256, 0, st>>>(kb.n, make_double2(1, 0), kb.hy.as<double2>(), y + kb.off);
+    c->launches += 3;
+    PB_CHECK_LAUNCH();
+    return PB_OK;
+}
 }  // namespace
 
 int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts &o, double ctol,
                         double gtol, double *zmat, pb_sweep_stats *stats, pb_hstats *hs)
 {
-    if (c->capacitance && c->ncell > 0) {
-        pb_set_error("compression = 1 with capacitance (H-matrix of the charge block) is not built in this "
-                     "library; use the dense sweep");
+    const int ns = (int)c->seg.size(), N = c->nfull, offS = c->offS, n1 = c->offS, np = (int)c->port.size();
+    const int cap = (c->capacitance && c->ncell > 0) ? 1 : 0;
+    const int nc = cap ? c->ncell : 0, offQ = c->nunknown;
+    if (ns <= 0 || N <= 0) { pb_set_error("compressed sweep: empty system"); return PB_ERR_ARG; }
+    if (N != offS + ns + nc || (cap && offQ != offS + ns)) {
+        pb_set_error("compressed sweep: unexpected unknown layout");
         return PB_ERR_UNSUP;
     }
-    const int ns = (int)c->seg.size(), N = c->nfull, offS = c->offS, n1 = c->offS, np = (int)c->port.size();
-    if (ns <= 0 || N <= 0) { pb_set_error("compressed sweep: empty system"); return PB_ERR_ARG; }
-    if (N != offS + ns) { pb_set_error("compressed sweep: unexpected unknown layout"); return PB_ERR_UNSUP; }
     const cudaStream_t st = c->stream;
     const int fill32 = (o.fill_prec == PB_PREC_MIXED);
     *hs = pb_hstats();
 
-    // cluster tree over the segment midpoints (hmat_build, hmatrix.c:617-634)
-    std::vector<double> pts(3 * (size_t)ns);
-    for (int i = 0; i < ns; i++)
-        for (int q = 0; q < 3; q++) pts[3 * i + q] = 0.5 * (c->seg[i].x1[q] + c->seg[i].x2[q]);
-    pb_htree T;
-    pb_htree_build(T, ns, pts.data());
-    const int nl = (int)T.leafid.size();
-    // leaf index of every perm position, leaf start positions
-    std::vector<int> leaf_of(ns), leaf_lo(nl), leaf_hi(nl);
-    for (int r = 0; r < nl; r++) {
-        leaf_lo[r] = T.lo[T.leafid[r]];
-        leaf_hi[r] = T.hi[T.leafid[r]];
-        for (int i = leaf_lo[r]; i < leaf_hi[r]; i++) leaf_of[i] = r;
-        if (leaf_hi[r] - leaf_lo[r] > PB_PC_MAXM) {
-            pb_set_error("compressed sweep: leaf of %d cells exceeds %d (coincident cells?)", leaf_hi[r] - leaf_lo[r], PB_PC_MAXM);
-            return PB_ERR_UNSUP;
+    // compressed blocks: Lp over the segment midpoints (hmat_build, hmatrix.c:617-634) and,
+    // with capacitance, P over the cell points (hmat_build_pot, potential.c:158-165)
+    std::vector<KBlock> kbs(1 + cap);
+    {
+        std::vector<double> pts(3 * (size_t)ns);
+        for (int i = 0; i < ns; i++)
+            for (int q = 0; q < 3; q++) pts[3 * i + q] = 0.5 * (c->seg[i].x1[q] + c->seg[i].x2[q]);
+        kbs[0].off = offS;
+        kbs[0].n = ns;
+        PB_TRY(kb_setup(kbs[0], pts.data(), st));
+    }
+    if (cap) {
+        // cell point: length-weighted centroid of its sub-cell midpoints (potential.c:98-111)
+        std::vector<double> cpt(3 * (size_t)nc);
+        for (int i = 0; i < nc; i++) {
+            double w = 0, x[3] = {0, 0, 0};
+            for (int e = c->csoff[i]; e < c->csoff[i + 1]; e++) {
+                const pb_cell_t &s = c->chg[c->csidx[e]];
+                for (int q = 0; q < 3; q++) x[q] += s.len * 0.5 * (s.x1[q] + s.x2[q]);
+                w += s.len;
+            }
+            for (int q = 0; q < 3; q++) cpt[3 * i + q] = w > 0 ? x[q] / w : 0;
         }
-    }
-    const int nfar = (int)T.fr.size(), nnear = (int)T.nr.size();
-    hs->nfar = nfar;
-    hs->nnear = nnear;
-
-    // ACA workspace per far block
-    std::vector<AcaBlk> ab(nfar);
-    long long uo = 0, vo = 0, so = 0;
-    for (int b = 0; b < nfar; b++) {
-        AcaBlk &B = ab[b];
-        B.r0 = T.lo[T.fr[b]];
-        B.m = T.hi[T.fr[b]] - B.r0;
-        B.c0 = T.lo[T.fc[b]];
-        B.nn = T.hi[T.fc[b]] - B.c0;
-        B.lim = std::min(std::min(B.m, B.nn), PB_HM_MAXIT);
-        B.uoff = uo;
-        B.voff = vo;
-        B.soff = so;
-        B.pad = 0;
-        uo += (long long)B.lim * B.m;
-        vo += (long long)B.lim * B.nn;
-        so += B.m;
+        kbs[1].off = offQ;
+        kbs[1].n = nc;
+        PB_TRY(kb_setup(kbs[1], cpt.data(), st));
     }
 
-    Dev bK, bSt, bZint, bFreq, bX, bB, bR, bW, bZ, bHy, bVk, bDot, bU1, bWb, bUb;
+    Dev bK, bSt, bKP, bStP, bIg, bZint, bFreq, bX, bB, bR, bW, bZ, bVk, bDot, bU1;
     PB_TRY(bK.alloc(sizeof(double2) * (size_t)ns * ns));
     PB_TRY(bSt.alloc(sizeof(double) * (size_t)ns * ns));
+    if (cap) {
+        PB_TRY(bKP.alloc(sizeof(double2) * (size_t)nc * nc));
+        PB_TRY(bStP.alloc(sizeof(double) * (size_t)nc * nc));
+        if (c->retardation) PB_TRY(bIg.alloc(sizeof(double2) * c->chg.size() * c->chg.size()));
+    }
     PB_TRY(bZint.alloc(sizeof(double2) * (size_t)ns));
     PB_TRY(bFreq.alloc(sizeof(double)));
-    HDev H;
-    PB_TRY(upload(H.perm, T.perm, st));
-    PB_TRY(upload(H.aca, ab, st));
-    PB_TRY(H.rank.alloc(sizeof(int) * std::max(1, nfar)));
-    PB_TRY(H.U.alloc(sizeof(double2) * (size_t)std::max(1LL, uo)));
-    PB_TRY(H.V.alloc(sizeof(double2) * (size_t)std::max(1LL, vo)));
-    PB_TRY(H.rused.alloc(sizeof(int) * (size_t)std::max(1LL, so)));
-    PB_TRY(H.urep.alloc(sizeof(double) * (size_t)std::max(1LL, so)));
-    PB_TRY(upload(H.leaf_of, leaf_of, st));
-
     const int m = 60;                           // GMRES_MAXIT (iterative.c:29)
     PB_TRY(bX.alloc(sizeof(double2) * (size_t)N));
     PB_TRY(bB.alloc(sizeof(double2) * (size_t)N));
     PB_TRY(bR.alloc(sizeof(double2) * (size_t)N));
     PB_TRY(bW.alloc(sizeof(double2) * (size_t)N));
     PB_TRY(bZ.alloc(sizeof(double2) * (size_t)N));
-    PB_TRY(bHy.alloc(sizeof(double2) * (size_t)ns));
     PB_TRY(bVk.alloc(sizeof(double2) * (size_t)(m + 1) * N));
     PB_TRY(bDot.alloc(sizeof(double2) * 4));
     PB_TRY(bU1.alloc(sizeof(double2) * (size_t)std::max(1, n1)));
-    PB_TRY(bWb.alloc(sizeof(double2) * (size_t)ns));
-    PB_TRY(bUb.alloc(sizeof(double2) * (size_t)ns));
 
     double t_fill = 0, t_aca = 0, t_pc = 0, t_gm = 0, samples = 0;
     long gm_its = 0;
@@ -628,7 +810,7 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
     for (int ifr = 0; ifr < nfreq; ifr++) {
         const double f = freq[ifr], om = 2 * PB_PI * f;
         const double kw = c->retardation ? om / PB_C0 : 0.0;
-        // ---- dense kernel block Lp(f) and Z_int(f)
+        // ---- dense kernel blocks Lp(f) (and P(f)), Z_int(f)
         tick();
         PB_CUDA(cudaMemcpyAsync(bFreq.p, &f, sizeof(double), cudaMemcpyHostToDevice, st));
         PB_TRY(pb_zint(c->g, c->skin, 1, bFreq.as<double>(), bZint.as<double2>(), st, &c->launches));
@@ -638,95 +820,32 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
             ea.out = bK.as<double2>();
             ea.out_stride = (long long)ns * ns;
             PB_TRY(pb_lp_corr(c->g, 1, &kw, fill32, bSt.as<double>(), PB_EPI_STORE, ea, st, &c->launches, nullptr));
+            if (cap) {
+                PB_TRY(pb_pot_static(c->g, kw, bStP.as<double>(), st, &c->launches));
+                PB_TRY(pb_pot_corr(c->g, 1, &kw, fill32, bStP.as<double>(), bKP.as<double2>(), (long long)nc * nc,
+                                   c->retardation ? bIg.as<double2>() : nullptr, st, &c->launches, nullptr));
+            }
             if (kw > 0) {
                 PB_TRY(pb_count_samples(c->g, kw, &lp_samp, &p_samp, st));
-                samples += lp_samp;
+                samples += lp_samp + (cap ? p_samp : 0);
             }
         }
         tock(t_fill);
-        // ---- H-matrix of -jw Lp: ACA on far blocks, dense copies of the rest
+        // ---- H-matrices (the kernel blocks are rebuilt each frequency: solve.c:254-277)
         tick();
-        if (nfar > 0) {
-            k_aca<<<nfar, 256, 0, st>>>(bK.as<double2>(), ns, H.perm.as<int>(), H.aca.as<AcaBlk>(), H.U.as<double2>(),
-                                        H.V.as<double2>(), H.rused.as<int>(), H.urep.as<double>(), ctol,
-                                        H.rank.as<int>());
-            c->launches++;
-            PB_CHECK_LAUNCH();
+        pb_hstats hf;
+        kbs[0].scale = make_double2(0, -om);        // -jw Lp (solve.c:262)
+        PB_TRY(kb_compress(kbs[0], bK.as<double2>(), ctol, c, &hf));
+        if (cap) {
+            kbs[1].scale = make_double2(1, 0);      // P (solve.c:275)
+            PB_TRY(kb_compress(kbs[1], bKP.as<double2>(), ctol, c, &hf));
         }
-        std::vector<int> rank(std::max(1, nfar));
-        if (nfar > 0) PB_CUDA(cudaMemcpyAsync(rank.data(), H.rank.p, sizeof(int) * nfar, cudaMemcpyDeviceToHost, st));
-        PB_CUDA(cudaStreamSynchronize(st));
-        // dense blocks: near + far blocks that did not compress; low-rank list
-        std::vector<DBlk> db;
-        std::vector<FBlk> fb;
-        std::vector<int> db_row, fb_row;            // row cluster of each
-        long long doff = 0, toff = 0;
-        size_t nz = 0;
-        for (int q = 0; q < nnear; q++) {
-            DBlk B{T.lo[T.nr[q]], T.hi[T.nr[q]] - T.lo[T.nr[q]], T.lo[T.nc[q]], T.hi[T.nc[q]] - T.lo[T.nc[q]], doff};
-            doff += (long long)B.m * B.nn;
-            db.push_back(B);
-            db_row.push_back(T.nr[q]);
-        }
-        int ndf = 0, rmax = 0;
-        for (int b = 0; b < nfar; b++) {
-            const AcaBlk &A = ab[b];
-            if (rank[b] <= 0) {
-                DBlk B{A.r0, A.m, A.c0, A.nn, doff};
-                doff += (long long)A.m * A.nn;
-                db.push_back(B);
-                db_row.push_back(T.fr[b]);
-                ndf++;
-            } else {
-                FBlk B{A.r0, A.m, A.c0, A.nn, A.uoff, A.voff, rank[b], (int)toff};
-                toff += rank[b];
-                fb.push_back(B);
-                fb_row.push_back(T.fr[b]);
-                rmax = std::max(rmax, rank[b]);
-                nz += (size_t)rank[b] * (A.m + A.nn);
-            }
-        }
-        nz += (size_t)doff;
-        hs->ndense_far = ndf;
-        hs->max_rank = std::max(hs->max_rank, rmax);
-        hs->mem_mb = (double)nz * 16 / (1024.0 * 1024.0);
-        hs->dense_mb = (double)ns * ns * 16 / (1024.0 * 1024.0);
-        // per-leaf block lists (blocks whose row cluster contains the leaf, registration order)
-        std::vector<int> dn_off(nl + 1, 0), fr_off(nl + 1, 0), dn_idx, fr_idx;
-        {
-            std::vector<std::vector<int>> dl(nl), fl(nl);
-            for (size_t q = 0; q < db.size(); q++)
-                for (int r = leaf_of[db[q].r0]; r < nl && leaf_lo[r] < db[q].r0 + db[q].m; r++) dl[r].push_back((int)q);
-            for (size_t q = 0; q < fb.size(); q++)
-                for (int r = leaf_of[fb[q].r0]; r < nl && leaf_lo[r] < fb[q].r0 + fb[q].m; r++) fl[r].push_back((int)q);
-            for (int r = 0; r < nl; r++) {
-                dn_off[r + 1] = dn_off[r] + (int)dl[r].size();
-                fr_off[r + 1] = fr_off[r] + (int)fl[r].size();
-                dn_idx.insert(dn_idx.end(), dl[r].begin(), dl[r].end());
-                fr_idx.insert(fr_idx.end(), fl[r].begin(), fl[r].end());
-            }
-        }
-        // the H-matrix holds -jw Lp (scale of the Lp block, solve.c:262); the low-rank
-        // factors are scaled on the fly in the product (t carries the factor)
-        const double2 scale = make_double2(0, -om);
-        PB_TRY(upload(H.dblk, db, st));
-        PB_TRY(H.D.alloc(sizeof(double2) * (size_t)std::max(1LL, doff)));
-        if (!db.empty()) {
-            k_gather<<<(unsigned)db.size(), 256, 0, st>>>(bK.as<double2>(), ns, H.perm.as<int>(), H.dblk.as<DBlk>(),
-                                                          scale, H.D.as<double2>());
-            c->launches++;
-            PB_CHECK_LAUNCH();
-        }
-        PB_TRY(upload(H.fblk, fb, st));
-        PB_TRY(H.t.alloc(sizeof(double2) * (size_t)std::max(1LL, toff)));
-        PB_TRY(upload(H.dn_off, dn_off, st));
-        PB_TRY(upload(H.dn_idx, dn_idx, st));
-        PB_TRY(upload(H.fr_off, fr_off, st));
-        PB_TRY(upload(H.fr_idx, fr_idx, st));
+        hf.max_rank = std::max(hf.max_rank, hs->max_rank);
+        *hs = hf;
         tock(t_aca);
 
-        // ---- sparse part (mna_sparse): stamps of the augmented system + -Z_int on the
-        // segment diagonal, as CSR in registration order
+        // ---- sparse part (mna_sparse, mna.c:317-325): stamps of the augmented system and
+        // -Z_int on the segment diagonal, CSR in registration order
         tick();
         std::vector<zc> zint(ns);
         PB_CUDA(cudaMemcpyAsync(zint.data(), bZint.p, sizeof(double2) * ns, cudaMemcpyDeviceToHost, st));
@@ -754,85 +873,64 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
         PB_TRY(upload(bCol, col, st));
         PB_TRY(upload(bVal, val, st));
 
-        // ---- preconditioner (pc_build): D_r = leaf diagonal block of -jw Lp + same-leaf
-        // sparse entries; B / C couplings; Schur S = S11 - sum B D^-1 C; LU(S) on the device
-        std::vector<int> lof(nl + 1, 0), lidx(ns), dpiv(ns);
-        std::vector<long long> dof(nl + 1, 0);
-        for (int r = 0; r < nl; r++) {
-            const int mm = leaf_hi[r] - leaf_lo[r];
-            lof[r + 1] = lof[r] + mm;
-            dof[r + 1] = dof[r] + (long long)mm * mm;
-            for (int a = 0; a < mm; a++) lidx[lof[r] + a] = T.perm[leaf_lo[r] + a];
-        }
-        std::vector<zc> dlu(std::max<long long>(1, dof[nl]));
-        {
-            std::vector<DBlk> lb(nl);
-            for (int r = 0; r < nl; r++) {
-                const int mm = leaf_hi[r] - leaf_lo[r];
-                lb[r] = DBlk{leaf_lo[r], mm, leaf_lo[r], mm, dof[r]};
-            }
-            Dev bLb, bLd;
-            PB_TRY(upload(bLb, lb, st));
-            PB_TRY(bLd.alloc(sizeof(double2) * (size_t)std::max<long long>(1, dof[nl])));
-            k_gather<<<nl, 256, 0, st>>>(bK.as<double2>(), ns, H.perm.as<int>(), bLb.as<DBlk>(), scale, bLd.as<double2>());
-            c->launches++;
-            PB_CHECK_LAUNCH();
-            PB_CUDA(cudaMemcpyAsync(dlu.data(), bLd.p, sizeof(double2) * dof[nl], cudaMemcpyDeviceToHost, st));
-            PB_CUDA(cudaStreamSynchronize(st));
-        }
-        // unknown -> (leaf, position in leaf) for the segment block
-        std::vector<int> sleaf(ns), spos(ns);
-        for (int r = 0; r < nl; r++)
-            for (int e = lof[r]; e < lof[r + 1]; e++) { sleaf[lidx[e]] = r; spos[lidx[e]] = e - lof[r]; }
+        // ---- preconditioner (pc_build, precond.c:138-391)
+        std::vector<int> ublk(N, -1), upos(N, -1);
+        for (int b = 0; b < (int)kbs.size(); b++)
+            for (int i = 0; i < kbs[b].n; i++) { ublk[kbs[b].off + i] = b; upos[kbs[b].off + i] = i; }
         std::vector<zc> S((size_t)std::max(1, n1) * std::max(1, n1), zc(0, 0));
-        std::vector<int> bri, bci, cri, cci;
-        std::vector<zc> bval, cval;
+        for (auto &kb : kbs) {
+            kb.bri.clear(); kb.bci.clear(); kb.bval.clear();
+            kb.cri.clear(); kb.cci.clear(); kb.cval.clear();
+        }
         for (int i = 0; i < N; i++)
             for (int e = ro[i]; e < ro[i + 1]; e++) {
                 const int j = col[e];
                 const zc v = val[e];
                 if (i < n1 && j < n1) S[(size_t)i * n1 + j] += v;
-                else if (i < n1) { bri.push_back(i); bci.push_back(j - offS); bval.push_back(v); }
-                else if (j < n1) { cri.push_back(i - offS); cci.push_back(j); cval.push_back(v); }
-                else {
-                    const int k = i - offS, l = j - offS;
-                    if (sleaf[k] == sleaf[l]) {
-                        const int r = sleaf[k], mm = lof[r + 1] - lof[r];
-                        dlu[dof[r] + (long long)spos[k] * mm + spos[l]] += v;
+                else if (i < n1) { KBlock &kb = kbs[ublk[j]]; kb.bri.push_back(i); kb.bci.push_back(upos[j]); kb.bval.push_back(v); }
+                else if (j < n1) { KBlock &kb = kbs[ublk[i]]; kb.cri.push_back(upos[i]); kb.cci.push_back(j); kb.cval.push_back(v); }
+                else if (ublk[i] == ublk[j]) {
+                    KBlock &kb = kbs[ublk[i]];
+                    const int k = upos[i], l = upos[j];
+                    if (kb.sleaf[k] == kb.sleaf[l]) {
+                        const int r = kb.sleaf[k], mm = kb.lof[r + 1] - kb.lof[r];
+                        kb.dlu[kb.dof[r] + (long long)kb.spos[k] * mm + kb.spos[l]] += v;
                     }
                 }
             }
-        for (int r = 0; r < nl; r++) {
-            const int mm = lof[r + 1] - lof[r];
-            if (host_lu(mm, &dlu[dof[r]], &dpiv[lof[r]]) >= 0) {
-                pb_set_error("compressed sweep: preconditioner failed at f = %.5e Hz (floating node?)", f);
-                return PB_ERR_SINGULAR;
+        for (auto &kb : kbs)
+            for (int r = 0; r < kb.nl; r++) {
+                const int mm = kb.lof[r + 1] - kb.lof[r];
+                if (host_lu(mm, &kb.dlu[kb.dof[r]], &kb.dpiv[kb.lof[r]]) >= 0) {
+                    pb_set_error("compressed sweep: preconditioner failed at f = %.5e Hz (floating node?)", f);
+                    return PB_ERR_SINGULAR;
+                }
             }
-        }
-        // Schur complement, leaf by leaf (precond.c:275-364)
-        {
-            std::vector<int> coff(ns + 1, 0), cidx(cri.size()), boff(ns + 1, 0), bidx(bri.size());
-            for (size_t e = 0; e < cri.size(); e++) coff[cri[e] + 1]++;
-            for (int k = 0; k < ns; k++) coff[k + 1] += coff[k];
+        // Schur complement S = S11 - sum_b B_b D_b^-1 C_b, leaf by leaf (precond.c:275-364)
+        for (auto &kb : kbs) {
+            const int nb = kb.n;
+            std::vector<int> coff(nb + 1, 0), cidx(kb.cri.size()), boff(nb + 1, 0), bidx(kb.bri.size());
+            for (size_t e = 0; e < kb.cri.size(); e++) coff[kb.cri[e] + 1]++;
+            for (int k = 0; k < nb; k++) coff[k + 1] += coff[k];
             {
                 std::vector<int> pos(coff.begin(), coff.end() - 1);
-                for (size_t e = 0; e < cri.size(); e++) cidx[pos[cri[e]]++] = (int)e;
+                for (size_t e = 0; e < kb.cri.size(); e++) cidx[pos[kb.cri[e]]++] = (int)e;
             }
-            for (size_t e = 0; e < bri.size(); e++) boff[bci[e] + 1]++;
-            for (int k = 0; k < ns; k++) boff[k + 1] += boff[k];
+            for (size_t e = 0; e < kb.bri.size(); e++) boff[kb.bci[e] + 1]++;
+            for (int k = 0; k < nb; k++) boff[k + 1] += boff[k];
             {
                 std::vector<int> pos(boff.begin(), boff.end() - 1);
-                for (size_t e = 0; e < bri.size(); e++) bidx[pos[bci[e]]++] = (int)e;
+                for (size_t e = 0; e < kb.bri.size(); e++) bidx[pos[kb.bci[e]]++] = (int)e;
             }
             std::vector<int> tmap(std::max(1, n1), -1), tset;
             std::vector<zc> tb, colv(PB_PC_MAXM);
-            for (int r = 0; r < nl; r++) {
-                const int mm = lof[r + 1] - lof[r];
-                const int *idx = &lidx[lof[r]];
+            for (int r = 0; r < kb.nl; r++) {
+                const int mm = kb.lof[r + 1] - kb.lof[r];
+                const int *idx = &kb.lidx[kb.lof[r]];
                 tset.clear();
                 for (int a = 0; a < mm; a++)
                     for (int q = coff[idx[a]]; q < coff[idx[a] + 1]; q++) {
-                        const int j = cci[cidx[q]];
+                        const int j = kb.cci[cidx[q]];
                         if (tmap[j] < 0) { tmap[j] = (int)tset.size(); tset.push_back(j); }
                     }
                 const int t = (int)tset.size();
@@ -841,63 +939,67 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
                 for (int a = 0; a < mm; a++)
                     for (int q = coff[idx[a]]; q < coff[idx[a] + 1]; q++) {
                         const int e = cidx[q];
-                        tb[(size_t)a * t + tmap[cci[e]]] += cval[e];
+                        tb[(size_t)a * t + tmap[kb.cci[e]]] += kb.cval[e];
                     }
                 for (int cc = 0; cc < t; cc++) {
                     for (int a = 0; a < mm; a++) colv[a] = tb[(size_t)a * t + cc];
-                    host_lu_solve(mm, &dlu[dof[r]], &dpiv[lof[r]], colv.data());
+                    host_lu_solve(mm, &kb.dlu[kb.dof[r]], &kb.dpiv[kb.lof[r]], colv.data());
                     for (int a = 0; a < mm; a++) tb[(size_t)a * t + cc] = colv[a];
                 }
                 for (int a = 0; a < mm; a++)
                     for (int q = boff[idx[a]]; q < boff[idx[a] + 1]; q++) {
                         const int e = bidx[q];
-                        const int i = bri[e];
-                        for (int cc = 0; cc < t; cc++) S[(size_t)i * n1 + tset[cc]] -= bval[e] * tb[(size_t)a * t + cc];
+                        const int i = kb.bri[e];
+                        for (int cc = 0; cc < t; cc++) S[(size_t)i * n1 + tset[cc]] -= kb.bval[e] * tb[(size_t)a * t + cc];
                     }
                 for (int cc = 0; cc < t; cc++) tmap[tset[cc]] = -1;
             }
-        }
-        // device copies: leaf factors, B as CSR over circuit rows, C as CSR over segment rows
-        PcDev P;
-        P.nleaf = nl;
-        P.n1 = n1;
-        PB_TRY(upload(P.lof, lof, st));
-        PB_TRY(upload(P.lidx, lidx, st));
-        PB_TRY(upload(P.dof, dof, st));
-        PB_TRY(upload(P.dlu, dlu, st));
-        PB_TRY(upload(P.dpiv, dpiv, st));
-        {
-            std::vector<int> bro(n1 + 1, 0), bcol2(bri.size()), cro(ns + 1, 0), ccol2(cri.size());
-            std::vector<zc> bval2(bri.size()), cval2(cri.size());
-            for (size_t e = 0; e < bri.size(); e++) bro[bri[e] + 1]++;
+            // device copies: leaf factors, B as CSR over circuit rows, C as CSR over block rows
+            std::vector<int> bro(n1 + 1, 0), bcol2(kb.bri.size()), cro(nb + 1, 0), ccol2(kb.cri.size());
+            std::vector<zc> bval2(kb.bri.size()), cval2(kb.cri.size());
+            for (size_t e = 0; e < kb.bri.size(); e++) bro[kb.bri[e] + 1]++;
             for (int i = 0; i < n1; i++) bro[i + 1] += bro[i];
             {
                 std::vector<int> pos(bro.begin(), bro.end() - 1);
-                for (size_t e = 0; e < bri.size(); e++) { const int p = pos[bri[e]]++; bcol2[p] = bci[e]; bval2[p] = bval[e]; }
+                for (size_t e = 0; e < kb.bri.size(); e++) {
+                    const int p = pos[kb.bri[e]]++;
+                    bcol2[p] = kb.bci[e];
+                    bval2[p] = kb.bval[e];
+                }
             }
-            for (size_t e = 0; e < cri.size(); e++) cro[cri[e] + 1]++;
-            for (int k = 0; k < ns; k++) cro[k + 1] += cro[k];
+            for (size_t e = 0; e < kb.cri.size(); e++) cro[kb.cri[e] + 1]++;
+            for (int k = 0; k < nb; k++) cro[k + 1] += cro[k];
             {
                 std::vector<int> pos(cro.begin(), cro.end() - 1);
-                for (size_t e = 0; e < cri.size(); e++) { const int p = pos[cri[e]]++; ccol2[p] = cci[e]; cval2[p] = cval[e]; }
+                for (size_t e = 0; e < kb.cri.size(); e++) {
+                    const int p = pos[kb.cri[e]]++;
+                    ccol2[p] = kb.cci[e];
+                    cval2[p] = kb.cval[e];
+                }
             }
-            PB_TRY(upload(P.bro, bro, st));
-            PB_TRY(upload(P.bcol, bcol2, st));
-            PB_TRY(upload(P.bval, bval2, st));
-            PB_TRY(upload(P.cro, cro, st));
-            PB_TRY(upload(P.ccol, ccol2, st));
-            PB_TRY(upload(P.cval, cval2, st));
+            PB_TRY(upload(kb.lof_d, kb.lof, st));
+            PB_TRY(upload(kb.lidx_d, kb.lidx, st));
+            PB_TRY(upload(kb.dof_d, kb.dof, st));
+            PB_TRY(upload(kb.dlu_d, kb.dlu, st));
+            PB_TRY(upload(kb.dpiv_d, kb.dpiv, st));
+            PB_TRY(upload(kb.bro, bro, st));
+            PB_TRY(upload(kb.bcol, bcol2, st));
+            PB_TRY(upload(kb.bv, bval2, st));
+            PB_TRY(upload(kb.cro, cro, st));
+            PB_TRY(upload(kb.ccol, ccol2, st));
+            PB_TRY(upload(kb.cv, cval2, st));
         }
+        Dev slu, spiv, sperm, sinfo;
         if (n1 > 0) {
-            PB_TRY(upload(P.slu, S, st));
-            PB_TRY(P.spiv.alloc(sizeof(int) * n1));
-            PB_TRY(P.sperm.alloc(sizeof(int) * n1));
-            PB_TRY(P.sinfo.alloc(sizeof(int)));
-            PB_TRY(pb_lu_factor<double>(&c->lu, n1, 1, P.slu.as<double2>(), n1, (long)n1 * n1, P.spiv.as<int>(),
-                                        P.sinfo.as<int>()));
-            PB_TRY(pb_lu_perm(&c->lu, n1, 1, P.spiv.as<int>(), P.sperm.as<int>()));
+            PB_TRY(upload(slu, S, st));
+            PB_TRY(spiv.alloc(sizeof(int) * n1));
+            PB_TRY(sperm.alloc(sizeof(int) * n1));
+            PB_TRY(sinfo.alloc(sizeof(int)));
+            PB_TRY(pb_lu_factor<double>(&c->lu, n1, 1, slu.as<double2>(), n1, (long)n1 * n1, spiv.as<int>(),
+                                        sinfo.as<int>()));
+            PB_TRY(pb_lu_perm(&c->lu, n1, 1, spiv.as<int>(), sperm.as<int>()));
             int info = -1;
-            PB_CUDA(cudaMemcpyAsync(&info, P.sinfo.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+            PB_CUDA(cudaMemcpyAsync(&info, sinfo.p, sizeof(int), cudaMemcpyDeviceToHost, st));
             PB_CUDA(cudaStreamSynchronize(st));
             if (info >= 0) {
                 pb_set_error("compressed sweep: preconditioner failed at f = %.5e Hz (floating node?)", f);
@@ -907,50 +1009,37 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
         tock(t_pc);
 
         // ---- operators on device vectors
-        const unsigned gN = ceil_div(N, TB), gS = ceil_div(ns, TB);
-        tick();
-        // scale the low-rank factors once: U_b <- scale * U_b
-        if (!fb.empty()) {
-            for (const FBlk &B : fb) {
-                const long long cnt = (long long)B.rank * B.m;
-                k_axpy_c<<<ceil_div(cnt, TB), TB, 0, st>>>((int)cnt, make_double2(scale.x - 1.0, scale.y),
-                                                           H.U.as<double2>() + B.uoff, H.U.as<double2>() + B.uoff);
-            }
-            c->launches += fb.size();
-            PB_CHECK_LAUNCH();
-        }
-        auto opA = [&](const double2 *x, double2 *y) -> int {   // y = S x + scale H x_seg
+        const unsigned gN = ceil_div(N, TB);
+        auto opA = [&](const double2 *x, double2 *y) -> int {   // mna_apply (mna.c:347-364)
             k_spmv<<<gN, TB, 0, st>>>(N, bRo.as<int>(), bCol.as<int>(), bVal.as<double2>(), x, y);
-            if (!fb.empty())
-                k_hmv_t<<<(unsigned)fb.size(), 128, 0, st>>>(H.fblk.as<FBlk>(), H.V.as<double2>(), H.perm.as<int>(),
-                                                             x + offS, H.t.as<double2>());
-            k_hmv_y<<<ceil_div((long long)ns * 32, TB), TB, 0, st>>>(
-                ns, H.perm.as<int>(), H.leaf_of.as<int>(), H.dn_off.as<int>(), H.dn_idx.as<int>(), H.dblk.as<DBlk>(),
-                H.D.as<double2>(), H.fr_off.as<int>(), H.fr_idx.as<int>(), H.fblk.as<FBlk>(), H.U.as<double2>(),
-                H.t.as<double2>(), x + offS, bHy.as<double2>());
-            k_axpy_c<<<gS, TB, 0, st>>>(ns, make_double2(1, 0), bHy.as<double2>(), y + offS);
-            c->launches += 4;
-            PB_CHECK_LAUNCH();
+            c->launches++;
+            for (auto &kb : kbs) PB_TRY(kb_apply(kb, x, y, c));
             return PB_OK;
         };
-        auto opM = [&](double2 *z) -> int {                        // z <- M^-1 z (pc_apply)
+        auto opM = [&](double2 *z) -> int {                     // pc_apply (precond.c:407-435)
             if (n1 > 0) PB_CUDA(cudaMemcpyAsync(bU1.p, z, sizeof(double2) * n1, cudaMemcpyDeviceToDevice, st));
-            k_leaf_solve<<<ceil_div(nl, 64), 64, 0, st>>>(nl, P.lof.as<int>(), P.lidx.as<int>(), P.dof.as<long long>(),
-                                                         P.dlu.as<double2>(), P.dpiv.as<int>(), z + offS, bWb.as<double2>());
-            if (n1 > 0) {
-                k_csr_sub<<<ceil_div(n1, TB), TB, 0, st>>>(n1, P.bro.as<int>(), P.bcol.as<int>(), P.bval.as<double2>(),
-                                                           bWb.as<double2>(), bU1.as<double2>());
-                PB_TRY(pb_lu_solve_batched<double>(&c->lu, n1, 1, 1, P.slu.as<double2>(), n1, (long)n1 * n1,
-                                                   P.sperm.as<int>(), bU1.as<double2>(), z));
+            for (auto &kb : kbs) {
+                k_leaf_solve<<<ceil_div(kb.nl, 64), 64, 0, st>>>(kb.nl, kb.lof_d.as<int>(), kb.lidx_d.as<int>(),
+                                                                kb.dof_d.as<long long>(), kb.dlu_d.as<double2>(),
+                                                                kb.dpiv_d.as<int>(), z + kb.off, kb.wb.as<double2>());
+                if (n1 > 0)
+                    k_csr_sub<<<ceil_div(n1, TB), TB, 0, st>>>(n1, kb.bro.as<int>(), kb.bcol.as<int>(),
+                                                               kb.bv.as<double2>(), kb.wb.as<double2>(), bU1.as<double2>());
+                c->launches += 2;
             }
-            PB_CUDA(cudaMemcpyAsync(bUb.p, z + offS, sizeof(double2) * ns, cudaMemcpyDeviceToDevice, st));
             if (n1 > 0)
-                k_csr_sub<<<gS, TB, 0, st>>>(ns, P.cro.as<int>(), P.ccol.as<int>(), P.cval.as<double2>(), z,
-                                             bUb.as<double2>());
-            k_leaf_solve<<<ceil_div(nl, 64), 64, 0, st>>>(nl, P.lof.as<int>(), P.lidx.as<int>(), P.dof.as<long long>(),
-                                                         P.dlu.as<double2>(), P.dpiv.as<int>(), bUb.as<double2>(),
-                                                         z + offS);
-            c->launches += 5;
+                PB_TRY(pb_lu_solve_batched<double>(&c->lu, n1, 1, 1, slu.as<double2>(), n1, (long)n1 * n1,
+                                                   sperm.as<int>(), bU1.as<double2>(), z));
+            for (auto &kb : kbs) {
+                PB_CUDA(cudaMemcpyAsync(kb.ub.p, z + kb.off, sizeof(double2) * kb.n, cudaMemcpyDeviceToDevice, st));
+                if (n1 > 0)
+                    k_csr_sub<<<ceil_div(kb.n, TB), TB, 0, st>>>(kb.n, kb.cro.as<int>(), kb.ccol.as<int>(),
+                                                                 kb.cv.as<double2>(), z, kb.ub.as<double2>());
+                k_leaf_solve<<<ceil_div(kb.nl, 64), 64, 0, st>>>(kb.nl, kb.lof_d.as<int>(), kb.lidx_d.as<int>(),
+                                                                kb.dof_d.as<long long>(), kb.dlu_d.as<double2>(),
+                                                                kb.dpiv_d.as<int>(), kb.ub.as<double2>(), z + kb.off);
+                c->launches += 2;
+            }
             PB_CHECK_LAUNCH();
             return PB_OK;
         };
@@ -965,6 +1054,7 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
         };
 
         // ---- every port excitation: matrix-free GMRES (gmres_hmat, iterative.c:285-354)
+        tick();
         for (int j = 0; j < np; j++) {
             std::vector<zc> bh(N, zc(0, 0));
             const int i1 = c->nodemap[c->port[j].n1], i2 = c->nodemap[c->port[j].n2];
@@ -978,7 +1068,6 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
             int total = 0;
             bool done = bnorm <= 0;
             for (int cyc = 0; cyc < 10 && !done; cyc++) {
-                // true residual
                 if (cyc == 0) PB_CUDA(cudaMemcpyAsync(bR.p, bB.p, sizeof(double2) * N, cudaMemcpyDeviceToDevice, st));
                 else {
                     PB_TRY(opA(bX.as<double2>(), bR.as<double2>()));
@@ -987,7 +1076,7 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
                     PB_TRY(dot(bR.as<double2>(), bR.as<double2>(), rr));
                     if (sqrt(rr.real()) <= tolabs) { done = true; break; }
                 }
-                // one cycle (gmres_cycle, iterative.c:83-196)
+                // one cycle (gmres_cycle, iterative.c:83-196), modified Gram-Schmidt as there
                 zc rr;
                 PB_TRY(dot(bR.as<double2>(), bR.as<double2>(), rr));
                 const double beta = sqrt(rr.real());
@@ -1001,7 +1090,7 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
                     PB_CUDA(cudaMemcpyAsync(bZ.p, Vk + (long long)jj * N, sizeof(double2) * N, cudaMemcpyDeviceToDevice, st));
                     PB_TRY(opM(bZ.as<double2>()));
                     PB_TRY(opA(bZ.as<double2>(), bW.as<double2>()));
-                    for (int i = 0; i <= jj; i++) {           // modified Gram-Schmidt
+                    for (int i = 0; i <= jj; i++) {
                         zc hij;
                         PB_TRY(dot(Vk + (long long)i * N, bW.as<double2>(), hij));
                         h[i + (size_t)jj * (m + 1)] = hij;
@@ -1051,7 +1140,6 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
             gm_its += total;
             gm_max = std::max(gm_max, total);
             nrhs++;
-            // Z column j: port voltages
             std::vector<zc> xh(N);
             PB_CUDA(cudaMemcpyAsync(xh.data(), bX.p, sizeof(double2) * N, cudaMemcpyDeviceToHost, st));
             PB_CUDA(cudaStreamSynchronize(st));
@@ -1073,7 +1161,6 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
     hs->gmres_rhs = nrhs;
     if (stats) {
         memset(stats, 0, sizeof(*stats));
-        stats->t_static_ms = 0;
         stats->t_corr_ms = t_fill;
         stats->t_assemble_ms = t_aca;
         stats->t_lu_ms = t_pc;

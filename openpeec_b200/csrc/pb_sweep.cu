@@ -230,13 +230,30 @@ __global__ void k_axpy(double2 *x, const double2 *d, long long n)
 }
 
 // ---------------------------------------------------------------- helpers
+// Device buffer of one sweep call; with a context slot the storage stays with the context
+// for the next call (grow-only).
 struct DevBuf {
     void *p = nullptr;
-    ~DevBuf() { if (p) cudaFree(p); }
+    pb_cache_slot *slot = nullptr;
+    DevBuf() = default;
+    explicit DevBuf(pb_cache_slot *s) : slot(s) {}
+    ~DevBuf() { if (p && !slot) cudaFree(p); }
     int alloc(size_t bytes)
     {
-        if (p) { cudaFree(p); p = nullptr; }
         if (bytes == 0) bytes = 16;
+        if (slot) {
+            if (slot->cap < bytes) {
+                if (slot->p) cudaFree(slot->p);
+                slot->p = nullptr;
+                slot->cap = 0;
+                cudaError_t e = cudaMalloc(&slot->p, bytes);
+                if (e != cudaSuccess) { slot->p = nullptr; return pb_cuda_fail(e, "cudaMalloc", __FILE__, __LINE__); }
+                slot->cap = bytes;
+            }
+            p = slot->p;
+            return PB_OK;
+        }
+        if (p) { cudaFree(p); p = nullptr; }
         cudaError_t e = cudaMalloc(&p, bytes);
         if (e != cudaSuccess) { p = nullptr; return pb_cuda_fail(e, "cudaMalloc", __FILE__, __LINE__); }
         return PB_OK;
@@ -329,19 +346,21 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
                          (c->retardation ? (double)PB_FMAX * c->chg.size() * c->chg.size() * 16 : 0.0);
     int B = o.batch;
     if (B <= 0) {
-        const double avail = 0.80 * (double)fr - fixed - 256e6;
+        double cached = 0;                       // storage this context already holds
+        for (const auto &slot : c->cache) cached += (double)slot.cap;
+        const double avail = 0.80 * ((double)fr + cached) - fixed - 256e6;
         B = (int)std::max(1.0, std::floor(avail / perf));
         B = std::min(B, 256);
     }
     B = std::max(1, std::min(B, nfreq));
 
-    DevBuf bM64, bM32, bP, bLp, bStLp, bStP, bZint, bPiv, bPerm, bInfo, bRhs, bX, bR, bD, bRn, bBn,
-        bFreq, bZ, bPC;
+    pb_cache_slot *cs = c->cache;
+    DevBuf bM64(cs + 0), bM32(cs + 1), bP(cs + 2), bLp(cs + 3), bStLp(cs + 4), bStP(cs + 5), bZint(cs + 6), bPiv(cs + 7), bPerm(cs + 8), bInfo(cs + 9), bRhs(cs + 10), bX(cs + 11), bR(cs + 12), bD(cs + 13), bRn(cs + 14), bBn(cs + 15), bFreq(cs + 16), bZ(cs + 17), bPC(cs + 18);
     PB_TRY(bM64.alloc((size_t)B * n2 * 16));
     if (mixed) PB_TRY(bM32.alloc((size_t)B * n2 * 8));
     // real-embedded right operands of the tensor-core trailing updates: the largest is
     // k x nc complex with k + nc = n, i.e. at most n^2/4 entries -> 4 * n^2/4 floats
-    DevBuf bEmb;
+    DevBuf bEmb(cs + 19);
     struct EmbGuard {
         pb_lu_engine *e;
         ~EmbGuard() { e->emb = nullptr; e->emb_cap = 0; }
@@ -352,7 +371,7 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
         c->lu.emb_cap = (size_t)B * n2 * 4;
     }
     PB_TRY(bP.alloc((size_t)B * nc * nc * 16 + 16));
-    DevBuf bIg;                                  // sub-cell P corrections of one fill chunk
+    DevBuf bIg(cs + 20);                                  // sub-cell P corrections of one fill chunk
     if (c->capacitance && nc > 0 && c->retardation)
         PB_TRY(bIg.alloc((size_t)PB_FMAX * c->chg.size() * c->chg.size() * 16));
     if (form == PB_FORM_FULL) PB_TRY(bLp.alloc((size_t)B * ns * ns * 16 + 16));
@@ -367,7 +386,7 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
     PB_TRY(bX.alloc(vb));
     PB_TRY(bR.alloc(vb));
     PB_TRY(bD.alloc(vb));
-    DevBuf bXn, bAn;
+    DevBuf bXn(cs + 21), bAn(cs + 22);
     PB_TRY(bXn.alloc((size_t)B * nr * 8));
     PB_TRY(bAn.alloc((size_t)B * 8));
     PB_TRY(bRn.alloc((size_t)B * nr * 8));

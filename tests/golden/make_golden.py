@@ -150,6 +150,9 @@ frequency = 1e6 2e9 1 log
 end
 """
     make_comp_case("bars_small", bars, [1e6, 2e9])
+    make_comp_case("compress_cap", sample("compress_cap.peec"), [1e6])
+    make_comp_case("cap_retarded", configs.cfg2(16, 8, 512).replace("capacitance = 1", "capacitance = 1\ncompression = 1 1e-6"),
+                   [3.2e8, 1.28e9])
 
 
 def pw_cases():

@@ -6,7 +6,10 @@ Fixtures: tests/golden/comp/*.npz, written by tests/golden/make_golden.py from t
 reference's own compressed solve and its dense solve of the same input (compression key
 removed): the sample compress_wire (200-segment wire) and compress_plate (16 x 16 sheet
 with mixed cell orientations, the case that needs ACA's restarts from unrepresented
-rows), and a 12 x 12 x 4 volume-bar stack with retardation at 1 MHz and 2 GHz.
+rows), a 12 x 12 x 4 volume-bar stack with retardation at 1 MHz and 2 GHz, the sample
+compress_cap (capacitive sheet: charge unknowns, H-matrices of Lp and P, two-block
+preconditioner) and the 16 x 8 plate + wire over ground with capacitance, retardation and
+skin effect.
 
 Bar: Z within 1e-5 of the reference's compressed Z (the same algorithm on entries equal
 to ~1e-15, so the same blocks and nearly the same low-rank factors), and within the
@@ -21,7 +24,7 @@ import pytest
 from conftest import load_golden
 
 pytestmark = pytest.mark.gpu
-CASES = ["compress_wire", "compress_plate", "bars_small"]
+CASES = ["compress_wire", "compress_plate", "bars_small", "compress_cap", "cap_retarded"]
 
 
 def rel(a, b):
@@ -62,10 +65,14 @@ def test_compressed_wire_known_answer():
     assert abs(z[0, 0, 0].real / 5.48810e-3 - 1) <= 5e-3
 
 
-def test_compressed_rejects_capacitance(golden):
-    from openpeec_b200 import api
-    prob, fx = golden("cfg2_small")
+def test_compressed_capacitive_exact_at_small_scale(golden):
+    """With every block near (no approximation at this size) the charge formulation of the
+    compressed path is the dense system itself: Z equals the dense sweep to round-off
+    (the reference's 'compress cap exact' check, peec_check.sh:754-771)."""
+    from openpeec_b200 import abi, api
+    prob, fx = golden("dipole_halfwave")
     with api.Context(prob) as ctx:
-        with pytest.raises(api.PbError) as e:
-            ctx.sweep(fx["freqs"][:1], compress=1)
-    assert e.value.code == 5
+        zc, st = ctx.sweep(fx["freqs"], fill_prec=abi.PREC_FP64, lu=abi.LU_FP64, compress=1)
+        zd, _ = ctx.sweep(fx["freqs"], fill_prec=abi.PREC_FP64, lu=abi.LU_FP64)
+    assert st["hmat_far"] == 0
+    assert np.all(rel(zc, zd) <= 1e-9), rel(zc, zd)
