@@ -1,5 +1,6 @@
 // pb_ctx.cuh — the opaque context behind pb_ctx* (include/peec_b200.h).
 #pragma once
+#include <map>
 #include <vector>
 #include "pb_common.cuh"
 #include "pb_fill.cuh"
@@ -57,6 +58,8 @@ struct pb_ctx {
     int *d_cellnode = nullptr;                 // [ncell] matrix index of the cell's node (-1 = ref)
 
     pb_cache_slot cache[PB_CACHE_SLOTS];
+    // correction samples (Lp, P) per quadrature-level signature, for the statistics
+    std::map<std::vector<long>, std::pair<double, double>> sample_counts;
 
     long launches = 0;
 };

@@ -472,7 +472,18 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
                 if (c->capacitance && nc > 0) PB_TRY(pb_pot_static(c->g, kw0, bStP.as<double>(), st, &c->launches));
                 PB_TRY(pb_lp_static(c->g, kw0, bStLp.as<double>(), st, &c->launches));
                 tStatic.stop(st);
-                if (kw0 > 0) PB_TRY(pb_count_samples(c->g, kw0, &lp_samp, &p_samp, st));
+                if (kw0 > 0) {
+                    // exact quadrature-sample count of this level (statistics only): it depends
+                    // on the geometry and the level signature, so the context keeps it
+                    auto it = c->sample_counts.find(sig);
+                    if (it == c->sample_counts.end()) {
+                        PB_TRY(pb_count_samples(c->g, kw0, &lp_samp, &p_samp, st));
+                        c->sample_counts[sig] = std::make_pair(lp_samp, p_samp);
+                    } else {
+                        lp_samp = it->second.first;
+                        p_samp = it->second.second;
+                    }
+                }
                 else lp_samp = p_samp = 0;
                 cur_sig = sig;
                 static_valid = true;
