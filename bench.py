@@ -358,6 +358,58 @@ def run_reference(args, ws, rank):
     }
 
 
+def run_barstack(args):
+    """Second workload (not the headline line): the compressed path on the volume-cell bar
+    stack (40 x 40 x 0.2 mm, 96 x 96 x 4 cells = 74,496 current cells, retardation, ACA
+    tolerance 1e-6, GMRES relative residual 1e-10). `--steps` frequencies of its 32
+    log-spaced points are timed after one warm-up frequency, first with the plain
+    leaf-block + circuit-Schur preconditioner, then with the learned correction trained
+    on the GPU from plain-method samples of seeded smaller stacks of the family. The time
+    is the host wall clock around the synchronous pb_sweep call: the path interleaves
+    device kernels with host work (tree, leaf LUs, Schur assembly, GMRES Givens)."""
+    from openpeec_b200 import pc_learn
+    nx, ny, nz = (int(v) for v in args.barstack.split("x"))
+    prob = geometry.build(geometry.parse_peec(configs.cfg4(nx, ny, nz)))
+    allf = prob.freqs()
+    pick = np.unique(np.linspace(0, len(allf) - 1, max(1, args.steps)).round().astype(int))
+    freqs = allf[pick]
+    t0 = time.time()
+    fam = pc_learn.plate_family(seed=0, count=6)
+    X, T = pc_learn.collect([p for _, p in fam])
+    w, hist = pc_learn.train(X, T, steps=3000, want_loss=True)
+    t_train = time.time() - t0
+    out = {"plain": [], "learned": []}
+    with api.Context(prob) as ctx:
+        ctx.sweep(freqs[:1])                                  # warm-up (allocations, static part)
+        for tag, wts in (("plain", None), ("learned", w)):
+            for f in freqs:
+                t0 = time.perf_counter()
+                z, st = ctx.sweep([f], pc_mlp=wts)
+                dt = time.perf_counter() - t0
+                out[tag].append({"f_hz": float(f), "s": dt, "gmres_its": st["gmres_its_max"],
+                                 "fallbacks": st["pc_mlp_fallbacks"], "zin": [float(z[0, 0, 0].real), float(z[0, 0, 0].imag)]})
+        last = st
+    tp = sum(r["s"] for r in out["plain"])
+    its_p = [r["gmres_its"] for r in out["plain"]]
+    its_l = [r["gmres_its"] for r in out["learned"]]
+    return {
+        "metric": "bar-stack compressed sweep freq-points/s (H-matrix + GMRES)", "value": len(freqs) / tp,
+        "unit": UNIT, "n_gpus": 1, "steps": len(freqs), "warmup": 1, "ms_per_step": 1e3 * tp / len(freqs),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64 (f32 for the learned network)",
+        "data": "synthetic (seeded geometry from the .peec text)", "timing": "host wall clock around synchronous pb_sweep",
+        "config": {"workload": "bar stack 40x40x0.2 mm %dx%dx%d, retardation, 32 log freqs 1 MHz - 2 GHz, ACA 1e-6" % (nx, ny, nz),
+                   "current_cells": len(prob.seg), "freqs_hz": [float(f) for f in freqs]},
+        "hmat": {"far": last["hmat_far"], "near": last["hmat_near"], "max_rank": last["hmat_max_rank"],
+                 "mb": last["hmat_mb"], "dense_mb": last["hmat_dense_mb"]},
+        "gmres_its": {"plain": its_p, "learned": its_l,
+                      "ratio_plain_over_learned": float(sum(its_p) / max(1, sum(its_l)))},
+        "learned": {"train_samples": int(len(X)), "train_s": t_train, "loss_first_last": [float(hist[0]), float(hist[-1])],
+                    "target_var": float(T.var(0).mean()), "fallbacks": [r["fallbacks"] for r in out["learned"]],
+                    "s_per_freq": sum(r["s"] for r in out["learned"]) / len(freqs)},
+        "per_freq": out,
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -370,8 +422,14 @@ def main():
     ap.add_argument("--grid", default="64x32", help="plate grid; not 64x32 only for profiling captures")
     ap.add_argument("--accel", type=int, default=0,
                     help="LU reuse: one FP32 factorisation per ACCEL frequencies, GMRES for the rest (0 = every frequency)")
+    ap.add_argument("--barstack", default="",
+                    help="NXxNYxNZ: time the compressed path on the bar stack instead (e.g. 96x96x4)")
     args = ap.parse_args()
     ws, rank = dist_env()
+    if args.barstack:
+        if rank == 0:
+            print(json.dumps(run_barstack(args)), flush=True)
+        return
     if args.impl == "reference":
         line = run_reference(args, ws, rank)
         if line is not None:

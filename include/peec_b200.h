@@ -131,6 +131,10 @@ typedef struct {
                                with capacitance the charge block P is compressed too */
     int    pad_;
     double ctol;            /* ACA relative tolerance (0 = 1e-6, the reference's default) */
+    const float *pc_mlp;    /* compressed path: weights (pb_mlp_nparam() floats) of the learned
+                               correction of the preconditioner's leaf blocks, NULL = plain
+                               preconditioner; the plain one is the fall back whenever the
+                               corrected one fails (singular leaf, GMRES not converged) */
 } pb_sweep_opts;
 
 typedef struct {
@@ -156,6 +160,8 @@ typedef struct {
     int    hmat_far, hmat_near;        /* compressed path: far (low-rank) and near blocks */
     int    hmat_max_rank, hmat_dense_far; /* largest ACA rank; far blocks kept dense      */
     double hmat_mb, hmat_dense_mb;     /* H-matrix storage vs the dense Lp block [MiB]  */
+    int    pc_mlp_fallbacks;           /* frequencies that fell back to the plain preconditioner */
+    int    pad2_;
 } pb_sweep_stats;
 
 const char *pb_last_error(void);
@@ -247,6 +253,26 @@ int  pb_lu_decomp_batched_dev(int n, int nb, double *a_dev, int *piv_dev, int *i
  */
 int  pb_lp_fill_noalloc(int nseg, const pb_cell_t *seg_dev, int gp, double gpz, double kw,
                         int prec, double *lp_dev);
+
+/*
+ * Learned preconditioner correction (no counterpart in the reference; the plain method is
+ * precond.c:138-391). A 12 -> 128 -> 128 -> 2 tanh MLP maps the features of a current cell
+ * to a correction y of the diagonal of its leaf block, D_ii <- D_ii (1 + y_0 + j y_1).
+ * Weights are pb_mlp_nparam() floats: W1[128][12], b1, W2[128][128], b2, W3[2][128], b3.
+ *
+ * pb_pc_samples: training data of one structure at one frequency: x [nseg][12] features,
+ *   t [nseg][2] targets (S_r - D_r)_ii / D_ii with S_r = ((A_LL^-1)_rr)^-1, the leaf block
+ *   that reproduces the diagonal blocks of the inverse of the whole Lp block (dense inverse
+ *   on the GPU, for training-sized structures).
+ * pb_mlp_train: full-batch Adam on the GPU (hand-written forward / backward kernels); w is
+ *   the initial and final weights, loss_hist [steps] may be NULL.
+ * pb_mlp_grad: mean-squared-error loss and its gradient (for gradient checks).
+ */
+int  pb_mlp_nparam(void);
+int  pb_pc_samples(pb_ctx *ctx, double freq, const pb_sweep_opts *opts, float *x, float *t);
+int  pb_mlp_train(float *w, int n, const float *x, const float *t, int steps, float lr, float *loss_hist);
+int  pb_mlp_grad(const float *w, int n, const float *x, const float *t, float *grad, float *loss);
+int  pb_mlp_predict(const float *w, int n, const float *x, float *y);
 
 /* Measured FP32 FMA throughput of the current GPU in TFLOP/s (dependent FMA chains on
  * every SM): the denominator of the fill kernels' roofline. */

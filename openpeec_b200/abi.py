@@ -57,7 +57,7 @@ class PbSweepOpts(C.Structure):
         ("fill_prec", C.c_int), ("lu", C.c_int), ("form", C.c_int), ("batch", C.c_int),
         ("refine_tol", C.c_double), ("refine_maxit", C.c_int), ("verbose", C.c_int),
         ("corr_freqs", C.c_int), ("accel", C.c_int), ("compress", C.c_int), ("pad_", C.c_int),
-        ("ctol", C.c_double),
+        ("ctol", C.c_double), ("pc_mlp", C.c_void_p),
     ]
 
 
@@ -75,6 +75,7 @@ class PbSweepStats(C.Structure):
         ("gmres_refactored", C.c_int), ("gmres_its_avg", C.c_double),
         ("hmat_far", C.c_int), ("hmat_near", C.c_int), ("hmat_max_rank", C.c_int),
         ("hmat_dense_far", C.c_int), ("hmat_mb", C.c_double), ("hmat_dense_mb", C.c_double),
+        ("pc_mlp_fallbacks", C.c_int), ("pad2_", C.c_int),
     ]
 
     def as_dict(self):
@@ -140,6 +141,11 @@ def lib():
     L.pb_fp32_peak.argtypes = [C.POINTER(C.c_double)]
     L.pb_lp_fill_noalloc.argtypes = [C.c_int, _vp, C.c_int, C.c_double, C.c_double, C.c_int, _vp]
     L.pb_device_sync.restype = C.c_int
+    L.pb_mlp_nparam.restype = C.c_int
+    L.pb_pc_samples.argtypes = [_vp, C.c_double, C.POINTER(PbSweepOpts), _vp, _vp]
+    L.pb_mlp_train.argtypes = [_vp, C.c_int, _vp, _vp, C.c_int, C.c_float, _vp]
+    L.pb_mlp_grad.argtypes = [_vp, C.c_int, _vp, _vp, _vp, _vp]
+    L.pb_mlp_predict.argtypes = [_vp, C.c_int, _vp, _vp]
     _lib = L
     return L
 

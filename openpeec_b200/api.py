@@ -65,7 +65,12 @@ class Context:
 
     def sweep(self, freqs, fill_prec=abi.PREC_MIXED, lu=abi.LU_TC, form=abi.FORM_AUTO,
               batch=0, refine_tol=0.0, refine_maxit=0, want_segi=False, zmat_out=None,
-              corr_freqs=0, verbose=0, accel=0, compress=0, ctol=0.0):
+              corr_freqs=0, verbose=0, accel=None, compress=None, ctol=None, pc_mlp=None):
+        """pb_sweep. accel / compress / ctol = None take the .peec file's acceleration and
+        compression keys."""
+        accel = getattr(self.prob, "accel", 0) if accel is None else accel
+        compress = getattr(self.prob, "compress", 0) if compress is None else compress
+        ctol = getattr(self.prob, "ctol", 0.0) if ctol is None else ctol
         freqs = np.ascontiguousarray(freqs, np.float64)
         npt = len(self.prob.port)
         z = zmat_out if zmat_out is not None else np.zeros((len(freqs), npt, npt), np.complex128)
@@ -73,6 +78,9 @@ class Context:
         o = abi.PbSweepOpts(int(fill_prec), int(lu), int(form), int(batch), float(refine_tol),
                             int(refine_maxit), int(verbose), int(corr_freqs), int(accel),
                             int(compress), 0, float(ctol))
+        if pc_mlp is not None:
+            pc_mlp = np.ascontiguousarray(pc_mlp, np.float32)
+            o.pc_mlp = pc_mlp.ctypes.data
         st = abi.PbSweepStats()
         _check(abi.lib().pb_sweep(self.h, len(freqs), freqs.ctypes.data, C.byref(o),
                                   z.ctypes.data, None if segi is None else segi.ctypes.data,
@@ -91,7 +99,7 @@ class Context:
         npt = len(self.prob.port)
         voc = np.zeros((npt, len(freqs)), np.complex128)
         seg = np.zeros((len(freqs), self.nseg), np.complex128) if want_segi else None
-        o = abi.PbSweepOpts(int(fill_prec), int(lu), int(form), int(batch), 0.0, 0, 0, 0, int(accel), 0, 0, 0.0)
+        o = abi.PbSweepOpts(int(fill_prec), int(lu), int(form), int(batch), 0.0, 0, 0, 0, int(accel), 0, 0, 0.0, None)
         w = abi.PbPlanewave(float(pw[0]), float(pw[1]), int(pw[2]), 0, float(pw[3]),
                             float(pw[4]) if len(pw) > 4 else 0.0)
         st = abi.PbSweepStats()
@@ -101,6 +109,64 @@ class Context:
         if want_segi:
             return voc, seg, st.as_dict()
         return voc, st.as_dict()
+
+
+    def pc_samples(self, freq, fill_prec=abi.PREC_MIXED, ctol=0.0):
+        """Training samples of the learned preconditioner correction at one frequency:
+        (features [nseg, 12], targets [nseg, 2]) (pb_pc_samples)."""
+        x = np.zeros((self.nseg, 12), np.float32)
+        t = np.zeros((self.nseg, 2), np.float32)
+        o = abi.PbSweepOpts(int(fill_prec), int(abi.LU_FP64), 0, 0, 0.0, 0, 0, 0, 0, 1, 0, float(ctol))
+        _check(abi.lib().pb_pc_samples(self.h, float(freq), C.byref(o), x.ctypes.data, t.ctypes.data))
+        return x, t
+
+
+MLP_IN, MLP_H, MLP_OUT = 12, 128, 2
+
+
+def mlp_nparam():
+    return abi.lib().pb_mlp_nparam()
+
+
+def mlp_init(seed=0):
+    """Initial weights (uniform +-1/sqrt(fan_in), biases 0) in the library's layout."""
+    rng = np.random.default_rng(seed)
+    parts = []
+    for fin, fout in ((MLP_IN, MLP_H), (MLP_H, MLP_H), (MLP_H, MLP_OUT)):
+        parts.append(rng.uniform(-1, 1, (fout, fin)).astype(np.float32).ravel() / np.float32(np.sqrt(fin)))
+        parts.append(np.zeros(fout, np.float32))
+    w = np.concatenate(parts).astype(np.float32)
+    assert w.size == mlp_nparam()
+    return w
+
+
+def mlp_train(w, x, t, steps=2000, lr=1e-3, want_loss=False):
+    w = np.ascontiguousarray(w, np.float32).copy()
+    x = np.ascontiguousarray(x, np.float32)
+    t = np.ascontiguousarray(t, np.float32)
+    hist = np.zeros(steps, np.float32) if want_loss else None
+    _check(abi.lib().pb_mlp_train(w.ctypes.data, len(x), x.ctypes.data, t.ctypes.data, int(steps),
+                                  float(lr), None if hist is None else hist.ctypes.data))
+    return (w, hist) if want_loss else w
+
+
+def mlp_grad(w, x, t):
+    w = np.ascontiguousarray(w, np.float32)
+    x = np.ascontiguousarray(x, np.float32)
+    t = np.ascontiguousarray(t, np.float32)
+    g = np.zeros(mlp_nparam(), np.float32)
+    loss = C.c_float()
+    _check(abi.lib().pb_mlp_grad(w.ctypes.data, len(x), x.ctypes.data, t.ctypes.data, g.ctypes.data,
+                                 C.byref(loss)))
+    return float(loss.value), g
+
+
+def mlp_predict(w, x):
+    w = np.ascontiguousarray(w, np.float32)
+    x = np.ascontiguousarray(x, np.float32)
+    y = np.zeros((len(x), MLP_OUT), np.float32)
+    _check(abi.lib().pb_mlp_predict(w.ctypes.data, len(x), x.ctypes.data, y.ctypes.data))
+    return y
 
 
 def lu_decomp(a):

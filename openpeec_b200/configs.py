@@ -9,6 +9,10 @@ cfg3  batch of random thin-wire polylines: per instance numpy.random.default_rng
       20-400 segments random-walked in a 10 cm cube (steps 2-8 mm), radius 0.1-2 mm, port
       across a gap cut into the first segment; capacitance, retardation,
       64 log frequencies 50 MHz - 3 GHz
+cfg4  volume-cell bar stack for the compressed (H-matrix + GMRES) path: copper plate
+      40 x 40 mm, 0.2 mm thick, 96 x 96 grid x 4 layers (74,496 current cells), retardation,
+      32 log frequencies 1 MHz - 2 GHz, ACA tolerance 1e-6; fed across the diagonal
+      (node 1 at one corner, node 2 at the opposite one, as the compressed plate sample)
 Scaled-down variants of cfg2 (plate grid na x nb) serve the parity tests.
 """
 import numpy as np
@@ -73,3 +77,17 @@ def cfg3_instance(seed, i, nmin=20, nmax=400, nfreq=64):
         lines.append(f"wire = {f(pts[k])} {f(pts[k + 1])} {radius:.12g} 5.8e7 1")
     lines += ["port = 1 2 50", f"frequency = 5e7 3e9 {nfreq - 1} log", "end", ""]
     return "\n".join(lines)
+
+
+def cfg4(nx=96, ny=96, nz=4, nfreq=32, L=0.04, W=0.04, t=2e-4):
+    return f"""OpenPEEC 1 0
+title = bar stack {L * 1e3:g}x{W * 1e3:g} mm, {t * 1e3:g} mm thick, {nx}x{ny}x{nz} cells
+compression = 1 1e-6
+retardation = 1
+plate = 0 0 0  {L:.10g} 0 0  0 {W:.10g} 0  {t:.10g} 5.8e7 {nx} {ny} {nz}
+node = 1 0 0 0
+node = 2 {L:.10g} {W:.10g} 0
+port = 1 2 50
+frequency = 1e6 2e9 {nfreq - 1} log
+end
+"""

@@ -1,5 +1,6 @@
 // pb_api.cu — C entry points of the batched core (include/peec_b200.h).
 #include "pb_ctx.cuh"
+#include "pb_hmat.cuh"
 #include <algorithm>
 #include <cmath>
 #include <cstdarg>
@@ -372,6 +373,18 @@ int pb_sweep(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts *opts
     if (!c) { pb_set_error("pb_sweep: null context"); return PB_ERR_ARG; }
     PB_CUDA(cudaSetDevice(c->dev));
     return pb_sweep_impl(c, nfreq, freq, opts, zmat, segi, stats, nullptr, nullptr, nullptr);
+}
+
+int pb_pc_samples(pb_ctx *c, double freq, const pb_sweep_opts *opts, float *x, float *t)
+{
+    if (!c || !x || !t || !(freq > 0)) { pb_set_error("pb_pc_samples: bad argument"); return PB_ERR_ARG; }
+    PB_CUDA(cudaSetDevice(c->dev));
+    pb_sweep_opts o;
+    memset(&o, 0, sizeof(o));
+    if (opts) o = *opts;
+    else o.fill_prec = PB_PREC_MIXED;
+    pb_hstats hs;
+    return pb_sweep_compressed(c, 1, &freq, o, o.ctol > 0 ? o.ctol : 1e-6, 1e-10, nullptr, nullptr, &hs, x, t);
 }
 
 int pb_planewave(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts *opts,

@@ -37,5 +37,8 @@ struct pb_hstats {
 // block is filled on the device, compressed (ACA on the far blocks), the sparse part and
 // the preconditioner are built, and every port excitation is solved by matrix-free
 // right-preconditioned GMRES(60) to the relative residual tol.
+// With sample_x / sample_t (nfreq = 1) no system is solved: the features of every current
+// cell and the targets of the learned preconditioner correction are written instead.
 int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts &o,
-                        double ctol, double gtol, double *zmat, pb_sweep_stats *stats, pb_hstats *hs);
+                        double ctol, double gtol, double *zmat, pb_sweep_stats *stats, pb_hstats *hs,
+                        float *sample_x = nullptr, float *sample_t = nullptr);

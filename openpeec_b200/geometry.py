@@ -40,6 +40,7 @@ class PeecInput:
         self.gmin = 0.0
         self.maxid = 0
         self.planewave = None    # (theta_deg, phi_deg, pol, amp, phase_deg)
+        self.compress, self.ctol, self.accel = 0, 0.0, 0
         self.unsupported = []
 
 
@@ -121,8 +122,12 @@ def parse_peec(text):
             if pol not in (1, 2) or amp <= 0:
                 raise ValueError("planewave: polarisation 1/2 and amplitude > 0")
             p.planewave = (float(a[0]), float(a[1]), pol, amp, float(a[4]) if len(a) > 4 else 0.0)
-        elif key in ("quad", "disk", "dielectric", "mutual", "isource",
-                     "compression", "acceleration"):
+        elif key == "compression":         # compression = 1 [tol] (input_data.c, solve.c:251-294)
+            p.compress = int(a[0])
+            p.ctol = float(a[1]) if len(a) > 1 else 0.0
+        elif key == "acceleration":        # acceleration = 1 (solve.c:47-64)
+            p.accel = int(a[0])
+        elif key in ("quad", "disk", "dielectric", "mutual", "isource"):
             p.unsupported.append(key)
     return p
 
@@ -313,7 +318,8 @@ def build(p: PeecInput) -> Problem:
                    np.array(chgnode, dtype=np.int32), np.zeros(0), maxid, port, lump,
                    capacitance=p.capacitance, retardation=p.retardation, skin=p.skin,
                    gp=p.gp, gpz=p.gpz, gmin=p.gmin, f0=p.f0, f1=p.f1, nfreq=p.nfreq,
-                   flog=p.flog, title=p.title, planewave=p.planewave)
+                   flog=p.flog, title=p.title, planewave=p.planewave, compress=p.compress,
+                   ctol=p.ctol, accel=p.accel)
 
 
 def load_peec(path) -> Problem:
