@@ -387,6 +387,8 @@ def run_barstack(args):
                 z, st = ctx.sweep([f], pc_mlp=wts)
                 dt = time.perf_counter() - t0
                 out[tag].append({"f_hz": float(f), "s": dt, "gmres_its": st["gmres_its_max"],
+                                 "phases_ms": {"fill": st["t_corr_ms"], "compress": st["t_assemble_ms"],
+                                               "precond": st["t_lu_ms"], "gmres": st["t_refine_ms"]},
                                  "fallbacks": st["pc_mlp_fallbacks"], "zin": [float(z[0, 0, 0].real), float(z[0, 0, 0].imag)]})
         last = st
     tp = sum(r["s"] for r in out["plain"])

@@ -10,6 +10,7 @@
 // repeated sweeps of one structure do not reallocate their batch buffers.
 struct pb_cache_slot { void *p = nullptr; size_t cap = 0; };
 #define PB_CACHE_SLOTS 32
+#define PB_SLOT_COMP0  24     // slots [24, 32) hold the compressed path's dense kernel blocks
 
 // One additive contribution to an MNA entry whose value scales as val * {1, jw, -jw}.
 enum { ST_CONST = 0, ST_JW = 1, ST_MJW = 2 };
@@ -60,6 +61,9 @@ struct pb_ctx {
     pb_cache_slot cache[PB_CACHE_SLOTS];
     // correction samples (Lp, P) per quadrature-level signature, for the statistics
     std::map<std::vector<long>, std::pair<double, double>> sample_counts;
+    // compressed path: level signature whose static parts the held slots contain
+    std::vector<long> comp_sig;
+    bool comp_static_valid = false;
 
     long launches = 0;
 };

@@ -468,6 +468,28 @@ struct Dev {
     template <typename T> T *as() const { return (T *)p; }
 };
 
+// Device buffer held by a context slot across calls (grow-only)
+struct Held {
+    pb_cache_slot *s;
+    void *p = nullptr;
+    explicit Held(pb_cache_slot *slot) : s(slot) {}
+    int alloc(size_t b)
+    {
+        if (b == 0) b = 16;
+        if (s->cap < b) {
+            if (s->p) cudaFree(s->p);
+            s->p = nullptr;
+            s->cap = 0;
+            cudaError_t e = cudaMalloc(&s->p, b);
+            if (e != cudaSuccess) { s->p = nullptr; return pb_cuda_fail(e, "cudaMalloc", __FILE__, __LINE__); }
+            s->cap = b;
+        }
+        p = s->p;
+        return PB_OK;
+    }
+    template <typename T> T *as() const { return (T *)p; }
+};
+
 template <typename T> int upload(Dev &d, const std::vector<T> &v, cudaStream_t s)
 {
     PB_TRY(d.alloc(sizeof(T) * std::max<size_t>(1, v.size())));
@@ -903,12 +925,18 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
         PB_TRY(kb_setup(kbs[1], cpt.data(), st));
     }
 
-    Dev bK, bSt, bKP, bStP, bIg, bZint, bFreq, bX, bB, bR, bW, bZ, bVk, bDot, bU1;
+    // dense kernel blocks and their static parts stay with the context between calls; the
+    // static parts are valid while the quadrature-level signature does not change
+    pb_cache_slot *cs = c->cache + PB_SLOT_COMP0;
+    Held bK(cs + 0), bSt(cs + 1), bKP(cs + 2), bStP(cs + 3), bIg(cs + 4);
+    Dev bZint, bFreq, bX, bB, bR, bW, bZ, bVk, bDot, bU1;
+    const size_t stat_bytes = sizeof(double) * (size_t)ns * ns, statP_bytes = sizeof(double) * (size_t)nc * nc;
+    if (cs[1].cap < stat_bytes || (cap && cs[3].cap < statP_bytes)) c->comp_static_valid = false;
     PB_TRY(bK.alloc(sizeof(double2) * (size_t)ns * ns));
-    PB_TRY(bSt.alloc(sizeof(double) * (size_t)ns * ns));
+    PB_TRY(bSt.alloc(stat_bytes));
     if (cap) {
         PB_TRY(bKP.alloc(sizeof(double2) * (size_t)nc * nc));
-        PB_TRY(bStP.alloc(sizeof(double) * (size_t)nc * nc));
+        PB_TRY(bStP.alloc(statP_bytes));
         if (c->retardation) PB_TRY(bIg.alloc(sizeof(double2) * c->chg.size() * c->chg.size()));
     }
     PB_TRY(bZint.alloc(sizeof(double2) * (size_t)ns));
@@ -948,18 +976,34 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
         PB_CUDA(cudaMemcpyAsync(bFreq.p, &f, sizeof(double), cudaMemcpyHostToDevice, st));
         PB_TRY(pb_zint(c->g, c->skin, 1, bFreq.as<double>(), bZint.as<double2>(), st, &c->launches));
         if (ifr == 0 || c->retardation) {
-            PB_TRY(pb_lp_static(c->g, kw, bSt.as<double>(), st, &c->launches));
+            std::vector<long> sig;
+            level_signature(c, kw, sig);
+            sig.push_back(cap);
+            if (!c->comp_static_valid || sig != c->comp_sig) {
+                c->comp_static_valid = false;
+                PB_TRY(pb_lp_static(c->g, kw, bSt.as<double>(), st, &c->launches));
+                if (cap) PB_TRY(pb_pot_static(c->g, kw, bStP.as<double>(), st, &c->launches));
+                c->comp_sig = sig;
+                c->comp_static_valid = true;
+            }
             pb_epi_args ea;
             ea.out = bK.as<double2>();
             ea.out_stride = (long long)ns * ns;
             PB_TRY(pb_lp_corr(c->g, 1, &kw, fill32, bSt.as<double>(), PB_EPI_STORE, ea, st, &c->launches, nullptr));
             if (cap) {
-                PB_TRY(pb_pot_static(c->g, kw, bStP.as<double>(), st, &c->launches));
                 PB_TRY(pb_pot_corr(c->g, 1, &kw, fill32, bStP.as<double>(), bKP.as<double2>(), (long long)nc * nc,
                                    c->retardation ? bIg.as<double2>() : nullptr, st, &c->launches, nullptr));
             }
             if (kw > 0) {
-                PB_TRY(pb_count_samples(c->g, kw, &lp_samp, &p_samp, st));
+                sig.pop_back();
+                auto it = c->sample_counts.find(sig);
+                if (it == c->sample_counts.end()) {
+                    PB_TRY(pb_count_samples(c->g, kw, &lp_samp, &p_samp, st));
+                    c->sample_counts[sig] = std::make_pair(lp_samp, p_samp);
+                } else {
+                    lp_samp = it->second.first;
+                    p_samp = it->second.second;
+                }
                 samples += lp_samp + (cap ? p_samp : 0);
             }
         }

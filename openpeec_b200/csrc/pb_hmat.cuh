@@ -22,6 +22,10 @@ struct pb_htree {
     std::vector<int> leafid;                    // leaf clusters in perm order
 };
 
+// Quadrature-level signature of a wavenumber (pb_sweep.cu): equal signatures mean equal
+// static parts of the kernel blocks.
+void level_signature(const pb_ctx *c, double kw, std::vector<long> &sig);
+
 // Builds the tree over pts[3n] and splits the (root, root) block.
 void pb_htree_build(pb_htree &t, int n, const double *pts);
 

@@ -264,7 +264,7 @@ struct DevBuf {
 // Quadrature-level signature of a wavenumber: floor(kw * size) over the distinct cell
 // sizes that can be a pair's lmax (partial.c:166-173, 216-227). Equal signatures mean
 // every pair uses the same nsub, hence the same static part.
-static void level_signature(const pb_ctx *c, double kw, std::vector<long> &sig)
+void level_signature(const pb_ctx *c, double kw, std::vector<long> &sig)
 {
     sig.clear();
     sig.push_back(kw > 0 ? 1 : 0);
@@ -347,7 +347,7 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
     int B = o.batch;
     if (B <= 0) {
         double cached = 0;                       // storage this context already holds
-        for (const auto &slot : c->cache) cached += (double)slot.cap;
+        for (int q = 0; q < PB_SLOT_COMP0; q++) cached += (double)c->cache[q].cap;
         const double avail = 0.80 * ((double)fr + cached) - fixed - 256e6;
         B = (int)std::max(1.0, std::floor(avail / perf));
         B = std::min(B, 256);
