@@ -298,6 +298,7 @@ void pb_destroy(pb_ctx *c)
                     c->d_fe_st, c->d_cellnode};
     for (void *p : ptrs) if (p) cudaFree(p);
     for (auto &slot : c->cache) if (slot.p) cudaFree(slot.p);
+    if (c->comp_schur_reg) cudaHostUnregister(c->comp_schur_reg);
     pb_lu_engine_free(&c->lu);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;

@@ -1,5 +1,6 @@
 // pb_ctx.cuh — the opaque context behind pb_ctx* (include/peec_b200.h).
 #pragma once
+#include <complex>
 #include <map>
 #include <vector>
 #include "pb_common.cuh"
@@ -64,6 +65,10 @@ struct pb_ctx {
     // compressed path: level signature whose static parts the held slots contain
     std::vector<long> comp_sig;
     bool comp_static_valid = false;
+    // compressed path: host copy of the dense circuit Schur complement, page-locked once
+    // (cudaHostRegister) so that its per-frequency upload runs at full link speed
+    std::vector<std::complex<double>> comp_schur;
+    void *comp_schur_reg = nullptr;
 
     long launches = 0;
 };

@@ -16,6 +16,9 @@
 //     on the device,
 //   * matrix-free right-preconditioned GMRES(60) with true-residual restarts (gmres_hmat,
 //     iterative.c:285-354).
+#include <chrono>
+#include <thread>
+#include <cstdio>
 #include "pb_hmat.cuh"
 #include "pb_mlp.cuh"
 #include <algorithm>
@@ -414,28 +417,51 @@ __global__ void __launch_bounds__(1024) k_dotc(int n, const double2 *a, const do
 
 // ================================================================ device: preconditioner apply
 // z[idx] = D_r^-1 u[idx] for every leaf r (one thread per leaf; m <= PB_PC_MAXM)
-__global__ void k_leaf_solve(int nleaf, const int *lof, const int *lidx, const long long *dof, const double2 *dlu,
-                             const int *dpiv, const double2 *u, double2 *z)
+__global__ void __launch_bounds__(256) k_leaf_solve(int nleaf, const int *lof, const int *lidx, const long long *dof,
+                                                    const double2 *dlu, const int *dpiv, const double2 *u, double2 *z)
 {
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    // one warp per leaf: lane q holds rows q and q + 32 (PB_PC_MAXM = 64); the row
+    // interchanges run serially in shared memory, then column-oriented substitution with
+    // each solved entry broadcast by a shuffle (blk_dsolve, precond.c:394-404)
+    static_assert(PB_PC_MAXM <= 64, "two rows per lane");
+    __shared__ double2 cs[8][PB_PC_MAXM];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int r = blockIdx.x * 8 + w;
     if (r >= nleaf) return;
     const int m = lof[r + 1] - lof[r];
     const int *idx = lidx + lof[r];
     const double2 *a = dlu + dof[r];
     const int *piv = dpiv + lof[r];
-    double2 c[PB_PC_MAXM];
-    for (int q = 0; q < m; q++) c[q] = u[idx[q]];
-    for (int q = 0; q < m; q++) {                   // row interchanges (lu.c:68-96)
-        const int p = piv[q];
-        if (p != q) { const double2 t = c[q]; c[q] = c[p]; c[p] = t; }
+    double2 *c = cs[w];
+    for (int q = lane; q < m; q += 32) c[q] = u[idx[q]];
+    __syncwarp();
+    if (lane == 0)
+        for (int q = 0; q < m; q++) {               // row interchanges (lu.c:68-96)
+            const int p = piv[q];
+            if (p != q) { const double2 t = c[q]; c[q] = c[p]; c[p] = t; }
+        }
+    __syncwarp();
+    double2 v0 = lane < m ? c[lane] : make_double2(0, 0);
+    double2 v1 = lane + 32 < m ? c[lane + 32] : make_double2(0, 0);
+    for (int j = 0; j < m; j++) {                   // forward, unit lower
+        double2 xj = j >= 32 ? v1 : v0;
+        xj.x = __shfl_sync(0xffffffffu, xj.x, j & 31);
+        xj.y = __shfl_sync(0xffffffffu, xj.y, j & 31);
+        if (lane > j && lane < m) v0 = csub(v0, cmul(a[lane * m + j], xj));
+        if (lane + 32 > j && lane + 32 < m) v1 = csub(v1, cmul(a[(lane + 32) * m + j], xj));
     }
-    for (int i = 0; i < m; i++)
-        for (int j = 0; j < i; j++) c[i] = csub(c[i], cmul(a[i * m + j], c[j]));
-    for (int i = m - 1; i >= 0; i--) {
-        for (int j = i + 1; j < m; j++) c[i] = csub(c[i], cmul(a[i * m + j], c[j]));
-        c[i] = cdiv64(c[i], a[i * m + i]);
+    for (int j = m - 1; j >= 0; j--) {              // backward, upper with diagonal
+        const bool hi = j >= 32;
+        double2 xj = hi ? v1 : v0;
+        if (lane == (j & 31)) xj = cdiv64(xj, a[j * m + j]);
+        xj.x = __shfl_sync(0xffffffffu, xj.x, j & 31);
+        xj.y = __shfl_sync(0xffffffffu, xj.y, j & 31);
+        if (lane == (j & 31)) { if (hi) v1 = xj; else v0 = xj; }
+        if (lane < j) v0 = csub(v0, cmul(a[lane * m + j], xj));
+        if (lane + 32 < j) v1 = csub(v1, cmul(a[(lane + 32) * m + j], xj));
     }
-    for (int q = 0; q < m; q++) z[idx[q]] = c[q];
+    if (lane < m) z[idx[lane]] = v0;
+    if (lane + 32 < m) z[idx[lane + 32]] = v1;
 }
 
 // w[i] -= sum_e val[e] x[col[e]] over row i of a CSR matrix
@@ -467,6 +493,21 @@ struct Dev {
     }
     template <typename T> T *as() const { return (T *)p; }
 };
+
+// Zero a large host array with several threads (the circuit Schur complement is n1^2).
+void par_zero(std::vector<zc> &v)
+{
+    const size_t n = v.size();
+    const unsigned nt = n < (1u << 22) ? 1u : std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    if (nt == 1) { std::fill(v.begin(), v.end(), zc(0, 0)); return; }
+    std::vector<std::thread> th;
+    for (unsigned t = 0; t < nt; t++)
+        th.emplace_back([&v, n, nt, t]() {
+            const size_t a = n * t / nt, b = n * (t + 1) / nt;
+            std::fill(v.begin() + a, v.begin() + b, zc(0, 0));
+        });
+    for (auto &x : th) x.join();
+}
 
 // Device buffer held by a context slot across calls (grow-only)
 struct Held {
@@ -968,6 +1009,9 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
     double lp_samp = 0, p_samp = 0;
     const unsigned TB = 256;
 
+    struct CTrip { int i, j; zc v; };
+    std::vector<zc> &S = c->comp_schur;         // circuit Schur complement (host)
+    std::vector<CTrip> s11;                     // its circuit-only stamps
     for (int ifr = 0; ifr < nfreq; ifr++) {
         const double f = freq[ifr], om = 2 * PB_PI * f;
         const double kw = c->retardation ? om / PB_C0 : 0.0;
@@ -1024,6 +1068,14 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
         // ---- sparse part (mna_sparse, mna.c:317-325): stamps of the augmented system and
         // -Z_int on the segment diagonal, CSR in registration order
         tick();
+        auto hc0 = std::chrono::steady_clock::now();
+        auto mark = [&](const char *what) {         // host-clock sub-phases (verbose)
+            if (!o.verbose) return;
+            const auto t = std::chrono::steady_clock::now();
+            fprintf(stderr, "[compressed f=%.5g] %-14s %9.1f ms\n", f, what,
+                    std::chrono::duration<double, std::milli>(t - hc0).count());
+            hc0 = t;
+        };
         std::vector<zc> zint(ns);
         PB_CUDA(cudaMemcpyAsync(zint.data(), bZint.p, sizeof(double2) * ns, cudaMemcpyDeviceToHost, st));
         PB_CUDA(cudaStreamSynchronize(st));
@@ -1050,11 +1102,29 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
         PB_TRY(upload(bCol, col, st));
         PB_TRY(upload(bVal, val, st));
 
+        mark("sparse part");
         // ---- preconditioner (pc_build, precond.c:138-391)
         std::vector<int> ublk(N, -1), upos(N, -1);
         for (int b = 0; b < (int)kbs.size(); b++)
             for (int i = 0; i < kbs[b].n; i++) { ublk[kbs[b].off + i] = b; upos[kbs[b].off + i] = i; }
-        std::vector<zc> S((size_t)std::max(1, n1) * std::max(1, n1), zc(0, 0));
+        // dense Schur complement on the host, held (page-locked) by the context: first touch
+        // of a fresh n1^2 array and a pageable upload cost more than its assembly
+        const size_t n1sq = (size_t)std::max(1, n1) * std::max(1, n1);
+        if (S.size() != n1sq) {
+            if (c->comp_schur_reg) cudaHostUnregister(c->comp_schur_reg);
+            c->comp_schur_reg = nullptr;
+            S.assign(n1sq, zc(0, 0));
+            if (n1sq >= ((size_t)1 << 20)) {
+                if (cudaHostRegister(S.data(), sizeof(zc) * n1sq, cudaHostRegisterDefault) == cudaSuccess)
+                    c->comp_schur_reg = S.data();
+                else
+                    cudaGetLastError();             // stays pageable
+            }
+        } else {
+            par_zero(S);
+        }
+        mark("Schur zero");
+        s11.clear();
         for (auto &kb : kbs) {
             kb.bri.clear(); kb.bci.clear(); kb.bval.clear();
             kb.cri.clear(); kb.cci.clear(); kb.cval.clear();
@@ -1063,7 +1133,7 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
             for (int e = ro[i]; e < ro[i + 1]; e++) {
                 const int j = col[e];
                 const zc v = val[e];
-                if (i < n1 && j < n1) S[(size_t)i * n1 + j] += v;
+                if (i < n1 && j < n1) { S[(size_t)i * n1 + j] += v; s11.push_back({i, j, v}); }
                 else if (i < n1) { KBlock &kb = kbs[ublk[j]]; kb.bri.push_back(i); kb.bci.push_back(upos[j]); kb.bval.push_back(v); }
                 else if (j < n1) { KBlock &kb = kbs[ublk[i]]; kb.cri.push_back(upos[i]); kb.cci.push_back(j); kb.cval.push_back(v); }
                 else if (ublk[i] == ublk[j]) {
@@ -1075,14 +1145,16 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
                     }
                 }
             }
-        // plain leaf blocks and S11, kept for the fall back from the learned correction
-        const std::vector<zc> S11 = S;
+        mark("stamps split");
+        // plain leaf blocks (and the S11 entries above), kept for the fall back from the
+        // learned correction
         std::vector<std::vector<zc>> dplain(kbs.size());
         for (size_t b = 0; b < kbs.size(); b++) dplain[b] = kbs[b].dlu;
         if (sample_x) {                         // training samples instead of a solve
             PB_TRY(pc_samples(c, kbs[0], zint, om, bK.as<double2>(), sample_x, sample_t));
             return PB_OK;
         }
+        mark("Schur init");
         bool use_mlp = o.pc_mlp != nullptr;
         if (use_mlp) {
             PB_TRY(apply_mlp(c, kbs[0], zint, om, o.pc_mlp, use_mlp));
@@ -1090,9 +1162,10 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
         }
         auto restore_plain = [&]() {
             for (size_t b = 0; b < kbs.size(); b++) kbs[b].dlu = dplain[b];
-            S = S11;
+            par_zero(S);
+            for (const auto &t : s11) S[(size_t)t.i * n1 + t.j] += t.v;
         };
-        Dev slu, spiv, sperm, sinfo;
+        Dev slu, spiv, sperm, sinfo, sinv;
         auto build_pc = [&]() -> int {
             for (auto &kb : kbs)
                 for (int r = 0; r < kb.nl; r++) {
@@ -1102,6 +1175,7 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
                         return PB_ERR_SINGULAR;
                     }
                 }
+            mark("leaf LU");
             // Schur complement S = S11 - sum_b B_b D_b^-1 C_b, leaf by leaf (precond.c:275-364)
             for (auto &kb : kbs) {
                 const int nb = kb.n;
@@ -1185,8 +1259,11 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
                 PB_TRY(upload(kb.ccol, ccol2, st));
                 PB_TRY(upload(kb.cv, cval2, st));
             }
+            mark("Schur assembly");
             if (n1 > 0) {
                 PB_TRY(upload(slu, S, st));
+                if (o.verbose) PB_CUDA(cudaStreamSynchronize(st));
+                mark("Schur upload");
                 PB_TRY(spiv.alloc(sizeof(int) * n1));
                 PB_TRY(sperm.alloc(sizeof(int) * n1));
                 PB_TRY(sinfo.alloc(sizeof(int)));
@@ -1201,6 +1278,12 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
                     return PB_ERR_SINGULAR;
                 }
             }
+            // above PB_SCHUR_INV circuit unknowns the explicit inverse: every GMRES step then
+            // applies it as one bandwidth-bound product instead of two sequential substitutions
+            if (n1 > PB_SCHUR_INV) PB_TRY(sinv.alloc(sizeof(double2) * (size_t)n1 * n1));
+            if (n1 > PB_SCHUR_INV) PB_TRY(pb_lu_inverse(&c->lu, n1, slu.as<double2>(), n1, sperm.as<int>(), sinv.as<double2>()));
+            if (o.verbose) PB_CUDA(cudaStreamSynchronize(st));
+            mark("Schur LU");
             return PB_OK;
         };
         {
@@ -1217,6 +1300,17 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
 
         // ---- operators on device vectors
         const unsigned gN = ceil_div(N, TB);
+        // verbose >= 2: device time of the operators inside GMRES (synchronising)
+        double t_opM = 0, t_opA = 0, t_leaf = 0, t_schur = 0;
+        auto timed = [&](double &acc, const auto &fn) -> int {
+            if (o.verbose < 2) return fn();
+            PB_CUDA(cudaStreamSynchronize(st));
+            const auto t0 = std::chrono::steady_clock::now();
+            const int r = fn();
+            PB_CUDA(cudaStreamSynchronize(st));
+            acc += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+            return r;
+        };
         auto opA = [&](const double2 *x, double2 *y) -> int {   // mna_apply (mna.c:347-364)
             k_spmv<<<gN, TB, 0, st>>>(N, bRo.as<int>(), bCol.as<int>(), bVal.as<double2>(), x, y);
             c->launches++;
@@ -1226,7 +1320,7 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
         auto opM = [&](double2 *z) -> int {                     // pc_apply (precond.c:407-435)
             if (n1 > 0) PB_CUDA(cudaMemcpyAsync(bU1.p, z, sizeof(double2) * n1, cudaMemcpyDeviceToDevice, st));
             for (auto &kb : kbs) {
-                k_leaf_solve<<<ceil_div(kb.nl, 64), 64, 0, st>>>(kb.nl, kb.lof_d.as<int>(), kb.lidx_d.as<int>(),
+                k_leaf_solve<<<ceil_div(kb.nl, 8), 256, 0, st>>>(kb.nl, kb.lof_d.as<int>(), kb.lidx_d.as<int>(),
                                                                 kb.dof_d.as<long long>(), kb.dlu_d.as<double2>(),
                                                                 kb.dpiv_d.as<int>(), z + kb.off, kb.wb.as<double2>());
                 if (n1 > 0)
@@ -1235,14 +1329,17 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
                 c->launches += 2;
             }
             if (n1 > 0)
-                PB_TRY(pb_lu_solve_batched<double>(&c->lu, n1, 1, 1, slu.as<double2>(), n1, (long)n1 * n1,
-                                                   sperm.as<int>(), bU1.as<double2>(), z));
+                PB_TRY(timed(t_schur, [&]() {
+                    return n1 > PB_SCHUR_INV ? pb_gemv(&c->lu, n1, sinv.as<double2>(), bU1.as<double2>(), z)
+                                             : pb_lu_solve_batched<double>(&c->lu, n1, 1, 1, slu.as<double2>(), n1,
+                                                                           (long)n1 * n1, sperm.as<int>(), bU1.as<double2>(), z);
+                }));
             for (auto &kb : kbs) {
                 PB_CUDA(cudaMemcpyAsync(kb.ub.p, z + kb.off, sizeof(double2) * kb.n, cudaMemcpyDeviceToDevice, st));
                 if (n1 > 0)
                     k_csr_sub<<<ceil_div(kb.n, TB), TB, 0, st>>>(kb.n, kb.cro.as<int>(), kb.ccol.as<int>(),
                                                                  kb.cv.as<double2>(), z, kb.ub.as<double2>());
-                k_leaf_solve<<<ceil_div(kb.nl, 64), 64, 0, st>>>(kb.nl, kb.lof_d.as<int>(), kb.lidx_d.as<int>(),
+                k_leaf_solve<<<ceil_div(kb.nl, 8), 256, 0, st>>>(kb.nl, kb.lof_d.as<int>(), kb.lidx_d.as<int>(),
                                                                 kb.dof_d.as<long long>(), kb.dlu_d.as<double2>(),
                                                                 kb.dpiv_d.as<int>(), kb.ub.as<double2>(), z + kb.off);
                 c->launches += 2;
@@ -1295,8 +1392,8 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
                 int iters = -1, jj = 0;
                 for (jj = 0; jj < m; jj++) {
                     PB_CUDA(cudaMemcpyAsync(bZ.p, Vk + (long long)jj * N, sizeof(double2) * N, cudaMemcpyDeviceToDevice, st));
-                    PB_TRY(opM(bZ.as<double2>()));
-                    PB_TRY(opA(bZ.as<double2>(), bW.as<double2>()));
+                    PB_TRY(timed(t_opM, [&]() { return opM(bZ.as<double2>()); }));
+                    PB_TRY(timed(t_opA, [&]() { return opA(bZ.as<double2>(), bW.as<double2>()); }));
                     for (int i = 0; i <= jj; i++) {
                         zc hij;
                         PB_TRY(dot(Vk + (long long)i * N, bW.as<double2>(), hij));
@@ -1378,6 +1475,10 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
             }
         }
         tock(t_gm);
+        mark("GMRES");
+        if (o.verbose >= 2)
+            fprintf(stderr, "[compressed f=%.5g] GMRES: preconditioner %.1f ms (Schur solves %.1f ms), matvec %.1f ms, %d its\n",
+                    f, t_opM, t_schur, t_opA, gm_max);
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

@@ -9,6 +9,7 @@
 #define PB_HM_MAXIT 200     // largest ACA rank before a block is kept dense (hmatrix.c:39)
 #define PB_HM_PROBE 4       // restarts from unrepresented rows (hmatrix.c:40)
 #define PB_PC_MAXM  64      // largest leaf the preconditioner factorises (precond.c:41)
+#define PB_SCHUR_INV 1024   // circuit Schur complements above this order are applied as an explicit inverse
 
 // Cluster tree and block partition (built on the host: ct_build / hm_split,
 // hmatrix.c:91-227) plus the per-leaf block lists of the matrix-vector product.

@@ -583,6 +583,63 @@ template int pb_lu_solve_mapped<double>(pb_lu_engine *, int, int, int, const dou
 template int pb_lu_solve_batched<float>(pb_lu_engine *, int, int, int, const float2 *, int, long, const int *, const double2 *, double2 *);
 template int pb_lu_solve_batched<double>(pb_lu_engine *, int, int, int, const double2 *, int, long, const int *, const double2 *, double2 *);
 
+// ---------------------------------------------------------------- explicit inverse
+// For one FP64 system whose factors serve many solves (the circuit Schur complement of the
+// compressed path's preconditioner) the explicit inverse turns every later solve into one
+// bandwidth-bound matrix-vector product. A^-1 = U^-1 L^-1 P: X starts as P (X[i][perm[i]]
+// = 1) and two cuBLAS triangular solves with n right-hand sides apply L^-1 and U^-1. The
+// factors are row-major, which cuBLAS (column-major) sees transposed: L Y = P becomes
+// Y^T L^T = P^T (right side, upper, unit) and U X = Y becomes X^T U^T = Y^T (right side,
+// lower); the row-major buffer then holds X.
+__global__ void k_inv_init(int n, const int *perm, double2 *X)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) X[(long long)i * n + perm[i]] = make_double2(1, 0);
+}
+
+int pb_lu_inverse(pb_lu_engine *e, int n, const double2 *lu, int ld, const int *perm, double2 *X)
+{
+    if (n <= 0) return PB_OK;
+    PB_CUDA(cudaMemsetAsync(X, 0, sizeof(double2) * (size_t)n * n, e->stream));
+    k_inv_init<<<ceil_div(n, 256), 256, 0, e->stream>>>(n, perm, X);
+    PB_CHECK_LAUNCH();
+    const cuDoubleComplex one = make_cuDoubleComplex(1, 0);
+    cublasStatus_t s = cublasZtrsm(e->blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_UNIT,
+                                   n, n, &one, (const cuDoubleComplex *)lu, ld, (cuDoubleComplex *)X, n);
+    if (s == CUBLAS_STATUS_SUCCESS)
+        s = cublasZtrsm(e->blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, n, n,
+                        &one, (const cuDoubleComplex *)lu, ld, (cuDoubleComplex *)X, n);
+    e->launches += 3;
+    if (s != CUBLAS_STATUS_SUCCESS) { pb_set_error("triangular solve for the inverse failed (%d)", (int)s); return PB_ERR_CUDA; }
+    return PB_OK;
+}
+
+// y = X r, X row-major n x n: one warp per row (coalesced row reads, r from L2)
+__global__ void __launch_bounds__(256) k_gemv_rm(int n, const double2 *__restrict__ X, const double2 *__restrict__ r,
+                                                 double2 *__restrict__ y)
+{
+    const int i = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (i >= n) return;
+    const double2 *row = X + (long long)i * n;
+    double2 acc = make_double2(0, 0);
+    for (int c = lane; c < n; c += 32) acc = cadd(acc, cmul(row[c], r[c]));
+    for (int o = 16; o > 0; o >>= 1) {
+        acc.x += __shfl_down_sync(0xffffffffu, acc.x, o);
+        acc.y += __shfl_down_sync(0xffffffffu, acc.y, o);
+    }
+    if (lane == 0) y[i] = acc;
+}
+
+int pb_gemv(pb_lu_engine *e, int n, const double2 *X, const double2 *r, double2 *y)
+{
+    if (n <= 0) return PB_OK;
+    if ((const void *)r == (const void *)y) { pb_set_error("pb_gemv: r and y must differ"); return PB_ERR_ARG; }
+    k_gemv_rm<<<ceil_div(n, 8), 256, 0, e->stream>>>(n, X, r, y);
+    e->launches++;
+    PB_CHECK_LAUNCH();
+    return PB_OK;
+}
+
 // ---------------------------------------------------------------- FP64 residual
 // r = b - A x ; 8 warps per block, each warp one row at a time; x staged in smem.
 __device__ __forceinline__ void atomic_max_pos(double *addr, double v)

@@ -47,6 +47,12 @@ int pb_lu_solve_batched(pb_lu_engine *e, int n, int nb, int nrhs,
                         const typename cplx_t<TF>::type *lu, int ld, long stride,
                         const int *perm, const double2 *r, double2 *x);
 
+// Explicit inverse X = A^-1 (row-major n x n, device) of one FP64 system from its factors
+// (pb_lu_factor / pb_lu_perm), for a matrix whose factors serve many solves.
+int pb_lu_inverse(pb_lu_engine *e, int n, const double2 *lu, int ld, const int *perm, double2 *X);
+// y = X r for a row-major n x n FP64 complex X (r and y must not alias).
+int pb_gemv(pb_lu_engine *e, int n, const double2 *X, const double2 *r, double2 *y);
+
 // Same with an indirection: CTA row y solves system sys[y] (vector slot, nullptr = y)
 // with the factors of matrix lu_of[system] (nullptr = the system itself).
 template <typename TF>

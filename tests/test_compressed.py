@@ -76,3 +76,19 @@ def test_compressed_capacitive_exact_at_small_scale(golden):
         zd, _ = ctx.sweep(fx["freqs"], fill_prec=abi.PREC_FP64, lu=abi.LU_FP64)
     assert st["hmat_far"] == 0
     assert np.all(rel(zc, zd) <= 1e-9), rel(zc, zd)
+
+
+def test_compressed_large_circuit_schur():
+    """A sheet with more than 1024 circuit unknowns (32 x 32 x 1: 1089 nodes) applies the
+    circuit Schur complement as an explicit inverse (one matrix-vector product per GMRES
+    step). GMRES must converge in the first cycle as with the substitution, and Z must agree
+    with the dense sweep of the same structure within the compression error (ACA tolerance
+    1e-6)."""
+    from openpeec_b200 import abi, api, configs, geometry
+    prob = geometry.build(geometry.parse_peec(configs.cfg4(32, 32, 1, 2)))
+    with api.Context(prob) as ctx:
+        assert ctx.nnode > 1024
+        zc, st = ctx.sweep([1e6, 1e9], fill_prec=abi.PREC_FP64, compress=1)
+        zd, _ = ctx.sweep([1e6, 1e9], fill_prec=abi.PREC_FP64, lu=abi.LU_FP64, compress=0)
+    assert 0 < st["gmres_its_max"] <= 60, st["gmres_its_max"]
+    assert np.all(rel(zc, zd) <= 1e-4), rel(zc, zd)
