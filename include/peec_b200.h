@@ -219,6 +219,25 @@ int  pb_planewave(pb_ctx *ctx, int nfreq, const double *freq, const pb_sweep_opt
                   const pb_planewave_t *pw, double *voc, double *segipw, pb_sweep_stats *stats);
 
 /*
+ * Independent sources (reference src_t, include/peec.h:43; vsource / isource keys,
+ * src/input_data.c:175-192). isvsrc = 1: voltage source amp at phase_deg; the k-th
+ * voltage source is the k-th PB_LUMP_V element of the problem (its branch row, mna.c:77).
+ * isvsrc = 0: current source, the current flowing inside the source from n1 to n2 (the
+ * SPICE convention of mna_rhs_sources, src/mna.c:470-489).
+ */
+typedef struct { int n1, n2, isvsrc, pad_; double amp, phase_deg; } pb_source_t;
+
+/*
+ * The extra solve of solve.c:392-396: the right-hand side of mna_rhs_sources
+ * (src/mna.c:471-489) through the dense full-form MNA at every frequency. vnode
+ * [nfreq][maxid+1] complex gets the node voltages print_vnode reports
+ * (src/solve.c:102-112): x[nodemap[id]], 0 for the reference node and for ids without a
+ * matrix row. Not built for the compressed path (PB_ERR_UNSUP).
+ */
+int  pb_sources(pb_ctx *ctx, int nfreq, const double *freq, const pb_sweep_opts *opts, int nsrc,
+                const pb_source_t *src, double *vnode, pb_sweep_stats *stats);
+
+/*
  * Dense complex LU with partial pivoting on a host matrix, executed on the GPU
  * (reference lu_decomp, src/lu.c:16-66): row-major a[n*n] complex is replaced by L\U,
  * piv[k] = row swapped with row k at step k. Returns -1 on success or the 0-based row of

@@ -87,6 +87,12 @@ class PbPlanewave(C.Structure):
                 ("pad_", C.c_int), ("amp", C.c_double), ("phase_deg", C.c_double)]
 
 
+class PbSource(C.Structure):
+    """pb_source_t (include/peec_b200.h)."""
+    _fields_ = [("n1", C.c_int), ("n2", C.c_int), ("isvsrc", C.c_int), ("pad_", C.c_int),
+                ("amp", C.c_double), ("phase_deg", C.c_double)]
+
+
 def ptr(a):
     """Address of a contiguous numpy array (None for None / empty)."""
     if a is None or a.size == 0:
@@ -141,6 +147,8 @@ def lib():
     L.pb_fp32_peak.argtypes = [C.POINTER(C.c_double)]
     L.pb_lp_fill_noalloc.argtypes = [C.c_int, _vp, C.c_int, C.c_double, C.c_double, C.c_int, _vp]
     L.pb_device_sync.restype = C.c_int
+    L.pb_sources.argtypes = [_vp, C.c_int, _vp, C.POINTER(PbSweepOpts), C.c_int, _vp, _vp,
+                             C.POINTER(PbSweepStats)]
     L.pb_mlp_nparam.restype = C.c_int
     L.pb_pc_samples.argtypes = [_vp, C.c_double, C.POINTER(PbSweepOpts), _vp, _vp]
     L.pb_mlp_train.argtypes = [_vp, C.c_int, _vp, _vp, C.c_int, C.c_float, _vp]

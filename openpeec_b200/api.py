@@ -111,6 +111,22 @@ class Context:
         return voc, st.as_dict()
 
 
+    def sources(self, freqs, sources=None, fill_prec=abi.PREC_MIXED, lu=abi.LU_TC, batch=0):
+        """Independent-source excitation (pb_sources): node voltages [nfreq, maxid+1] as
+        the reference's print_vnode reports them, and the stats. sources: (isvsrc, n1, n2,
+        amp, phase_deg) tuples; None takes the problem's own vsource/isource list."""
+        src = self.prob.sources if sources is None else sources
+        arr = (abi.PbSource * len(src))(*[abi.PbSource(int(n1), int(n2), int(v), 0, float(a), float(ph))
+                                          for v, n1, n2, a, ph in src])
+        freqs = np.ascontiguousarray(freqs, np.float64)
+        vn = np.zeros((len(freqs), self.prob.maxid + 1), np.complex128)
+        o = abi.PbSweepOpts(int(fill_prec), int(lu), int(abi.FORM_FULL), int(batch), 0.0, 0, 0, 0, 0, 0, 0, 0.0,
+                            None)
+        st = abi.PbSweepStats()
+        _check(abi.lib().pb_sources(self.h, len(freqs), freqs.ctypes.data, C.byref(o), len(src),
+                                    C.cast(arr, C.c_void_p), vn.ctypes.data, C.byref(st)))
+        return vn, st.as_dict()
+
     def pc_samples(self, freq, fill_prec=abi.PREC_MIXED, ctol=0.0):
         """Training samples of the learned preconditioner correction at one frequency:
         (features [nseg, 12], targets [nseg, 2]) (pb_pc_samples)."""

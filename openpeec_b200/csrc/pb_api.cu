@@ -28,7 +28,8 @@ int pb_cuda_fail(cudaError_t e, const char *what, const char *file, int line)
 
 int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts *opts,
                   double *zmat, double *segi, pb_sweep_stats *stats,
-                  const pb_planewave_t *pw, double *voc, double *segipw);
+                  const pb_planewave_t *pw, double *voc, double *segipw,
+                  const double *rhs_fixed = nullptr, double *vnode = nullptr);
 
 extern "C" const char *pb_last_error(void) { return g_err.c_str(); }
 
@@ -396,6 +397,52 @@ int pb_planewave(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts *
     if (!(pw->amp > 0)) { pb_set_error("pb_planewave: amplitude must be > 0"); return PB_ERR_ARG; }
     PB_CUDA(cudaSetDevice(c->dev));
     return pb_sweep_impl(c, nfreq, freq, opts, nullptr, nullptr, stats, pw, voc, segipw);
+}
+
+int pb_sources(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts *opts, int nsrc,
+               const pb_source_t *src, double *vnode, pb_sweep_stats *stats)
+{
+    if (!c || nsrc <= 0 || !src || !vnode) { pb_set_error("pb_sources: bad argument"); return PB_ERR_ARG; }
+    PB_CUDA(cudaSetDevice(c->dev));
+    pb_sweep_opts o;
+    memset(&o, 0, sizeof(o));
+    if (opts) o = *opts;
+    else { o.fill_prec = PB_PREC_MIXED; o.lu = PB_LU_TC; }
+    if (o.compress) { pb_set_error("pb_sources: not built for the compressed path"); return PB_ERR_UNSUP; }
+    if (o.form == PB_FORM_REDUCED) { pb_set_error("pb_sources: node voltages need the full MNA form"); return PB_ERR_ARG; }
+    o.form = PB_FORM_FULL;
+    // right-hand side of mna_rhs_sources (src/mna.c:471-489), frequency independent
+    std::vector<int> vl;
+    for (size_t i = 0; i < c->lump.size(); i++)
+        if (c->lump[i].kind == PB_LUMP_V) vl.push_back((int)i);
+    std::vector<double> b(2 * (size_t)c->nfull, 0.0);
+    size_t nv = 0;
+    for (int k = 0; k < nsrc; k++) {
+        const pb_source_t &e = src[k];
+        if (e.n1 < 0 || e.n2 < 0 || e.n1 > c->maxid || e.n2 > c->maxid) {
+            pb_set_error("pb_sources: source %d has a node outside 0..%d", k, c->maxid);
+            return PB_ERR_ARG;
+        }
+        const double ph = e.phase_deg * PB_PI / 180, vr = e.amp * cos(ph), vi = e.amp * sin(ph);
+        if (e.isvsrc) {
+            if (nv >= vl.size() || c->lump[vl[nv]].n1 != e.n1 || c->lump[vl[nv]].n2 != e.n2) {
+                pb_set_error("pb_sources: voltage source %d is not the %zu-th PB_LUMP_V element of the problem", k, nv);
+                return PB_ERR_ARG;
+            }
+            const size_t r = (size_t)(c->offV + nv++);
+            b[2 * r] = vr;
+            b[2 * r + 1] = vi;
+        } else {
+            const int i1 = c->nodemap[e.n1], i2 = c->nodemap[e.n2];
+            if (i1 >= 0) { b[2 * (size_t)i1] -= vr; b[2 * (size_t)i1 + 1] -= vi; }
+            if (i2 >= 0) { b[2 * (size_t)i2] += vr; b[2 * (size_t)i2 + 1] += vi; }
+        }
+    }
+    if (nv != vl.size()) {
+        pb_set_error("pb_sources: %zu voltage sources for %zu PB_LUMP_V elements", nv, vl.size());
+        return PB_ERR_ARG;
+    }
+    return pb_sweep_impl(c, nfreq, freq, &o, nullptr, nullptr, stats, nullptr, nullptr, nullptr, b.data(), vnode);
 }
 
 // ---------------------------------------------------------------- dense LU entry points

@@ -651,7 +651,7 @@ __device__ __forceinline__ void atomic_max_pos(double *addr, double v)
 __global__ void __launch_bounds__(256)
 k_residual(const double2 *a, int n, int ld, long long stride, const double2 *bv,
            const double2 *xv, double2 *rv, double *rn, double *bn, double *xn, double *an,
-           int nrhs, int rows_per_block, const int *sys)
+           int nrhs, int rows_per_block, const int *sys, double *cw)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     double2 *xs = reinterpret_cast<double2 *>(smraw);     // [nrhs][n]
@@ -678,16 +678,18 @@ k_residual(const double2 *a, int n, int ld, long long stride, const double2 *bv,
             if (lane == 0) atomic_max_pos(&an[b], sa);
         }
         for (int q = 0; q < nrhs; q++) {
-            double sr = 0, si = 0;
+            double sr = 0, si = 0, sa = 0;
             const double2 *x = xs + q * n;
             for (int c = lane; c < n; c += 32) {
                 const double2 av = row[c], xx = x[c];
                 sr += av.x * xx.x - av.y * xx.y;
                 si += av.x * xx.y + av.y * xx.x;
+                if (cw) sa += (fabs(av.x) + fabs(av.y)) * (fabs(xx.x) + fabs(xx.y));
             }
             for (int o = 16; o > 0; o >>= 1) {
                 sr += __shfl_down_sync(0xffffffffu, sr, o);
                 si += __shfl_down_sync(0xffffffffu, si, o);
+                if (cw) sa += __shfl_down_sync(0xffffffffu, sa, o);
             }
             if (lane == 0) {
                 const long long idx = ((long long)b * nrhs + q) * n + r;
@@ -697,6 +699,10 @@ k_residual(const double2 *a, int n, int ld, long long stride, const double2 *bv,
                     rv[idx] = res;
                     atomic_max_pos(&rn[b * nrhs + q], fmax(fabs(res.x), fabs(res.y)));
                     atomic_max_pos(&bn[b * nrhs + q], fmax(fabs(bb.x), fabs(bb.y)));
+                    if (cw) {                                // componentwise (Oettli-Prager)
+                        const double num = fabs(res.x) + fabs(res.y), den = sa + fabs(bb.x) + fabs(bb.y);
+                        atomic_max_pos(&cw[b * nrhs + q], den > 0 ? num / den : (num > 0 ? 1.0 : 0.0));
+                    }
                 } else {
                     rv[idx] = make_double2(sr, si);          // product only: r = A x
                 }
@@ -707,9 +713,10 @@ k_residual(const double2 *a, int n, int ld, long long stride, const double2 *bv,
 
 int pb_residual(pb_lu_engine *e, int n, int nb, int nrhs, const double2 *a, int ld, long stride,
                 const double2 *b, const double2 *x, double2 *r, double *rn, double *bn, double *xn,
-                double *an)
+                double *an, double *cw)
 {
     PB_CUDA(cudaMemsetAsync(rn, 0, sizeof(double) * nb * nrhs, e->stream));
+    if (cw) PB_CUDA(cudaMemsetAsync(cw, 0, sizeof(double) * nb * nrhs, e->stream));
     PB_CUDA(cudaMemsetAsync(bn, 0, sizeof(double) * nb * nrhs, e->stream));
     if (an) PB_CUDA(cudaMemsetAsync(an, 0, sizeof(double) * nb, e->stream));
     const size_t smem = (size_t)nrhs * n * sizeof(double2);
@@ -723,7 +730,7 @@ int pb_residual(pb_lu_engine *e, int n, int nb, int nrhs, const double2 *a, int 
     }
     const int rpb = 64;
     dim3 g(ceil_div(n, rpb), nb);
-    k_residual<<<g, 256, smem, e->stream>>>(a, n, ld, stride, b, x, r, rn, bn, xn, an, nrhs, rpb, nullptr);
+    k_residual<<<g, 256, smem, e->stream>>>(a, n, ld, stride, b, x, r, rn, bn, xn, an, nrhs, rpb, nullptr, cw);
     e->launches++;
     PB_CHECK_LAUNCH();
     return PB_OK;
@@ -748,7 +755,7 @@ int pb_residual_mapped(pb_lu_engine *e, int n, int nb, int nrhs, const double2 *
     }
     const int rpb = 64;
     dim3 g(ceil_div(n, rpb), nb);
-    k_residual<<<g, 256, smem, e->stream>>>(a, n, ld, stride, b, x, r, rn, bn, xn, an, nrhs, rpb, sys);
+    k_residual<<<g, 256, smem, e->stream>>>(a, n, ld, stride, b, x, r, rn, bn, xn, an, nrhs, rpb, sys, nullptr);
     e->launches++;
     PB_CHECK_LAUNCH();
     return PB_OK;
@@ -770,7 +777,7 @@ int pb_matvec_mapped(pb_lu_engine *e, int n, int nb, int nrhs, const double2 *a,
     const int rpb = 64;
     dim3 g(ceil_div(n, rpb), nb);
     k_residual<<<g, 256, smem, e->stream>>>(a, n, ld, stride, nullptr, x, y, nullptr, nullptr, nullptr,
-                                            nullptr, nrhs, rpb, sys);
+                                            nullptr, nrhs, rpb, sys, nullptr);
     e->launches++;
     PB_CHECK_LAUNCH();
     return PB_OK;

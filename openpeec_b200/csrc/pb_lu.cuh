@@ -73,7 +73,9 @@ int pb_matvec_mapped(pb_lu_engine *e, int n, int nb, int nrhs, const double2 *a,
 
 // r = b - A x for nb FP64 matrices, nrhs vectors each; also writes the infinity norms
 // (max |re|,|im| component) of r, b and x per vector into rn, bn, xn [nb*nrhs] and,
-// when an != nullptr, the infinity norm of each matrix (max row sum of |re|+|im|).
+// when an != nullptr, the infinity norm of each matrix (max row sum of |re|+|im|); when
+// cw != nullptr, the componentwise backward error max_i |r_i| / (|A||x| + |b|)_i per vector
+// (Oettli-Prager, with |z| measured as |re|+|im|).
 int pb_residual(pb_lu_engine *e, int n, int nb, int nrhs, const double2 *a, int ld,
                 long stride, const double2 *b, const double2 *x, double2 *r, double *rn,
-                double *bn, double *xn, double *an);
+                double *bn, double *xn, double *an, double *cw = nullptr);

@@ -159,6 +159,13 @@ __global__ void k_rhs_full(int nb, int np, int n, const int *pm, double2 *rhs)
     rhs[idx] = make_double2(v, 0);
 }
 
+// one frequency-independent right-hand side for every system of the batch
+__global__ void k_rhs_copy(int nb, int n, const double2 *b, double2 *rhs)
+{
+    const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (idx < (long long)nb * n) rhs[idx] = b[idx % n];
+}
+
 __global__ void k_z_full(int nb, int np, int nx, int n, const int *pm, const double2 *x, double2 *z)
 {
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
@@ -299,7 +306,8 @@ struct PhaseTimer {
 
 int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts *opts_in,
                   double *zmat, double *segi, pb_sweep_stats *stats,
-                  const pb_planewave_t *pw, double *voc, double *segipw)
+                  const pb_planewave_t *pw, double *voc, double *segipw,
+                  const double *rhs_fixed, double *vnode)
 {
     pb_sweep_opts o;
     if (opts_in) o = *opts_in;
@@ -308,6 +316,7 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
            o.compress = 0; o.pad_ = 0; o.ctol = 0; }
     if (o.compress) {
         if (pw) { pb_set_error("plane-wave excitation is not built for the compressed path"); return PB_ERR_UNSUP; }
+        if (rhs_fixed) { pb_set_error("source excitation is not built for the compressed path"); return PB_ERR_UNSUP; }
         if (nfreq <= 0 || freq == nullptr) { pb_set_error("pb_sweep: no frequencies"); return PB_ERR_ARG; }
         pb_hstats hs;
         return pb_sweep_compressed(c, nfreq, freq, o, o.ctol > 0 ? o.ctol : 1e-6,
@@ -330,7 +339,8 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
     const long launches0 = c->launches + c->lu.launches;
 
     const int ns = (int)c->seg.size(), nc = c->ncell, np = (int)c->port.size();
-    const int nr = pw ? 1 : np;                  // right-hand sides per frequency
+    if (rhs_fixed && form != PB_FORM_FULL) { pb_set_error("source excitation needs the full MNA form"); return PB_ERR_ARG; }
+    const int nr = (pw || rhs_fixed) ? 1 : np;   // right-hand sides per frequency
     const int n = (form == PB_FORM_REDUCED) ? ns : c->nfull;
     const cudaStream_t st = c->stream;
     if (n <= 0) { pb_set_error("pb_sweep: empty system"); return PB_ERR_ARG; }
@@ -391,6 +401,8 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
     PB_TRY(bAn.alloc((size_t)B * 8));
     PB_TRY(bRn.alloc((size_t)B * nr * 8));
     PB_TRY(bBn.alloc((size_t)B * nr * 8));
+    DevBuf bCw(cs + 23);                          // componentwise backward errors (full form)
+    PB_TRY(bCw.alloc((size_t)B * nr * 8));
     PB_TRY(bFreq.alloc((size_t)B * 8));
     PB_TRY(bZ.alloc((size_t)B * np * nr * 16 + 16));
     PB_TRY(bPC.alloc((size_t)2 * (np + 1) * 4));
@@ -410,6 +422,11 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
     pc.push_back(-1);                            // plane wave: no current injection
     pc.push_back(-1);
     PB_CUDA(cudaMemcpyAsync(bPC.p, pc.data(), sizeof(int) * 2 * (np + 1), cudaMemcpyHostToDevice, st));
+    DevBuf bFix;                                  // the source right-hand side (pb_sources)
+    if (rhs_fixed) {
+        PB_TRY(bFix.alloc(sizeof(double2) * (size_t)n));
+        PB_CUDA(cudaMemcpyAsync(bFix.p, rhs_fixed, sizeof(double2) * (size_t)n, cudaMemcpyHostToDevice, st));
+    }
     PwArgs pwa;
     if (pw) {
         if (pw->pol != 1 && pw->pol != 2) { pb_set_error("pb_planewave: polarisation must be 1 or 2"); return PB_ERR_ARG; }
@@ -579,7 +596,9 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
         // right-hand sides
         tRef.start(st);
         const long long nv = (long long)nb * nr * n;
-        if (pw) {
+        if (rhs_fixed) {
+            k_rhs_copy<<<ceil_div(nv, 256), 256, 0, st>>>(nb, n, bFix.as<double2>(), bRhs.as<double2>());
+        } else if (pw) {
             k_rhs_planewave<<<ceil_div(nv, 256), 256, 0, st>>>(nb, n, ns, form == PB_FORM_REDUCED, c->offS,
                                                                c->g.seg.cell, bFreq.as<double>(), c->gp, c->gpz,
                                                                pwa, bRhs.as<double2>());
@@ -667,8 +686,12 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
             // Iterative refinement in FP64 against the FP64 matrix:
             //   x_0 = LU^-1 b,  r = b - A x,  x += LU^-1 r,
             // until the normwise backward error eta = |r| / (|A| |x| + |b|) (infinity norms)
-            // reaches the level of an FP64 factorisation. A frequency whose iteration
-            // stalls above that is re-solved with an FP64 LU (stats->fp64_fallbacks).
+            // reaches the level of an FP64 factorisation. The full form mixes rows of very
+            // different scale (charge rows with P ~ 1e10, KCL rows with entries 1), where a
+            // small normwise error leaves the small rows inaccurate: there the componentwise
+            // error max_i |r_i| / (|A||x| + |b|)_i must reach that level too. A frequency
+            // whose iteration stalls above it is re-solved with an FP64 LU
+            // (stats->fp64_fallbacks).
             const int mb = nb - nd;
             const long long vo = (long long)nd * nr * n;
             double2 *m64 = bM64.as<double2>() + nd * nn;
@@ -679,17 +702,19 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
             PB_TRY(pb_lu_solve_batched<float>(&c->lu, n, mb, nr, m32, n, nn, perm, bRhs.as<double2>() + vo,
                                               bX.as<double2>() + vo));
             const double eta_tol = std::max(1e-14, 8.0 * std::sqrt((double)n) * 1.1e-16);
-            std::vector<double> prev(nb, 1e300);
+            const bool cwise = (form == PB_FORM_FULL);
+            std::vector<double> prev(nb, 1e300), cwh((size_t)mb * nr, 0.0);
             for (int q = nd; q < nb; q++) if (state[q] == 1) state[q] = 0;
             int it = 0;
             for (it = 1; it <= maxit + 1; it++) {
                 PB_TRY(pb_residual(&c->lu, n, mb, nr, m64, n, nn, bRhs.as<double2>() + vo, bX.as<double2>() + vo,
                                    bR.as<double2>() + vo, bRn.as<double>(), bBn.as<double>(), bXn.as<double>(),
-                                   it == 1 ? bAn.as<double>() : nullptr));
+                                   it == 1 ? bAn.as<double>() : nullptr, cwise ? bCw.as<double>() : nullptr));
                 PB_CUDA(cudaMemcpyAsync(rnh.data(), bRn.p, sizeof(double) * mb * nr, cudaMemcpyDeviceToHost, st));
                 PB_CUDA(cudaMemcpyAsync(bnh.data(), bBn.p, sizeof(double) * mb * nr, cudaMemcpyDeviceToHost, st));
                 PB_CUDA(cudaMemcpyAsync(xnh.data(), bXn.p, sizeof(double) * mb * nr, cudaMemcpyDeviceToHost, st));
                 if (it == 1) PB_CUDA(cudaMemcpyAsync(anh.data(), bAn.p, sizeof(double) * mb, cudaMemcpyDeviceToHost, st));
+                if (cwise) PB_CUDA(cudaMemcpyAsync(cwh.data(), bCw.p, sizeof(double) * mb * nr, cudaMemcpyDeviceToHost, st));
                 PB_CUDA(cudaStreamSynchronize(st));
                 int active = 0;
                 for (int q = 0; q < mb; q++) {
@@ -699,6 +724,7 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
                         const int v = q * nr + j;
                         const double den = anh[q] * xnh[v] + bnh[v];
                         eta = std::max(eta, den > 0 ? rnh[v] / den : 0.0);
+                        if (cwise) eta = std::max(eta, cwh[v]);
                     }
                     if (eta <= eta_tol) { state[nd + q] = 1; maxres = std::max(maxres, eta); }
                     else if (eta > 0.5 * prev[nd + q] || it > maxit) state[nd + q] = 2;
@@ -760,7 +786,20 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
         // port voltages per excitation: Z columns (1 A at port j) or the open-circuit
         // voltages of the plane-wave excitation (no injection: excitation cells -1)
         const int *pcx = pw ? bPC.as<int>() + 2 * np : bPC.as<int>();
-        if (form == PB_FORM_REDUCED) {
+        if (rhs_fixed) {
+            // node voltages of the source excitation (print_vnode, solve.c:102-112)
+            std::vector<double2> xh((size_t)nb * n);
+            PB_CUDA(cudaMemcpyAsync(xh.data(), bX.p, sizeof(double2) * xh.size(), cudaMemcpyDeviceToHost, st));
+            PB_CUDA(cudaStreamSynchronize(st));
+            const int nid = c->maxid + 1;
+            for (int q = 0; q < nb; q++)
+                for (int id = 0; id < nid; id++) {
+                    const int m = c->nodemap[id];
+                    const double2 v = m >= 0 ? xh[(size_t)q * n + m] : make_double2(0, 0);
+                    vnode[2 * ((size_t)(b0 + q) * nid + id)] = v.x;
+                    vnode[2 * ((size_t)(b0 + q) * nid + id) + 1] = v.y;
+                }
+        } else if (form == PB_FORM_REDUCED) {
             dim3 g(nr, np, nb);
             k_z_reduced<<<g, 256, 0, st>>>(np, nr, n, nc, bP.as<double2>(), (long long)nc * nc, c->d_inc_off,
                                            c->d_inc_seg, bPC.as<int>(), pcx, bX.as<double2>(), bFreq.as<double>(),

@@ -2,7 +2,7 @@
 
 Covers the keys the sweep hot path needs for thin-wire / bar / plate structures:
 title, node, wire, bar, plate (incl. the volume layers of ndiv_t >= 2), port,
-resistor, capacitor, inductor, vsource, frequency, nodetol, skineffect, capacitance,
+resistor, capacitor, inductor, vsource, isource, frequency, nodetol, skineffect, capacitance,
 retardation, groundplane, gmin, grading. Unknown keys are ignored (as the reference's
 parser does, src/input_data.c:555). quad / disk / dielectric / planewave structures are
 not built here (their cells come from the reference's own builder in the fixtures).
@@ -41,6 +41,7 @@ class PeecInput:
         self.maxid = 0
         self.planewave = None    # (theta_deg, phi_deg, pol, amp, phase_deg)
         self.compress, self.ctol, self.accel = 0, 0.0, 0
+        self.sources = []        # (isvsrc, n1, n2, amp, phase_deg), file order
         self.unsupported = []
 
 
@@ -95,9 +96,12 @@ def parse_peec(text):
             n1, n2 = int(a[1]), int(a[2])
             p.lumps.append((PB_LUMP_L, n1, n2, float(a[3])))
             p.maxid = max(p.maxid, n1, n2)
-        elif key == "vsource":             # vsource = n1 n2 amp [phase]
+        elif key in ("vsource", "isource"):  # n1 n2 amp [phase_deg] (input_data.c:175-192)
             n1, n2 = int(a[0]), int(a[1])
-            p.lumps.append((PB_LUMP_V, n1, n2, float(a[2])))
+            amp, ph = float(a[2]), float(a[3]) if len(a) > 3 else 0.0
+            if key == "vsource":
+                p.lumps.append((PB_LUMP_V, n1, n2, amp))
+            p.sources.append((1 if key == "vsource" else 0, n1, n2, amp, ph))
             p.maxid = max(p.maxid, n1, n2)
         elif key == "frequency":
             p.f0, p.f1 = float(a[0]), float(a[1])
@@ -127,7 +131,7 @@ def parse_peec(text):
             p.ctol = float(a[1]) if len(a) > 1 else 0.0
         elif key == "acceleration":        # acceleration = 1 (solve.c:47-64)
             p.accel = int(a[0])
-        elif key in ("quad", "disk", "dielectric", "mutual", "isource"):
+        elif key in ("quad", "disk", "dielectric", "mutual"):
             p.unsupported.append(key)
     return p
 
@@ -319,7 +323,7 @@ def build(p: PeecInput) -> Problem:
                    capacitance=p.capacitance, retardation=p.retardation, skin=p.skin,
                    gp=p.gp, gpz=p.gpz, gmin=p.gmin, f0=p.f0, f1=p.f1, nfreq=p.nfreq,
                    flog=p.flog, title=p.title, planewave=p.planewave, compress=p.compress,
-                   ctol=p.ctol, accel=p.accel)
+                   ctol=p.ctol, accel=p.accel, sources=p.sources)
 
 
 def load_peec(path) -> Problem:

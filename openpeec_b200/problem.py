@@ -19,7 +19,7 @@ class Problem:
     def __init__(self, seg, chg, chgnode, pv, maxid, port, lump=None, mut=None,
                  capacitance=0, retardation=0, skin=0, gp=0, gpz=0.0, gmin=0.0,
                  f0=0.0, f1=0.0, nfreq=1, flog=0, title="", planewave=None, compress=0, ctol=0.0,
-                 accel=0):
+                 accel=0, sources=None):
         self.seg = np.ascontiguousarray(seg, dtype=CELL_DTYPE)
         self.chg = np.ascontiguousarray(chg, dtype=CELL_DTYPE)
         self.chgnode = np.ascontiguousarray(chgnode, dtype=np.int32)
@@ -38,6 +38,8 @@ class Problem:
         self.planewave = tuple(planewave) if planewave is not None else None
         # solver keys of the .peec file (compression = 1 [tol], acceleration = 1)
         self.compress, self.ctol, self.accel = int(compress), float(ctol), int(accel)
+        # independent sources (isvsrc, n1, n2, amp, phase_deg) in file order (src_t)
+        self.sources = [tuple(x) for x in sources] if sources is not None else []
 
     # include/peec.h:241-248
     def freq_at(self, i):

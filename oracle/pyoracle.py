@@ -190,6 +190,8 @@ class RefLib:
             L.rh_solve.argtypes = [_vp, _vp]
             L.rh_voc.argtypes = [_vp, _vp, _vp, _vp]
             L.rh_voc.restype = C.c_int
+            L.rh_vnode.argtypes = [_vp, C.c_double, _vp]
+            L.rh_vnode.restype = C.c_int
             L.rh_set_freqs.argtypes = [_vp, C.c_double, C.c_double, C.c_int, C.c_int]
             L.rh_lu_decomp.argtypes = [C.c_int, _vp, _vp]
             L.rh_lu_solve.argtypes = [C.c_int, _vp, _vp, _vp]
@@ -300,6 +302,15 @@ class RefLib:
         if r == 0:
             return None
         return voc, (seg if r == 2 else None), pwp
+
+    def vnode(self, f):
+        """Node voltages [maxid+1] of the independent-source excitation at f (rh_vnode:
+        the reference's own fill, MNA, mna_rhs_sources and LU)."""
+        out = np.zeros(self.maxid + 1, np.complex128)
+        r = self.lib().rh_vnode(self.h, float(f), out.ctypes.data)
+        if r != -1:
+            raise RuntimeError("rh_vnode status %d" % r)
+        return out
 
     @classmethod
     def set_threads(cls, n):

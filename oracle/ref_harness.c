@@ -262,6 +262,38 @@ int rh_voc(void *hv, double *voc, double *segipw, double *pwp)
     return 1 + (p->segipw != NULL);
 }
 
+/* Node voltages of the independent-source excitation at f, computed the way the dense
+ * path of solve() does it (solve.c:243-248, 296-299, 392-396): lp_fill / pot_fill at f,
+ * mna_assemble, mna_rhs_sources, lu_decomp / lu_solve. out [2*(maxid+1)] = x[nodemap[id]],
+ * 0 where nodemap < 0, as print_vnode (solve.c:102-112) reports them. Returns -2 without
+ * sources, -3 on allocation failure, else lu_decomp's status (-1 = regular). */
+int rh_vnode(void *hv, double f, double *out)
+{
+    rh_t *h = (rh_t *)hv;
+    peec_t *p = &h->p;
+    if (p->nsrc <= 0) return -2;
+    lp_fill(p, f, h->log);
+    if (pot_fill(p, f, h->log)) return -3;
+    const int n = p->nunknown;
+    d_complex_t *a = (d_complex_t *)malloc((size_t)n * n * sizeof(d_complex_t));
+    d_complex_t *b = (d_complex_t *)malloc((size_t)n * sizeof(d_complex_t));
+    int *piv = (int *)malloc((size_t)n * sizeof(int));
+    if (!a || !b || !piv) { free(a); free(b); free(piv); return -3; }
+    mna_assemble(p, f, a);
+    mna_rhs_sources(p, b);
+    const int r = lu_decomp(n, a, piv);
+    if (r < 0) {
+        lu_solve(n, a, piv, b);
+        for (int id = 0; id <= p->maxid; id++) {
+            const int m = p->nodemap[id];
+            out[2 * id] = m >= 0 ? b[m].r : 0;
+            out[2 * id + 1] = m >= 0 ? b[m].i : 0;
+        }
+    }
+    free(a); free(b); free(piv);
+    return r;
+}
+
 /* Restrict the sweep to [ifreq0, ifreq0+count) of the parsed list (for timing samples). */
 void rh_set_freqs(void *hv, double f0, double f1, int nfreq, int flog)
 {

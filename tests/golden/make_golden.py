@@ -103,6 +103,41 @@ def make_pw_case(name, peec_text, freqs, threads=8):
     print(name, "nseg", r.nseg, "voc", np.array(vocs).T.ravel()[:2], "->", out)
 
 
+def make_src_case(name, peec_text, freqs, threads=8):
+    """Independent-source case: the node voltages of the reference's source solve
+    (mna_rhs_sources through its dense MNA, solve.c:392-396) at each frequency, and the
+    source list as the package's parser reads it. Written to tests/golden/src/."""
+    from openpeec_b200 import geometry
+    with tempfile.NamedTemporaryFile("w", suffix=".peec", delete=False) as f:
+        f.write(peec_text)
+        path = f.name
+    RefLib.set_threads(threads)
+    r = RefLib(path)
+    prob = r.problem()
+    vn = np.array([r.vnode(fr) for fr in freqs])
+    srcs = np.array(geometry.parse_peec(peec_text).sources, dtype=np.float64).reshape(-1, 5)
+    os.unlink(path)
+    os.makedirs(os.path.join(HERE, "src"), exist_ok=True)
+    out = os.path.join(HERE, "src", name + ".npz")
+    tmp = os.path.join(HERE, name + "_prob.npz")
+    prob.save(tmp)
+    pz = dict(np.load(tmp))
+    os.unlink(tmp)
+    np.savez_compressed(out, **{"prob_" + k: v for k, v in pz.items()}, freqs=np.array(freqs),
+                        vnode=vn, sources=srcs, peec=np.array(peec_text))
+    print(name, "nseg", r.nseg, "vnode", vn[0, :3], "->", out)
+
+
+def src_cases():
+    rlc = sample("rlc_series.peec")
+    make_src_case("rlc_isource", rlc.replace("end", "isource = 0 1 1.0 30\nend"), [5.0329212e6, 1.0065842e7])
+    make_src_case("rlc_vsource", rlc.replace("end", "vsource = 1 0 2.0 0\nend"), [5.0329212e6, 1.0065842e7])
+    dip = sample("dipole_halfwave.peec")
+    make_src_case("dipole_isource", dip.replace("\nend", "\nisource = 2 1 1.0 0\nend"), [2.93e8, 6.0e8])
+    make_src_case("cfg2_isource", configs.cfg2(16, 8, 512).replace("\nend", "\nisource = 0 1 0.5 -45\nend"),
+                  [5e6, 6.4e8])
+
+
 def make_comp_case(name, peec_text, freqs, threads=16):
     """Compressed-path case: Z of the reference's compression = 1 solve (H-matrix + ACA,
     leaf-Schur preconditioner, GMRES) and Z of its dense solve of the same input with the
@@ -176,9 +211,13 @@ def main():
     ap.add_argument("--cfg2", action="store_true")
     ap.add_argument("--pw-only", action="store_true", help="only the plane-wave cases")
     ap.add_argument("--comp-only", action="store_true", help="only the compressed-path cases")
+    ap.add_argument("--src-only", action="store_true", help="only the independent-source cases")
     a = ap.parse_args()
     subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True,
                    stdout=subprocess.DEVNULL)
+    if a.src_only:
+        src_cases()
+        return
     if not a.comp_only:
         pw_cases()
     comp_cases()

@@ -64,6 +64,20 @@ def test_full_and_reduced_forms_agree(name, golden):
     assert zerr(zr, zf) <= 1e-9
 
 
+@pytest.mark.parametrize("name", ["dipole_halfwave", "cfg2_small"])
+def test_full_form_mixed_lu_refines_componentwise(golden, name):
+    """The full form mixes charge rows (P ~ 1e10) with KCL rows of entries 1. After one
+    refinement step of the FP32 factorisation the normwise backward error is already at FP64
+    level while the small rows are still off by 1e-5 (Z of the dipole was 1.7e-5 away);
+    the componentwise stopping rule keeps refining until Z is within 1e-6."""
+    prob, fx = golden(name)
+    with api.Context(prob) as ctx:
+        z64, _ = ctx.sweep(fx["freqs"], fill_prec=abi.PREC_FP64, lu=abi.LU_FP64, form=abi.FORM_REDUCED)
+        zf, sf = ctx.sweep(fx["freqs"], fill_prec=abi.PREC_FP64, lu=abi.LU_TC, form=abi.FORM_FULL)
+    assert sf["form_used"] == abi.FORM_FULL
+    assert zerr(zf, z64) <= 1e-6, (zerr(zf, z64), sf["max_iters"])
+
+
 def test_monopole_is_half_dipole(golden):
     """Image theory: the quarter-wave monopole over ground is the half-wave dipole / 2
     (reference check peec_check.sh:382-397, measured 3e-10 there)."""
