@@ -219,6 +219,28 @@ int  pb_planewave(pb_ctx *ctx, int nfreq, const double *freq, const pb_sweep_opt
                   const pb_planewave_t *pw, double *voc, double *segipw, pb_sweep_stats *stats);
 
 /*
+ * Far field of the sweep's port-1 currents (output_far, src/farfield.c:42-182): for every
+ * frequency and direction (theta = thmax*it/nth, it = 0..nth, thmax = pi, or pi/2 over a
+ * ground plane with image currents; phi = 2 pi ip/nph) the radiation vector of the current
+ * cells and r*E_theta, r*E_phi [V] (et, ep [nfreq][(nth+1)*nph] complex), the directivity
+ * and gain [dBi] (d_dbi, g_dbi, same shape, -600 below 1e-30; may be NULL), the radiated
+ * power (prad [nfreq]) and the input power 0.5 Re Zin (pin [nfreq]; zin NULL: 0).
+ * segi: port-1 segment currents, frequency f at segi + 2*f*seg_stride (complex doubles).
+ */
+int  pb_farfield(pb_ctx *ctx, int nfreq, const double *freq, const double *segi, long long seg_stride,
+                 const double *zin, int nth, int nph, double *et, double *ep, double *d_dbi,
+                 double *g_dbi, double *prad, double *pin);
+
+/*
+ * Transient synthesis (tran_synth / output_tran, src/transient.c:73-177) of nsig frequency
+ * responses h [nsig][nfreq] complex sampled at f_k = k df (f0 = df, f1 = f_max; else
+ * PB_ERR_ARG as tran_check): a Gaussian pulse att_db down at f_max, x [2*nfreq] the pulse
+ * itself, y [nsig][2*nfreq] the responses, at t_n = n dt, dt = 1/(2 f_max) (*dt_out).
+ */
+int  pb_transient(int nfreq, double f0, double f1, double att_db, int nsig, const double *h, double *x,
+                  double *y, double *dt_out);
+
+/*
  * Independent sources (reference src_t, include/peec.h:43; vsource / isource keys,
  * src/input_data.c:175-192). isvsrc = 1: voltage source amp at phase_deg; the k-th
  * voltage source is the k-th PB_LUMP_V element of the problem (its branch row, mna.c:77).

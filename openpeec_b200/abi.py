@@ -149,6 +149,9 @@ def lib():
     L.pb_device_sync.restype = C.c_int
     L.pb_sources.argtypes = [_vp, C.c_int, _vp, C.POINTER(PbSweepOpts), C.c_int, _vp, _vp,
                              C.POINTER(PbSweepStats)]
+    L.pb_farfield.argtypes = [_vp, C.c_int, _vp, _vp, C.c_longlong, _vp, C.c_int, C.c_int, _vp, _vp, _vp,
+                              _vp, _vp, _vp]
+    L.pb_transient.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, C.c_int, _vp, _vp, _vp, _vp]
     L.pb_mlp_nparam.restype = C.c_int
     L.pb_pc_samples.argtypes = [_vp, C.c_double, C.POINTER(PbSweepOpts), _vp, _vp]
     L.pb_mlp_train.argtypes = [_vp, C.c_int, _vp, _vp, C.c_int, C.c_float, _vp]

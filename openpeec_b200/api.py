@@ -127,6 +127,24 @@ class Context:
                                     C.cast(arr, C.c_void_p), vn.ctypes.data, C.byref(st)))
         return vn, st.as_dict()
 
+    def farfield(self, freqs, segi, zin, nth, nph):
+        """Far field of port-1 currents segi [nfreq, nseg] (or [nfreq, nport, nseg]: port 1
+        is taken) with input impedance zin [nfreq] (pb_farfield). Returns a dict of et, ep,
+        d_dbi, g_dbi [nfreq, (nth+1)*nph], prad, pin [nfreq]."""
+        freqs = np.ascontiguousarray(freqs, np.float64)
+        segi = np.ascontiguousarray(segi, np.complex128)
+        stride = segi.shape[-1] * (segi.shape[1] if segi.ndim == 3 else 1)
+        zin = np.ascontiguousarray(zin, np.complex128)
+        nf, nd = len(freqs), (nth + 1) * nph
+        out = {k: np.zeros((nf, nd), np.complex128) for k in ("et", "ep")}
+        out.update({k: np.zeros((nf, nd)) for k in ("d_dbi", "g_dbi")})
+        out.update({k: np.zeros(nf) for k in ("prad", "pin")})
+        _check(abi.lib().pb_farfield(self.h, nf, freqs.ctypes.data, segi.ctypes.data, stride, zin.ctypes.data,
+                                     int(nth), int(nph), out["et"].ctypes.data, out["ep"].ctypes.data,
+                                     out["d_dbi"].ctypes.data, out["g_dbi"].ctypes.data, out["prad"].ctypes.data,
+                                     out["pin"].ctypes.data))
+        return out
+
     def pc_samples(self, freq, fill_prec=abi.PREC_MIXED, ctol=0.0):
         """Training samples of the learned preconditioner correction at one frequency:
         (features [nseg, 12], targets [nseg, 2]) (pb_pc_samples)."""
@@ -135,6 +153,20 @@ class Context:
         o = abi.PbSweepOpts(int(fill_prec), int(abi.LU_FP64), 0, 0, 0.0, 0, 0, 0, 0, 1, 0, float(ctol))
         _check(abi.lib().pb_pc_samples(self.h, float(freq), C.byref(o), x.ctypes.data, t.ctypes.data))
         return x, t
+
+
+def transient(f0, f1, nfreq, h, att_db=40.0):
+    """Transient synthesis (pb_transient) of responses h [nsig, nfreq] on the sweep
+    f_k = k df: (x pulse [2 nfreq], y [nsig, 2 nfreq], dt)."""
+    h = np.ascontiguousarray(np.atleast_2d(h), np.complex128)
+    nsig = h.shape[0] if h.size else 0
+    x = np.zeros(2 * nfreq)
+    y = np.zeros((nsig, 2 * nfreq))
+    dt = C.c_double()
+    _check(abi.lib().pb_transient(int(nfreq), float(f0), float(f1), float(att_db), nsig,
+                                  h.ctypes.data if nsig else None, x.ctypes.data,
+                                  y.ctypes.data if nsig else None, C.byref(dt)))
+    return x, y, dt.value
 
 
 MLP_IN, MLP_H, MLP_OUT = 12, 128, 2

@@ -190,6 +190,10 @@ class RefLib:
             L.rh_solve.argtypes = [_vp, _vp]
             L.rh_voc.argtypes = [_vp, _vp, _vp, _vp]
             L.rh_voc.restype = C.c_int
+            L.rh_results.argtypes = [_vp, _vp, _vp, _vp]
+            L.rh_results.restype = C.c_int
+            L.rh_output_far.argtypes = [_vp, C.c_char_p]
+            L.rh_output_tran.argtypes = [_vp, C.c_char_p]
             L.rh_vnode.argtypes = [_vp, C.c_double, _vp]
             L.rh_vnode.restype = C.c_int
             L.rh_set_freqs.argtypes = [_vp, C.c_double, C.c_double, C.c_int, C.c_int]
@@ -302,6 +306,23 @@ class RefLib:
         if r == 0:
             return None
         return voc, (seg if r == 2 else None), pwp
+
+    def results(self):
+        """(zin [nport, nfreq], segi [nfreq, nport, nseg] or None, smat [nfreq, nport, nport])
+        of the last solve()."""
+        zin = np.zeros((self.nport, self.nfreq), np.complex128)
+        segi = np.zeros((self.nfreq, self.nport, self.nseg), np.complex128)
+        smat = np.zeros((self.nfreq, self.nport, self.nport), np.complex128)
+        r = self.lib().rh_results(self.h, zin.ctypes.data, segi.ctypes.data, smat.ctypes.data)
+        if r == 0:
+            raise RuntimeError("no results: solve() first")
+        return zin, (segi if r == 2 else None), smat
+
+    def output_csv(self, which, path):
+        """Run the reference's output_far ('far') or output_tran ('tran') into path."""
+        f = self.lib().rh_output_far if which == "far" else self.lib().rh_output_tran
+        if f(self.h, path.encode()) != 0:
+            raise RuntimeError("reference output_%s failed" % which)
 
     def vnode(self, f):
         """Node voltages [maxid+1] of the independent-source excitation at f (rh_vnode:

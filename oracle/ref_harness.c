@@ -294,6 +294,33 @@ int rh_vnode(void *hv, double f, double *out)
     return r;
 }
 
+/* Results of the last rh_solve that the post-processing reads: zin [2*nport*nfreq]
+ * (zin[j*nfreq+f]), segi [2*nfreq*nport*nseg] (DIDX order; when distribution or farfield
+ * is set), smat [2*nfreq*nport*nport] (ZIDX order). Returns 1 + (segi present). */
+int rh_results(void *hv, double *zin, double *segi, double *smat)
+{
+    const peec_t *p = &((rh_t *)hv)->p;
+    if (p->zin == NULL) return 0;
+    if (zin) memcpy(zin, p->zin, (size_t)p->nport * p->nfreq * sizeof(d_complex_t));
+    if (smat && p->smat) memcpy(smat, p->smat, (size_t)p->nfreq * p->nport * p->nport * sizeof(d_complex_t));
+    if (segi && p->segi) memcpy(segi, p->segi, (size_t)p->nfreq * p->nport * p->nseg * sizeof(d_complex_t));
+    return 1 + (p->segi != NULL);
+}
+
+/* The reference's own post-processing writers on the last rh_solve's results:
+ * output_far (farfield.c:42) and output_tran (transient.c:97) into the CSV file fn. */
+int rh_output_far(void *hv, const char *fn)
+{
+    rh_t *h = (rh_t *)hv;
+    return output_far(&h->p, fn, h->log);
+}
+
+int rh_output_tran(void *hv, const char *fn)
+{
+    rh_t *h = (rh_t *)hv;
+    return output_tran(&h->p, fn, h->log);
+}
+
 /* Restrict the sweep to [ifreq0, ifreq0+count) of the parsed list (for timing samples). */
 void rh_set_freqs(void *hv, double f0, double f1, int nfreq, int flog)
 {

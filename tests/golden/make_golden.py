@@ -128,6 +128,59 @@ def make_src_case(name, peec_text, freqs, threads=8):
     print(name, "nseg", r.nseg, "vnode", vn[0, :3], "->", out)
 
 
+def make_post_case(name, peec_text, which):
+    """Post-processing case: the reference's sweep, then its own output_far or output_tran
+    writer (parsed back from the CSV, 10 significant digits), together with the inputs
+    the writer read (port-1 segment currents, Zin, S, Voc). Written to tests/golden/post/."""
+    import csv
+    with tempfile.NamedTemporaryFile("w", suffix=".peec", delete=False) as f:
+        f.write(peec_text)
+        path = f.name
+    r = RefLib(path)
+    prob = r.problem()
+    r.solve()
+    zin, segi, smat = r.results()
+    pw = r.voc()
+    out = path + ".csv"
+    r.output_csv(which, out)
+    rows = list(csv.reader(open(out)))[1:]
+    os.unlink(out)
+    os.unlink(path)
+    extra = {}
+    if which == "far":
+        a = np.array([[float(v) for v in row] for row in rows])
+        extra = dict(ff_freq=a[:, 0], ff_th=a[:, 1], ff_ph=a[:, 2], et=a[:, 3] + 1j * a[:, 4],
+                     ep=a[:, 5] + 1j * a[:, 6], d_dbi=a[:, 7], g_dbi=a[:, 8])
+    else:
+        extra = dict(tr_type=np.array([row[0] for row in rows]), tr_i=np.array([int(row[1]) for row in rows]),
+                     tr_j=np.array([int(row[2]) for row in rows]), tr_t=np.array([float(row[3]) for row in rows]),
+                     tr_y=np.array([float(row[4]) for row in rows]))
+    os.makedirs(os.path.join(HERE, "post"), exist_ok=True)
+    dst = os.path.join(HERE, "post", name + ".npz")
+    tmp = os.path.join(HERE, name + "_prob.npz")
+    prob.save(tmp)
+    pz = dict(np.load(tmp))
+    os.unlink(tmp)
+    np.savez_compressed(dst, **{"prob_" + k: v for k, v in pz.items()}, freqs=np.array(r.freqs()), zin=zin,
+                        segi=segi if segi is not None else np.zeros(0), smat=smat,
+                        voc=pw[0] if pw is not None else np.zeros(0), peec=np.array(peec_text), **extra)
+    print(name, which, len(rows), "rows ->", dst)
+
+
+def post_cases():
+    make_post_case("ff_dipole", sample("dipole_ff.peec"), "far")
+    mono = sample("monopole_gp.peec").replace("groundplane = 0", "groundplane = 0\nfarfield = 12 16")
+    mono = "\n".join(l for l in mono.splitlines() if not l.startswith("frequency")).replace(
+        "\nend", "\nfrequency = 1.3e8 1.6e8 1\nend")
+    make_post_case("ff_monopole_gp", mono, "far")
+    plate = configs.cfg2(16, 8, 2, 6.4e8, 6.4e8).replace("capacitance = 1", "capacitance = 1\nfarfield = 8 12")
+    make_post_case("ff_plate_gp", plate, "far")
+    make_post_case("tran_tdr", sample("tdr_resistor.peec"), "tran")
+    make_post_case("tran_loop_pw", sample("loop_tran.peec"), "tran")
+    twop = configs.cfg2(16, 8, 32, 8e7, 8e7).replace("capacitance = 1", "capacitance = 1\ntransient = 1 60")
+    make_post_case("tran_plate", twop, "tran")
+
+
 def src_cases():
     rlc = sample("rlc_series.peec")
     make_src_case("rlc_isource", rlc.replace("end", "isource = 0 1 1.0 30\nend"), [5.0329212e6, 1.0065842e7])
@@ -212,11 +265,15 @@ def main():
     ap.add_argument("--pw-only", action="store_true", help="only the plane-wave cases")
     ap.add_argument("--comp-only", action="store_true", help="only the compressed-path cases")
     ap.add_argument("--src-only", action="store_true", help="only the independent-source cases")
+    ap.add_argument("--post-only", action="store_true", help="only the far-field / transient cases")
     a = ap.parse_args()
     subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True,
                    stdout=subprocess.DEVNULL)
     if a.src_only:
         src_cases()
+        return
+    if a.post_only:
+        post_cases()
         return
     if not a.comp_only:
         pw_cases()
