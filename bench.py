@@ -412,6 +412,92 @@ def run_barstack(args):
     }
 
 
+class _StdoutToStderr:
+    """The reference's C code prints progress with printf; keep the bench's stdout to the
+    one JSON line by sending file descriptor 1 to stderr meanwhile."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        os.dup2(2, 1)
+
+    def __exit__(self, *a):
+        import ctypes as _C
+        _C.CDLL(None).fflush(None)
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+
+
+def run_batch3(args):
+    """Third workload (not the headline line): config 3, a batch of uneven random thin-wire
+    structures (20-400 segments, capacitance + retardation, 64 log frequencies 50 MHz-3 GHz
+    each), swept by pb_sweep_many (concurrent streams from a size-ordered work queue) and,
+    for comparison, one pb_sweep after another. Geometry is resident (contexts created
+    before the timed region); the time is the host wall clock between device
+    synchronisations. The CPU reference solves a bounded sample of the instances with all
+    host threads and is scaled to the batch."""
+    import tempfile
+    n = args.batch3
+    texts = [configs.cfg3_instance(0, i) for i in range(n)]
+    probs = [geometry.build(geometry.parse_peec(t)) for t in texts]
+    ctxs = [api.Context(p) for p in probs]
+    freqs = [p.freqs() for p in probs]
+    L = abi.lib()
+    # warm-up: one full pass (per-context buffers, static parts and sample counts per
+    # quadrature-level signature), so both timed passes start from the same state
+    api.sweep_many(ctxs, freqs)
+    L.pb_device_sync()
+    t0 = time.perf_counter()
+    for c, f in zip(ctxs, freqs):
+        c.sweep(f)
+    L.pb_device_sync()
+    t_serial = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    zs, st = api.sweep_many(ctxs, freqs, want_stats=True)
+    L.pb_device_sync()
+    t_many = time.perf_counter() - t0
+    pts = sum(len(f) for f in freqs)
+    nseg = [len(p.seg) for p in probs]
+    # CPU reference on a bounded sample: every 16th instance at 8 of its frequencies
+    from oracle import pyoracle
+    ncpu = os.cpu_count() or 1
+    ref_s, ref_pts = 0.0, 0
+    for i in range(0, n, 16):
+        with tempfile.NamedTemporaryFile("w", suffix=".peec", delete=False) as fh:
+            fh.write(texts[i])
+            path = fh.name
+        try:
+            with _StdoutToStderr():
+                r = pyoracle.RefLib(path)
+                r.set_threads(ncpu)
+                fs = freqs[i][::8]
+                r.set_freqs(fs[0], fs[-1], len(fs), 1)
+                t0 = time.perf_counter()
+                r.solve()
+                ref_s += time.perf_counter() - t0
+            ref_pts += len(fs)
+        finally:
+            os.unlink(path)
+        if ref_s > 20:
+            break
+    for c in ctxs:
+        c.close()
+    return {
+        "metric": "config-3 batch instance-freq-points/s (fill+solve)", "value": pts / t_many, "unit": "points/s",
+        "n_gpus": 1, "steps": 1, "warmup": 1, "ms_per_step": 1e3 * t_many, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64 (mixed fill, tensor-core LU, FP64 refinement)",
+        "data": "synthetic (seeded random polylines from the .peec text)",
+        "timing": "host wall clock between device synchronisations",
+        "config": {"workload": "%d random thin-wire structures, %d-%d segments, 64 log freqs 50 MHz-3 GHz each"
+                   % (n, min(nseg), max(nseg)), "points": pts},
+        "serial_pb_sweep": {"value": pts / t_serial, "s": t_serial},
+        "concurrency_gain": t_serial / t_many,
+        "max_refine_iters": max(s["max_iters"] for s in st),
+        "cpu_baseline": {"value": ref_pts / ref_s if ref_s > 0 else None, "unit": "points/s", "cores": ncpu,
+                         "kind": "reference", "sample": "%d points: every 16th instance at every 8th frequency" % ref_pts},
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -424,6 +510,8 @@ def main():
     ap.add_argument("--grid", default="64x32", help="plate grid; not 64x32 only for profiling captures")
     ap.add_argument("--accel", type=int, default=0,
                     help="LU reuse: one FP32 factorisation per ACCEL frequencies, GMRES for the rest (0 = every frequency)")
+    ap.add_argument("--batch3", type=int, default=0,
+                    help="N: time config 3 (N random thin-wire structures) through pb_sweep_many instead")
     ap.add_argument("--barstack", default="",
                     help="NXxNYxNZ: time the compressed path on the bar stack instead (e.g. 96x96x4)")
     args = ap.parse_args()
@@ -431,6 +519,10 @@ def main():
     if args.barstack:
         if rank == 0:
             print(json.dumps(run_barstack(args)), flush=True)
+        return
+    if args.batch3:
+        if rank == 0:
+            print(json.dumps(run_batch3(args)), flush=True)
         return
     if args.impl == "reference":
         line = run_reference(args, ws, rank)

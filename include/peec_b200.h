@@ -219,6 +219,19 @@ int  pb_planewave(pb_ctx *ctx, int nfreq, const double *freq, const pb_sweep_opt
                   const pb_planewave_t *pw, double *voc, double *segipw, pb_sweep_stats *stats);
 
 /*
+ * Many structures at once (config-3 style batches of small, uneven structures; the
+ * reference solves them one after another). Instance k sweeps nfreq[k] frequencies freq[k]
+ * through ctx[k] exactly as pb_sweep(ctx[k], ...) would (same kernels, same order: the
+ * results are bit-identical), zmat[k] as pb_sweep's zmat (may be NULL), stats [ninst] or
+ * NULL. Instances run concurrently on their own streams, largest first, from a shared work
+ * queue served by nthreads host threads (0 = min(16, ninst)). The contexts must be
+ * distinct. Returns the first failing instance's status, with "instance k: " in front of
+ * its message; the others still run.
+ */
+int  pb_sweep_many(int ninst, pb_ctx *const *ctx, const int *nfreq, const double *const *freq,
+                   const pb_sweep_opts *opts, double *const *zmat, pb_sweep_stats *stats, int nthreads);
+
+/*
  * Far field of the sweep's port-1 currents (output_far, src/farfield.c:42-182): for every
  * frequency and direction (theta = thmax*it/nth, it = 0..nth, thmax = pi, or pi/2 over a
  * ground plane with image currents; phi = 2 pi ip/nph) the radiation vector of the current

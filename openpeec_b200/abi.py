@@ -152,6 +152,7 @@ def lib():
     L.pb_farfield.argtypes = [_vp, C.c_int, _vp, _vp, C.c_longlong, _vp, C.c_int, C.c_int, _vp, _vp, _vp,
                               _vp, _vp, _vp]
     L.pb_transient.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, C.c_int, _vp, _vp, _vp, _vp]
+    L.pb_sweep_many.argtypes = [C.c_int, _vp, _vp, _vp, C.POINTER(PbSweepOpts), _vp, _vp, C.c_int]
     L.pb_mlp_nparam.restype = C.c_int
     L.pb_pc_samples.argtypes = [_vp, C.c_double, C.POINTER(PbSweepOpts), _vp, _vp]
     L.pb_mlp_train.argtypes = [_vp, C.c_int, _vp, _vp, C.c_int, C.c_float, _vp]

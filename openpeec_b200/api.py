@@ -155,6 +155,24 @@ class Context:
         return x, t
 
 
+def sweep_many(ctxs, freqs, fill_prec=abi.PREC_MIXED, lu=abi.LU_TC, nthreads=0, want_stats=False):
+    """pb_sweep_many: every context sweeps its own frequency list (freqs: one list per
+    context) concurrently. Returns the Z matrices [nfreq_k, nport_k, nport_k] per context
+    (and the per-instance stats)."""
+    n = len(ctxs)
+    fl = [np.ascontiguousarray(f, np.float64) for f in freqs]
+    zs = [np.zeros((len(f), len(c.prob.port), len(c.prob.port)), np.complex128) for c, f in zip(ctxs, fl)]
+    hs = (C.c_void_p * n)(*[c.h for c in ctxs])
+    nf = (C.c_int * n)(*[len(f) for f in fl])
+    fp = (C.c_void_p * n)(*[f.ctypes.data for f in fl])
+    zp = (C.c_void_p * n)(*[z.ctypes.data for z in zs])
+    st = (abi.PbSweepStats * n)()
+    o = abi.PbSweepOpts(int(fill_prec), int(lu), 0, 0, 0.0, 0, 0, 0, 0, 0, 0, 0.0, None)
+    _check(abi.lib().pb_sweep_many(n, C.cast(hs, C.c_void_p), C.cast(nf, C.c_void_p), C.cast(fp, C.c_void_p),
+                                   C.byref(o), C.cast(zp, C.c_void_p), C.cast(st, C.c_void_p), int(nthreads)))
+    return (zs, [s.as_dict() for s in st]) if want_stats else zs
+
+
 def transient(f0, f1, nfreq, h, att_db=40.0):
     """Transient synthesis (pb_transient) of responses h [nsig, nfreq] on the sweep
     f_k = k df: (x pulse [2 nfreq], y [nsig, 2 nfreq], dt)."""

@@ -1,3 +1,5 @@
+#include <atomic>
+#include <thread>
 // pb_api.cu — C entry points of the batched core (include/peec_b200.h).
 #include "pb_ctx.cuh"
 #include "pb_hmat.cuh"
@@ -283,6 +285,10 @@ int pb_create(const pb_problem_t *prob, pb_ctx **out)
         if ((r = pb_build_qpts(g.seg, c->seg.data(), c->pv.data(), g.pv, s))) return fail(r);
         if ((r = pb_build_qpts(g.chg, c->chg.data(), c->pv.data(), g.pv, s))) return fail(r);
     }
+    {
+        cudaError_t e = cudaMalloc(&c->d_count, 2 * sizeof(unsigned long long));
+        if (e != cudaSuccess) { c->d_count = nullptr; return fail(pb_cuda_fail(e, "cudaMalloc", __FILE__, __LINE__)); }
+    }
     if ((r = pb_lu_engine_init(&c->lu, s))) return fail(r);
     if (cudaStreamSynchronize(s) != cudaSuccess) return fail(pb_cuda_fail(cudaGetLastError(), "upload", __FILE__, __LINE__));
     *out = c;
@@ -296,7 +302,7 @@ void pb_destroy(pb_ctx *c)
     void *ptrs[] = {c->g.seg.cell, c->g.seg.qpt, c->g.seg.qoff, c->g.chg.cell, c->g.chg.qpt,
                     c->g.chg.qoff, c->g.pv, c->g.csoff, c->g.csidx, c->g.carea, c->g.seg_ca,
                     c->g.seg_cb, c->d_inc_off, c->d_inc_seg, c->d_fe_row, c->d_fe_col, c->d_fe_off,
-                    c->d_fe_st, c->d_cellnode};
+                    c->d_fe_st, c->d_cellnode, c->d_count};
     for (void *p : ptrs) if (p) cudaFree(p);
     for (auto &slot : c->cache) if (slot.p) cudaFree(slot.p);
     if (c->comp_schur_reg) cudaHostUnregister(c->comp_schur_reg);
@@ -375,6 +381,57 @@ int pb_sweep(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts *opts
     if (!c) { pb_set_error("pb_sweep: null context"); return PB_ERR_ARG; }
     PB_CUDA(cudaSetDevice(c->dev));
     return pb_sweep_impl(c, nfreq, freq, opts, zmat, segi, stats, nullptr, nullptr, nullptr);
+}
+
+int pb_sweep_many(int ninst, pb_ctx *const *ctx, const int *nfreq, const double *const *freq,
+                  const pb_sweep_opts *opts, double *const *zmat, pb_sweep_stats *stats, int nthreads)
+{
+    if (ninst <= 0 || !ctx || !nfreq || !freq) { pb_set_error("pb_sweep_many: bad argument"); return PB_ERR_ARG; }
+    {
+        std::vector<const pb_ctx *> seen(ctx, ctx + ninst);
+        std::sort(seen.begin(), seen.end());
+        for (int k = 0; k < ninst; k++)
+            if (!seen[k] || (k > 0 && seen[k] == seen[k - 1])) {
+                pb_set_error("pb_sweep_many: null or repeated context");
+                return PB_ERR_ARG;
+            }
+    }
+    // work queue: largest system first, so the long instances start early
+    std::vector<int> order(ninst);
+    for (int k = 0; k < ninst; k++) order[k] = k;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        return (double)ctx[a]->nfull * ctx[a]->nfull * nfreq[a] > (double)ctx[b]->nfull * ctx[b]->nfull * nfreq[b];
+    });
+    const int nt = std::max(1, std::min(nthreads > 0 ? nthreads : 16, ninst));
+    std::atomic<int> next{0};
+    std::vector<int> rc(ninst, PB_OK);
+    std::vector<std::string> msg(ninst);
+    auto worker = [&]() {
+        pb_mem_share = nt;
+        for (;;) {
+            const int q = next.fetch_add(1);
+            if (q >= ninst) return;
+            const int k = order[q];
+            cudaError_t e = cudaSetDevice(ctx[k]->dev);
+            int r = e == cudaSuccess ? PB_OK : pb_cuda_fail(e, "cudaSetDevice", __FILE__, __LINE__);
+            if (r == PB_OK)
+                r = pb_sweep_impl(ctx[k], nfreq[k], freq[k], opts, zmat ? zmat[k] : nullptr, nullptr,
+                                  stats ? &stats[k] : nullptr, nullptr, nullptr, nullptr);
+            rc[k] = r;
+            if (r != PB_OK) msg[k] = pb_last_error();
+        }
+    };
+    std::vector<std::thread> th;
+    for (int t = 1; t < nt; t++) th.emplace_back(worker);
+    worker();
+    pb_mem_share = 1;
+    for (auto &x : th) x.join();
+    for (int k = 0; k < ninst; k++)
+        if (rc[k] != PB_OK) {
+            pb_set_error("instance %d: %s", k, msg[k].c_str());
+            return rc[k];
+        }
+    return PB_OK;
 }
 
 int pb_pc_samples(pb_ctx *c, double freq, const pb_sweep_opts *opts, float *x, float *t)

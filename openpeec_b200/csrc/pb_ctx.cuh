@@ -58,6 +58,7 @@ struct pb_ctx {
     int *d_fe_row = nullptr, *d_fe_col = nullptr, *d_fe_off = nullptr;
     pb_stamp *d_fe_st = nullptr;
     int *d_cellnode = nullptr;                 // [ncell] matrix index of the cell's node (-1 = ref)
+    unsigned long long *d_count = nullptr;     // [2] quadrature-sample counters (statistics)
 
     pb_cache_slot cache[PB_CACHE_SLOTS];
     // correction samples (Lp, P) per quadrature-level signature, for the statistics
@@ -72,3 +73,7 @@ struct pb_ctx {
 
     long launches = 0;
 };
+
+// Number of sweeps that run concurrently from this host thread's pb_sweep_many: the dense
+// sweep sizes its frequency batch from the free device memory divided by it.
+extern thread_local int pb_mem_share;

@@ -17,6 +17,7 @@
 //   come from FP64 once per term and frequency group; each sample only rotates them by
 //   the small angle k delta / 2. The sample loop has no FP64 arithmetic.
 // * Epilogue: store Lp / P, or assemble the reduced MNA matrix directly.
+#include <atomic>
 #include "pb_fill.cuh"
 #include "pb_geom.cuh"
 #include <vector>
@@ -854,17 +855,17 @@ __global__ void k_count(pb_fill_geom g, double kw, unsigned long long *out)
     atomicAdd(&out[1], acc_p);
 }
 
+// d_count: two counters of device memory owned by the caller (no allocation here: a
+// cudaFree would synchronise the whole device under concurrent sweeps)
 int pb_count_samples(const pb_fill_geom &g, double kw, double *lp_samples, double *p_samples,
-                     cudaStream_t s)
+                     cudaStream_t s, unsigned long long *d_count)
 {
-    unsigned long long *d = nullptr, h[2] = {0, 0};
-    PB_CUDA(cudaMalloc(&d, 16));
+    unsigned long long *d = d_count, h[2] = {0, 0};
     PB_CUDA(cudaMemsetAsync(d, 0, 16, s));
     const long long T = (long long)g.seg.n * (g.seg.n + 1) / 2 + (long long)g.ncell * (g.ncell + 1) / 2;
     if (T > 0) k_count<<<grid_for(T, 256), 256, 0, s>>>(g, kw, d);
     cudaError_t e = cudaMemcpyAsync(h, d, 16, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    cudaFree(d);
     if (e != cudaSuccess) return pb_cuda_fail(e, "pb_count_samples", __FILE__, __LINE__);
     *lp_samples = (double)h[0];
     *p_samples = (double)h[1];
@@ -998,7 +999,7 @@ static int launch_corr(const pb_fill_geom &g, const KArg &k, const double *st, c
     const int n = SET == PB_SET_LP ? g.seg.n : g.chg.n;
     const long long T = (long long)n * (n + 1) / 2;
     constexpr size_t smem = corr_smem_bytes<R, F>();
-    static bool attr_set = false;
+    static std::atomic<bool> attr_set{false};   // set once, before any launch relies on it
     if (!attr_set) {
         PB_CUDA(cudaFuncSetAttribute(k_corr<R, F, SET, EPI, EQ, RED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         attr_set = true;

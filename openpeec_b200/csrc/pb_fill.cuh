@@ -64,7 +64,7 @@ int pb_pot_corr(const pb_fill_geom &g, int nf, const double *kw, int use_fp32,
 // Exact number of correction quadrature samples of one Lp / P fill at wavenumber kw
 // (used for throughput and roofline accounting).
 int pb_count_samples(const pb_fill_geom &g, double kw, double *lp_samples, double *p_samples,
-                     cudaStream_t s);
+                     cudaStream_t s, unsigned long long *d_count);
 
 // Internal impedance per segment (skin.c:112-133, mna.c:128-138, mna.c:254-258).
 int pb_zint(const pb_fill_geom &g, int skin, int nf, const double *freq, double2 *zint,

@@ -1042,7 +1042,7 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
                 sig.pop_back();
                 auto it = c->sample_counts.find(sig);
                 if (it == c->sample_counts.end()) {
-                    PB_TRY(pb_count_samples(c->g, kw, &lp_samp, &p_samp, st));
+                    PB_TRY(pb_count_samples(c->g, kw, &lp_samp, &p_samp, st, c->d_count));
                     c->sample_counts[sig] = std::make_pair(lp_samp, p_samp);
                 } else {
                     lp_samp = it->second.first;

@@ -7,6 +7,7 @@
 // the reference's rule in src/lu.c:19-30); everything above the leaves is row swaps,
 // a unit-lower triangular solve and a complex GEMM trailing update.
 // Row-major storage, like the reference (a[i*n+j]).
+#include <atomic>
 #include "pb_lu.cuh"
 #include <climits>
 #include <cuComplex.h>
@@ -323,7 +324,7 @@ template <typename T, int SW>
 static int launch_leaf(pb_lu_engine *e, T2_t<T> *a, int n, int ld, long long stride, int nb,
                        int k0, int w, int *piv, int *info, size_t smem)
 {
-    static bool attr_set = false;
+    static std::atomic<bool> attr_set{false};   // set once, before any launch relies on it
     if (!attr_set) {
         int dev = 0, cap = 0;
         cudaGetDevice(&dev);
@@ -355,7 +356,7 @@ static int trsm_rec(pb_lu_engine *e, T2_t<T> *a, int ld, long long stride, int n
 {
     if (c1 <= c0 || w <= 0) return PB_OK;
     if (w <= 64) {
-        static bool attr_set = false;
+        static std::atomic<bool> attr_set{false};   // set once, before any launch relies on it
         if (!attr_set) {
             PB_CUDA(cudaFuncSetAttribute(k_trsm_small<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (64 * 64 + 64 * 64) * (int)sizeof(T2_t<T>)));
@@ -564,7 +565,7 @@ int pb_lu_solve_mapped(pb_lu_engine *e, int n, int nb, int nrhs, const T2_t<TF> 
 {
     if (nb <= 0) return PB_OK;
     const size_t smem = (size_t)n * sizeof(T2_t<TF>);
-    static bool attr_set = false;
+    static std::atomic<bool> attr_set{false};   // set once, before any launch relies on it
     if (!attr_set) {
         int dev = 0, cap = 0;
         cudaGetDevice(&dev);
@@ -720,7 +721,7 @@ int pb_residual(pb_lu_engine *e, int n, int nb, int nrhs, const double2 *a, int 
     PB_CUDA(cudaMemsetAsync(bn, 0, sizeof(double) * nb * nrhs, e->stream));
     if (an) PB_CUDA(cudaMemsetAsync(an, 0, sizeof(double) * nb, e->stream));
     const size_t smem = (size_t)nrhs * n * sizeof(double2);
-    static bool attr_set = false;
+    static std::atomic<bool> attr_set{false};   // set once, before any launch relies on it
     if (!attr_set) {
         int dev = 0, cap = 0;
         cudaGetDevice(&dev);
@@ -745,7 +746,7 @@ int pb_residual_mapped(pb_lu_engine *e, int n, int nb, int nrhs, const double2 *
     if (an) PB_CUDA(cudaMemsetAsync(an, 0, sizeof(double) * nall, e->stream));
     if (nb <= 0) return PB_OK;
     const size_t smem = (size_t)nrhs * n * sizeof(double2);
-    static bool attr_set = false;
+    static std::atomic<bool> attr_set{false};   // set once, before any launch relies on it
     if (!attr_set) {
         int dev = 0, cap = 0;
         cudaGetDevice(&dev);
@@ -766,7 +767,7 @@ int pb_matvec_mapped(pb_lu_engine *e, int n, int nb, int nrhs, const double2 *a,
 {
     if (nb <= 0) return PB_OK;
     const size_t smem = (size_t)nrhs * n * sizeof(double2);
-    static bool attr_set = false;
+    static std::atomic<bool> attr_set{false};   // set once, before any launch relies on it
     if (!attr_set) {
         int dev = 0, cap = 0;
         cudaGetDevice(&dev);

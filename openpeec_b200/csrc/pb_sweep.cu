@@ -271,6 +271,8 @@ struct DevBuf {
 // Quadrature-level signature of a wavenumber: floor(kw * size) over the distinct cell
 // sizes that can be a pair's lmax (partial.c:166-173, 216-227). Equal signatures mean
 // every pair uses the same nsub, hence the same static part.
+thread_local int pb_mem_share = 1;
+
 void level_signature(const pb_ctx *c, double kw, std::vector<long> &sig)
 {
     sig.clear();
@@ -358,7 +360,8 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
     if (B <= 0) {
         double cached = 0;                       // storage this context already holds
         for (int q = 0; q < PB_SLOT_COMP0; q++) cached += (double)c->cache[q].cap;
-        const double avail = 0.80 * ((double)fr + cached) - fixed - 256e6;
+        // concurrent instances (pb_sweep_many) share the free memory
+        const double avail = 0.80 * ((double)fr + cached) / pb_mem_share - fixed - 256e6;
         B = (int)std::max(1.0, std::floor(avail / perf));
         B = std::min(B, 256);
     }
@@ -494,7 +497,7 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
                     // on the geometry and the level signature, so the context keeps it
                     auto it = c->sample_counts.find(sig);
                     if (it == c->sample_counts.end()) {
-                        PB_TRY(pb_count_samples(c->g, kw0, &lp_samp, &p_samp, st));
+                        PB_TRY(pb_count_samples(c->g, kw0, &lp_samp, &p_samp, st, c->d_count));
                         c->sample_counts[sig] = std::make_pair(lp_samp, p_samp);
                     } else {
                         lp_samp = it->second.first;
