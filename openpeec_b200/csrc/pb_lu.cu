@@ -332,7 +332,11 @@ static int launch_leaf(pb_lu_engine *e, T2_t<T> *a, int n, int ld, long long str
         PB_CUDA(cudaFuncSetAttribute(k_lu_leaf<T, SW>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap - 1024));
         attr_set = true;
     }
-    k_lu_leaf<T, SW><<<nb, 1024, smem, e->stream>>>(a, n, ld, stride, k0, w, piv, info);
+    // the panel has m = n - k0 rows: a CTA no wider than the panel (at least 128 threads)
+    // lets several small systems share an SM (batches of small structures); the pivot
+    // search and the updates do not depend on the thread count, so results are unchanged
+    const int m = n - k0, nt = std::min(1024, std::max(128, (m + 31) / 32 * 32));
+    k_lu_leaf<T, SW><<<nb, nt, smem, e->stream>>>(a, n, ld, stride, k0, w, piv, info);
     e->launches++;
     PB_CHECK_LAUNCH();
     return PB_OK;
