@@ -743,9 +743,10 @@ int pb_residual(pb_lu_engine *e, int n, int nb, int nrhs, const double2 *a, int 
 
 int pb_residual_mapped(pb_lu_engine *e, int n, int nb, int nrhs, const double2 *a, int ld, long stride,
                        const double2 *b, const double2 *x, double2 *r, double *rn, double *bn, double *xn,
-                       double *an, int nall, const int *sys)
+                       double *an, int nall, const int *sys, double *cw)
 {
     PB_CUDA(cudaMemsetAsync(rn, 0, sizeof(double) * nall * nrhs, e->stream));
+    if (cw) PB_CUDA(cudaMemsetAsync(cw, 0, sizeof(double) * nall * nrhs, e->stream));
     PB_CUDA(cudaMemsetAsync(bn, 0, sizeof(double) * nall * nrhs, e->stream));
     if (an) PB_CUDA(cudaMemsetAsync(an, 0, sizeof(double) * nall, e->stream));
     if (nb <= 0) return PB_OK;
@@ -760,7 +761,7 @@ int pb_residual_mapped(pb_lu_engine *e, int n, int nb, int nrhs, const double2 *
     }
     const int rpb = 64;
     dim3 g(ceil_div(n, rpb), nb);
-    k_residual<<<g, 256, smem, e->stream>>>(a, n, ld, stride, b, x, r, rn, bn, xn, an, nrhs, rpb, sys, nullptr);
+    k_residual<<<g, 256, smem, e->stream>>>(a, n, ld, stride, b, x, r, rn, bn, xn, an, nrhs, rpb, sys, cw);
     e->launches++;
     PB_CHECK_LAUNCH();
     return PB_OK;

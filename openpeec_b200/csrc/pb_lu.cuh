@@ -65,7 +65,7 @@ int pb_lu_solve_mapped(pb_lu_engine *e, int n, int nb, int nrhs,
 // systems are left at 0.
 int pb_residual_mapped(pb_lu_engine *e, int n, int nb, int nrhs, const double2 *a, int ld, long stride,
                        const double2 *b, const double2 *x, double2 *r, double *rn, double *bn, double *xn,
-                       double *an, int nall, const int *sys);
+                       double *an, int nall, const int *sys, double *cw = nullptr);
 
 // y = A x for the nb systems sys[0..nb) (nullptr = 0..nb), nrhs vectors each.
 int pb_matvec_mapped(pb_lu_engine *e, int n, int nb, int nrhs, const double2 *a, int ld, long stride,

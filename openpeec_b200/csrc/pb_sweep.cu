@@ -236,6 +236,16 @@ __global__ void k_axpy(double2 *x, const double2 *d, long long n)
     if (i < n) { x[i].x += d[i].x; x[i].y += d[i].y; }
 }
 
+// x += d for the systems sys[blockIdx.y] (m = entries per system)
+__global__ void k_axpy_sys(double2 *x, const double2 *d, long long m, const int *sys)
+{
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    const long long o = (long long)sys[blockIdx.y] * m + i;
+    x[o].x += d[o].x;
+    x[o].y += d[o].y;
+}
+
 // ---------------------------------------------------------------- helpers
 // Device buffer of one sweep call; with a context slot the storage stays with the context
 // for the next call (grow-only).
@@ -406,6 +416,8 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
     PB_TRY(bBn.alloc((size_t)B * nr * 8));
     DevBuf bCw(cs + 23);                          // componentwise backward errors (full form)
     PB_TRY(bCw.alloc((size_t)B * nr * 8));
+    DevBuf bSys(cs + 24);                         // systems still refining
+    PB_TRY(bSys.alloc((size_t)B * sizeof(int)));
     PB_TRY(bFreq.alloc((size_t)B * 8));
     PB_TRY(bZ.alloc((size_t)B * np * nr * 16 + 16));
     PB_TRY(bPC.alloc((size_t)2 * (np + 1) * 4));
@@ -708,11 +720,19 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
             const bool cwise = (form == PB_FORM_FULL);
             std::vector<double> prev(nb, 1e300), cwh((size_t)mb * nr, 0.0);
             for (int q = nd; q < nb; q++) if (state[q] == 1) state[q] = 0;
+            // only the systems still refining are touched after the first pass (the
+            // stragglers near the FP64 fallback take up to a dozen steps, most need 2-3)
+            std::vector<int> act;
             int it = 0;
             for (it = 1; it <= maxit + 1; it++) {
-                PB_TRY(pb_residual(&c->lu, n, mb, nr, m64, n, nn, bRhs.as<double2>() + vo, bX.as<double2>() + vo,
-                                   bR.as<double2>() + vo, bRn.as<double>(), bBn.as<double>(), bXn.as<double>(),
-                                   it == 1 ? bAn.as<double>() : nullptr, cwise ? bCw.as<double>() : nullptr));
+                act.clear();
+                for (int q = 0; q < mb; q++) if (state[nd + q] == 0) act.push_back(q);
+                if (act.empty()) break;
+                PB_CUDA(cudaMemcpyAsync(bSys.p, act.data(), sizeof(int) * act.size(), cudaMemcpyHostToDevice, st));
+                PB_TRY(pb_residual_mapped(&c->lu, n, (int)act.size(), nr, m64, n, nn, bRhs.as<double2>() + vo,
+                                          bX.as<double2>() + vo, bR.as<double2>() + vo, bRn.as<double>(),
+                                          bBn.as<double>(), bXn.as<double>(), it == 1 ? bAn.as<double>() : nullptr,
+                                          mb, bSys.as<int>(), cwise ? bCw.as<double>() : nullptr));
                 PB_CUDA(cudaMemcpyAsync(rnh.data(), bRn.p, sizeof(double) * mb * nr, cudaMemcpyDeviceToHost, st));
                 PB_CUDA(cudaMemcpyAsync(bnh.data(), bBn.p, sizeof(double) * mb * nr, cudaMemcpyDeviceToHost, st));
                 PB_CUDA(cudaMemcpyAsync(xnh.data(), bXn.p, sizeof(double) * mb * nr, cudaMemcpyDeviceToHost, st));
@@ -734,10 +754,14 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
                     else { prev[nd + q] = eta; active++; }
                 }
                 if (active == 0) break;
-                PB_TRY(pb_lu_solve_batched<float>(&c->lu, n, mb, nr, m32, n, nn, perm, bR.as<double2>() + vo,
-                                                  bD.as<double2>() + vo));
-                const long long mv = (long long)mb * nr * n;
-                k_axpy<<<ceil_div(mv, 256), 256, 0, st>>>(bX.as<double2>() + vo, bD.as<double2>() + vo, mv);
+                act.clear();
+                for (int q = 0; q < mb; q++) if (state[nd + q] == 0) act.push_back(q);
+                PB_CUDA(cudaMemcpyAsync(bSys.p, act.data(), sizeof(int) * act.size(), cudaMemcpyHostToDevice, st));
+                PB_TRY(pb_lu_solve_mapped<float>(&c->lu, n, (int)act.size(), nr, m32, n, nn, perm,
+                                                 bR.as<double2>() + vo, bD.as<double2>() + vo, bSys.as<int>(), nullptr));
+                const long long mv = (long long)nr * n;
+                k_axpy_sys<<<dim3(ceil_div(mv, 256), (unsigned)act.size()), 256, 0, st>>>(
+                    bX.as<double2>() + vo, bD.as<double2>() + vo, mv, bSys.as<int>());
                 c->launches++;
                 PB_CHECK_LAUNCH();
             }
