@@ -378,15 +378,16 @@ def run_barstack(args):
     X, T = pc_learn.collect([p for _, p in fam])
     w, hist = pc_learn.train(X, T, steps=3000, want_loss=True)
     t_train = time.time() - t0
-    out = {"plain": [], "learned": []}
+    out = {"plain": [], "learned": [], "two_level": []}
     with api.Context(prob) as ctx:
         ctx.sweep(freqs[:1])                                  # warm-up (allocations, static part)
-        for tag, wts in (("plain", None), ("learned", w)):
+        for tag, wts, coarse in (("plain", None, 0), ("learned", w, 0), ("two_level", None, 1)):
             for f in freqs:
                 t0 = time.perf_counter()
-                z, st = ctx.sweep([f], pc_mlp=wts)
+                z, st = ctx.sweep([f], pc_mlp=wts, pc_coarse=coarse)
                 dt = time.perf_counter() - t0
                 out[tag].append({"f_hz": float(f), "s": dt, "gmres_its": st["gmres_its_max"],
+                                 "coarse_n": st["pc_coarse_n"], "t_coarse_ms": st["t_coarse_ms"],
                                  "phases_ms": {"fill": st["t_corr_ms"], "compress": st["t_assemble_ms"],
                                                "precond": st["t_lu_ms"], "gmres": st["t_refine_ms"]},
                                  "fallbacks": st["pc_mlp_fallbacks"], "zin": [float(z[0, 0, 0].real), float(z[0, 0, 0].imag)]})
@@ -403,8 +404,12 @@ def run_barstack(args):
                    "current_cells": len(prob.seg), "freqs_hz": [float(f) for f in freqs]},
         "hmat": {"far": last["hmat_far"], "near": last["hmat_near"], "max_rank": last["hmat_max_rank"],
                  "mb": last["hmat_mb"], "dense_mb": last["hmat_dense_mb"]},
-        "gmres_its": {"plain": its_p, "learned": its_l,
-                      "ratio_plain_over_learned": float(sum(its_p) / max(1, sum(its_l)))},
+        "gmres_its": {"plain": its_p, "learned": its_l, "two_level": [r["gmres_its"] for r in out["two_level"]],
+                      "ratio_plain_over_learned": float(sum(its_p) / max(1, sum(its_l))),
+                      "ratio_plain_over_two_level": float(sum(its_p) / max(1, sum(r["gmres_its"] for r in out["two_level"])))},
+        "two_level": {"coarse_n": [r["coarse_n"] for r in out["two_level"]],
+                      "s_per_freq": sum(r["s"] for r in out["two_level"]) / len(freqs),
+                      "setup_ms": [r["t_coarse_ms"] for r in out["two_level"]]},
         "learned": {"train_samples": int(len(X)), "train_s": t_train, "loss_first_last": [float(hist[0]), float(hist[-1])],
                     "target_var": float(T.var(0).mean()), "fallbacks": [r["fallbacks"] for r in out["learned"]],
                     "s_per_freq": sum(r["s"] for r in out["learned"]) / len(freqs)},

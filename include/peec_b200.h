@@ -135,6 +135,11 @@ typedef struct {
                                correction of the preconditioner's leaf blocks, NULL = plain
                                preconditioner; the plain one is the fall back whenever the
                                corrected one fails (singular leaf, GMRES not converged) */
+    int pc_coarse;          /* compressed path: 1 = two-level preconditioner, a coarse
+                               correction over divergence-free coarse currents (one per leaf
+                               and current axis) applied before the plain preconditioner;
+                               0 = the plain preconditioner alone (the reference's) */
+    int pad3_;
 } pb_sweep_opts;
 
 typedef struct {
@@ -161,7 +166,8 @@ typedef struct {
     int    hmat_max_rank, hmat_dense_far; /* largest ACA rank; far blocks kept dense      */
     double hmat_mb, hmat_dense_mb;     /* H-matrix storage vs the dense Lp block [MiB]  */
     int    pc_mlp_fallbacks;           /* frequencies that fell back to the plain preconditioner */
-    int    pad2_;
+    int    pc_coarse_n;                /* coarse-space size of the two-level preconditioner */
+    double t_coarse_ms;                /* its set-up time (coarse basis and matrix) [ms]   */
 } pb_sweep_stats;
 
 const char *pb_last_error(void);

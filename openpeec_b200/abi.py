@@ -57,7 +57,7 @@ class PbSweepOpts(C.Structure):
         ("fill_prec", C.c_int), ("lu", C.c_int), ("form", C.c_int), ("batch", C.c_int),
         ("refine_tol", C.c_double), ("refine_maxit", C.c_int), ("verbose", C.c_int),
         ("corr_freqs", C.c_int), ("accel", C.c_int), ("compress", C.c_int), ("pad_", C.c_int),
-        ("ctol", C.c_double), ("pc_mlp", C.c_void_p),
+        ("ctol", C.c_double), ("pc_mlp", C.c_void_p), ("pc_coarse", C.c_int), ("pad3_", C.c_int),
     ]
 
 
@@ -75,7 +75,7 @@ class PbSweepStats(C.Structure):
         ("gmres_refactored", C.c_int), ("gmres_its_avg", C.c_double),
         ("hmat_far", C.c_int), ("hmat_near", C.c_int), ("hmat_max_rank", C.c_int),
         ("hmat_dense_far", C.c_int), ("hmat_mb", C.c_double), ("hmat_dense_mb", C.c_double),
-        ("pc_mlp_fallbacks", C.c_int), ("pad2_", C.c_int),
+        ("pc_mlp_fallbacks", C.c_int), ("pc_coarse_n", C.c_int), ("t_coarse_ms", C.c_double),
     ]
 
     def as_dict(self):

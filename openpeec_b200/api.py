@@ -65,7 +65,7 @@ class Context:
 
     def sweep(self, freqs, fill_prec=abi.PREC_MIXED, lu=abi.LU_TC, form=abi.FORM_AUTO,
               batch=0, refine_tol=0.0, refine_maxit=0, want_segi=False, zmat_out=None,
-              corr_freqs=0, verbose=0, accel=None, compress=None, ctol=None, pc_mlp=None):
+              corr_freqs=0, verbose=0, accel=None, compress=None, ctol=None, pc_mlp=None, pc_coarse=0):
         """pb_sweep. accel / compress / ctol = None take the .peec file's acceleration and
         compression keys."""
         accel = getattr(self.prob, "accel", 0) if accel is None else accel
@@ -81,6 +81,7 @@ class Context:
         if pc_mlp is not None:
             pc_mlp = np.ascontiguousarray(pc_mlp, np.float32)
             o.pc_mlp = pc_mlp.ctypes.data
+        o.pc_coarse = int(pc_coarse)
         st = abi.PbSweepStats()
         _check(abi.lib().pb_sweep(self.h, len(freqs), freqs.ctypes.data, C.byref(o),
                                   z.ctypes.data, None if segi is None else segi.ctypes.data,

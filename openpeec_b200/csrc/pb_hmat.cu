@@ -19,6 +19,7 @@
 #include <chrono>
 #include <thread>
 #include <cstdio>
+#include <cublas_v2.h>
 #include "pb_hmat.cuh"
 #include "pb_mlp.cuh"
 #include <algorithm>
@@ -462,6 +463,29 @@ __global__ void __launch_bounds__(256) k_leaf_solve(int nleaf, const int *lof, c
     }
     if (lane < m) z[idx[lane]] = v0;
     if (lane + 32 < m) z[idx[lane + 32]] = v1;
+}
+
+// Coarse right-hand sides of the two-level preconditioner: column g of W gets D v_g, with
+// v_g = +-1 on the cells of group g (one leaf, one current axis) and D the leaf block
+// (unfactored, row-major). One warp per group, lanes over the leaf's rows.
+__global__ void k_coarse_rhs(int ng, const int *goff, const int *gcell, const double *gsign, const int *cleaf,
+                             const int *cpos, const int *lof, const int *lidx, const long long *dof,
+                             const double2 *D, int off, long long N, double2 *W)
+{
+    const int g = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (g >= ng) return;
+    double2 *w = W + (long long)g * N + off;
+    for (int e = goff[g]; e < goff[g + 1]; e++) {
+        const int i = gcell[e], r = cleaf[i], a = cpos[i], mm = lof[r + 1] - lof[r];
+        const double sg = gsign[e];
+        for (int b = lane; b < mm; b += 32) {
+            const double2 d = D[dof[r] + (long long)b * mm + a];
+            double2 &t = w[lidx[lof[r] + b]];
+            t.x += sg * d.x;
+            t.y += sg * d.y;
+        }
+        __syncwarp();
+    }
 }
 
 // w[i] -= sum_e val[e] x[col[e]] over row i of a CSR matrix
@@ -925,7 +949,8 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
                         double gtol, double *zmat, pb_sweep_stats *stats, pb_hstats *hs, float *sample_x,
                         float *sample_t)
 {
-    int mlp_fallbacks = 0;
+    int mlp_fallbacks = 0, coarse_fallbacks = 0, coarse_n = 0;
+    double t_coarse = 0;
     const int ns = (int)c->seg.size(), N = c->nfull, offS = c->offS, n1 = c->offS, np = (int)c->port.size();
     const int cap = (c->capacitance && c->ncell > 0) ? 1 : 0;
     const int nc = cap ? c->ncell : 0, offQ = c->nunknown;
@@ -1357,6 +1382,131 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
             return PB_OK;
         };
 
+        // ---- two-level preconditioner (o.pc_coarse): a coarse correction over the
+        // divergence-free coarse currents W = M^-1 [0; D V], V one +-1 vector per (leaf,
+        // current axis) of the Lp block. M's Schur step makes every column satisfy the KCL
+        // rows exactly, so the coarse space holds loop currents (with their node
+        // potentials), which the leaf blocks cannot represent. Galerkin coarse matrix
+        // E = W^H A W (columns of A W in chunks), applied multiplicatively:
+        //   z1 = W E^-1 W^H r,  z = z1 + M^-1 (r - A z1).
+        int ncz = 0;
+        bool coarse_on = false;
+        Dev cW, cAW, cE, cEinv, cPiv, cPerm, cInfo, cT1, cT2, cC, cY, cGoff, cGcell, cGsign, cLeaf, cPos, cDpl;
+        auto build_coarse = [&]() -> int {
+            coarse_on = false;
+            if (!o.pc_coarse) return PB_OK;
+            tick();
+            KBlock &kb = kbs[0];
+            std::vector<int> goff(1, 0), gcell;
+            std::vector<double> gsign;
+            for (int r = 0; r < kb.nl; r++) {
+                std::vector<int> axc[3];
+                std::vector<double> axs[3];
+                for (int a = 0; a < kb.lof[r + 1] - kb.lof[r]; a++) {
+                    const int i = kb.lidx[kb.lof[r] + a];
+                    const pb_cell_t &sg = c->seg[i];
+                    int d = 0;
+                    double best = -1, t[3];
+                    for (int q = 0; q < 3; q++) {
+                        t[q] = (sg.x2[q] - sg.x1[q]) / sg.len;
+                        if (fabs(t[q]) > best) { best = fabs(t[q]); d = q; }
+                    }
+                    axc[d].push_back(i);
+                    axs[d].push_back(t[d] > 0 ? 1.0 : -1.0);
+                }
+                for (int d = 0; d < 3; d++)
+                    if (!axc[d].empty()) {
+                        gcell.insert(gcell.end(), axc[d].begin(), axc[d].end());
+                        gsign.insert(gsign.end(), axs[d].begin(), axs[d].end());
+                        goff.push_back((int)gcell.size());
+                    }
+            }
+            ncz = (int)goff.size() - 1;
+            if (ncz <= 0) return PB_OK;
+            PB_TRY(upload(cGoff, goff, st));
+            PB_TRY(upload(cGcell, gcell, st));
+            PB_TRY(upload(cGsign, gsign, st));
+            PB_TRY(upload(cLeaf, kb.sleaf, st));
+            PB_TRY(upload(cPos, kb.spos, st));
+            PB_TRY(upload(cDpl, dplain[0], st));
+            const size_t wsz = sizeof(double2) * (size_t)N * ncz;
+            PB_TRY(cW.alloc(wsz));
+            PB_CUDA(cudaMemsetAsync(cW.p, 0, wsz, st));
+            k_coarse_rhs<<<ceil_div(ncz, 8), 256, 0, st>>>(ncz, cGoff.as<int>(), cGcell.as<int>(), cGsign.as<double>(),
+                                                           cLeaf.as<int>(), cPos.as<int>(), kb.lof_d.as<int>(),
+                                                           kb.lidx_d.as<int>(), kb.dof_d.as<long long>(),
+                                                           cDpl.as<double2>(), kb.off, (long long)N, cW.as<double2>());
+            c->launches++;
+            PB_CHECK_LAUNCH();
+            for (int g = 0; g < ncz; g++) PB_TRY(opM(cW.as<double2>() + (size_t)g * N));
+            // E = W^H (A W), columns of A W in chunks
+            const int ck = (int)std::max<long long>(1, std::min<long long>(ncz, (1LL << 30) / ((long long)N * 16)));
+            PB_TRY(cAW.alloc(sizeof(double2) * (size_t)N * ck));
+            PB_TRY(cE.alloc(sizeof(double2) * (size_t)ncz * ncz));
+            const cuDoubleComplex one = make_cuDoubleComplex(1, 0), zero = make_cuDoubleComplex(0, 0);
+            for (int g0 = 0; g0 < ncz; g0 += ck) {
+                const int nb = std::min(ck, ncz - g0);
+                for (int q = 0; q < nb; q++)
+                    PB_TRY(opA(cW.as<double2>() + (size_t)(g0 + q) * N, cAW.as<double2>() + (size_t)q * N));
+                if (cublasZgemm(c->lu.blas, CUBLAS_OP_C, CUBLAS_OP_N, ncz, nb, N, &one,
+                                (const cuDoubleComplex *)cW.p, N, (const cuDoubleComplex *)cAW.p, N, &zero,
+                                (cuDoubleComplex *)cE.p + (size_t)g0 * ncz, ncz) != CUBLAS_STATUS_SUCCESS) {
+                    pb_set_error("two-level preconditioner: coarse matrix product failed");
+                    return PB_ERR_CUDA;
+                }
+                c->launches++;
+            }
+            // E is column-major, i.e. E^T row-major; the row-major inverse of E^T is E^-1
+            // column-major, which the coarse solve applies
+            PB_TRY(cPiv.alloc(sizeof(int) * ncz));
+            PB_TRY(cPerm.alloc(sizeof(int) * ncz));
+            PB_TRY(cInfo.alloc(sizeof(int)));
+            PB_TRY(cEinv.alloc(sizeof(double2) * (size_t)ncz * ncz));
+            PB_TRY(pb_lu_factor<double>(&c->lu, ncz, 1, cE.as<double2>(), ncz, (long)ncz * ncz, cPiv.as<int>(),
+                                        cInfo.as<int>()));
+            PB_TRY(pb_lu_perm(&c->lu, ncz, 1, cPiv.as<int>(), cPerm.as<int>()));
+            int info = -1;
+            PB_CUDA(cudaMemcpyAsync(&info, cInfo.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+            PB_CUDA(cudaStreamSynchronize(st));
+            if (info >= 0) {                     // singular coarse matrix: plain preconditioner
+                coarse_fallbacks++;
+                tock(t_coarse);
+                return PB_OK;
+            }
+            PB_TRY(pb_lu_inverse(&c->lu, ncz, cE.as<double2>(), ncz, cPerm.as<int>(), cEinv.as<double2>()));
+            PB_TRY(cT1.alloc(sizeof(double2) * N));
+            PB_TRY(cT2.alloc(sizeof(double2) * N));
+            PB_TRY(cC.alloc(sizeof(double2) * ncz));
+            PB_TRY(cY.alloc(sizeof(double2) * ncz));
+            coarse_on = true;
+            coarse_n = std::max(coarse_n, ncz);
+            tock(t_coarse);
+            return PB_OK;
+        };
+        PB_TRY(build_coarse());
+        auto opM2 = [&](double2 *z) -> int {
+            if (!coarse_on) return opM(z);
+            const cuDoubleComplex one = make_cuDoubleComplex(1, 0), zero = make_cuDoubleComplex(0, 0);
+            cublasStatus_t bs = cublasZgemv(c->lu.blas, CUBLAS_OP_C, N, ncz, &one, (const cuDoubleComplex *)cW.p, N,
+                                            (const cuDoubleComplex *)z, 1, &zero, (cuDoubleComplex *)cC.p, 1);
+            if (bs == CUBLAS_STATUS_SUCCESS)
+                bs = cublasZgemv(c->lu.blas, CUBLAS_OP_N, ncz, ncz, &one, (const cuDoubleComplex *)cEinv.p, ncz,
+                                 (const cuDoubleComplex *)cC.p, 1, &zero, (cuDoubleComplex *)cY.p, 1);
+            if (bs == CUBLAS_STATUS_SUCCESS)
+                bs = cublasZgemv(c->lu.blas, CUBLAS_OP_N, N, ncz, &one, (const cuDoubleComplex *)cW.p, N,
+                                 (const cuDoubleComplex *)cY.p, 1, &zero, (cuDoubleComplex *)cT1.p, 1);
+            if (bs != CUBLAS_STATUS_SUCCESS) { pb_set_error("two-level preconditioner: coarse solve failed"); return PB_ERR_CUDA; }
+            c->launches += 3;
+            PB_TRY(opA(cT1.as<double2>(), cT2.as<double2>()));
+            k_sub<<<gN, TB, 0, st>>>(N, z, cT2.as<double2>());                 // r - A z1
+            c->launches++;
+            PB_TRY(opM(cT2.as<double2>()));
+            k_axpy_c<<<gN, TB, 0, st>>>(N, make_double2(1, 0), cT1.as<double2>(), cT2.as<double2>());
+            c->launches++;
+            PB_CUDA(cudaMemcpyAsync(z, cT2.p, sizeof(double2) * N, cudaMemcpyDeviceToDevice, st));
+            PB_CHECK_LAUNCH();
+            return PB_OK;
+        };
         // ---- every port excitation: matrix-free GMRES (gmres_hmat, iterative.c:285-354)
         tick();
         auto solve_rhs = [&](int j, int &total, bool &done, int max_cycles) -> int {
@@ -1392,7 +1542,7 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
                 int iters = -1, jj = 0;
                 for (jj = 0; jj < m; jj++) {
                     PB_CUDA(cudaMemcpyAsync(bZ.p, Vk + (long long)jj * N, sizeof(double2) * N, cudaMemcpyDeviceToDevice, st));
-                    PB_TRY(timed(t_opM, [&]() { return opM(bZ.as<double2>()); }));
+                    PB_TRY(timed(t_opM, [&]() { return opM2(bZ.as<double2>()); }));
                     PB_TRY(timed(t_opA, [&]() { return opA(bZ.as<double2>(), bW.as<double2>()); }));
                     for (int i = 0; i <= jj; i++) {
                         zc hij;
@@ -1432,7 +1582,7 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
                 for (int l = 0; l < k; l++)
                     k_axpy_c<<<gN, TB, 0, st>>>(N, make_double2(y[l].real(), y[l].imag()), Vk + (long long)l * N,
                                                 bZ.as<double2>());
-                if (k > 0) PB_TRY(opM(bZ.as<double2>()));
+                if (k > 0) PB_TRY(opM2(bZ.as<double2>()));
                 k_axpy_c<<<gN, TB, 0, st>>>(N, make_double2(1, 0), bZ.as<double2>(), bX.as<double2>());
                 total += iters > 0 ? iters : m;
                 if (iters > 0) done = true;
@@ -1451,6 +1601,7 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
                 use_mlp = false;
                 mlp_fallbacks++;
                 PB_TRY(build_pc());
+                PB_TRY(build_coarse());
                 const int spent = total;
                 PB_TRY(solve_rhs(j, total, done, 10));
                 total += spent;
@@ -1506,6 +1657,8 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
         stats->hmat_mb = hs->mem_mb;
         stats->hmat_dense_mb = hs->dense_mb;
         stats->pc_mlp_fallbacks = mlp_fallbacks;
+        stats->pc_coarse_n = coarse_n;
+        stats->t_coarse_ms = t_coarse;
     }
     return PB_OK;
 }
