@@ -310,7 +310,9 @@ __global__ void k_gather(const double2 *K, int n, const int *perm, const DBlk *b
 }
 
 // ================================================================ device: H x vector
-struct FBlk { int r0, m, c0, nn; long long uoff, voff; int rank, toff; };
+// uoff: the block's U, scaled and row by row, in the compact Urm; usrc: its columns in the
+// ACA workspace U; voff: its V rows in the ACA workspace V.
+struct FBlk { int r0, m, c0, nn; long long uoff, voff; int rank, toff; long long usrc; };
 
 // t_b = V_b^T x (x in cell order)
 __global__ void k_hmv_t(const FBlk *fb, const double2 *V, const int *perm, const double2 *x, double2 *t)
@@ -329,6 +331,19 @@ __global__ void k_hmv_t(const FBlk *fb, const double2 *V, const int *perm, const
             si += __shfl_down_sync(0xffffffffu, si, o);
         }
         if (lane == 0) t[B.toff + l] = make_double2(sr, si);
+    }
+}
+
+// Far block b's U (m x rank, column by column as ACA writes it) scaled and stored row by
+// row in the compact Urm: Urm[uoff + row * rank + l] = scale U[usrc + l * m + row]. One CTA
+// per far block.
+__global__ void k_u_rowmajor(const FBlk *fb, const double2 *U, double2 scale, double2 *Urm)
+{
+    const FBlk B = fb[blockIdx.x];
+    const long long tot = (long long)B.m * B.rank;
+    for (long long e = threadIdx.x; e < tot; e += blockDim.x) {
+        const int row = (int)(e / B.rank), l = (int)(e - (long long)row * B.rank);
+        Urm[B.uoff + e] = cmul(scale, U[B.usrc + (long long)l * B.m + row]);
     }
 }
 
@@ -354,7 +369,7 @@ __global__ void k_hmv_y(int n, const int *perm, const int *leaf_of, const int *d
     for (int e = fr_off[L]; e < fr_off[L + 1]; e++) {
         const FBlk B = fb[fr_idx[e]];
         for (int l = lane; l < B.rank; l += 32) {
-            const double2 a = U[B.uoff + (long long)l * B.m + (r - B.r0)], b = t[B.toff + l];
+            const double2 a = U[B.uoff + (long long)(r - B.r0) * B.rank + l], b = t[B.toff + l];
             sr += a.x * b.x - a.y * b.y;
             si += a.x * b.y + a.y * b.x;
         }
@@ -366,9 +381,115 @@ __global__ void k_hmv_y(int n, const int *perm, const int *leaf_of, const int *d
     if (lane == 0) y[perm[r]] = make_double2(sr, si);
 }
 
-// ================================================================ device: sparse part, vectors
-__global__ void k_spmv(int n, const int *ro, const int *col, const double2 *val, const double2 *x, double2 *y)
+// H x for R vectors at once (the coarse-space set-up). The vectors are interleaved,
+// XT[p * R + q] = x_q[p], so the gather of one column index brings all R values in one
+// 16 R-byte segment; every matrix entry is read once per batch and applied to the R vectors
+// from registers. T and Y use the same layout.
+template <int R>
+__global__ void k_hmv_t_multi(const FBlk *fb, const double2 *V, const int *perm, const double2 *XT, double2 *TT)
 {
+    const FBlk B = fb[blockIdx.x];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int l = w; l < B.rank; l += nw) {
+        double sr[R], si[R];
+#pragma unroll
+        for (int q = 0; q < R; q++) sr[q] = si[q] = 0;
+        for (int j = lane; j < B.nn; j += 32) {
+            const double2 a = V[B.voff + (long long)l * B.nn + j];
+            const double2 *xp = XT + (long long)perm[B.c0 + j] * R;
+#pragma unroll
+            for (int q = 0; q < R; q++) {
+                const double2 b = xp[q];
+                sr[q] += a.x * b.x - a.y * b.y;
+                si[q] += a.x * b.y + a.y * b.x;
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < R; q++)
+            for (int o = 16; o > 0; o >>= 1) {
+                sr[q] += __shfl_down_sync(0xffffffffu, sr[q], o);
+                si[q] += __shfl_down_sync(0xffffffffu, si[q], o);
+            }
+        if (lane == 0)
+#pragma unroll
+            for (int q = 0; q < R; q++) TT[(long long)(B.toff + l) * R + q] = make_double2(sr[q], si[q]);
+    }
+}
+
+template <int R>
+__global__ void k_hmv_y_multi(int n, const int *perm, const int *leaf_of, const int *dn_off, const int *dn_idx,
+                              const DBlk *db, const double2 *D, const int *fr_off, const int *fr_idx, const FBlk *fb,
+                              const double2 *U, const double2 *TT, const double2 *XT, double2 *YT)
+{
+    const int r = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (r >= n) return;
+    const int L = leaf_of[r];
+    double sr[R], si[R];
+#pragma unroll
+    for (int q = 0; q < R; q++) sr[q] = si[q] = 0;
+    for (int e = dn_off[L]; e < dn_off[L + 1]; e++) {
+        const DBlk B = db[dn_idx[e]];
+        const double2 *row = D + B.off + (long long)(r - B.r0) * B.nn;
+        for (int j = lane; j < B.nn; j += 32) {
+            const double2 a = row[j];
+            const double2 *xp = XT + (long long)perm[B.c0 + j] * R;
+#pragma unroll
+            for (int q = 0; q < R; q++) {
+                const double2 b = xp[q];
+                sr[q] += a.x * b.x - a.y * b.y;
+                si[q] += a.x * b.y + a.y * b.x;
+            }
+        }
+    }
+    for (int e = fr_off[L]; e < fr_off[L + 1]; e++) {
+        const FBlk B = fb[fr_idx[e]];
+        for (int l = lane; l < B.rank; l += 32) {
+            const double2 a = U[B.uoff + (long long)(r - B.r0) * B.rank + l];
+            const double2 *tp = TT + (long long)(B.toff + l) * R;
+#pragma unroll
+            for (int q = 0; q < R; q++) {
+                const double2 b = tp[q];
+                sr[q] += a.x * b.x - a.y * b.y;
+                si[q] += a.x * b.y + a.y * b.x;
+            }
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < R; q++)
+        for (int o = 16; o > 0; o >>= 1) {
+            sr[q] += __shfl_down_sync(0xffffffffu, sr[q], o);
+            si[q] += __shfl_down_sync(0xffffffffu, si[q], o);
+        }
+    if (lane == 0)
+#pragma unroll
+        for (int q = 0; q < R; q++) YT[(long long)perm[r] * R + q] = make_double2(sr[q], si[q]);
+}
+
+// XT[p * R + q] = x_q[p] for q < nr, 0 for nr <= q < R (x_q at X + q * xs)
+__global__ void k_interleave(int n, int R, int nr, const double2 *X, long long xs, double2 *XT)
+{
+    const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (e >= (long long)n * R) return;
+    const int p = (int)(e / R), q = (int)(e % R);
+    XT[e] = q < nr ? X[q * xs + p] : make_double2(0, 0);
+}
+
+// y_q[p] += YT[p * R + q], q < nr
+__global__ void k_deinterleave_add(int n, int R, int nr, const double2 *YT, double2 *Y, long long ys)
+{
+    const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (e >= (long long)n * R) return;
+    const int p = (int)(e / R), q = (int)(e % R);
+    if (q < nr) Y[q * ys + p] = cadd(Y[q * ys + p], YT[e]);
+}
+
+// ================================================================ device: sparse part, vectors
+__global__ void k_spmv(int n, const int *ro, const int *col, const double2 *val, const double2 *x, double2 *y,
+                       long long xs = 0, long long ys = 0)
+{
+    x += blockIdx.y * xs;                               // vector blockIdx.y of a batch
+    y += blockIdx.y * ys;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double2 s = make_double2(0, 0);
@@ -419,8 +540,11 @@ __global__ void __launch_bounds__(1024) k_dotc(int n, const double2 *a, const do
 // ================================================================ device: preconditioner apply
 // z[idx] = D_r^-1 u[idx] for every leaf r (one thread per leaf; m <= PB_PC_MAXM)
 __global__ void __launch_bounds__(256) k_leaf_solve(int nleaf, const int *lof, const int *lidx, const long long *dof,
-                                                    const double2 *dlu, const int *dpiv, const double2 *u, double2 *z)
+                                                    const double2 *dlu, const int *dpiv, const double2 *u, double2 *z,
+                                                    long long us = 0, long long zs = 0)
 {
+    u += blockIdx.y * us;                               // vector blockIdx.y of a batch
+    z += blockIdx.y * zs;
     // one warp per leaf: lane q holds rows q and q + 32 (PB_PC_MAXM = 64); the row
     // interchanges run serially in shared memory, then column-oriented substitution with
     // each solved entry broadcast by a shuffle (blk_dsolve, precond.c:394-404)
@@ -489,8 +613,11 @@ __global__ void k_coarse_rhs(int ng, const int *goff, const int *gcell, const do
 }
 
 // w[i] -= sum_e val[e] x[col[e]] over row i of a CSR matrix
-__global__ void k_csr_sub(int n, const int *ro, const int *col, const double2 *val, const double2 *x, double2 *w)
+__global__ void k_csr_sub(int n, const int *ro, const int *col, const double2 *val, const double2 *x, double2 *w,
+                          long long xs = 0, long long ws = 0)
 {
+    x += blockIdx.y * xs;                               // vector blockIdx.y of a batch
+    w += blockIdx.y * ws;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double2 s = w[i];
@@ -611,7 +738,7 @@ struct KBlock {
     std::vector<int> leaf_of, leaf_lo, leaf_hi;
     std::vector<AcaBlk> ab;
     long long uo = 0, vo = 0, so = 0;
-    Dev perm, aca, rank, U, V, rused, urep, leaf_of_d;
+    Dev perm, aca, rank, U, V, rused, urep, leaf_of_d, Urm;
     // per build
     std::vector<DBlk> db;
     std::vector<FBlk> fb;
@@ -694,7 +821,7 @@ int kb_compress(KBlock &kb, const double2 *K, double ctol, pb_ctx *c, pb_hstats 
     PB_CUDA(cudaStreamSynchronize(st));
     kb.db.clear();
     kb.fb.clear();
-    long long doff = 0;
+    long long doff = 0, ucomp = 0;
     kb.toff = 0;
     size_t nz = 0;
     for (int q = 0; q < nnear; q++) {
@@ -710,7 +837,8 @@ int kb_compress(KBlock &kb, const double2 *K, double ctol, pb_ctx *c, pb_hstats 
             doff += (long long)A.m * A.nn;
             hs->ndense_far++;
         } else {
-            kb.fb.push_back(FBlk{A.r0, A.m, A.c0, A.nn, A.uoff, A.voff, rank[b], (int)kb.toff});
+            kb.fb.push_back(FBlk{A.r0, A.m, A.c0, A.nn, ucomp, A.voff, rank[b], (int)kb.toff, A.uoff});
+            ucomp += (long long)A.m * rank[b];
             kb.toff += rank[b];
             hs->max_rank = std::max(hs->max_rank, rank[b]);
             nz += (size_t)rank[b] * (A.m + A.nn);
@@ -747,16 +875,17 @@ int kb_compress(KBlock &kb, const double2 *K, double ctol, pb_ctx *c, pb_hstats 
         c->launches++;
         PB_CHECK_LAUNCH();
     }
-    // the low-rank factors carry the scale: U <- scale U
-    const double2 sm1 = make_double2(kb.scale.x - 1.0, kb.scale.y);
-    for (const FBlk &B : kb.fb) {
-        const long long cnt = (long long)B.rank * B.m;
-        k_axpy_c<<<ceil_div(cnt, 256), 256, 0, st>>>((int)cnt, sm1, kb.U.as<double2>() + B.uoff,
-                                                     kb.U.as<double2>() + B.uoff);
-        c->launches++;
-    }
-    PB_CHECK_LAUNCH();
+    // the low-rank factors carry the scale (U <- scale U) and are stored row by row in a
+    // compact array (U[row][l], only the ranks ACA reached): the matrix-vector product reads
+    // a row's rank entries with one warp, contiguously. One launch over all far blocks.
     PB_TRY(upload(kb.fblk, kb.fb, st));
+    if (!kb.fb.empty()) {
+        PB_TRY(kb.Urm.alloc(sizeof(double2) * (size_t)std::max(1LL, ucomp)));
+        k_u_rowmajor<<<(unsigned)kb.fb.size(), 256, 0, st>>>(kb.fblk.as<FBlk>(), kb.U.as<double2>(), kb.scale,
+                                                            kb.Urm.as<double2>());
+        c->launches++;
+        PB_CHECK_LAUNCH();
+    }
     PB_TRY(kb.t.alloc(sizeof(double2) * (size_t)std::max(1LL, kb.toff)));
     PB_TRY(upload(kb.dn_off, dn_off, st));
     PB_TRY(upload(kb.dn_idx, dn_idx, st));
@@ -806,7 +935,7 @@ int kb_apply(KBlock &kb, const double2 *x, double2 *y, pb_ctx *c)
                                                         x + kb.off, kb.t.as<double2>());
     k_hmv_y<<<ceil_div((long long)kb.n * 32, 256), 256, 0, st>>>(
         kb.n, kb.perm.as<int>(), kb.leaf_of_d.as<int>(), kb.dn_off.as<int>(), kb.dn_idx.as<int>(), kb.dblk.as<DBlk>(),
-        kb.D.as<double2>(), kb.fr_off.as<int>(), kb.fr_idx.as<int>(), kb.fblk.as<FBlk>(), kb.U.as<double2>(),
+        kb.D.as<double2>(), kb.fr_off.as<int>(), kb.fr_idx.as<int>(), kb.fblk.as<FBlk>(), kb.Urm.as<double2>(),
         kb.t.as<double2>(), x + kb.off, kb.hy.as<double2>());
     k_axpy_c<<<ceil_div(kb.n, 256), 256, 0, st>>>(kb.n, make_double2(1, 0), kb.hy.as<double2>(), y + kb.off);
     c->launches += 3;
@@ -1382,6 +1511,87 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
             return PB_OK;
         };
 
+        // ---- batched operators for the coarse-space set-up: R vectors at base + q N
+        Dev cU1, cU1b, cWB, cUB, cHY, cTm, cXT;
+        long long c_ts = 1;
+        constexpr int RM = 64, RA = 8;
+        auto coarse_buffers = [&]() -> int {
+            long long mxn = 1;
+            for (auto &kb : kbs) { mxn = std::max<long long>(mxn, kb.n); c_ts = std::max<long long>(c_ts, kb.toff); }
+            PB_TRY(cU1.alloc(sizeof(double2) * (size_t)std::max(1, n1) * RM));
+            PB_TRY(cU1b.alloc(sizeof(double2) * (size_t)std::max(1, n1) * RM));
+            PB_TRY(cWB.alloc(sizeof(double2) * (size_t)mxn * RM));
+            PB_TRY(cUB.alloc(sizeof(double2) * (size_t)mxn * RM));
+            PB_TRY(cHY.alloc(sizeof(double2) * (size_t)mxn * RA));
+            PB_TRY(cTm.alloc(sizeof(double2) * (size_t)c_ts * RA));
+            PB_TRY(cXT.alloc(sizeof(double2) * (size_t)mxn * RA));
+            return PB_OK;
+        };
+        auto opM_multi = [&](double2 *Z, int R) -> int {        // Z_q <- M^-1 Z_q, q < R <= RM
+            const size_t zb = sizeof(double2);
+            if (n1 > 0)
+                PB_CUDA(cudaMemcpy2DAsync(cU1.p, n1 * zb, Z, (size_t)N * zb, n1 * zb, R, cudaMemcpyDeviceToDevice, st));
+            for (auto &kb : kbs) {
+                k_leaf_solve<<<dim3(ceil_div(kb.nl, 8), R), 256, 0, st>>>(
+                    kb.nl, kb.lof_d.as<int>(), kb.lidx_d.as<int>(), kb.dof_d.as<long long>(), kb.dlu_d.as<double2>(),
+                    kb.dpiv_d.as<int>(), Z + kb.off, cWB.as<double2>(), (long long)N, (long long)kb.n);
+                if (n1 > 0)
+                    k_csr_sub<<<dim3(ceil_div(n1, TB), R), TB, 0, st>>>(n1, kb.bro.as<int>(), kb.bcol.as<int>(),
+                                                                        kb.bv.as<double2>(), cWB.as<double2>(),
+                                                                        cU1.as<double2>(), (long long)kb.n, (long long)n1);
+                c->launches += 2;
+            }
+            if (n1 > PB_SCHUR_INV) {
+                const cuDoubleComplex one = make_cuDoubleComplex(1, 0), zero = make_cuDoubleComplex(0, 0);
+                if (cublasZgemm(c->lu.blas, CUBLAS_OP_T, CUBLAS_OP_N, n1, R, n1, &one, (const cuDoubleComplex *)sinv.p,
+                                n1, (const cuDoubleComplex *)cU1.p, n1, &zero, (cuDoubleComplex *)Z, N) !=
+                    CUBLAS_STATUS_SUCCESS) {
+                    pb_set_error("two-level preconditioner: Schur product failed");
+                    return PB_ERR_CUDA;
+                }
+                c->launches++;
+            } else if (n1 > 0) {
+                PB_TRY(pb_lu_solve_batched<double>(&c->lu, n1, 1, R, slu.as<double2>(), n1, (long)n1 * n1,
+                                                   sperm.as<int>(), cU1.as<double2>(), cU1b.as<double2>()));
+                PB_CUDA(cudaMemcpy2DAsync(Z, (size_t)N * zb, cU1b.p, n1 * zb, n1 * zb, R, cudaMemcpyDeviceToDevice, st));
+            }
+            for (auto &kb : kbs) {
+                PB_CUDA(cudaMemcpy2DAsync(cUB.p, kb.n * zb, Z + kb.off, (size_t)N * zb, kb.n * zb, R,
+                                          cudaMemcpyDeviceToDevice, st));
+                if (n1 > 0)
+                    k_csr_sub<<<dim3(ceil_div(kb.n, TB), R), TB, 0, st>>>(kb.n, kb.cro.as<int>(), kb.ccol.as<int>(),
+                                                                          kb.cv.as<double2>(), Z, cUB.as<double2>(),
+                                                                          (long long)N, (long long)kb.n);
+                k_leaf_solve<<<dim3(ceil_div(kb.nl, 8), R), 256, 0, st>>>(
+                    kb.nl, kb.lof_d.as<int>(), kb.lidx_d.as<int>(), kb.dof_d.as<long long>(), kb.dlu_d.as<double2>(),
+                    kb.dpiv_d.as<int>(), cUB.as<double2>(), Z + kb.off, (long long)kb.n, (long long)N);
+                c->launches += 2;
+            }
+            PB_CHECK_LAUNCH();
+            return PB_OK;
+        };
+        auto opA_multi = [&](const double2 *X, double2 *Y, int R) -> int {   // Y_q = A X_q, q < R <= RA
+            k_spmv<<<dim3(gN, R), TB, 0, st>>>(N, bRo.as<int>(), bCol.as<int>(), bVal.as<double2>(), X, Y, (long long)N,
+                                               (long long)N);
+            c->launches++;
+            for (auto &kb : kbs) {
+                const long long ne = (long long)kb.n * RA;
+                k_interleave<<<ceil_div(ne, 256), 256, 0, st>>>(kb.n, RA, R, X + kb.off, (long long)N, cXT.as<double2>());
+                if (!kb.fb.empty())
+                    k_hmv_t_multi<RA><<<(unsigned)kb.fb.size(), 128, 0, st>>>(kb.fblk.as<FBlk>(), kb.V.as<double2>(),
+                                                                              kb.perm.as<int>(), cXT.as<double2>(),
+                                                                              cTm.as<double2>());
+                k_hmv_y_multi<RA><<<ceil_div((long long)kb.n * 32, 256), 256, 0, st>>>(
+                    kb.n, kb.perm.as<int>(), kb.leaf_of_d.as<int>(), kb.dn_off.as<int>(), kb.dn_idx.as<int>(),
+                    kb.dblk.as<DBlk>(), kb.D.as<double2>(), kb.fr_off.as<int>(), kb.fr_idx.as<int>(), kb.fblk.as<FBlk>(),
+                    kb.Urm.as<double2>(), cTm.as<double2>(), cXT.as<double2>(), cHY.as<double2>());
+                k_deinterleave_add<<<ceil_div(ne, 256), 256, 0, st>>>(kb.n, RA, R, cHY.as<double2>(), Y + kb.off,
+                                                                       (long long)N);
+                c->launches += 4;
+            }
+            PB_CHECK_LAUNCH();
+            return PB_OK;
+        };
         // ---- two-level preconditioner (o.pc_coarse): a coarse correction over the
         // divergence-free coarse currents W = M^-1 [0; D V], V one +-1 vector per (leaf,
         // current axis) of the Lp block. M's Schur step makes every column satisfy the KCL
@@ -1438,16 +1648,20 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
                                                            cDpl.as<double2>(), kb.off, (long long)N, cW.as<double2>());
             c->launches++;
             PB_CHECK_LAUNCH();
-            for (int g = 0; g < ncz; g++) PB_TRY(opM(cW.as<double2>() + (size_t)g * N));
-            // E = W^H (A W), columns of A W in chunks
+            PB_TRY(coarse_buffers());
+            for (int g0 = 0; g0 < ncz; g0 += RM) PB_TRY(opM_multi(cW.as<double2>() + (size_t)g0 * N, std::min(RM, ncz - g0)));
+            if (o.verbose) PB_CUDA(cudaStreamSynchronize(st));
+            mark("coarse basis");
+            // E = W^H (A W), columns of A W in chunks (batched products, 8 vectors at a time)
             const int ck = (int)std::max<long long>(1, std::min<long long>(ncz, (1LL << 30) / ((long long)N * 16)));
             PB_TRY(cAW.alloc(sizeof(double2) * (size_t)N * ck));
             PB_TRY(cE.alloc(sizeof(double2) * (size_t)ncz * ncz));
             const cuDoubleComplex one = make_cuDoubleComplex(1, 0), zero = make_cuDoubleComplex(0, 0);
             for (int g0 = 0; g0 < ncz; g0 += ck) {
                 const int nb = std::min(ck, ncz - g0);
-                for (int q = 0; q < nb; q++)
-                    PB_TRY(opA(cW.as<double2>() + (size_t)(g0 + q) * N, cAW.as<double2>() + (size_t)q * N));
+                for (int q0 = 0; q0 < nb; q0 += RA)
+                    PB_TRY(opA_multi(cW.as<double2>() + (size_t)(g0 + q0) * N, cAW.as<double2>() + (size_t)q0 * N,
+                                     std::min(RA, nb - q0)));
                 if (cublasZgemm(c->lu.blas, CUBLAS_OP_C, CUBLAS_OP_N, ncz, nb, N, &one,
                                 (const cuDoubleComplex *)cW.p, N, (const cuDoubleComplex *)cAW.p, N, &zero,
                                 (cuDoubleComplex *)cE.p + (size_t)g0 * ncz, ncz) != CUBLAS_STATUS_SUCCESS) {
@@ -1456,6 +1670,8 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
                 }
                 c->launches++;
             }
+            if (o.verbose) PB_CUDA(cudaStreamSynchronize(st));
+            mark("coarse matrix");
             // E is column-major, i.e. E^T row-major; the row-major inverse of E^T is E^-1
             // column-major, which the coarse solve applies
             PB_TRY(cPiv.alloc(sizeof(int) * ncz));
@@ -1481,6 +1697,7 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
             coarse_on = true;
             coarse_n = std::max(coarse_n, ncz);
             tock(t_coarse);
+            mark("coarse inverse");
             return PB_OK;
         };
         PB_TRY(build_coarse());

@@ -119,3 +119,17 @@ def test_two_level_cuts_iterations():
             z1, s1 = ctx.sweep([f], compress=1, pc_coarse=1)
             assert np.abs(z1 - z0).max() <= 1e-8 * np.abs(z0).max()
             assert 2 * s1["gmres_its_max"] <= s0["gmres_its_max"] + 1, (f, s0["gmres_its_max"], s1["gmres_its_max"])
+
+
+def test_two_level_large_circuit():
+    """A sheet with 1089 nodes: the coarse set-up then applies the explicit inverse of the
+    circuit Schur complement as one matrix product per batch of coarse vectors. Same Z as
+    the plain preconditioner, fewer iterations."""
+    from openpeec_b200 import api, configs, geometry
+    prob = geometry.build(geometry.parse_peec(configs.cfg4(32, 32, 1, 2)))
+    with api.Context(prob) as ctx:
+        assert ctx.nnode > 1024
+        z0, s0 = ctx.sweep([1e9], compress=1)
+        z1, s1 = ctx.sweep([1e9], compress=1, pc_coarse=1)
+    assert np.abs(z1 - z0).max() <= 1e-8 * np.abs(z0).max()
+    assert s1["gmres_its_max"] < s0["gmres_its_max"], (s0["gmres_its_max"], s1["gmres_its_max"])
