@@ -381,89 +381,104 @@ __global__ void k_hmv_y(int n, const int *perm, const int *leaf_of, const int *d
     if (lane == 0) y[perm[r]] = make_double2(sr, si);
 }
 
-// H x for R vectors at once (the coarse-space set-up). The vectors are interleaved,
-// XT[p * R + q] = x_q[p], so the gather of one column index brings all R values in one
-// 16 R-byte segment; every matrix entry is read once per batch and applied to the R vectors
-// from registers. T and Y use the same layout.
-template <int R>
-__global__ void k_hmv_t_multi(const FBlk *fb, const double2 *V, const int *perm, const double2 *XT, double2 *TT)
+// H x for 8 vectors at once (the coarse-space set-up), GEMM-shaped: the 8 vectors are
+// interleaved (XT[p * 8 + q] = x_q[p]); a CTA stages the 64-column tile of the vectors a
+// block needs in shared memory, and thread (row or rank index, q) accumulates its output
+// from the block entries, which the 8 threads of one row read from the same address.
+#define HM_R 8
+#define HM_TILE 64
+
+// T_b = V_b^T X over the columns of far block b (one CTA per far block)
+__global__ void __launch_bounds__(256)
+k_hmv_t_multi(const FBlk *fb, const double2 *V, const int *perm, const double2 *XT, double2 *TT)
 {
+    __shared__ double2 xs[HM_TILE * HM_R];
     const FBlk B = fb[blockIdx.x];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int l = w; l < B.rank; l += nw) {
-        double sr[R], si[R];
+    const int q = threadIdx.x & (HM_R - 1), ls = threadIdx.x >> 3;          // 32 rank slots
+    constexpr int NL = (PB_HM_MAXIT + 31) / 32;
+    double2 acc[NL];
 #pragma unroll
-        for (int q = 0; q < R; q++) sr[q] = si[q] = 0;
-        for (int j = lane; j < B.nn; j += 32) {
-            const double2 a = V[B.voff + (long long)l * B.nn + j];
-            const double2 *xp = XT + (long long)perm[B.c0 + j] * R;
+    for (int i = 0; i < NL; i++) acc[i] = make_double2(0, 0);
+    for (int j0 = 0; j0 < B.nn; j0 += HM_TILE) {
+        const int nt = min(HM_TILE, B.nn - j0);
+        __syncthreads();
+        for (int k = threadIdx.x; k < nt * HM_R; k += blockDim.x)
+            xs[k] = XT[(long long)perm[B.c0 + j0 + (k >> 3)] * HM_R + (k & (HM_R - 1))];
+        __syncthreads();
 #pragma unroll
-            for (int q = 0; q < R; q++) {
-                const double2 b = xp[q];
-                sr[q] += a.x * b.x - a.y * b.y;
-                si[q] += a.x * b.y + a.y * b.x;
+        for (int i = 0; i < NL; i++) {
+            const int l = ls + 32 * i;
+            if (l < B.rank) {
+                const double2 *v = V + B.voff + (long long)l * B.nn + j0;
+                double2 a = acc[i];
+                for (int jj = 0; jj < nt; jj++) a = cadd(a, cmul(v[jj], xs[jj * HM_R + q]));
+                acc[i] = a;
             }
         }
+    }
 #pragma unroll
-        for (int q = 0; q < R; q++)
-            for (int o = 16; o > 0; o >>= 1) {
-                sr[q] += __shfl_down_sync(0xffffffffu, sr[q], o);
-                si[q] += __shfl_down_sync(0xffffffffu, si[q], o);
-            }
-        if (lane == 0)
-#pragma unroll
-            for (int q = 0; q < R; q++) TT[(long long)(B.toff + l) * R + q] = make_double2(sr[q], si[q]);
+    for (int i = 0; i < NL; i++) {
+        const int l = ls + 32 * i;
+        if (l < B.rank) TT[(long long)(B.toff + l) * HM_R + q] = acc[i];
     }
 }
 
-template <int R>
-__global__ void k_hmv_y_multi(int n, const int *perm, const int *leaf_of, const int *dn_off, const int *dn_idx,
-                              const DBlk *db, const double2 *D, const int *fr_off, const int *fr_idx, const FBlk *fb,
-                              const double2 *U, const double2 *TT, const double2 *XT, double2 *YT)
+// Y rows of leaf L = near blocks x X + far blocks' U x T (one CTA per leaf, blocks in the
+// leaf's list order: deterministic)
+__global__ void __launch_bounds__(256)
+k_hmv_leaf_multi(const int *llo, const int *lhi, const int *perm, const int *dn_off, const int *dn_idx,
+                 const DBlk *db, const double2 *D, const int *fr_off, const int *fr_idx, const FBlk *fb,
+                 const double2 *U, const double2 *TT, const double2 *XT, double2 *YT)
 {
-    const int r = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
-    const int lane = threadIdx.x & 31;
-    if (r >= n) return;
-    const int L = leaf_of[r];
-    double sr[R], si[R];
-#pragma unroll
-    for (int q = 0; q < R; q++) sr[q] = si[q] = 0;
+    __shared__ double2 xs[HM_TILE * HM_R];
+    const int L = blockIdx.x, lo = llo[L], hi = lhi[L];
+    const int q = threadIdx.x & (HM_R - 1), rs = threadIdx.x >> 3;          // 32 row slots
+    double2 acc[2] = {make_double2(0, 0), make_double2(0, 0)};              // rows lo+rs, lo+rs+32
     for (int e = dn_off[L]; e < dn_off[L + 1]; e++) {
         const DBlk B = db[dn_idx[e]];
-        const double2 *row = D + B.off + (long long)(r - B.r0) * B.nn;
-        for (int j = lane; j < B.nn; j += 32) {
-            const double2 a = row[j];
-            const double2 *xp = XT + (long long)perm[B.c0 + j] * R;
+        for (int j0 = 0; j0 < B.nn; j0 += HM_TILE) {
+            const int nt = min(HM_TILE, B.nn - j0);
+            __syncthreads();
+            for (int k = threadIdx.x; k < nt * HM_R; k += blockDim.x)
+                xs[k] = XT[(long long)perm[B.c0 + j0 + (k >> 3)] * HM_R + (k & (HM_R - 1))];
+            __syncthreads();
 #pragma unroll
-            for (int q = 0; q < R; q++) {
-                const double2 b = xp[q];
-                sr[q] += a.x * b.x - a.y * b.y;
-                si[q] += a.x * b.y + a.y * b.x;
+            for (int h = 0; h < 2; h++) {
+                const int r = lo + rs + 32 * h;
+                if (r < hi && r >= B.r0 && r < B.r0 + B.m) {
+                    const double2 *row = D + B.off + (long long)(r - B.r0) * B.nn + j0;
+                    double2 a = acc[h];
+                    for (int jj = 0; jj < nt; jj++) a = cadd(a, cmul(row[jj], xs[jj * HM_R + q]));
+                    acc[h] = a;
+                }
             }
         }
     }
     for (int e = fr_off[L]; e < fr_off[L + 1]; e++) {
         const FBlk B = fb[fr_idx[e]];
-        for (int l = lane; l < B.rank; l += 32) {
-            const double2 a = U[B.uoff + (long long)(r - B.r0) * B.rank + l];
-            const double2 *tp = TT + (long long)(B.toff + l) * R;
+        for (int l0 = 0; l0 < B.rank; l0 += HM_TILE) {
+            const int nt = min(HM_TILE, B.rank - l0);
+            __syncthreads();
+            for (int k = threadIdx.x; k < nt * HM_R; k += blockDim.x)
+                xs[k] = TT[(long long)(B.toff + l0 + (k >> 3)) * HM_R + (k & (HM_R - 1))];
+            __syncthreads();
 #pragma unroll
-            for (int q = 0; q < R; q++) {
-                const double2 b = tp[q];
-                sr[q] += a.x * b.x - a.y * b.y;
-                si[q] += a.x * b.y + a.y * b.x;
+            for (int h = 0; h < 2; h++) {
+                const int r = lo + rs + 32 * h;
+                if (r < hi && r >= B.r0 && r < B.r0 + B.m) {
+                    const double2 *u = U + B.uoff + (long long)(r - B.r0) * B.rank + l0;
+                    double2 a = acc[h];
+                    for (int ll = 0; ll < nt; ll++) a = cadd(a, cmul(u[ll], xs[ll * HM_R + q]));
+                    acc[h] = a;
+                }
             }
         }
     }
 #pragma unroll
-    for (int q = 0; q < R; q++)
-        for (int o = 16; o > 0; o >>= 1) {
-            sr[q] += __shfl_down_sync(0xffffffffu, sr[q], o);
-            si[q] += __shfl_down_sync(0xffffffffu, si[q], o);
-        }
-    if (lane == 0)
-#pragma unroll
-        for (int q = 0; q < R; q++) YT[(long long)perm[r] * R + q] = make_double2(sr[q], si[q]);
+    for (int h = 0; h < 2; h++) {
+        const int r = lo + rs + 32 * h;
+        if (r < hi) YT[(long long)perm[r] * HM_R + q] = acc[h];
+    }
 }
 
 // XT[p * R + q] = x_q[p] for q < nr, 0 for nr <= q < R (x_q at X + q * xs)
@@ -738,7 +753,7 @@ struct KBlock {
     std::vector<int> leaf_of, leaf_lo, leaf_hi;
     std::vector<AcaBlk> ab;
     long long uo = 0, vo = 0, so = 0;
-    Dev perm, aca, rank, U, V, rused, urep, leaf_of_d, Urm;
+    Dev perm, aca, rank, U, V, rused, urep, leaf_of_d, Urm, leaf_lo_d, leaf_hi_d;
     // per build
     std::vector<DBlk> db;
     std::vector<FBlk> fb;
@@ -1513,8 +1528,9 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
 
         // ---- batched operators for the coarse-space set-up: R vectors at base + q N
         Dev cU1, cU1b, cWB, cUB, cHY, cTm, cXT;
+        double t_cm_t = 0, t_cm_y = 0, t_cm_g = 0;          // verbose >= 2: coarse-matrix kernels
         long long c_ts = 1;
-        constexpr int RM = 64, RA = 8;
+        constexpr int RM = 64, RA = HM_R;
         auto coarse_buffers = [&]() -> int {
             long long mxn = 1;
             for (auto &kb : kbs) { mxn = std::max<long long>(mxn, kb.n); c_ts = std::max<long long>(c_ts, kb.toff); }
@@ -1525,6 +1541,10 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
             PB_TRY(cHY.alloc(sizeof(double2) * (size_t)mxn * RA));
             PB_TRY(cTm.alloc(sizeof(double2) * (size_t)c_ts * RA));
             PB_TRY(cXT.alloc(sizeof(double2) * (size_t)mxn * RA));
+            for (auto &kb : kbs) {
+                PB_TRY(upload(kb.leaf_lo_d, kb.leaf_lo, st));
+                PB_TRY(upload(kb.leaf_hi_d, kb.leaf_hi, st));
+            }
             return PB_OK;
         };
         auto opM_multi = [&](double2 *Z, int R) -> int {        // Z_q <- M^-1 Z_q, q < R <= RM
@@ -1578,13 +1598,20 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
                 const long long ne = (long long)kb.n * RA;
                 k_interleave<<<ceil_div(ne, 256), 256, 0, st>>>(kb.n, RA, R, X + kb.off, (long long)N, cXT.as<double2>());
                 if (!kb.fb.empty())
-                    k_hmv_t_multi<RA><<<(unsigned)kb.fb.size(), 128, 0, st>>>(kb.fblk.as<FBlk>(), kb.V.as<double2>(),
+                    PB_TRY(timed(t_cm_t, [&]() {
+                        k_hmv_t_multi<<<(unsigned)kb.fb.size(), 256, 0, st>>>(kb.fblk.as<FBlk>(), kb.V.as<double2>(),
                                                                               kb.perm.as<int>(), cXT.as<double2>(),
                                                                               cTm.as<double2>());
-                k_hmv_y_multi<RA><<<ceil_div((long long)kb.n * 32, 256), 256, 0, st>>>(
-                    kb.n, kb.perm.as<int>(), kb.leaf_of_d.as<int>(), kb.dn_off.as<int>(), kb.dn_idx.as<int>(),
-                    kb.dblk.as<DBlk>(), kb.D.as<double2>(), kb.fr_off.as<int>(), kb.fr_idx.as<int>(), kb.fblk.as<FBlk>(),
-                    kb.Urm.as<double2>(), cTm.as<double2>(), cXT.as<double2>(), cHY.as<double2>());
+                        return PB_OK;
+                    }));
+                PB_TRY(timed(t_cm_y, [&]() {
+                    k_hmv_leaf_multi<<<kb.nl, 256, 0, st>>>(
+                        kb.leaf_lo_d.as<int>(), kb.leaf_hi_d.as<int>(), kb.perm.as<int>(), kb.dn_off.as<int>(),
+                        kb.dn_idx.as<int>(), kb.dblk.as<DBlk>(), kb.D.as<double2>(), kb.fr_off.as<int>(),
+                        kb.fr_idx.as<int>(), kb.fblk.as<FBlk>(), kb.Urm.as<double2>(), cTm.as<double2>(),
+                        cXT.as<double2>(), cHY.as<double2>());
+                    return PB_OK;
+                }));
                 k_deinterleave_add<<<ceil_div(ne, 256), 256, 0, st>>>(kb.n, RA, R, cHY.as<double2>(), Y + kb.off,
                                                                        (long long)N);
                 c->launches += 4;
@@ -1662,16 +1689,22 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
                 for (int q0 = 0; q0 < nb; q0 += RA)
                     PB_TRY(opA_multi(cW.as<double2>() + (size_t)(g0 + q0) * N, cAW.as<double2>() + (size_t)q0 * N,
                                      std::min(RA, nb - q0)));
-                if (cublasZgemm(c->lu.blas, CUBLAS_OP_C, CUBLAS_OP_N, ncz, nb, N, &one,
-                                (const cuDoubleComplex *)cW.p, N, (const cuDoubleComplex *)cAW.p, N, &zero,
-                                (cuDoubleComplex *)cE.p + (size_t)g0 * ncz, ncz) != CUBLAS_STATUS_SUCCESS) {
-                    pb_set_error("two-level preconditioner: coarse matrix product failed");
-                    return PB_ERR_CUDA;
-                }
+                PB_TRY(timed(t_cm_g, [&]() {
+                    if (cublasZgemm(c->lu.blas, CUBLAS_OP_C, CUBLAS_OP_N, ncz, nb, N, &one,
+                                    (const cuDoubleComplex *)cW.p, N, (const cuDoubleComplex *)cAW.p, N, &zero,
+                                    (cuDoubleComplex *)cE.p + (size_t)g0 * ncz, ncz) != CUBLAS_STATUS_SUCCESS) {
+                        pb_set_error("two-level preconditioner: coarse matrix product failed");
+                        return PB_ERR_CUDA;
+                    }
+                    return PB_OK;
+                }));
                 c->launches++;
             }
             if (o.verbose) PB_CUDA(cudaStreamSynchronize(st));
             mark("coarse matrix");
+            if (o.verbose >= 2)
+                fprintf(stderr, "[compressed f=%.5g] coarse matrix: V^T X %.1f ms, leaf rows %.1f ms, W^H AW %.1f ms\n", f,
+                        t_cm_t, t_cm_y, t_cm_g);
             // E is column-major, i.e. E^T row-major; the row-major inverse of E^T is E^-1
             // column-major, which the coarse solve applies
             PB_TRY(cPiv.alloc(sizeof(int) * ncz));
