@@ -76,7 +76,8 @@ class Clocks:
 
     def __init__(self):
         self.p = None
-        self.out = os.path.join(ROOT, "gpurun_out", "clocks_%d.csv" % os.getpid())
+        import tempfile
+        self.out = os.path.join(tempfile.gettempdir(), "pb_clocks_%d.csv" % os.getpid())
 
     def start(self):
         try:
@@ -147,7 +148,8 @@ def cpu_baseline(prob, budget_s=25.0):
     npairs = nseg * (nseg + 1) // 2
     kind = "reference" if pyoracle.ref_available() else "port"
     if kind == "reference":
-        path = os.path.join(ROOT, "gpurun_out", "_cfg2_%d.peec" % os.getpid())
+        import tempfile
+        path = os.path.join(tempfile.gettempdir(), "pb_cfg2_%d.peec" % os.getpid())
         os.makedirs(os.path.dirname(path), exist_ok=True)
         open(path, "w").write(configs.CFG2)
         ref = pyoracle.RefLib(path, light=True)
