@@ -383,7 +383,7 @@ def run_barstack(args):
     out = {"plain": [], "learned": [], "two_level": []}
     with api.Context(prob) as ctx:
         ctx.sweep(freqs[:1])                                  # warm-up (allocations, static part)
-        for tag, wts, coarse in (("plain", None, 0), ("learned", w, 0), ("two_level", None, 1)):
+        for tag, wts, coarse in (("plain", None, 0), ("learned", w, 0), ("two_level", None, args.coarse_level)):
             for f in freqs:
                 t0 = time.perf_counter()
                 z, st = ctx.sweep([f], pc_mlp=wts, pc_coarse=coarse)
@@ -409,7 +409,7 @@ def run_barstack(args):
         "gmres_its": {"plain": its_p, "learned": its_l, "two_level": [r["gmres_its"] for r in out["two_level"]],
                       "ratio_plain_over_learned": float(sum(its_p) / max(1, sum(its_l))),
                       "ratio_plain_over_two_level": float(sum(its_p) / max(1, sum(r["gmres_its"] for r in out["two_level"])))},
-        "two_level": {"coarse_n": [r["coarse_n"] for r in out["two_level"]],
+        "two_level": {"level": args.coarse_level, "coarse_n": [r["coarse_n"] for r in out["two_level"]],
                       "s_per_freq": sum(r["s"] for r in out["two_level"]) / len(freqs),
                       "setup_ms": [r["t_coarse_ms"] for r in out["two_level"]]},
         "learned": {"train_samples": int(len(X)), "train_s": t_train, "loss_first_last": [float(hist[0]), float(hist[-1])],
@@ -519,6 +519,8 @@ def main():
                     help="LU reuse: one FP32 factorisation per ACCEL frequencies, GMRES for the rest (0 = every frequency)")
     ap.add_argument("--batch3", type=int, default=0,
                     help="N: time config 3 (N random thin-wire structures) through pb_sweep_many instead")
+    ap.add_argument("--coarse-level", type=int, default=4,
+                    help="--barstack: aggregation level of the two-level preconditioner (1 = leaves)")
     ap.add_argument("--barstack", default="",
                     help="NXxNYxNZ: time the compressed path on the bar stack instead (e.g. 96x96x4)")
     args = ap.parse_args()

@@ -135,10 +135,12 @@ typedef struct {
                                correction of the preconditioner's leaf blocks, NULL = plain
                                preconditioner; the plain one is the fall back whenever the
                                corrected one fails (singular leaf, GMRES not converged) */
-    int pc_coarse;          /* compressed path: 1 = two-level preconditioner, a coarse
-                               correction over divergence-free coarse currents (one per leaf
-                               and current axis) applied before the plain preconditioner;
-                               0 = the plain preconditioner alone (the reference's) */
+    int pc_coarse;          /* compressed path: >= 1 = two-level preconditioner, a coarse
+                               correction over divergence-free coarse currents (one per
+                               aggregate and current axis; aggregates = the leaves for 1, their
+                               ancestors pc_coarse - 1 levels up otherwise) applied before the
+                               plain preconditioner; 0 = the plain preconditioner alone (the
+                               reference's) */
     int pad3_;
 } pb_sweep_opts;
 

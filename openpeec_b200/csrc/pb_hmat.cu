@@ -1634,23 +1634,42 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
             if (!o.pc_coarse) return PB_OK;
             tick();
             KBlock &kb = kbs[0];
+            // aggregates: the leaves (pc_coarse = 1) or their ancestors pc_coarse - 1 levels up
+            // (fewer, larger coarse vectors: cheaper set-up, weaker correction)
+            std::vector<int> parent(kb.T.lo.size(), -1);
+            for (size_t q = 0; q < kb.T.lo.size(); q++)
+                if (kb.T.left[q] >= 0) { parent[kb.T.left[q]] = (int)q; parent[kb.T.right[q]] = (int)q; }
+            std::vector<int> agg_of(kb.nl), aggs;
+            {
+                std::map<int, int> id;
+                for (int r = 0; r < kb.nl; r++) {
+                    int cl = kb.T.leafid[r];
+                    for (int up = 1; up < o.pc_coarse && parent[cl] >= 0; up++) cl = parent[cl];
+                    auto it = id.find(cl);
+                    if (it == id.end()) { id[cl] = (int)aggs.size(); agg_of[r] = (int)aggs.size(); aggs.push_back(cl); }
+                    else agg_of[r] = it->second;
+                }
+            }
+            std::vector<std::vector<int>> agg_leaves(aggs.size());
+            for (int r = 0; r < kb.nl; r++) agg_leaves[agg_of[r]].push_back(r);
             std::vector<int> goff(1, 0), gcell;
             std::vector<double> gsign;
-            for (int r = 0; r < kb.nl; r++) {
+            for (const auto &lv : agg_leaves) {
                 std::vector<int> axc[3];
                 std::vector<double> axs[3];
-                for (int a = 0; a < kb.lof[r + 1] - kb.lof[r]; a++) {
-                    const int i = kb.lidx[kb.lof[r] + a];
-                    const pb_cell_t &sg = c->seg[i];
-                    int d = 0;
-                    double best = -1, t[3];
-                    for (int q = 0; q < 3; q++) {
-                        t[q] = (sg.x2[q] - sg.x1[q]) / sg.len;
-                        if (fabs(t[q]) > best) { best = fabs(t[q]); d = q; }
+                for (int r : lv)
+                    for (int a = 0; a < kb.lof[r + 1] - kb.lof[r]; a++) {
+                        const int i = kb.lidx[kb.lof[r] + a];
+                        const pb_cell_t &sg = c->seg[i];
+                        int d = 0;
+                        double best = -1, t[3];
+                        for (int q = 0; q < 3; q++) {
+                            t[q] = (sg.x2[q] - sg.x1[q]) / sg.len;
+                            if (fabs(t[q]) > best) { best = fabs(t[q]); d = q; }
+                        }
+                        axc[d].push_back(i);
+                        axs[d].push_back(t[d] > 0 ? 1.0 : -1.0);
                     }
-                    axc[d].push_back(i);
-                    axs[d].push_back(t[d] > 0 ? 1.0 : -1.0);
-                }
                 for (int d = 0; d < 3; d++)
                     if (!axc[d].empty()) {
                         gcell.insert(gcell.end(), axc[d].begin(), axc[d].end());
