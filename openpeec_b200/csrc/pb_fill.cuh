@@ -62,9 +62,10 @@ int pb_pot_corr(const pb_fill_geom &g, int nf, const double *kw, int use_fp32,
                 cudaStream_t s, long *launches, double *samples);
 
 // Exact number of correction quadrature samples of one Lp / P fill at wavenumber kw
-// (used for throughput and roofline accounting).
+// (used for throughput and roofline accounting); kw_far32 > 0: as the FP32 path samples
+// a launch whose largest wavenumber is kw_far32 (0: the FP64 path).
 int pb_count_samples(const pb_fill_geom &g, double kw, double *lp_samples, double *p_samples,
-                     cudaStream_t s, unsigned long long *d_count);
+                     cudaStream_t s, unsigned long long *d_count, double kw_far32);
 
 // Internal impedance per segment (skin.c:112-133, mna.c:128-138, mna.c:254-258).
 int pb_zint(const pb_fill_geom &g, int skin, int nf, const double *freq, double2 *zint,

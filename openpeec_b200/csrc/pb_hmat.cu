@@ -1209,10 +1209,14 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
             }
             if (kw > 0) {
                 sig.pop_back();
-                auto it = c->sample_counts.find(sig);
+                std::vector<long> skey(sig);
+                long kbits = -2;                            // the FP32 path samples far ribbons less
+                if (fill32) std::memcpy(&kbits, &kw, sizeof kbits);
+                skey.push_back(kbits);
+                auto it = c->sample_counts.find(skey);
                 if (it == c->sample_counts.end()) {
-                    PB_TRY(pb_count_samples(c->g, kw, &lp_samp, &p_samp, st, c->d_count));
-                    c->sample_counts[sig] = std::make_pair(lp_samp, p_samp);
+                    PB_TRY(pb_count_samples(c->g, kw, &lp_samp, &p_samp, st, c->d_count, fill32 ? kw : 0.0));
+                    c->sample_counts[skey] = std::make_pair(lp_samp, p_samp);
                 } else {
                     lp_samp = it->second.first;
                     p_samp = it->second.second;

@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <cmath>
 #include <vector>
+#include <cstring>
 
 // ---------------------------------------------------------------- small kernels
 // rhs'[f][j][k] = (P b_j)[ca_k] - (P b_j)[cb_k],  b_j = e(pc1_j) - e(pc2_j)   (cells)
@@ -504,25 +505,34 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
                 if (c->capacitance && nc > 0) PB_TRY(pb_pot_static(c->g, kw0, bStP.as<double>(), st, &c->launches));
                 PB_TRY(pb_lp_static(c->g, kw0, bStLp.as<double>(), st, &c->launches));
                 tStatic.stop(st);
-                if (kw0 > 0) {
-                    // exact quadrature-sample count of this level (statistics only): it depends
-                    // on the geometry and the level signature, so the context keeps it
-                    auto it = c->sample_counts.find(sig);
-                    if (it == c->sample_counts.end()) {
-                        PB_TRY(pb_count_samples(c->g, kw0, &lp_samp, &p_samp, st, c->d_count));
-                        c->sample_counts[sig] = std::make_pair(lp_samp, p_samp);
-                    } else {
-                        lp_samp = it->second.first;
-                        p_samp = it->second.second;
-                    }
-                }
-                else lp_samp = p_samp = 0;
                 cur_sig = sig;
                 static_valid = true;
                 refreshes++;
             }
-            double kw[PB_FMAX];
-            for (int q = 0; q < nf; q++) kw[q] = c->retardation ? 2 * PB_PI * fb[f + q] / PB_C0 : 0.0;
+            double kw[PB_FMAX], kwmax = 0;
+            for (int q = 0; q < nf; q++) {
+                kw[q] = c->retardation ? 2 * PB_PI * fb[f + q] / PB_C0 : 0.0;
+                kwmax = std::max(kwmax, kw[q]);
+            }
+            if (kw0 > 0) {
+                // exact quadrature-sample count of this chunk (statistics only): it depends on
+                // the geometry, the level signature and, on the FP32 path (fewer samples for
+                // far ribbons), the chunk's largest wavenumber; the context keeps it
+                std::vector<long> skey(sig);
+                long kbits = -2;
+                if (fill32) std::memcpy(&kbits, &kwmax, sizeof kbits);
+                skey.push_back(kbits);
+                auto it = c->sample_counts.find(skey);
+                if (it == c->sample_counts.end()) {
+                    PB_TRY(pb_count_samples(c->g, kw0, &lp_samp, &p_samp, st, c->d_count, fill32 ? kwmax : 0.0));
+                    c->sample_counts[skey] = std::make_pair(lp_samp, p_samp);
+                } else {
+                    lp_samp = it->second.first;
+                    p_samp = it->second.second;
+                }
+            } else {
+                lp_samp = p_samp = 0;
+            }
             tCorr.start(st);
             if (c->capacitance && nc > 0)
                 PB_TRY(pb_pot_corr(c->g, nf, kw, fill32, bStP.as<double>(), bP.as<double2>() + (long long)f * nc * nc,

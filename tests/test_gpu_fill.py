@@ -104,6 +104,32 @@ def test_entries_match_reference_golden(name, golden):
                 assert err(got, fx["p_v"][ik], np.max(np.abs(pm)), dv) <= 1e-5, name
 
 
+def test_mixed_fill_far_ribbon_rule():
+    """FP32 path: ribbon pairs with centre distance >= 10 x the largest cell dimension lmax
+    and k lmax <= 0.1 take the 2-point Gauss-Legendre product rule (16 samples for the
+    reference's 256). Entries stay within the mixed bar up to the bound (k lmax = 0.0999),
+    the FP64 path keeps the full rule, and the FP32 sweep counts fewer samples. The
+    100 x 50 mm plate at 32 x 16 cells over ground: 62 % of the direct pairs are far."""
+    from openpeec_b200 import configs, geometry
+    prob = geometry.build(geometry.parse_peec(configs.cfg2(32, 16, 2)))
+    o, od = Oracle(prob), direct_oracle(prob)
+    seg = prob.seg
+    lmax = max(np.max(seg["len"]), np.max(seg["wid"]))
+    with api.Context(prob) as ctx:
+        for kl in (0.02, 0.0999):
+            kw = kl / lmax
+            ref, dref = o.lp_fill(kw), od.lp_fill(kw) if od else None
+            assert entry_err(ctx.lp_fill(kw, abi.PREC_MIXED), ref, abi.PREC_MIXED, dref) <= 1e-5, kl
+            assert entry_err(ctx.lp_fill(kw, abi.PREC_FP64), ref) <= 1e-9, kl
+            if prob.capacitance:
+                ref, dref = o.pot_fill(kw), od.pot_fill(kw) if od else None
+                assert entry_err(ctx.pot_fill(kw, abi.PREC_MIXED), ref, abi.PREC_MIXED, dref) <= 1e-5, kl
+        f = np.array([0.05 / lmax * C0 / (2 * np.pi)])
+        _, s32 = ctx.sweep(f, fill_prec=abi.PREC_MIXED)
+        _, s64 = ctx.sweep(f, fill_prec=abi.PREC_FP64)
+        assert 0 < s32["corr_samples"] < 0.6 * s64["corr_samples"]
+
+
 def test_mixed_fill_normwise_error(golden):
     """Normwise entry error of the mixed fill: max |dL| / max |L| <= 1e-7 (same for P)."""
     prob, fx = golden("cfg2_small")
