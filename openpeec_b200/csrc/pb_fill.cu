@@ -662,6 +662,57 @@ __device__ __forceinline__ void prefetch_l1(const void *p)
     asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
 }
 
+// One term of a far pair (2-point rule) on a half-warp: lane l of half h takes sample
+// (i, j, m, q) = bits 0..3 of l & 15 of the term T_h; the half's phase bases sit at
+// base + h * nbase. T is null for a half whose pair has fewer terms.
+template <int F, int EQ, int RED>
+__device__ void run_far2(const Term<float> *T, const KArg &k, Acc<float, F> &a, int lane, float4 *bases)
+{
+    constexpr int NB = nbase<F, EQ>();
+    const int hl = lane & 15;
+    float4 *base = bases + (lane >> 4) * NB;
+    __syncwarp();                                   // previous term's bases no longer read
+    if (T && hl < NB) {
+        const double kh = EQ ? (hl < NB - 1 ? k.kh[8 * hl] : k.dkh) : k.kh[hl];
+        double sn, cs;
+        sincos(kh * T->D, &sn, &cs);
+        const float sh = (float)sn, ch = (float)cs;
+        base[hl] = make_float4(sh, ch, (float)(sn - (double)sh), (float)(cs - (double)ch));
+    }
+    __syncwarp();
+    if (T) {
+        const float g = 0.577350269189625765f;      // 1/sqrt(3), weights 1
+        const float xi = (hl & 1) ? g : -g, xj = (hl & 2) ? g : -g;
+        const float xm = (hl & 4) ? g : -g, xq = (hl & 8) ? g : -g;
+        const float a1 = 0.5f * T->L1 * xi, b1 = 0.5f * T->W1 * xj, a2 = 0.5f * T->L2 * xm, b2 = 0.5f * T->W2 * xq;
+        const float cd[3] = {T->cdf[0], T->cdf[1], T->cdf[2]};
+        float p[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) p[c] = fmaf(a2, T->u2[c], fmaf(b2, T->v2[c], -fmaf(a1, T->u1[c], b1 * T->v1[c])));
+        sample32<F, EQ, RED>(a, k, base, cd, 0.f, T->Df, T->Dlo, p[0], p[1], p[2], (float)(-2.0 * T->sc));
+    }
+}
+
+// reduce_select for two pairs at once: lane f of half h sums frequency f over the 16
+// lanes of half h (F <= 16).
+template <int F>
+__device__ __forceinline__ void reduce_halves(Acc<float, F> &a, int lane, double &cr, double &ci)
+{
+    a.flush();
+    __syncwarp();
+    cr = ci = 0;
+    const int hl = lane & 15, h0 = lane & 16;
+    if (hl < F) {
+        const double *base = a.tot - lane + h0;
+#pragma unroll 8
+        for (int l = 0; l < 16; l++) {
+            cr += base[(2 * hl) * 32 + l];
+            ci += base[(2 * hl + 1) * 32 + l];
+        }
+    }
+    __syncwarp();
+}
+
 template <typename R, int F>
 constexpr size_t corr_smem_bytes()
 {
@@ -689,6 +740,8 @@ k_corr(pb_fill_geom g, KArg k, const double *st, pb_epi_args ea, double2 *ig, lo
     const int n = set.n;
     const long long T = (long long)n * (n + 1) / 2;
     const double coef = PB_MU0 / (4 * PB_PI);
+    // far pairs two at a time: each half-warp needs its own phase bases
+    constexpr bool PAIR_FAR = sizeof(R) == 4 && 2 * nbase<F, EQ>() <= PB_FMAX + 1;
     const double kw0 = k.kw[0];
     const int nf = k.nf;
     const long long stride = (long long)gridDim.x * PB_CORR_WARPS * PB_GROUP;
@@ -731,43 +784,29 @@ k_corr(pb_fill_geom g, KArg k, const double *st, pb_epi_args ea, double2 *ig, lo
                     nt++;
                 }
             }
-            hdr[lane] = TaskHdr{i, j, nt, 0};
+            int far = nt > 0;
+            for (int q = 0; q < nt; q++) far &= terms[2 * lane + q].ty == TT_RIBBON2;
+            hdr[lane] = TaskHdr{i, j, nt, far};
         }
         __syncwarp();
-        // ---- samples of the 32 pairs, one after the other
-        for (int tk = 0; tk < PB_GROUP; tk++) {
-            if (g0 + tk >= T) break;
-            const TaskHdr h = hdr[tk];
-            if (EPI == PB_EPI_REDUCED && SET == PB_SET_LP && lane < nf) {
-                // the epilogue's scattered P(f) reads: start them into L1 now, so that they
-                // arrive while the samples run instead of stalling the warp afterwards
+        // the epilogue's scattered P(f) reads: start them into L1 before the samples, so that
+        // they arrive while the samples run instead of stalling the warp afterwards
+        auto prefetch_p = [&](const TaskHdr &h, int f) {
+            if (EPI == PB_EPI_REDUCED && SET == PB_SET_LP && f < nf) {
                 const int ca = g.seg_ca[h.i], cb = g.seg_cb[h.i], da = g.seg_ca[h.j], db = g.seg_cb[h.j];
-                const double2 *P = ea.pm + lane * ea.pm_stride;
+                const double2 *P = ea.pm + f * ea.pm_stride;
                 const int nc = g.ncell;
                 if (ca >= 0 && da >= 0) prefetch_l1(P + (long long)ca * nc + da);
                 if (ca >= 0 && db >= 0) prefetch_l1(P + (long long)ca * nc + db);
                 if (cb >= 0 && da >= 0) prefetch_l1(P + (long long)cb * nc + da);
                 if (cb >= 0 && db >= 0) prefetch_l1(P + (long long)cb * nc + db);
             }
-            double cr = 0, cim = 0;
-            if (h.nterm > 0) {               // warp-uniform; e.g. perpendicular Lp pairs have none
-                Acc<R, F> acc;
-                acc.init(tot + lane);
-                for (int q = 0; q < h.nterm; q++) {
-                    if constexpr (sizeof(R) == 4) {
-                        run_term32<F, EQ, RED>(terms[2 * tk + q], k, acc, lane, bases);
-                    } else {
-                        const Term<R> tm = terms[2 * tk + q];
-                        run_term<R, F, EQ>(tm, k, acc, lane);
-                    }
-                }
-                reduce_select<F>(acc, lane, cr, cim);
-            }
-            const int f = lane, i = h.i, j = h.j;
-            if (f >= nf) continue;
+        };
+        // one entry (pair i, j) at frequency f from its correction cr + j cim
+        auto emit = [&](int i, int j, int f, double cr, double cim) {
             if (SET == PB_SET_IG) {
                 ig[f * igs + (long long)i * n + j] = make_double2(cr, cim);
-                continue;
+                return;
             }
             const double lr = st[(long long)i * n + j] + cr, li = cim;
             if (EPI == PB_EPI_STORE) {
@@ -797,6 +836,51 @@ k_corr(pb_fill_geom g, KArg k, const double *st, pb_epi_args ea, double2 *ig, lo
                     m2[(long long)i * n + j] = make_float2((float)vr, (float)vi);
                     m2[(long long)j * n + i] = make_float2((float)vr, (float)vi);
                 }
+            }
+        };
+        // ---- samples of the 16 pairs, one after the other (far pairs below, two at a time)
+        for (int tk = 0; tk < PB_GROUP; tk++) {
+            if (g0 + tk >= T) break;
+            const TaskHdr h = hdr[tk];
+            if (PAIR_FAR && h.pad) continue;
+            prefetch_p(h, lane);
+            double cr = 0, cim = 0;
+            if (h.nterm > 0) {               // warp-uniform; e.g. perpendicular Lp pairs have none
+                Acc<R, F> acc;
+                acc.init(tot + lane);
+                for (int q = 0; q < h.nterm; q++) {
+                    if constexpr (sizeof(R) == 4) {
+                        run_term32<F, EQ, RED>(terms[2 * tk + q], k, acc, lane, bases);
+                    } else {
+                        const Term<R> tm = terms[2 * tk + q];
+                        run_term<R, F, EQ>(tm, k, acc, lane);
+                    }
+                }
+                reduce_select<F>(acc, lane, cr, cim);
+            }
+            if (lane < nf) emit(h.i, h.j, lane, cr, cim);
+        }
+        // ---- far pairs (2-point rule, 16 samples per term): two pairs at once, one per
+        // half-warp, so that no lane idles and one transposed reduction serves both
+        if constexpr (PAIR_FAR) {
+            unsigned fm = __ballot_sync(0xffffffffu, lane < PB_GROUP && g0 + lane < T && hdr[lane].pad);
+            const int half = lane >> 4, hl = lane & 15;
+            while (fm) {                                    // warp-uniform
+                const int ta = __ffs(fm) - 1;
+                fm &= fm - 1;
+                int tb = -1;
+                if (fm) { tb = __ffs(fm) - 1; fm &= fm - 1; }
+                const int tk = half ? tb : ta;
+                const int nq = max(hdr[ta].nterm, tb >= 0 ? hdr[tb].nterm : 0);
+                TaskHdr h{0, 0, 0, 0};
+                if (tk >= 0) { h = hdr[tk]; prefetch_p(h, hl); }
+                Acc<R, F> acc;
+                acc.init(tot + lane);
+                for (int q = 0; q < nq; q++)
+                    run_far2<F, EQ, RED>(q < h.nterm ? &terms[2 * tk + q] : nullptr, k, acc, lane, bases);
+                double cr, cim;
+                reduce_halves<F>(acc, lane, cr, cim);
+                if (tk >= 0 && hl < nf) emit(h.i, h.j, hl, cr, cim);
             }
         }
         __syncwarp();
