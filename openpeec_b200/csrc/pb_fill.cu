@@ -51,6 +51,10 @@ struct KArg {
     int step_tiny;       // |dkh| * (bound on |delta|) < 0.01: two-term step sine/cosine
 };                       // (selects the RED instance of the FP32 kernels)
 
+// 3-point Gauss-Legendre rule (nodes 0, +-sqrt(3/5); weights 8/9, 5/9) for separated
+// ribbon pairs on the FP32 path; the nodes in FP32, the weights in FP64.
+__constant__ float cXG3f[3] = {-0.7745966692414834f, 0.0f, 0.7745966692414834f};
+__constant__ double cWG3[3] = {5.0 / 9.0, 8.0 / 9.0, 5.0 / 9.0};
 // FP32 copies of the 4- and 8-point Gauss-Legendre nodes and weights (the FP64 tables
 // cXG4/cWG4/cXG8/cWG8 rounded to nearest), for uniform loads in the FP32 sample loops.
 __constant__ float cXG4f[4] = {-0.8611363115940526f, -0.3399810435848563f, 0.3399810435848563f, 0.8611363115940526f};
@@ -251,28 +255,35 @@ __device__ __forceinline__ void accum(Acc<double, F> &a, const KArg &k, double r
 // One (possibly mirrored) pair term reduced to what its sample loop needs, in the
 // precision of that loop. Built from the FP64 cells just before the loop so that the
 // cells are not live during it.
-enum { TT_RIBBON = 0, TT_WIRE = 1, TT_POLY = 2, TT_RIBBON2 = 3 };
+enum { TT_RIBBON = 0, TT_WIRE = 1, TT_POLY = 2, TT_RIBBON2 = 3, TT_RIBBON3 = 4 };
 
-// Well-separated ribbon pairs on the FP32 path: a single sub-square (nsub = 1), centre
-// distance >= PB_FAR2_RATIO times the largest cell dimension lmax, and k * lmax <=
-// PB_FAR2_KL at every wavenumber of the launch. There the correction integrand
-// (e^{-jkR}-1)/R is smooth over both cells: the 2-point Gauss-Legendre product rule (16
-// samples) has a remainder of order (k lmax)^4 / 1000 of the entry, against the
-// reference's 4-point rule (256 samples). Measured on the benchmark plate (every parallel
-// pair with ratio >= 10, direct and image): 3e-8 of the entry at k lmax = 0.086, 2e-9 at
-// a quarter of it. Without the k lmax bound a coarser plate at k lmax = 0.225 erred by
-// 2.6e-6 of the direct + image terms, as the estimate says; the bound keeps the rule at
-// <= 1e-7. The FP64 (plain) path keeps the reference's 4-point rule everywhere.
+// Separated ribbon pairs on the FP32 path: a single sub-square (nsub = 1) and k * lmax <=
+// PB_FAR_KL at every wavenumber of the launch (lmax: the largest cell dimension). There
+// the correction integrand (e^{-jkR}-1)/R is smooth over both cells, and lower-order
+// Gauss-Legendre product rules than the reference's 4-point rule (256 samples) agree with
+// it to far below the FP32 rounding of the correction:
+//   centre distance >= PB_FAR2_RATIO lmax: 2-point rule (16 samples),
+//   centre distance >= PB_FAR3_RATIO lmax: 3-point rule (81 samples).
+// Measured on the benchmark plate at k lmax = 0.1 (parallel pairs, direct and image,
+// relative to |static| + |correction|): 2-point <= 6.7e-8 at ratio 8-10 (remainder
+// ~(k lmax)^4 / 1000); 3-point <= 2.6e-9 at ratio 3-4, 7e-10 at 4-5. Without the k lmax
+// bound a coarser plate at k lmax = 0.225 erred by 2.6e-6 with the 2-point rule. The FP64
+// (plain) path keeps the reference's 4-point rule everywhere.
 #define PB_FAR2_RATIO 10.0
-#define PB_FAR2_KL 0.1
-__device__ __forceinline__ bool ribbon_far2(const Cell &s1, const Cell &s2, int nsub, const double *c1,
-                                            const double *c2, double kwmax)
+#define PB_FAR3_RATIO 3.0
+#define PB_FAR_KL 0.1
+// 4 (the reference's rule), 3 or 2: the product rule of a ribbon pair on the FP32 path
+__device__ __forceinline__ int ribbon_rule32(const Cell &s1, const Cell &s2, int nsub, const double *c1,
+                                             const double *c2, double kwmax)
 {
-    if (nsub != 1) return false;
+    if (nsub != 1) return 4;
     const double lmax = fmax(fmax(s1.len, s2.len), fmax(s1.wid, s2.wid));
-    if (kwmax * lmax > PB_FAR2_KL) return false;
+    if (kwmax * lmax > PB_FAR_KL) return 4;
     const double dx = c2[0] - c1[0], dy = c2[1] - c1[1], dz = c2[2] - c1[2];
-    return dx * dx + dy * dy + dz * dz >= (PB_FAR2_RATIO * lmax) * (PB_FAR2_RATIO * lmax);
+    const double d2 = dx * dx + dy * dy + dz * dz;
+    if (d2 >= (PB_FAR2_RATIO * lmax) * (PB_FAR2_RATIO * lmax)) return 2;
+    if (d2 >= (PB_FAR3_RATIO * lmax) * (PB_FAR3_RATIO * lmax)) return 3;
+    return 4;
 }
 // Centre offset of a term in the form its sample loop reads it.
 template <typename R> struct TermOffset;
@@ -329,8 +340,11 @@ __device__ void make_term(Term<R> &T, const Cell &s1, const Cell &s2, int same, 
         T.L1 = (R)s1.len; T.W1 = (R)s1.wid; T.L2 = (R)s2.len; T.W2 = (R)s2.wid;
         T.sc = scale * s1.len * s2.len / (16.0 * nsub * nsub);   // any product rule: weights sum to 16
         T.nsub = nsub;
-        if constexpr (sizeof(R) == 4)
-            if (ribbon_far2(s1, s2, nsub, c1d, c2d, kwmax)) T.ty = TT_RIBBON2;
+        if constexpr (sizeof(R) == 4) {
+            const int rule = ribbon_rule32(s1, s2, nsub, c1d, c2d, kwmax);
+            if (rule == 2) T.ty = TT_RIBBON2;
+            if (rule == 3) T.ty = TT_RIBBON3;
+        }
     } else {                                               // gauss_kernel mode 1, partial.c:61-99
         T.ty = TT_WIRE;
         const Cell &b = wire_self ? s1 : s2;
@@ -497,6 +511,21 @@ __device__ void run_term32(const Term<float> &T, const KArg &k, Acc<float, F> &a
 #pragma unroll
             for (int c = 0; c < 3; c++) p[c] = fmaf(a2, T.u2[c], fmaf(b2, T.v2[c], -fmaf(a1, T.u1[c], b1 * T.v1[c])));
             sample32<F, EQ, RED>(a, k, base, cd, 0.f, D, Dlo, p[0], p[1], p[2], (float)(-2.0 * T.sc));
+        }
+    } else if (T.ty == TT_RIBBON3) {                // separated ribbons: 3-point rule
+        if (lane < 27) {                            // lane = i + 3 j + 9 m; q = 0..2 in the loop
+            const int i = lane % 3, j = (lane / 3) % 3, m = lane / 9;
+            const float a1 = 0.5f * T.L1 * cXG3f[i], b1 = 0.5f * T.W1 * cXG3f[j], a2 = 0.5f * T.L2 * cXG3f[m];
+            const double wijm = cWG3[i] * cWG3[j] * cWG3[m] * (-2.0 * T.sc);
+            float Q[3];
+#pragma unroll
+            for (int c = 0; c < 3; c++) Q[c] = fmaf(a2, T.u2[c], -fmaf(a1, T.u1[c], b1 * T.v1[c]));
+#pragma unroll 1
+            for (int q = 0; q < 3; q++) {
+                const float b2 = 0.5f * T.W2 * cXG3f[q];
+                sample32<F, EQ, RED>(a, k, base, cd, 0.f, D, Dlo, fmaf(b2, T.v2[0], Q[0]), fmaf(b2, T.v2[1], Q[1]),
+                                     fmaf(b2, T.v2[2], Q[2]), (float)(wijm * cWG3[q]));
+            }
         }
     } else if (T.ty == TT_WIRE) {                   // gauss_kernel mode 1, partial.c:61-99
         const int lj = lane & 7, li = lane >> 3;
@@ -934,7 +963,9 @@ __device__ __forceinline__ long long pair_samples(const Cell &s1, const Cell &s2
             double t[3], w[3], nv[3], c1[3], c2[3];
             frame(s1, t, w, nv, c1);
             frame(s2, t, w, nv, c2);
-            if (ribbon_far2(s1, s2, n, c1, c2, kwf)) return 16;
+            const int rule = ribbon_rule32(s1, s2, n, c1, c2, kwf);
+            if (rule == 2) return 16;
+            if (rule == 3) return 81;
         }
         return 256LL * n * n;
     }

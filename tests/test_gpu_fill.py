@@ -105,9 +105,10 @@ def test_entries_match_reference_golden(name, golden):
 
 
 def test_mixed_fill_far_ribbon_rule():
-    """FP32 path: ribbon pairs with centre distance >= 10 x the largest cell dimension lmax
-    and k lmax <= 0.1 take the 2-point Gauss-Legendre product rule (16 samples for the
-    reference's 256). Entries stay within the mixed bar up to the bound (k lmax = 0.0999),
+    """FP32 path: ribbon pairs with k lmax <= 0.1 (lmax: the largest cell dimension) take
+    lower-order Gauss-Legendre product rules than the reference's 4-point rule (256
+    samples): the 2-point rule (16) at centre distance >= 10 lmax, the 3-point rule (81)
+    at >= 3 lmax. Entries stay within the mixed bar up to the bound (k lmax = 0.0999),
     the FP64 path keeps the full rule, and the FP32 sweep counts fewer samples. The
     100 x 50 mm plate at 32 x 16 cells over ground: 62 % of the direct pairs are far."""
     from openpeec_b200 import configs, geometry
