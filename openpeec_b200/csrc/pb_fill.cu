@@ -440,7 +440,7 @@ __device__ void run_term(const Term<R> &T, const KArg &k, Acc<R, F> &a, int lane
 // FP64 path (sample s = l + 32 t of each sub-square), but with the lane-fixed parts of the
 // point (and of its weight) hoisted out of the loops; the phase bases sin/cos(kh D) of the
 // term are computed in FP64 by the first lanes into the warp's `base` slots.
-template <int F, int EQ, int RED>
+template <int F, int EQ, int RED, bool HAS2>
 __device__ void run_term32(const Term<float> &T, const KArg &k, Acc<float, F> &a, int lane,
                            float4 *base)
 {
@@ -501,7 +501,7 @@ __device__ void run_term32(const Term<float> &T, const KArg &k, Acc<float, F> &a
                 }
             }
         }
-    } else if (T.ty == TT_RIBBON2) {                // well-separated ribbons: 2-point rule
+    } else if (HAS2 && T.ty == TT_RIBBON2) {        // well-separated ribbons: 2-point rule
         if (lane < 16) {
             const float g = 0.577350269189625765f;  // 1/sqrt(3), weights 1
             const float xi = (lane & 1) ? g : -g, xj = (lane & 2) ? g : -g;
@@ -815,6 +815,9 @@ k_corr(pb_fill_geom g, KArg k, const double *st, pb_epi_args ea, double2 *ig, lo
             }
             int far = nt > 0;
             for (int q = 0; q < nt; q++) far &= terms[2 * lane + q].ty == TT_RIBBON2;
+            if (!far)                       // a pair that mixes rules takes the 3-point rule for its
+                for (int q = 0; q < nt; q++)    // far terms: one sample loop less in the near path
+                    if (terms[2 * lane + q].ty == TT_RIBBON2) terms[2 * lane + q].ty = TT_RIBBON3;
             hdr[lane] = TaskHdr{i, j, nt, far};
         }
         __syncwarp();
@@ -867,50 +870,57 @@ k_corr(pb_fill_geom g, KArg k, const double *st, pb_epi_args ea, double2 *ig, lo
                 }
             }
         };
-        // ---- samples of the 16 pairs, one after the other (far pairs below, two at a time)
-        for (int tk = 0; tk < PB_GROUP; tk++) {
-            if (g0 + tk >= T) break;
-            const TaskHdr h = hdr[tk];
-            if (PAIR_FAR && h.pad) continue;
-            prefetch_p(h, lane);
-            double cr = 0, cim = 0;
-            if (h.nterm > 0) {               // warp-uniform; e.g. perpendicular Lp pairs have none
-                Acc<R, F> acc;
-                acc.init(tot + lane);
-                for (int q = 0; q < h.nterm; q++) {
-                    if constexpr (sizeof(R) == 4) {
-                        run_term32<F, EQ, RED>(terms[2 * tk + q], k, acc, lane, bases);
-                    } else {
-                        const Term<R> tm = terms[2 * tk + q];
-                        run_term<R, F, EQ>(tm, k, acc, lane);
-                    }
-                }
-                reduce_select<F>(acc, lane, cr, cim);
-            }
-            if (lane < nf) emit(h.i, h.j, lane, cr, cim);
-        }
-        // ---- far pairs (2-point rule, 16 samples per term): two pairs at once, one per
+        // ---- samples of the 16 pairs: other pairs one after the other with the whole warp,
+        // then the far pairs (2-point rule, 16 samples per term) two at a time, one per
         // half-warp, so that no lane idles and one transposed reduction serves both
-        if constexpr (PAIR_FAR) {
-            unsigned fm = __ballot_sync(0xffffffffu, lane < PB_GROUP && g0 + lane < T && hdr[lane].pad);
-            const int half = lane >> 4, hl = lane & 15;
-            while (fm) {                                    // warp-uniform
-                const int ta = __ffs(fm) - 1;
-                fm &= fm - 1;
-                int tb = -1;
-                if (fm) { tb = __ffs(fm) - 1; fm &= fm - 1; }
-                const int tk = half ? tb : ta;
-                const int nq = max(hdr[ta].nterm, tb >= 0 ? hdr[tb].nterm : 0);
-                TaskHdr h{0, 0, 0, 0};
-                if (tk >= 0) { h = hdr[tk]; prefetch_p(h, hl); }
-                Acc<R, F> acc;
-                acc.init(tot + lane);
-                for (int q = 0; q < nq; q++)
-                    run_far2<F, EQ, RED>(q < h.nterm ? &terms[2 * tk + q] : nullptr, k, acc, lane, bases);
-                double cr, cim;
-                reduce_halves<F>(acc, lane, cr, cim);
-                if (tk >= 0 && hl < nf) emit(h.i, h.j, hl, cr, cim);
+        const bool valid = lane < PB_GROUP && g0 + lane < T;
+        unsigned far_m = PAIR_FAR ? __ballot_sync(0xffffffffu, valid && hdr[lane].pad) : 0u;
+        unsigned near_m = __ballot_sync(0xffffffffu, valid) & ~far_m;
+        const int half = lane >> 4, hl = lane & 15;
+        while (near_m | far_m) {                           // warp-uniform
+            int tk, f;
+            double cr = 0, cim = 0;
+            if (near_m) {
+                tk = __ffs(near_m) - 1;
+                near_m &= near_m - 1;
+                f = lane;
+                const TaskHdr h = hdr[tk];
+                prefetch_p(h, f);
+                if (h.nterm > 0) {           // warp-uniform; e.g. perpendicular Lp pairs have none
+                    Acc<R, F> acc;
+                    acc.init(tot + lane);
+                    for (int q = 0; q < h.nterm; q++) {
+                        if constexpr (sizeof(R) == 4) {
+                            run_term32<F, EQ, RED, !PAIR_FAR>(terms[2 * tk + q], k, acc, lane, bases);
+                        } else {
+                            const Term<R> tm = terms[2 * tk + q];
+                            run_term<R, F, EQ>(tm, k, acc, lane);
+                        }
+                    }
+                    reduce_select<F>(acc, lane, cr, cim);
+                }
+            } else {
+                if constexpr (PAIR_FAR) {
+                    const int ta = __ffs(far_m) - 1;
+                    far_m &= far_m - 1;
+                    int tb = -1;
+                    if (far_m) { tb = __ffs(far_m) - 1; far_m &= far_m - 1; }
+                    tk = half ? tb : ta;
+                    f = hl;
+                    const int nq = max(hdr[ta].nterm, tb >= 0 ? hdr[tb].nterm : 0);
+                    const int nt = tk >= 0 ? hdr[tk].nterm : 0;
+                    if (tk >= 0) prefetch_p(hdr[tk], f);
+                    Acc<R, F> acc;
+                    acc.init(tot + lane);
+                    for (int q = 0; q < nq; q++)
+                        run_far2<F, EQ, RED>(q < nt ? &terms[2 * tk + q] : nullptr, k, acc, lane, bases);
+                    reduce_halves<F>(acc, lane, cr, cim);
+                } else {
+                    tk = -1;
+                    f = 0;
+                }
             }
+            if (tk >= 0 && f < nf) emit(hdr[tk].i, hdr[tk].j, f, cr, cim);
         }
         __syncwarp();
     }
@@ -950,8 +960,9 @@ __global__ void k_pot_aggr(pb_fill_geom g, int nf, const double *st, const doubl
 
 static int grid_for(long long work, int per_block, int blocks_per_sm = 8);
 // ---------------------------------------------------------------- sample counting
+// Samples of one term; r2 counts the terms on the 2-point rule (kwf > 0: the FP32 path).
 __device__ __forceinline__ long long pair_samples(const Cell &s1, const Cell &s2, int same, double kw,
-                                                  const pb_dev_cells &set, int i1, int i2, double kwf)
+                                                  const pb_dev_cells &set, int i1, int i2, double kwf, int &r2)
 {
     if (same && s1.wid <= 0 && s1.npv <= 0) { const int n = corr_nsub(s1, s1, kw); return 64LL * n * n; }
     const int ty = pair_type(s1, s2);
@@ -964,7 +975,7 @@ __device__ __forceinline__ long long pair_samples(const Cell &s1, const Cell &s2
             frame(s1, t, w, nv, c1);
             frame(s2, t, w, nv, c2);
             const int rule = ribbon_rule32(s1, s2, n, c1, c2, kwf);
-            if (rule == 2) return 16;
+            if (rule == 2) { r2++; return 16; }
             if (rule == 3) return 81;
         }
         return 256LL * n * n;
@@ -972,6 +983,10 @@ __device__ __forceinline__ long long pair_samples(const Cell &s1, const Cell &s2
     const int n = corr_nsub(s1, s2, kw);
     return 64LL * n * n;
 }
+
+// A pair whose terms do not all take the 2-point rule runs its 2-point terms on the 3-point
+// rule (the k_corr set-up does the same).
+__device__ __forceinline__ long long mixed_fix(int nterm, int r2) { return r2 < nterm ? r2 * (81LL - 16) : 0; }
 
 __global__ void k_count(pb_fill_geom g, double kw, unsigned long long *out, double kwf)
 {
@@ -987,17 +1002,28 @@ __global__ void k_count(pb_fill_geom g, double kw, unsigned long long *out, doub
             load_cell(si, g.seg.cell, g.pv, i, 0, g.gpz);
             double t1[3], t2[3];
             tangent(si, t1);
+            int nt = 0, r2 = 0;
             if (i == j) {
-                acc_lp += pair_samples(si, si, 1, kw, g.seg, i, i, kwf);
+                acc_lp += pair_samples(si, si, 1, kw, g.seg, i, i, kwf, r2);
+                nt++;
                 const double tdm = t1[0] * t1[0] + t1[1] * t1[1] - t1[2] * t1[2];
-                if (g.gp && tdm != 0) { load_cell(sj, g.seg.cell, g.pv, i, 1, g.gpz); acc_lp += pair_samples(si, sj, 0, kw, g.seg, i, i, kwf); }
+                if (g.gp && tdm != 0) {
+                    load_cell(sj, g.seg.cell, g.pv, i, 1, g.gpz);
+                    acc_lp += pair_samples(si, sj, 0, kw, g.seg, i, i, kwf, r2);
+                    nt++;
+                }
             } else {
                 load_cell(sj, g.seg.cell, g.pv, j, 0, g.gpz);
                 tangent(sj, t2);
                 const double tdot = dot3(t1, t2), tdm = t1[0] * t2[0] + t1[1] * t2[1] - t1[2] * t2[2];
-                if (tdot != 0) acc_lp += pair_samples(si, sj, 0, kw, g.seg, i, j, kwf);
-                if (g.gp && tdm != 0) { load_cell(sj, g.seg.cell, g.pv, j, 1, g.gpz); acc_lp += pair_samples(si, sj, 0, kw, g.seg, i, j, kwf); }
+                if (tdot != 0) { acc_lp += pair_samples(si, sj, 0, kw, g.seg, i, j, kwf, r2); nt++; }
+                if (g.gp && tdm != 0) {
+                    load_cell(sj, g.seg.cell, g.pv, j, 1, g.gpz);
+                    acc_lp += pair_samples(si, sj, 0, kw, g.seg, i, j, kwf, r2);
+                    nt++;
+                }
             }
+            acc_lp += mixed_fix(nt, r2);
         } else {
             int ci, cj;
             tri_index(t - T1, nc, ci, cj);
@@ -1007,8 +1033,10 @@ __global__ void k_count(pb_fill_geom g, double kw, unsigned long long *out, doub
                     Cell sa, sb;
                     load_cell(sa, g.chg.cell, g.pv, a, 0, g.gpz);
                     load_cell(sb, g.chg.cell, g.pv, b, 0, g.gpz);
-                    acc_p += pair_samples(sa, sb, a == b, kw, g.chg, a, b, kwf);
-                    if (g.gp) { load_cell(sb, g.chg.cell, g.pv, b, 1, g.gpz); acc_p += pair_samples(sa, sb, 0, kw, g.chg, a, b, kwf); }
+                    int r2 = 0;
+                    acc_p += pair_samples(sa, sb, a == b, kw, g.chg, a, b, kwf, r2);
+                    if (g.gp) { load_cell(sb, g.chg.cell, g.pv, b, 1, g.gpz); acc_p += pair_samples(sa, sb, 0, kw, g.chg, a, b, kwf, r2); }
+                    acc_p += mixed_fix(g.gp ? 2 : 1, r2);
                 }
         }
     }
