@@ -182,6 +182,22 @@ def test_tensor_core_lu_matches_plain_path():
     assert zerr(zs, zp) <= 1e-6
 
 
+@pytest.mark.parametrize("nf,log", [(16, True), (8, True), (16, False)])
+def test_far_ribbon_rules_every_launch_shape(nf, log):
+    """The lower-order rules for separated ribbon pairs run in every FP32 launch shape:
+    16 or 8 frequencies per launch, log-spaced (phase bases per frequency; at 16 the far
+    pairs run one per warp) or equally spaced (angle recurrence; far pairs two per warp).
+    Mid-size plate, 100-300 MHz (k lmax <= 0.02): Z within 1e-6 of the plain FP64 path."""
+    from openpeec_b200 import configs, geometry
+    prob = geometry.build(geometry.parse_peec(configs.cfg2(32, 16, 2)))
+    f = np.geomspace(1e8, 3e8, nf) if log else np.linspace(1e8, 3e8, nf)
+    with api.Context(prob) as ctx:
+        zp, sp = ctx.sweep(f, fill_prec=abi.PREC_FP64, lu=abi.LU_FP64)
+        zm, sm = ctx.sweep(f, fill_prec=abi.PREC_MIXED, lu=abi.LU_TC)
+    assert sm["corr_samples"] < 0.6 * sp["corr_samples"], (sm, sp)
+    assert zerr(zm, zp) <= 1e-6, (zerr(zm, zp), sm)
+
+
 @pytest.mark.parametrize("name", ["cfg2_small", "dipole_halfwave", "strip_dipole_ret", "cfg3_small_0", "rlc_series"])
 def test_accel_gmres_matches_reference(name, golden):
     """LU reuse (the reference's acceleration = 1): one FP32 LU per 2 frequencies, GMRES
