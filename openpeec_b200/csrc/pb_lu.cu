@@ -11,6 +11,7 @@
 #include "pb_lu.cuh"
 #include <climits>
 #include <cuComplex.h>
+#include <dlfcn.h>
 
 template <typename T> using T2_t = typename cplx_t<T>::type;
 
@@ -247,6 +248,20 @@ __global__ void k_embed_right(const float2 *__restrict__ b, int k, int nc, int l
 // real form was measured slower on B200 (launch and split overheads dominate).
 static const int kTcMinDim = 128;
 
+// cublasSetEmulationStrategy exists from cuBLAS 12.9 on. It is looked up in the
+// libcublas.so.12 this process has loaded rather than linked: a host may have loaded an
+// older copy first (e.g. a Python framework's bundled cuBLAS), and the library must still
+// load there. Without it the trailing updates stay on the SIMT complex GEMM.
+typedef cublasStatus_t (*pb_set_emulation_fn)(cublasHandle_t, cublasEmulationStrategy_t);
+static pb_set_emulation_fn set_emulation()
+{
+    static const pb_set_emulation_fn fn = []() -> pb_set_emulation_fn {
+        void *h = dlopen("libcublas.so.12", RTLD_LAZY | RTLD_NOLOAD);
+        return h ? reinterpret_cast<pb_set_emulation_fn>(dlsym(h, "cublasSetEmulationStrategy")) : nullptr;
+    }();
+    return fn;
+}
+
 template <>
 int gemm_sub<float>(pb_lu_engine *e, int m, int nc, int k, const float2 *A, int lda,
                     const float2 *B, int ldb, float2 *Cm, int ldc, long long stride, int nb)
@@ -254,6 +269,8 @@ int gemm_sub<float>(pb_lu_engine *e, int m, int nc, int k, const float2 *A, int 
     if (m <= 0 || nc <= 0 || k <= 0) return PB_OK;
     cublasStatus_t s;
     const size_t need = (size_t)nb * 4 * (size_t)k * nc * sizeof(float);
+    const pb_set_emulation_fn set_emu = set_emulation();
+    if (!set_emu) e->tc_disabled = 1;
     if (e->gemm_kind == PB_GEMM_TC && !e->tc_disabled && e->emb && need <= e->emb_cap &&
         m >= kTcMinDim && nc >= kTcMinDim && k >= kTcMinDim) {
         k_embed_right<<<dim3(ceil_div(nc, 128), k, nb), 128, 0, e->stream>>>(B, k, nc, ldb, stride, e->emb);
@@ -261,14 +278,14 @@ int gemm_sub<float>(pb_lu_engine *e, int m, int nc, int k, const float2 *A, int 
         e->launches++;
         const float ra = -1.0f, rb = 1.0f;
         cublasSetMathMode(e->blas, CUBLAS_DEFAULT_MATH);
-        cublasSetEmulationStrategy(e->blas, CUBLAS_EMULATION_STRATEGY_EAGER);
+        set_emu(e->blas, CUBLAS_EMULATION_STRATEGY_EAGER);
         // row-major real C (m x 2nc) -= A (m x 2k) * Bemb (2k x 2nc); cuBLAS is
         // column-major, so it computes the transpose: C^T = Bemb^T A^T.
         s = cublasGemmStridedBatchedEx(
             e->blas, CUBLAS_OP_N, CUBLAS_OP_N, 2 * nc, m, 2 * k, &ra, e->emb, CUDA_R_32F, 2 * nc,
             4LL * k * nc, A, CUDA_R_32F, 2 * lda, 2 * stride, &rb, Cm, CUDA_R_32F, 2 * ldc, 2 * stride, nb,
             CUBLAS_COMPUTE_32F_EMULATED_16BFX9, CUBLAS_GEMM_DEFAULT);
-        cublasSetEmulationStrategy(e->blas, CUBLAS_EMULATION_STRATEGY_DEFAULT);
+        set_emu(e->blas, CUBLAS_EMULATION_STRATEGY_DEFAULT);
         cublasSetMathMode(e->blas, CUBLAS_PEDANTIC_MATH);
         e->launches++;
         if (s == CUBLAS_STATUS_SUCCESS) return PB_OK;

@@ -4,6 +4,7 @@ import ctypes as C
 import os
 import re
 import subprocess
+import sys
 
 import numpy as np
 import pytest
@@ -84,3 +85,23 @@ def test_bad_arguments_rejected():
     h = C.c_void_p()
     s.nport = 0
     assert abi.lib().pb_create(C.byref(s), C.byref(h)) == abi.PB_ERR_ARG
+
+
+def test_loads_after_an_older_cublas():
+    """A host that loaded another libcublas.so.12 first keeps it for every later library
+    (the loader matches the soname). PyTorch's bundled cuBLAS (12.8) lacks
+    cublasSetEmulationStrategy (12.9), so the library resolves it at run time instead of
+    linking it, and loads either way (the BF16x9 updates then fall back to the SIMT GEMM)."""
+    try:
+        import nvidia.cublas
+    except ImportError:
+        pytest.skip("no second cuBLAS in this environment")
+    d = os.path.join(list(nvidia.cublas.__path__)[0], "lib")
+    if not os.path.exists(os.path.join(d, "libcublas.so.12")):
+        pytest.skip("no second cuBLAS in this environment")
+    code = ("import ctypes, os, sys; d = sys.argv[1]; "
+            "ctypes.CDLL(os.path.join(d, 'libcublasLt.so.12'), mode=ctypes.RTLD_GLOBAL); "
+            "ctypes.CDLL(os.path.join(d, 'libcublas.so.12'), mode=ctypes.RTLD_GLOBAL); "
+            "from openpeec_b200 import abi; abi.lib(); print('loaded')")
+    r = subprocess.run([sys.executable, "-c", code, d], cwd=ROOT, capture_output=True, text=True, timeout=240)
+    assert r.returncode == 0 and "loaded" in r.stdout, r.stderr[-2000:]
