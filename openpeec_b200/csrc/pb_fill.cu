@@ -271,7 +271,6 @@ enum { TT_RIBBON = 0, TT_WIRE = 1, TT_POLY = 2, TT_RIBBON2 = 3, TT_RIBBON3 = 4 }
 // (plain) path keeps the reference's 4-point rule everywhere.
 #define PB_FAR2_RATIO 10.0
 #define PB_FAR3_RATIO 3.0
-#define PB_FAR_KL 0.1
 // 4 (the reference's rule), 3 or 2: the product rule of a ribbon pair on the FP32 path
 __device__ __forceinline__ int ribbon_rule32(const Cell &s1, const Cell &s2, int nsub, const double *c1,
                                              const double *c2, double kwmax)

@@ -26,6 +26,9 @@ struct pb_fill_geom {
 };
 
 #define PB_FMAX 16
+// FP32 path: lower-order product rules for separated ribbon pairs only where k * lmax <=
+// PB_FAR_KL at every wavenumber of a launch (lmax: the pair's largest cell dimension)
+#define PB_FAR_KL 0.1
 
 // Epilogue of the Lp correction kernel.
 enum { PB_EPI_STORE = 0, PB_EPI_REDUCED = 1 };

@@ -1210,9 +1210,7 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
             if (kw > 0) {
                 sig.pop_back();
                 std::vector<long> skey(sig);
-                long kbits = -2;                            // the FP32 path samples far ribbons less
-                if (fill32) std::memcpy(&kbits, &kw, sizeof kbits);
-                skey.push_back(kbits);
+                skey.push_back(fill32 ? far_rule_key(c, kw) : -1);   // FP32: lower-order rules
                 auto it = c->sample_counts.find(skey);
                 if (it == c->sample_counts.end()) {
                     PB_TRY(pb_count_samples(c->g, kw, &lp_samp, &p_samp, st, c->d_count, fill32 ? kw : 0.0));

@@ -26,6 +26,10 @@ struct pb_htree {
 // Quadrature-level signature of a wavenumber (pb_sweep.cu): equal signatures mean equal
 // static parts of the kernel blocks.
 void level_signature(const pb_ctx *c, double kw, std::vector<long> &sig);
+// Key of the FP32 path's choice of lower-order ribbon rules at largest wavenumber kwmax:
+// the number of cells with kwmax * max(len, wid) > PB_FAR_KL. Wavenumbers with equal keys
+// give every pair the same rule, hence the same sample count.
+long far_rule_key(const pb_ctx *c, double kwmax);
 
 // Builds the tree over pts[3n] and splits the (root, root) block.
 void pb_htree_build(pb_htree &t, int n, const double *pts);

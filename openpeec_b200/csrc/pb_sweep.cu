@@ -19,7 +19,6 @@
 #include <algorithm>
 #include <cmath>
 #include <vector>
-#include <cstring>
 
 // ---------------------------------------------------------------- small kernels
 // rhs'[f][j][k] = (P b_j)[ca_k] - (P b_j)[cb_k],  b_j = e(pc1_j) - e(pc2_j)   (cells)
@@ -284,6 +283,14 @@ struct DevBuf {
 // every pair uses the same nsub, hence the same static part.
 thread_local int pb_mem_share = 1;
 
+long far_rule_key(const pb_ctx *c, double kwmax)
+{
+    long n = 0;
+    for (const auto *v : {&c->seg, &c->chg})
+        for (const auto &s : *v) n += kwmax * std::max(s.len, s.wid) > PB_FAR_KL;
+    return n;
+}
+
 void level_signature(const pb_ctx *c, double kw, std::vector<long> &sig)
 {
     sig.clear();
@@ -517,11 +524,10 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
             if (kw0 > 0) {
                 // exact quadrature-sample count of this chunk (statistics only): it depends on
                 // the geometry, the level signature and, on the FP32 path (fewer samples for
-                // far ribbons), the chunk's largest wavenumber; the context keeps it
+                // separated ribbons), which cells the chunk's largest wavenumber admits to
+                // the lower-order rules; the context keeps it per key
                 std::vector<long> skey(sig);
-                long kbits = -2;
-                if (fill32) std::memcpy(&kbits, &kwmax, sizeof kbits);
-                skey.push_back(kbits);
+                skey.push_back(fill32 ? far_rule_key(c, kwmax) : -1);
                 auto it = c->sample_counts.find(skey);
                 if (it == c->sample_counts.end()) {
                     PB_TRY(pb_count_samples(c->g, kw0, &lp_samp, &p_samp, st, c->d_count, fill32 ? kwmax : 0.0));
