@@ -774,50 +774,58 @@ k_corr(pb_fill_geom g, KArg k, const double *st, pb_epi_args ea, double2 *ig, lo
     const int nf = k.nf;
     const long long stride = (long long)gridDim.x * PB_CORR_WARPS * PB_GROUP;
     for (long long g0 = ((long long)blockIdx.x * PB_CORR_WARPS + wib) * PB_GROUP; g0 < T; g0 += stride) {
-        // ---- set-up: lane -> pair g0 + lane
-        const long long t = g0 + lane;
-        if (lane < PB_GROUP && t < T) {
-            int i, j;
+        // ---- set-up: lane -> term (lane >> 4) of pair g0 + (lane & 15): the direct term on
+        // the lower half-warp, the ground-plane image on the upper one
+        static_assert(PB_GROUP == 16, "set-up maps two terms of 16 pairs onto the 32 lanes");
+        const int pl = lane & 15, term = lane >> 4;
+        const long long t = g0 + pl;
+        int i = 0, j = 0, ok = 0;
+        if (t < T) {
             tri_index(t, n, i, j);
-            int nt = 0;
-            if (kw0 > 0) {
-                for (int term = 0; term < 2; term++) {
-                    if (term == 1 && !g.gp) break;
-                    Cell si, sj;
-                    load_cell(si, set.cell, g.pv, i, 0, g.gpz);
-                    load_cell(sj, set.cell, g.pv, j, term, g.gpz);
-                    double wgt, a1, a2;
-                    if (SET == PB_SET_LP) {                 // partial.c:392-423
-                        double t1[3], t2[3];
-                        tangent(si, t1);
-                        if (i == j) {
-                            wgt = term == 0 ? 1.0 : -(t1[0] * t1[0] + t1[1] * t1[1] - t1[2] * t1[2]);
-                        } else {
-                            Cell u;
-                            load_cell(u, set.cell, g.pv, j, 0, g.gpz);
-                            tangent(u, t2);
-                            wgt = term == 0 ? dot3(t1, t2) : -(t1[0] * t2[0] + t1[1] * t2[1] - t1[2] * t2[2]);
-                        }
-                        wgt *= coef;
-                        a1 = set.cell[i].aL;
-                        a2 = set.cell[j].aL;
-                    } else {                                // potential.c:219-236
-                        wgt = term == 0 ? 1.0 : -1.0;
-                        a1 = set.cell[i].aP;
-                        a2 = set.cell[j].aP;
+            if (kw0 > 0 && (term == 0 || g.gp)) {
+                Cell si, sj;
+                load_cell(si, set.cell, g.pv, i, 0, g.gpz);
+                load_cell(sj, set.cell, g.pv, j, term, g.gpz);
+                double wgt, a1, a2;
+                if (SET == PB_SET_LP) {                     // partial.c:392-423
+                    double t1[3], t2[3];
+                    tangent(si, t1);
+                    if (i == j) {
+                        wgt = term == 0 ? 1.0 : -(t1[0] * t1[0] + t1[1] * t1[1] - t1[2] * t1[2]);
+                    } else {
+                        Cell u;
+                        load_cell(u, set.cell, g.pv, j, 0, g.gpz);
+                        tangent(u, t2);
+                        wgt = term == 0 ? dot3(t1, t2) : -(t1[0] * t2[0] + t1[1] * t2[1] - t1[2] * t2[2]);
                     }
-                    if (wgt == 0) continue;
-                    make_term<R>(terms[2 * lane + nt], si, sj, (i == j && term == 0), a1, a2, wgt, kw0, k.kwmax,
+                    wgt *= coef;
+                    a1 = set.cell[i].aL;
+                    a2 = set.cell[j].aL;
+                } else {                                    // potential.c:219-236
+                    wgt = term == 0 ? 1.0 : -1.0;
+                    a1 = set.cell[i].aP;
+                    a2 = set.cell[j].aP;
+                }
+                if (wgt != 0) {
+                    make_term<R>(terms[2 * pl + term], si, sj, (i == j && term == 0), a1, a2, wgt, kw0, k.kwmax,
                                  set, i, j);
-                    nt++;
+                    ok = 1;
                 }
             }
+        }
+        const int ok_img = __shfl_down_sync(0xffffffffu, ok, 16);
+        __syncwarp();                                       // both halves' terms written
+        if (lane < PB_GROUP && t < T) {
+            if (!ok && ok_img) terms[2 * pl] = terms[2 * pl + 1];   // image only: to slot 0
+            const int nt = ok + ok_img;
             int far = nt > 0;
             for (int q = 0; q < nt; q++) far &= terms[2 * lane + q].ty == TT_RIBBON2;
             if (!far)                       // a pair that mixes rules takes the 3-point rule for its
                 for (int q = 0; q < nt; q++)    // far terms: one sample loop less in the near path
                     if (terms[2 * lane + q].ty == TT_RIBBON2) terms[2 * lane + q].ty = TT_RIBBON3;
-            hdr[lane] = TaskHdr{i, j, nt, far};
+            // term-less pairs (e.g. perpendicular Lp cells) run with the far pairs, two at a
+            // time: they need only the epilogue, which then serves two pairs per pass
+            hdr[lane] = TaskHdr{i, j, nt, far || nt == 0};
         }
         __syncwarp();
         // the epilogue's scattered P(f) reads: start them into L1 before the samples, so that
@@ -870,8 +878,9 @@ k_corr(pb_fill_geom g, KArg k, const double *st, pb_epi_args ea, double2 *ig, lo
             }
         };
         // ---- samples of the 16 pairs: other pairs one after the other with the whole warp,
-        // then the far pairs (2-point rule, 16 samples per term) two at a time, one per
-        // half-warp, so that no lane idles and one transposed reduction serves both
+        // then the far pairs (2-point rule, 16 samples per term) and the term-less pairs two
+        // at a time, one per half-warp, so that no lane idles and one transposed reduction
+        // and one epilogue pass serve both
         const bool valid = lane < PB_GROUP && g0 + lane < T;
         unsigned far_m = PAIR_FAR ? __ballot_sync(0xffffffffu, valid && hdr[lane].pad) : 0u;
         unsigned near_m = __ballot_sync(0xffffffffu, valid) & ~far_m;
@@ -909,11 +918,13 @@ k_corr(pb_fill_geom g, KArg k, const double *st, pb_epi_args ea, double2 *ig, lo
                     const int nq = max(hdr[ta].nterm, tb >= 0 ? hdr[tb].nterm : 0);
                     const int nt = tk >= 0 ? hdr[tk].nterm : 0;
                     if (tk >= 0) prefetch_p(hdr[tk], f);
-                    Acc<R, F> acc;
-                    acc.init(tot + lane);
-                    for (int q = 0; q < nq; q++)
-                        run_far2<F, EQ, RED>(q < nt ? &terms[2 * tk + q] : nullptr, k, acc, lane, bases);
-                    reduce_halves<F>(acc, lane, cr, cim);
+                    if (nq > 0) {                          // warp-uniform; 0: two term-less pairs
+                        Acc<R, F> acc;
+                        acc.init(tot + lane);
+                        for (int q = 0; q < nq; q++)
+                            run_far2<F, EQ, RED>(q < nt ? &terms[2 * tk + q] : nullptr, k, acc, lane, bases);
+                        reduce_halves<F>(acc, lane, cr, cim);
+                    }
                 } else {
                     tk = -1;
                     f = 0;
