@@ -670,11 +670,12 @@ k_pot_static(pb_fill_geom g, double kw, double *st)
 }
 
 // ---------------------------------------------------------------- correction kernels
-// One warp owns a group of 32 consecutive upper-triangle pairs. Set-up: lane l builds the
-// (at most two) term descriptors of pair l of the group - the FP64 dispatch, frames and
-// quadrature choice - into shared memory. Then the whole warp sweeps the samples of the
-// 32 pairs one after the other (lanes split the samples), so the FP64 set-up costs one
-// lane-evaluation per pair instead of 32.
+// One warp owns a group of PB_GROUP = 16 consecutive upper-triangle pairs. Set-up: lane p
+// builds the direct term descriptor of pair p of the group and lane 16 + p its
+// ground-plane image - the FP64 dispatch, frames and quadrature choice - into shared
+// memory. Then the warp sweeps the samples: pairs with a near term one after the other
+// with all 32 lanes (lanes split the samples), far and term-less pairs two at a time,
+// one per half-warp. The FP64 set-up so costs one lane-evaluation per term.
 #define PB_CORR_WARPS 4
 #ifndef PB_CORR_MINB
 #define PB_CORR_MINB 4      // resident blocks per SM the register budget is sized for
@@ -683,7 +684,7 @@ k_pot_static(pb_fill_geom g, double kw, double *st)
 
 enum { PB_SET_LP = 0, PB_SET_IG = 1 };
 
-struct TaskHdr { int i, j, nterm, pad; };
+struct TaskHdr { int i, j, nterm, half; };   // half: far or term-less, runs on a half-warp
 
 __device__ __forceinline__ void prefetch_l1(const void *p)
 {
@@ -882,7 +883,7 @@ k_corr(pb_fill_geom g, KArg k, const double *st, pb_epi_args ea, double2 *ig, lo
         // at a time, one per half-warp, so that no lane idles and one transposed reduction
         // and one epilogue pass serve both
         const bool valid = lane < PB_GROUP && g0 + lane < T;
-        unsigned far_m = PAIR_FAR ? __ballot_sync(0xffffffffu, valid && hdr[lane].pad) : 0u;
+        unsigned far_m = PAIR_FAR ? __ballot_sync(0xffffffffu, valid && hdr[lane].half) : 0u;
         unsigned near_m = __ballot_sync(0xffffffffu, valid) & ~far_m;
         const int half = lane >> 4, hl = lane & 15;
         while (near_m | far_m) {                           // warp-uniform
