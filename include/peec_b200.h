@@ -100,6 +100,8 @@ typedef struct pb_ctx pb_ctx;
 #define PB_LU_FP64     0     /* FP64 panels + FP64 trailing updates                      */
 #define PB_LU_FP32     1     /* FP32 panels + FP32 SIMT trailing updates, FP64 refinement */
 #define PB_LU_TC       2     /* FP32 panels + tensor-core trailing updates, FP64 refinement */
+#define PB_LU_TC_CUBLAS 3    /* comparison baseline: as PB_LU_TC, with cuBLAS's BF16x9 FP32
+                                emulation in place of the library's tcgen05 update kernel  */
 
 /* MNA formulation inside the sweep. */
 #define PB_FORM_AUTO    0    /* reduced when applicable, else full                       */
@@ -298,6 +300,28 @@ int  pb_lu_solve(int n, const double *a, const int *piv, double *b);
  * info[b] = -1 or the zero-pivot row of matrix b. Device pointers (cudaMalloc'd).
  */
 int  pb_lu_decomp_batched_dev(int n, int nb, double *a_dev, int *piv_dev, int *info_host);
+
+/*
+ * The mixed-precision factorisation of the sweep on device memory: nb matrices of order
+ * n, row-major, complex FP32 (interleaved re/im), stride n*n, factorised in place with
+ * the pivot rule of lu_decomp (src/lu.c:16-66); lu = PB_LU_TC (tensor-core trailing
+ * updates), PB_LU_FP32 (SIMT updates) or PB_LU_TC_CUBLAS. info_host[b] as above.
+ */
+int  pb_lu_decomp_batched32_dev(int n, int nb, float *a_dev, int *piv_dev, int *info_host, int lu);
+
+/*
+ * The trailing update of the factorisation (the row update of lu_decomp, src/lu.c:54-62,
+ * for a block of rows and columns at once): C[b] -= A[b] * B[b] for b < nb, complex FP32
+ * (interleaved re/im), row-major, leading dimensions and batch stride in complex
+ * elements, device pointers; C is m x nc, A m x k, B k x nc. kind = PB_LU_TC: the
+ * library's tcgen05 kernel (split-TF32, 3 products, FP32 accumulation); it needs
+ * m, nc >= 128, k >= 16, even leading dimensions and batch stride and 16-byte aligned
+ * pointers, else PB_ERR_UNSUP (inside the factorisation such updates go to the SIMT
+ * kernel). PB_LU_FP32: the SIMT kernel, any shape. PB_LU_TC_CUBLAS: cuBLAS's BF16x9 FP32
+ * emulation. Runs on the default stream; returns 0 once the update is queued, or PB_ERR_*.
+ */
+int  pb_cgemm_sub_batched_dev(int m, int nc, int k, const float *a_dev, int lda, const float *b_dev,
+                              int ldb, float *c_dev, int ldc, long long stride, int nb, int kind);
 
 /*
  * Partial-inductance fill that allocates nothing. It has no counterpart in the reference

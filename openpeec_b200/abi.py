@@ -32,7 +32,7 @@ MUT_DTYPE = np.dtype([("l1", "<i4"), ("l2", "<i4"), ("k", "<f8")])
 PB_LUMP_R, PB_LUMP_C, PB_LUMP_L, PB_LUMP_V = 0, 1, 2, 3
 PB_OK, PB_ERR_ARG, PB_ERR_CUDA, PB_ERR_SINGULAR, PB_ERR_NOCONV, PB_ERR_UNSUP = range(6)
 PREC_FP64, PREC_MIXED = 0, 1
-LU_FP64, LU_FP32, LU_TC = 0, 1, 2
+LU_FP64, LU_FP32, LU_TC, LU_TC_CUBLAS = 0, 1, 2, 3
 FORM_AUTO, FORM_FULL, FORM_REDUCED = 0, 1, 2
 
 _vp = C.c_void_p
@@ -145,6 +145,9 @@ def lib():
     L.pb_lu_solve.argtypes = [C.c_int, _vp, _vp, _vp]
     L.pb_lu_decomp_batched_dev.argtypes = [C.c_int, C.c_int, _vp, _vp, _vp]
     L.pb_fp32_peak.argtypes = [C.POINTER(C.c_double)]
+    L.pb_lu_decomp_batched32_dev.argtypes = [C.c_int, C.c_int, _vp, _vp, _vp, C.c_int]
+    L.pb_cgemm_sub_batched_dev.argtypes = [C.c_int, C.c_int, C.c_int, _vp, C.c_int, _vp, C.c_int, _vp, C.c_int,
+                                           C.c_longlong, C.c_int, C.c_int]
     L.pb_lp_fill_noalloc.argtypes = [C.c_int, _vp, C.c_int, C.c_double, C.c_double, C.c_int, _vp]
     L.pb_device_sync.restype = C.c_int
     L.pb_sources.argtypes = [_vp, C.c_int, _vp, C.POINTER(PbSweepOpts), C.c_int, _vp, _vp,

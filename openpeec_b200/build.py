@@ -18,7 +18,8 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
          "-ccbin", "/usr/bin/g++"]
-SOURCES = ["pb_api.cu", "pb_fill.cu", "pb_lu.cu", "pb_sweep.cu", "pb_gmres.cu", "pb_hmat.cu", "pb_mlp.cu", "pb_post.cu", "pb_noalloc.cu"]
+SOURCES = ["pb_api.cu", "pb_fill.cu", "pb_lu.cu", "pb_tcgemm.cu", "pb_sweep.cu", "pb_gmres.cu", "pb_hmat.cu",
+           "pb_mlp.cu", "pb_post.cu", "pb_noalloc.cu"]
 # The fill keeps multiply and add separate (as the reference's CPU build does) so that the
 # quadrature-order decisions (e.g. rc/lmax > 2) and the cancellation-prone FP64 closed
 # forms round like the reference; the hot accumulations use explicit fma().

@@ -1,8 +1,10 @@
 #include <atomic>
 #include <thread>
 // pb_api.cu — C entry points of the batched core (include/peec_b200.h).
+#include <mutex>
 #include "pb_ctx.cuh"
 #include "pb_hmat.cuh"
+#include "pb_tcgemm.cuh"
 #include <algorithm>
 #include <cmath>
 #include <cstdarg>
@@ -520,6 +522,83 @@ int pb_lu_decomp_batched_dev(int n, int nb, double *a_dev, int *piv_dev, int *in
     }
     cudaFree(info);
     pb_lu_engine_free(&e);
+    return r;
+}
+
+int pb_lu_decomp_batched32_dev(int n, int nb, float *a_dev, int *piv_dev, int *info_host, int lu)
+{
+    if (n <= 0 || nb <= 0 || !a_dev || !piv_dev || !info_host) { pb_set_error("pb_lu_decomp_batched32_dev: bad argument"); return PB_ERR_ARG; }
+    if (lu != PB_LU_TC && lu != PB_LU_FP32 && lu != PB_LU_TC_CUBLAS) { pb_set_error("pb_lu_decomp_batched32_dev: bad kind %d", lu); return PB_ERR_ARG; }
+    PB_TRY(need_device());
+    pb_lu_engine e;
+    PB_TRY(pb_lu_engine_init(&e, nullptr));
+    e.gemm_kind = lu == PB_LU_TC ? PB_GEMM_TC : lu == PB_LU_FP32 ? PB_GEMM_FP32 : PB_GEMM_TC_BLAS;
+    int *info = nullptr;
+    float *emb = nullptr;
+    cudaError_t ce = cudaMalloc(&info, sizeof(int) * nb);
+    if (ce == cudaSuccess && lu == PB_LU_TC_CUBLAS) {
+        e.emb_cap = (size_t)nb * n * n * sizeof(float);      // largest embedded right operand
+        ce = cudaMalloc(&emb, e.emb_cap);
+        e.emb = emb;
+    }
+    if (ce != cudaSuccess) { cudaFree(info); pb_lu_engine_free(&e); return pb_cuda_fail(ce, "cudaMalloc", __FILE__, __LINE__); }
+    int r = pb_lu_factor<float>(&e, n, nb, (float2 *)a_dev, n, (long)n * n, piv_dev, info);
+    if (r == PB_OK) {
+        ce = cudaMemcpy(info_host, info, sizeof(int) * nb, cudaMemcpyDeviceToHost);
+        if (ce != cudaSuccess) r = pb_cuda_fail(ce, "cudaMemcpy", __FILE__, __LINE__);
+    }
+    cudaFree(info);
+    cudaFree(emb);
+    pb_lu_engine_free(&e);
+    return r;
+}
+
+int pb_cgemm_sub_batched_dev(int m, int nc, int k, const float *a_dev, int lda, const float *b_dev, int ldb,
+                             float *c_dev, int ldc, long long stride, int nb, int kind)
+{
+    if (m < 0 || nc < 0 || k < 0 || nb < 0 || (m && nc && k && nb && (!a_dev || !b_dev || !c_dev)) ||
+        lda < k || ldb < nc || ldc < nc || (nb > 1 && stride < (long long)m * ldc)) {
+        pb_set_error("pb_cgemm_sub_batched_dev: bad argument");
+        return PB_ERR_ARG;
+    }
+    if (kind != PB_LU_TC && kind != PB_LU_FP32 && kind != PB_LU_TC_CUBLAS) { pb_set_error("pb_cgemm_sub_batched_dev: bad kind %d", kind); return PB_ERR_ARG; }
+    PB_TRY(need_device());
+    if (kind == PB_LU_TC && m > 0 && nc > 0 && k > 0 && nb > 0 &&
+        (m < 128 || nc < 128 || k < 16 ||
+         !pb_cgemm_tc_ok((const float2 *)a_dev, lda, (const float2 *)b_dev, ldb, (const float2 *)c_dev, ldc, stride, nb))) {
+        pb_set_error("pb_cgemm_sub_batched_dev: the tensor-core kernel needs m, nc >= 128, k >= 16, even leading "
+                     "dimensions and batch stride, and 16-byte aligned pointers");
+        return PB_ERR_UNSUP;
+    }
+    static pb_lu_engine eng;                 // one engine per process for this entry point
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lk(mu);
+    if (!eng.blas) PB_TRY(pb_lu_engine_init(&eng, nullptr));
+    eng.gemm_kind = kind == PB_LU_TC ? PB_GEMM_TC : kind == PB_LU_FP32 ? PB_GEMM_FP32 : PB_GEMM_TC_BLAS;
+    float *emb = nullptr;
+    if (kind == PB_LU_TC_CUBLAS) {
+        eng.emb_cap = (size_t)nb * 4 * k * nc * sizeof(float);
+        PB_CUDA(cudaMalloc(&emb, eng.emb_cap));
+        eng.emb = emb;
+    }
+    int r = pb_cgemm_sub(&eng, m, nc, k, (const float2 *)a_dev, lda, (const float2 *)b_dev, ldb, (float2 *)c_dev,
+                         ldc, stride, nb);
+    if (kind == PB_LU_TC_CUBLAS) {
+        cudaStreamSynchronize(nullptr);
+        cudaFree(emb);
+        eng.emb = nullptr;
+        eng.emb_cap = 0;
+    }
+    if (r == PB_OK && eng.tc_used && eng.tc_err) {
+        eng.tc_used = 0;
+        int h = 0;
+        PB_CUDA(cudaMemcpy(&h, eng.tc_err, sizeof(int), cudaMemcpyDeviceToHost));
+        if (h) {
+            cudaMemset(eng.tc_err, 0, sizeof(int));
+            pb_set_error("tensor-core update: a pipeline wait timed out");
+            r = PB_ERR_CUDA;
+        }
+    }
     return r;
 }
 

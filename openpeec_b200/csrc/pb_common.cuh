@@ -2,6 +2,7 @@
 // error plumbing, device-side cell frames).
 #pragma once
 #include <cuda_runtime.h>
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <cmath>
@@ -56,6 +57,32 @@ template <typename T2> __host__ __device__ __forceinline__ T2 cinv(T2 z)
 }
 template <typename T2> __host__ __device__ __forceinline__ double cmag1(T2 z)
 { return fabs((double)z.x) + fabs((double)z.y); }       // pivot measure, lu.c:10-13
+
+// ------------------------------------------------------------------ kernel attributes
+// cudaFuncSetAttribute acts on the current device only. A process that drives several
+// devices (one context per device, e.g. pb_sweep_many over contexts on different GPUs)
+// must set a kernel's shared-memory opt-in on each of them, so the flag that skips the
+// repeated call is a bit mask over device indices; devices >= 64 set it on every call.
+template <typename K>
+static inline int pb_smem_optin(K kernel, int bytes, std::atomic<unsigned long long> &done)
+{
+    int dev = 0;
+    PB_CUDA(cudaGetDevice(&dev));
+    const unsigned long long bit = (dev >= 0 && dev < 64) ? (1ull << dev) : 0ull;
+    if (bit && (done.load(std::memory_order_acquire) & bit)) return PB_OK;
+    PB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    if (bit) done.fetch_or(bit, std::memory_order_release);
+    return PB_OK;
+}
+
+// Largest dynamic shared memory one block may opt in to on the current device.
+static inline int pb_smem_cap()
+{
+    int dev = 0, cap = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&cap, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    return cap;
+}
 
 // ------------------------------------------------------------------ misc
 static inline unsigned ceil_div(long a, long b) { return (unsigned)((a + b - 1) / b); }

@@ -1199,11 +1199,8 @@ static int launch_corr(const pb_fill_geom &g, const KArg &k, const double *st, c
     const int n = SET == PB_SET_LP ? g.seg.n : g.chg.n;
     const long long T = (long long)n * (n + 1) / 2;
     constexpr size_t smem = corr_smem_bytes<R, F>();
-    static std::atomic<bool> attr_set{false};   // set once, before any launch relies on it
-    if (!attr_set) {
-        PB_CUDA(cudaFuncSetAttribute(k_corr<R, F, SET, EPI, EQ, RED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr_set = true;
-    }
+    static std::atomic<unsigned long long> attr_set{0};   // per device, before any launch relies on it
+    PB_TRY(pb_smem_optin(k_corr<R, F, SET, EPI, EQ, RED>, (int)smem, attr_set));
     const int grid = grid_for((T + PB_GROUP - 1) / PB_GROUP, PB_CORR_WARPS, PB_CORR_MINB);
     k_corr<R, F, SET, EPI, EQ, RED><<<grid, 32 * PB_CORR_WARPS, smem, s>>>(g, k, st, ea, ig, igs);
     PB_CHECK_LAUNCH();

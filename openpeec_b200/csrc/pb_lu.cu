@@ -9,6 +9,7 @@
 // Row-major storage, like the reference (a[i*n+j]).
 #include <atomic>
 #include "pb_lu.cuh"
+#include "pb_tcgemm.cuh"
 #include <climits>
 #include <cuComplex.h>
 #include <dlfcn.h>
@@ -262,46 +263,147 @@ static pb_set_emulation_fn set_emulation()
     return fn;
 }
 
+// Complex FP32 update C -= A * B on the SIMT pipes, for updates thinner than the
+// tensor-core kernel's 128 x 128 x 16 tile: 64 x 64 complex outputs per 256-thread block,
+// 4 x 4 per thread, k staged in shared memory 16 at a time, FP32 fused multiply-adds.
+__global__ void __launch_bounds__(256)
+k_cgemm_simt(const float2 *__restrict__ A, int lda, const float2 *__restrict__ B, int ldb,
+             float2 *__restrict__ C, int ldc, long long stride, int m, int nc, int k)
+{
+    __shared__ float2 As[16][65];               // [kk][row], padded against bank conflicts
+    __shared__ float2 Bs[16][64];               // [kk][col]
+    const long long bo = (long long)blockIdx.z * stride;
+    A += bo;
+    B += bo;
+    C += bo;
+    const int m0 = blockIdx.y * 64, n0 = blockIdx.x * 64;
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    float2 acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) acc[i][j] = make_float2(0.f, 0.f);
+    for (int k0 = 0; k0 < k; k0 += 16) {
+        for (int e = threadIdx.x; e < 1024; e += 256) {
+            const int r = e >> 4, kk = e & 15;
+            As[kk][r] = (m0 + r < m && k0 + kk < k) ? A[(long long)(m0 + r) * lda + k0 + kk] : make_float2(0.f, 0.f);
+            const int kb = e >> 6, c = e & 63;
+            Bs[kb][c] = (k0 + kb < k && n0 + c < nc) ? B[(long long)(k0 + kb) * ldb + n0 + c] : make_float2(0.f, 0.f);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < 16; kk++) {
+            float2 a[4], b[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) a[i] = As[kk][ty + 16 * i];
+#pragma unroll
+            for (int j = 0; j < 4; j++) b[j] = Bs[kk][tx + 16 * j];
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    acc[i][j].x = fmaf(a[i].x, b[j].x, fmaf(-a[i].y, b[j].y, acc[i][j].x));
+                    acc[i][j].y = fmaf(a[i].x, b[j].y, fmaf(a[i].y, b[j].x, acc[i][j].y));
+                }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const int r = m0 + ty + 16 * i;
+        if (r >= m) continue;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int c = n0 + tx + 16 * j;
+            if (c >= nc) continue;
+            float2 &v = C[(long long)r * ldc + c];
+            v.x -= acc[i][j].x;
+            v.y -= acc[i][j].y;
+        }
+    }
+}
+
+// cuBLAS's BF16x9 FP32 emulation of the update as one real GEMM (comparison baseline,
+// PB_GEMM_TC_BLAS). Returns PB_ERR_UNSUP when the library or the scratch cannot serve it.
+static int gemm_sub_cublas_bf16x9(pb_lu_engine *e, int m, int nc, int k, const float2 *A, int lda,
+                                  const float2 *B, int ldb, float2 *Cm, int ldc, long long stride, int nb)
+{
+    const size_t need = (size_t)nb * 4 * (size_t)k * nc * sizeof(float);
+    const pb_set_emulation_fn set_emu = set_emulation();
+    if (!set_emu) e->tc_disabled = 1;
+    if (e->tc_disabled || !e->emb || need > e->emb_cap || m < kTcMinDim || nc < kTcMinDim || k < kTcMinDim)
+        return PB_ERR_UNSUP;
+    k_embed_right<<<dim3(ceil_div(nc, 128), k, nb), 128, 0, e->stream>>>(B, k, nc, ldb, stride, e->emb);
+    PB_CHECK_LAUNCH();
+    e->launches++;
+    const float ra = -1.0f, rb = 1.0f;
+    cublasSetMathMode(e->blas, CUBLAS_DEFAULT_MATH);
+    set_emu(e->blas, CUBLAS_EMULATION_STRATEGY_EAGER);
+    // row-major real C (m x 2nc) -= A (m x 2k) * Bemb (2k x 2nc); cuBLAS is
+    // column-major, so it computes the transpose: C^T = Bemb^T A^T.
+    const cublasStatus_t s = cublasGemmStridedBatchedEx(
+        e->blas, CUBLAS_OP_N, CUBLAS_OP_N, 2 * nc, m, 2 * k, &ra, e->emb, CUDA_R_32F, 2 * nc,
+        4LL * k * nc, A, CUDA_R_32F, 2 * lda, 2 * stride, &rb, Cm, CUDA_R_32F, 2 * ldc, 2 * stride, nb,
+        CUBLAS_COMPUTE_32F_EMULATED_16BFX9, CUBLAS_GEMM_DEFAULT);
+    set_emu(e->blas, CUBLAS_EMULATION_STRATEGY_DEFAULT);
+    cublasSetMathMode(e->blas, CUBLAS_PEDANTIC_MATH);
+    e->launches++;
+    if (s == CUBLAS_STATUS_SUCCESS) return PB_OK;
+    if (s != CUBLAS_STATUS_NOT_SUPPORTED) {
+        pb_set_error("BF16x9 real GEMM failed (%d)", (int)s);
+        return PB_ERR_CUDA;
+    }
+    e->tc_disabled = 1;                     // library without the emulation: SIMT from now on
+    return PB_ERR_UNSUP;
+}
+
+int pb_cgemm_sub(pb_lu_engine *e, int m, int nc, int k, const float2 *A, int lda, const float2 *B,
+                 int ldb, float2 *Cm, int ldc, long long stride, int nb)
+{
+    if (m <= 0 || nc <= 0 || k <= 0 || nb <= 0) return PB_OK;
+    if (e->gemm_kind == PB_GEMM_TC && m >= 128 && nc >= 128 && k >= 16 &&
+        pb_cgemm_tc_ok(A, lda, B, ldb, Cm, ldc, stride, nb)) {
+        if (!e->tc_err) {
+            PB_CUDA(cudaMalloc(&e->tc_err, sizeof(int)));
+            PB_CUDA(cudaMemsetAsync(e->tc_err, 0, sizeof(int), e->stream));
+        }
+        e->launches++;
+        e->tc_used = 1;
+        return pb_cgemm_tc(m, nc, k, A, lda, B, ldb, Cm, ldc, stride, nb, e->tc_err, e->stream);
+    }
+    if (e->gemm_kind == PB_GEMM_TC_BLAS) {
+        const int r = gemm_sub_cublas_bf16x9(e, m, nc, k, A, lda, B, ldb, Cm, ldc, stride, nb);
+        if (r != PB_ERR_UNSUP) return r;
+    }
+    k_cgemm_simt<<<dim3(ceil_div(nc, 64), ceil_div(m, 64), nb), 256, 0, e->stream>>>(A, lda, B, ldb, Cm, ldc,
+                                                                                       stride, m, nc, k);
+    e->launches++;
+    PB_CHECK_LAUNCH();
+    return PB_OK;
+}
+
+// The tensor-core kernel reports a timed-out pipeline wait through a device flag; read it
+// (one stream synchronisation) after a factorisation that used the kernel.
+static int check_tc(pb_lu_engine *e)
+{
+    if (!e->tc_used || !e->tc_err) return PB_OK;
+    e->tc_used = 0;
+    int h = 0;
+    PB_CUDA(cudaMemcpyAsync(&h, e->tc_err, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
+    PB_CUDA(cudaStreamSynchronize(e->stream));
+    if (h) {
+        PB_CUDA(cudaMemsetAsync(e->tc_err, 0, sizeof(int), e->stream));
+        pb_set_error("tensor-core trailing update: a pipeline wait timed out; the factorisation is invalid");
+        return PB_ERR_CUDA;
+    }
+    return PB_OK;
+}
+
 template <>
 int gemm_sub<float>(pb_lu_engine *e, int m, int nc, int k, const float2 *A, int lda,
                     const float2 *B, int ldb, float2 *Cm, int ldc, long long stride, int nb)
 {
-    if (m <= 0 || nc <= 0 || k <= 0) return PB_OK;
-    cublasStatus_t s;
-    const size_t need = (size_t)nb * 4 * (size_t)k * nc * sizeof(float);
-    const pb_set_emulation_fn set_emu = set_emulation();
-    if (!set_emu) e->tc_disabled = 1;
-    if (e->gemm_kind == PB_GEMM_TC && !e->tc_disabled && e->emb && need <= e->emb_cap &&
-        m >= kTcMinDim && nc >= kTcMinDim && k >= kTcMinDim) {
-        k_embed_right<<<dim3(ceil_div(nc, 128), k, nb), 128, 0, e->stream>>>(B, k, nc, ldb, stride, e->emb);
-        PB_CHECK_LAUNCH();
-        e->launches++;
-        const float ra = -1.0f, rb = 1.0f;
-        cublasSetMathMode(e->blas, CUBLAS_DEFAULT_MATH);
-        set_emu(e->blas, CUBLAS_EMULATION_STRATEGY_EAGER);
-        // row-major real C (m x 2nc) -= A (m x 2k) * Bemb (2k x 2nc); cuBLAS is
-        // column-major, so it computes the transpose: C^T = Bemb^T A^T.
-        s = cublasGemmStridedBatchedEx(
-            e->blas, CUBLAS_OP_N, CUBLAS_OP_N, 2 * nc, m, 2 * k, &ra, e->emb, CUDA_R_32F, 2 * nc,
-            4LL * k * nc, A, CUDA_R_32F, 2 * lda, 2 * stride, &rb, Cm, CUDA_R_32F, 2 * ldc, 2 * stride, nb,
-            CUBLAS_COMPUTE_32F_EMULATED_16BFX9, CUBLAS_GEMM_DEFAULT);
-        set_emu(e->blas, CUBLAS_EMULATION_STRATEGY_DEFAULT);
-        cublasSetMathMode(e->blas, CUBLAS_PEDANTIC_MATH);
-        e->launches++;
-        if (s == CUBLAS_STATUS_SUCCESS) return PB_OK;
-        if (s != CUBLAS_STATUS_NOT_SUPPORTED) {
-            pb_set_error("BF16x9 real GEMM failed (%d)", (int)s);
-            return PB_ERR_CUDA;
-        }
-        e->tc_disabled = 1;                     // library without the emulation: SIMT from now on
-    }
-    const cuComplex alpha = make_cuComplex(-1, 0), beta = make_cuComplex(1, 0);
-    s = cublasCgemmStridedBatched(
-        e->blas, CUBLAS_OP_N, CUBLAS_OP_N, nc, m, k, &alpha, (const cuComplex *)B, ldb,
-        stride, (const cuComplex *)A, lda, stride, &beta, (cuComplex *)Cm, ldc, stride, nb);
-    e->launches++;
-    if (s != CUBLAS_STATUS_SUCCESS) { pb_set_error("complex FP32 GEMM failed (%d)", (int)s); return PB_ERR_CUDA; }
-    return PB_OK;
+    return pb_cgemm_sub(e, m, nc, k, A, lda, B, ldb, Cm, ldc, stride, nb);
 }
 
 int pb_lu_engine_init(pb_lu_engine *e, cudaStream_t s)
@@ -320,6 +422,8 @@ void pb_lu_engine_free(pb_lu_engine *e)
 {
     if (e->blas) cublasDestroy(e->blas);
     e->blas = nullptr;
+    if (e->tc_err) cudaFree(e->tc_err);
+    e->tc_err = nullptr;
 }
 
 // ---------------------------------------------------------------- recursion
@@ -341,14 +445,8 @@ template <typename T, int SW>
 static int launch_leaf(pb_lu_engine *e, T2_t<T> *a, int n, int ld, long long stride, int nb,
                        int k0, int w, int *piv, int *info, size_t smem)
 {
-    static std::atomic<bool> attr_set{false};   // set once, before any launch relies on it
-    if (!attr_set) {
-        int dev = 0, cap = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&cap, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-        PB_CUDA(cudaFuncSetAttribute(k_lu_leaf<T, SW>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap - 1024));
-        attr_set = true;
-    }
+    static std::atomic<unsigned long long> attr_set{0};   // per device, before any launch relies on it
+    PB_TRY(pb_smem_optin(k_lu_leaf<T, SW>, pb_smem_cap() - 1024, attr_set));
     // the panel has m = n - k0 rows: a CTA no wider than the panel (at least 128 threads)
     // lets several small systems share an SM (batches of small structures); the pivot
     // search and the updates do not depend on the thread count, so results are unchanged
@@ -377,12 +475,8 @@ static int trsm_rec(pb_lu_engine *e, T2_t<T> *a, int ld, long long stride, int n
 {
     if (c1 <= c0 || w <= 0) return PB_OK;
     if (w <= 64) {
-        static std::atomic<bool> attr_set{false};   // set once, before any launch relies on it
-        if (!attr_set) {
-            PB_CUDA(cudaFuncSetAttribute(k_trsm_small<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (64 * 64 + 64 * 64) * (int)sizeof(T2_t<T>)));
-            attr_set = true;
-        }
+        static std::atomic<unsigned long long> attr_set{0};   // per device
+        PB_TRY(pb_smem_optin(k_trsm_small<T>, (64 * 64 + 64 * 64) * (int)sizeof(T2_t<T>), attr_set));
         const size_t smem = (size_t)(w * w + w * 64) * sizeof(T2_t<T>);
         dim3 g(ceil_div(c1 - c0, 64), nb);
         k_trsm_small<T><<<g, 64, smem, e->stream>>>(a, ld, stride, r0, w, c0, c1);
@@ -437,7 +531,8 @@ int pb_lu_factor(pb_lu_engine *e, int n, int nb, T2_t<T> *a, int ld, long stride
         pb_set_error("LU order %d exceeds the shared-memory panel capacity of this build", n);
         return PB_ERR_UNSUP;
     }
-    return lu_rec<T>(e, a, n, ld, stride, nb, 0, n, piv, info, sw, smem);
+    PB_TRY(lu_rec<T>(e, a, n, ld, stride, nb, 0, n, piv, info, sw, smem));
+    return check_tc(e);
 }
 template int pb_lu_factor<float>(pb_lu_engine *, int, int, float2 *, int, long, int *, int *);
 template int pb_lu_factor<double>(pb_lu_engine *, int, int, double2 *, int, long, int *, int *);
@@ -586,14 +681,8 @@ int pb_lu_solve_mapped(pb_lu_engine *e, int n, int nb, int nrhs, const T2_t<TF> 
 {
     if (nb <= 0) return PB_OK;
     const size_t smem = (size_t)n * sizeof(T2_t<TF>);
-    static std::atomic<bool> attr_set{false};   // set once, before any launch relies on it
-    if (!attr_set) {
-        int dev = 0, cap = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&cap, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-        PB_CUDA(cudaFuncSetAttribute(k_lu_solve<TF>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap - 20480));
-        attr_set = true;
-    }
+    static std::atomic<unsigned long long> attr_set{0};   // per device
+    PB_TRY(pb_smem_optin(k_lu_solve<TF>, pb_smem_cap() - 20480, attr_set));
     dim3 g(nrhs, nb);
     k_lu_solve<TF><<<g, 1024, smem, e->stream>>>(lu, n, ld, stride, perm, r, x, nrhs, sys, lu_of);
     e->launches++;
@@ -733,6 +822,9 @@ k_residual(const double2 *a, int n, int ld, long long stride, const double2 *bv,
     }
 }
 
+// devices on which k_residual's shared-memory opt-in is set
+static std::atomic<unsigned long long> g_residual_attr{0};
+
 int pb_residual(pb_lu_engine *e, int n, int nb, int nrhs, const double2 *a, int ld, long stride,
                 const double2 *b, const double2 *x, double2 *r, double *rn, double *bn, double *xn,
                 double *an, double *cw)
@@ -742,14 +834,7 @@ int pb_residual(pb_lu_engine *e, int n, int nb, int nrhs, const double2 *a, int 
     PB_CUDA(cudaMemsetAsync(bn, 0, sizeof(double) * nb * nrhs, e->stream));
     if (an) PB_CUDA(cudaMemsetAsync(an, 0, sizeof(double) * nb, e->stream));
     const size_t smem = (size_t)nrhs * n * sizeof(double2);
-    static std::atomic<bool> attr_set{false};   // set once, before any launch relies on it
-    if (!attr_set) {
-        int dev = 0, cap = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&cap, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-        PB_CUDA(cudaFuncSetAttribute(k_residual, cudaFuncAttributeMaxDynamicSharedMemorySize, cap));
-        attr_set = true;
-    }
+    PB_TRY(pb_smem_optin(k_residual, pb_smem_cap(), g_residual_attr));
     const int rpb = 64;
     dim3 g(ceil_div(n, rpb), nb);
     k_residual<<<g, 256, smem, e->stream>>>(a, n, ld, stride, b, x, r, rn, bn, xn, an, nrhs, rpb, nullptr, cw);
@@ -768,14 +853,7 @@ int pb_residual_mapped(pb_lu_engine *e, int n, int nb, int nrhs, const double2 *
     if (an) PB_CUDA(cudaMemsetAsync(an, 0, sizeof(double) * nall, e->stream));
     if (nb <= 0) return PB_OK;
     const size_t smem = (size_t)nrhs * n * sizeof(double2);
-    static std::atomic<bool> attr_set{false};   // set once, before any launch relies on it
-    if (!attr_set) {
-        int dev = 0, cap = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&cap, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-        PB_CUDA(cudaFuncSetAttribute(k_residual, cudaFuncAttributeMaxDynamicSharedMemorySize, cap));
-        attr_set = true;
-    }
+    PB_TRY(pb_smem_optin(k_residual, pb_smem_cap(), g_residual_attr));
     const int rpb = 64;
     dim3 g(ceil_div(n, rpb), nb);
     k_residual<<<g, 256, smem, e->stream>>>(a, n, ld, stride, b, x, r, rn, bn, xn, an, nrhs, rpb, sys, cw);
@@ -789,14 +867,7 @@ int pb_matvec_mapped(pb_lu_engine *e, int n, int nb, int nrhs, const double2 *a,
 {
     if (nb <= 0) return PB_OK;
     const size_t smem = (size_t)nrhs * n * sizeof(double2);
-    static std::atomic<bool> attr_set{false};   // set once, before any launch relies on it
-    if (!attr_set) {
-        int dev = 0, cap = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&cap, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-        PB_CUDA(cudaFuncSetAttribute(k_residual, cudaFuncAttributeMaxDynamicSharedMemorySize, cap));
-        attr_set = true;
-    }
+    PB_TRY(pb_smem_optin(k_residual, pb_smem_cap(), g_residual_attr));
     const int rpb = 64;
     dim3 g(ceil_div(n, rpb), nb);
     k_residual<<<g, 256, smem, e->stream>>>(a, n, ld, stride, nullptr, x, y, nullptr, nullptr, nullptr,

@@ -5,11 +5,13 @@
 
 // Trailing-update engine of the LU.
 enum pb_gemm_kind {
-    PB_GEMM_FP64 = 0,   // complex FP64 GEMM
-    PB_GEMM_FP32 = 1,   // complex FP32 GEMM, SIMT
-    PB_GEMM_TC   = 2,   // complex FP32 GEMM as one real FP32 GEMM on the tensor cores
-                        // (BF16x9 FP32 emulation: each FP32 operand split into 3 BF16
-                        // terms, FP32 accumulation); SIMT for thin updates
+    PB_GEMM_FP64 = 0,   // complex FP64 GEMM (cuBLAS ZGEMM: the plain FP64 path)
+    PB_GEMM_FP32 = 1,   // complex FP32 GEMM, the library's own SIMT kernel
+    PB_GEMM_TC   = 2,   // complex FP32 GEMM on the tensor cores: the library's tcgen05
+                        // kernel (split-TF32, 3 products, FP32 accumulation in TMEM,
+                        // pb_tcgemm.cu); the SIMT kernel for updates thinner than its tile
+    PB_GEMM_TC_BLAS = 3 // comparison baseline: cuBLAS's BF16x9 FP32 emulation of the same
+                        // update as one real GEMM (B expanded to 2x2 real blocks)
 };
 
 struct pb_lu_engine {
@@ -17,14 +19,21 @@ struct pb_lu_engine {
     cudaStream_t stream = nullptr;
     int gemm_kind = PB_GEMM_FP64;
     long launches = 0;         // kernels launched (own kernels + library calls)
-    // Scratch for PB_GEMM_TC: the k x nc complex right operand expanded to the real
+    // Scratch for PB_GEMM_TC_BLAS: the k x nc complex right operand expanded to the real
     // 2k x 2nc matrix [[re, im], [-im, re]] per entry, nb of them (4*k*nc floats each).
     // Owned by the caller (the sweep sizes it at 4*n*n bytes per matrix); without it, or
-    // when an update needs more, the update runs as a SIMT complex GEMM.
+    // when an update needs more, the update runs on the SIMT kernel.
     float *emb = nullptr;
     size_t emb_cap = 0;        // bytes
     int tc_disabled = 0;       // set if the library rejects the emulated compute type
+    int *tc_err = nullptr;     // device flag: a pipeline wait of the tensor-core kernel timed out
+    int tc_used = 0;           // the tensor-core kernel ran since the flag was last checked
 };
+
+// C (m x nc) -= A (m x k) * B (k x nc), complex FP32, row-major, batched with one stride,
+// on the engine's stream with the engine's kernel choice (PB_GEMM_FP32 / TC / TC_BLAS).
+int pb_cgemm_sub(pb_lu_engine *e, int m, int nc, int k, const float2 *A, int lda, const float2 *B,
+                 int ldb, float2 *C, int ldc, long long stride, int nb);
 
 int pb_lu_engine_init(pb_lu_engine *e, cudaStream_t s);
 void pb_lu_engine_free(pb_lu_engine *e);

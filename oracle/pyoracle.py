@@ -37,6 +37,15 @@ def ref_available():
     return os.path.exists(REF_SO)
 
 
+def reference_root():
+    """The reference checkout, where one is present: $PEEC_REFERENCE, else a directory
+    named `reference` beside the repository. None when neither exists (e.g. on a machine
+    that only has the prebuilt oracle/_ref files)."""
+    env = os.environ.get("PEEC_REFERENCE")
+    cand = env if env else os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")
+    return cand if os.path.isdir(os.path.join(cand, "src")) else None
+
+
 class Oracle:
     """CPU restatement of the reference hot path on a Problem."""
     _L = None

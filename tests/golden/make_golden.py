@@ -26,9 +26,11 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
 from openpeec_b200 import configs  # noqa: E402
-from oracle.pyoracle import RefLib  # noqa: E402
+from oracle.pyoracle import RefLib, reference_root  # noqa: E402
 
-REF = os.environ.get("PEEC_REFERENCE", "/root/reference")
+REF = reference_root()
+if REF is None:
+    sys.exit("make_golden.py needs the reference checkout: set PEEC_REFERENCE")
 C0 = 2.99792458e8
 
 

@@ -47,8 +47,10 @@ def test_oracle_lu_rule():
                                 "loop_square.peec", "plate_skin_layers.peec"])
 def test_oracle_vs_live_reference(fn):
     import os
-    path = os.path.join(os.environ.get("PEEC_REFERENCE", "/root/reference"), "data", "sample", fn)
-    if not os.path.exists(path):
+    from oracle.pyoracle import reference_root
+    root = reference_root()
+    path = os.path.join(root, "data", "sample", fn) if root else ""
+    if not root or not os.path.exists(path):
         pytest.skip("reference samples not present")
     r = RefLib(path)
     prob = r.problem()
