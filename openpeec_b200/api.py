@@ -92,15 +92,17 @@ class Context:
 
 
     def planewave(self, freqs, pw, fill_prec=abi.PREC_MIXED, lu=abi.LU_TC, form=abi.FORM_AUTO,
-                  batch=0, accel=0, want_segi=False):
+                  batch=0, accel=0, want_segi=False, compress=0, ctol=0.0):
         """Plane-wave incidence (pb_planewave): pw = (theta_deg, phi_deg, pol, amp,
         phase_deg). Returns voc [nport, nfreq] (open-circuit port voltages), the induced
-        segment currents [nfreq, nseg] when want_segi, and the stats."""
+        segment currents [nfreq, nseg] when want_segi, and the stats. compress = 1 solves
+        on the compressed path (H-matrix + GMRES)."""
         freqs = np.ascontiguousarray(freqs, np.float64)
         npt = len(self.prob.port)
         voc = np.zeros((npt, len(freqs)), np.complex128)
         seg = np.zeros((len(freqs), self.nseg), np.complex128) if want_segi else None
-        o = abi.PbSweepOpts(int(fill_prec), int(lu), int(form), int(batch), 0.0, 0, 0, 0, int(accel), 0, 0, 0.0, None)
+        o = abi.PbSweepOpts(int(fill_prec), int(lu), int(form), int(batch), 0.0, 0, 0, 0, int(accel),
+                            int(compress), 0, float(ctol), None)
         w = abi.PbPlanewave(float(pw[0]), float(pw[1]), int(pw[2]), 0, float(pw[3]),
                             float(pw[4]) if len(pw) > 4 else 0.0)
         st = abi.PbSweepStats()

@@ -13,6 +13,13 @@ cfg4  volume-cell bar stack for the compressed (H-matrix + GMRES) path: copper p
       40 x 40 mm, 0.2 mm thick, 96 x 96 grid x 4 layers (74,496 current cells), retardation,
       32 log frequencies 1 MHz - 2 GHz, ACA tolerance 1e-6; fed across the diagonal
       (node 1 at one corner, node 2 at the opposite one, as the compressed plate sample)
+cfg5  mixed conductor / dielectric full-wave structure above a ground plane (z = 0):
+      6 disks (r = 10 mm, 8 rings x 32 sectors) and 4 convex quads (sides 20-40 mm,
+      24 x 24 grid) at seeded positions in a 60 mm box, one horizontal panel per height
+      level so that none intersects another, and a dielectric brick 30 x 30 x 1.6 mm,
+      epsr 4.4, 30 x 30 x 2 cells, 2 mm above the ground plane (every charge cell strictly
+      above z = 0); capacitance, retardation; plane wave theta 30, phi 45 deg, 1 V/m, plus
+      a port between the centres of the first two disks; 256 frequencies, df = 10 MHz
 Scaled-down variants of cfg2 (plate grid na x nb) serve the parity tests.
 """
 import numpy as np
@@ -91,3 +98,44 @@ port = 1 2 50
 frequency = 1e6 2e9 {nfreq - 1} log
 end
 """
+
+
+def cfg5(seed=0, ndisk=6, nquad=4, disk_grid=(8, 32), quad_grid=24, brick=(30, 30, 2),
+         nfreq=256, f0=1e7, df=1e7):
+    """Config 5 as .peec text; smaller counts and grids give the scaled-down variants
+    (ndisk >= 2: the port joins the centres of the first two disks)."""
+    rng = np.random.default_rng(seed)
+    f = lambda v: " ".join("%.9g" % x for x in v)
+    box = 0.06
+    # brick 30 x 30 x 1.6 mm centred in the box, 2 mm above the ground plane
+    bx = by = 0.5 * (box - 0.03)
+    lines = ["OpenPEEC 1 0",
+             f"title = cfg5 seed {seed}: {ndisk} disks, {nquad} quads, dielectric brick over ground",
+             "capacitance = 1", "retardation = 1", "groundplane = 0",
+             f"dielectric = {bx:.9g} {by:.9g} 0.002  0.03 0 0  0 0.03 0  0.0016 4.4 "
+             f"{brick[0]} {brick[1]} {brick[2]}"]
+    # one panel per height level between 6 mm and 58 mm, in a shuffled order
+    kinds = ["disk"] * ndisk + ["quad"] * nquad
+    levels = np.linspace(0.006, 0.058, len(kinds))
+    order = rng.permutation(len(kinds))
+    disks = []
+    for lev, kidx in zip(levels, order):
+        if kinds[kidx] == "disk":
+            c = np.array([rng.uniform(0.012, box - 0.012), rng.uniform(0.012, box - 0.012), lev])
+            disks.append(c)
+            lines.append(f"disk = {f(c)}  0 0 1  0.01 3.5e-5 5.8e7 {disk_grid[0]} {disk_grid[1]}")
+        else:
+            # a convex quadrilateral: an a x b rectangle (sides 20-40 mm) with each corner
+            # moved by less than 15 % of the shorter side, inside the box
+            a, b = rng.uniform(0.02, 0.04, 2)
+            jit = 0.15 * min(a, b) * rng.uniform(-1, 1, (4, 2))
+            x0, y0 = rng.uniform(0, box - a), rng.uniform(0, box - b)
+            v = np.array([[0, 0], [a, 0], [a, b], [0, b]]) + jit
+            v[:, 0] = np.clip(v[:, 0] + x0, 0, box)
+            v[:, 1] = np.clip(v[:, 1] + y0, 0, box)
+            pts = " ".join(f(np.array([p[0], p[1], lev])) for p in v)
+            lines.append(f"quad = {pts}  3.5e-5 5.8e7 {quad_grid} {quad_grid}")
+    lines += [f"node = 1 {f(disks[0])}", f"node = 2 {f(disks[1])}", "port = 1 2 50",
+              "planewave = 30 45 1 1.0",
+              f"frequency = {f0:.10g} {f0 + (nfreq - 1) * df:.10g} {nfreq - 1}", "end", ""]
+    return "\n".join(lines)

@@ -66,6 +66,11 @@ struct pb_ctx {
     // compressed path: level signature whose static parts the held slots contain
     std::vector<long> comp_sig;
     bool comp_static_valid = false;
+    // dense path: level signature of the FP64 static tables in cache slots 4 (Lp) and
+    // 5 (P), and the slot storage they were written to (a reallocated slot is invalid)
+    std::vector<long> dense_sig;
+    bool dense_static_valid = false;
+    const void *dense_static_ptr[2] = {nullptr, nullptr};
     // compressed path: host copy of the dense circuit Schur complement, page-locked once
     // (cudaHostRegister) so that its per-frequency upload runs at full link speed
     std::vector<std::complex<double>> comp_schur;

@@ -207,11 +207,37 @@ __device__ __forceinline__ void accum32(Acc<float, F> &a, const KArg &k, const f
     if (++a.cnt == PB_FLUSH) a.flush();
 }
 
+// A sample whose two points nearly coincide (R < D / 32: overlapping cells, e.g. the
+// crossing current cells of a quad panel): the phase kh R is formed from the direct FP32
+// R per frequency. Rotating the term's bases by kh dl there (dl = R - D ~ -D) leaves an
+// absolute phase error ~kh D 1e-7 against a phase of only kh R, and sin(kh R) / R takes
+// that error relative to R (it was 1e8 times the entry on a quad panel of config 5).
+template <int F>
+__device__ __forceinline__ void accum32_near(Acc<float, F> &a, const KArg &k, float r2, float ra, float qw)
+{
+    if (r2 > 0) {
+        const float q = __fdividef(qw, ra);
+#pragma unroll
+        for (int f = 0; f < F; f++) {
+            float s, c;
+            sincos_f32<1>(k.khf[f] * ra, s, c);
+            const float t = q * s;
+            a.pr[f] = fmaf(t, s, a.pr[f]);
+            a.pi[f] = fmaf(t, c, a.pi[f]);
+        }
+    } else {
+#pragma unroll
+        for (int f = 0; f < F; f++) a.pi[f] = fmaf(qw, k.khf[f], a.pi[f]);
+    }
+    if (++a.cnt == PB_FLUSH) a.flush();
+}
+
 // One sample of the FP32 path from its in-cell offset p (R = |cd + p|, plus the wire
 // kernel's a^2): dl = R - D = p.(p + 2 cd) / (R + D) with R + D from R^2 in FP32
 // (v = cd + p), then R = D + dl with D as FP32 head + tail, so that 1/R carries no
 // rounding shared by all samples of the term. Where D + dl cancels (a sample next to
-// the other cell of an adjacent pair) the direct FP32 R is taken instead.
+// the other cell of an adjacent pair) the direct FP32 R is taken instead, and where the
+// two points nearly coincide the phase too (accum32_near).
 template <int F, int EQ, int RED>
 __device__ __forceinline__ void sample32(Acc<float, F> &a, const KArg &k, const float4 *base,
                                          const float *cd, float a2, float D, float Dlo, float px,
@@ -221,6 +247,10 @@ __device__ __forceinline__ void sample32(Acc<float, F> &a, const KArg &k, const 
     const float r2 = fmaf(vx, vx, fmaf(vy, vy, fmaf(vz, vz, a2)));
     const float e = fmaf(px, fmaf(2.f, cd[0], px), fmaf(py, fmaf(2.f, cd[1], py), pz * fmaf(2.f, cd[2], pz)));
     const float ra = r2 * rsqrtf(r2);
+    if (!(ra >= 0.03125f * D)) {                  // also r2 = 0 (ra is then NaN)
+        accum32_near<F>(a, k, r2, r2 > 0 ? ra : 0.f, qw);
+        return;
+    }
     const float dl = __fdividef(e, ra + D);
     const float rd = D + (dl + Dlo);
     const float r = rd > 0.5f * ra ? rd : ra;

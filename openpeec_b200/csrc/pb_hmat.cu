@@ -1091,7 +1091,7 @@ int pc_samples(pb_ctx *c, KBlock &kb, const std::vector<zc> &zint, double om, co
 
 int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts &o, double ctol,
                         double gtol, double *zmat, pb_sweep_stats *stats, pb_hstats *hs, float *sample_x,
-                        float *sample_t)
+                        float *sample_t, const pb_planewave_t *pw, double *voc, double *segipw)
 {
     int mlp_fallbacks = 0, coarse_fallbacks = 0, coarse_n = 0;
     double t_coarse = 0;
@@ -1780,12 +1780,18 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
         };
         // ---- every port excitation: matrix-free GMRES (gmres_hmat, iterative.c:285-354)
         tick();
+        // j >= 0: 1 A into port j (mna_rhs_port, mna.c:367-376); j < 0: the plane wave
         auto solve_rhs = [&](int j, int &total, bool &done, int max_cycles) -> int {
-            std::vector<zc> bh(N, zc(0, 0));
-            const int i1 = c->nodemap[c->port[j].n1], i2 = c->nodemap[c->port[j].n2];
-            if (i1 >= 0) bh[i1] += 1.0;
-            if (i2 >= 0) bh[i2] -= 1.0;
-            PB_CUDA(cudaMemcpyAsync(bB.p, bh.data(), sizeof(double2) * N, cudaMemcpyHostToDevice, st));
+            if (j >= 0) {
+                std::vector<zc> bh(N, zc(0, 0));
+                const int i1 = c->nodemap[c->port[j].n1], i2 = c->nodemap[c->port[j].n2];
+                if (i1 >= 0) bh[i1] += 1.0;
+                if (i2 >= 0) bh[i2] -= 1.0;
+                PB_CUDA(cudaMemcpyAsync(bB.p, bh.data(), sizeof(double2) * N, cudaMemcpyHostToDevice, st));
+            } else {
+                PB_TRY(pb_pw_rhs_full(c, pw, bFreq.as<double>(), N, offS, bB.as<double2>(), st));
+                c->launches++;
+            }
             PB_CUDA(cudaMemsetAsync(bX.p, 0, sizeof(double2) * N, st));
             zc bb;
             PB_TRY(dot(bB.as<double2>(), bB.as<double2>(), bb));
@@ -1860,7 +1866,7 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
             }
             return PB_OK;
         };
-        for (int j = 0; j < np; j++) {
+        for (int j = pw ? -1 : 0; j < (pw ? 0 : np); j++) {
             int total = 0;
             bool done = false;
             // with the learned correction the true residual judges after one cycle: not
@@ -1887,6 +1893,20 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
             std::vector<zc> xh(N);
             PB_CUDA(cudaMemcpyAsync(xh.data(), bX.p, sizeof(double2) * N, cudaMemcpyDeviceToHost, st));
             PB_CUDA(cudaStreamSynchronize(st));
+            if (j < 0) {
+                // open-circuit port voltages and branch currents of the wave (solve.c:372-389)
+                for (int i = 0; i < np && voc; i++) {
+                    const int k1 = c->nodemap[c->port[i].n1], k2 = c->nodemap[c->port[i].n2];
+                    const zc v = (k1 < 0 ? zc(0, 0) : xh[k1]) - (k2 < 0 ? zc(0, 0) : xh[k2]);
+                    voc[2 * ((size_t)i * nfreq + ifr)] = v.real();
+                    voc[2 * ((size_t)i * nfreq + ifr) + 1] = v.imag();
+                }
+                for (int k = 0; k < ns && segipw; k++) {
+                    segipw[2 * ((size_t)ifr * ns + k)] = xh[offS + k].real();
+                    segipw[2 * ((size_t)ifr * ns + k) + 1] = xh[offS + k].imag();
+                }
+                continue;
+            }
             for (int i = 0; i < np; i++) {
                 const int k1 = c->nodemap[c->port[i].n1], k2 = c->nodemap[c->port[i].n2];
                 const zc v = (k1 < 0 ? zc(0, 0) : xh[k1]) - (k2 < 0 ? zc(0, 0) : xh[k2]);

@@ -48,6 +48,15 @@ struct pb_hstats {
 // right-preconditioned GMRES(60) to the relative residual tol.
 // With sample_x / sample_t (nfreq = 1) no system is solved: the features of every current
 // cell and the targets of the learned preconditioner correction are written instead.
+// pw != nullptr: one plane-wave excitation per frequency instead of the port excitations
+// (mna_rhs_planewave, src/mna.c:434-468): voc [nport][nfreq] open-circuit port voltages,
+// segipw [nfreq][nseg] branch currents (either may be nullptr), zmat unused.
 int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts &o,
                         double ctol, double gtol, double *zmat, pb_sweep_stats *stats, pb_hstats *hs,
-                        float *sample_x = nullptr, float *sample_t = nullptr);
+                        float *sample_x = nullptr, float *sample_t = nullptr,
+                        const pb_planewave_t *pw = nullptr, double *voc = nullptr, double *segipw = nullptr);
+
+// Plane-wave right-hand side of the full MNA form at one frequency (freq_dev: one double in
+// device memory): -EMF on the branch rows offS + k, zero elsewhere (n rows).
+int pb_pw_rhs_full(const pb_ctx *c, const pb_planewave_t *pw, const double *freq_dev, int n, int offS,
+                   double2 *rhs, cudaStream_t st);

@@ -64,7 +64,9 @@ template <typename T2> __device__ __forceinline__ T2 safe_inv(T2 z)
 // ---------------------------------------------------------------- leaf panel
 // Factor columns [k0, k0+w) (w <= 32) over rows [k0, n) of matrix blockIdx.x, SW
 // columns at a time in shared memory. Swaps are applied to the leaf's own columns only.
-template <typename T, int SW>
+// G = true (orders whose panel column does not fit in shared memory, FP64 above ~14 000
+// unknowns): the SW columns are worked on in place in global memory instead.
+template <typename T, int SW, bool G>
 __global__ void __launch_bounds__(1024)
 k_lu_leaf(T2_t<T> *a, int n, int ld, long long stride, int k0, int w, int *piv, int *info)
 {
@@ -73,25 +75,30 @@ k_lu_leaf(T2_t<T> *a, int n, int ld, long long stride, int k0, int w, int *piv, 
     __shared__ double red_m[33];
     __shared__ int red_i[33];
     const int m = n - k0;
-    T2 *sp = reinterpret_cast<T2 *>(smraw);       // [m][SW]
-    T2 *urow = sp + (size_t)m * SW;                // [SW][32]
+    T2 *spm = reinterpret_cast<T2 *>(smraw);      // [m][SW] (G = false)
+    T2 *urow = G ? spm : spm + (size_t)m * SW;     // [SW][32]
     const int b = blockIdx.x, tid = threadIdx.x, nt = blockDim.x;
     a += (long long)b * stride;
     piv += (long long)b * n;
 
     for (int s0 = 0; s0 < w; s0 += SW) {
         const int sw = min(SW, w - s0), c0 = k0 + s0;
-        for (int e = tid; e < m * sw; e += nt) {
-            const int r = e / sw, t = e - r * sw;
-            sp[r * SW + t] = a[(long long)(k0 + r) * ld + c0 + t];
-        }
+        // element (r, t) of the sub-panel: row k0 + r, column c0 + t
+        auto P = [&](int r, int t) -> T2 & {
+            return G ? a[(long long)(k0 + r) * ld + c0 + t] : spm[r * SW + t];
+        };
+        if (!G)
+            for (int e = tid; e < m * sw; e += nt) {
+                const int r = e / sw, t = e - r * sw;
+                spm[r * SW + t] = a[(long long)(k0 + r) * ld + c0 + t];
+            }
         __syncthreads();
         for (int t = 0; t < sw; t++) {
             const int c = c0 + t;
             double bm = -1.0;
             int bi = INT_MAX;
             for (int r = c + tid; r < n; r += nt) {
-                const double mm = cmag1(sp[(r - k0) * SW + t]);
+                const double mm = cmag1(P(r - k0, t));
                 if (mm > bm) { bm = mm; bi = r; }
             }
             block_argmax(bm, bi, red_m, red_i);
@@ -104,7 +111,7 @@ k_lu_leaf(T2_t<T> *a, int n, int ld, long long stride, int k0, int w, int *piv, 
                 for (int e = tid; e < w; e += nt) {
                     const int col = k0 + e;
                     if (col >= c0 && col < c0 + sw) {
-                        T2 *x = &sp[(c - k0) * SW + (col - c0)], *y = &sp[(ip - k0) * SW + (col - c0)];
+                        T2 *x = &P(c - k0, col - c0), *y = &P(ip - k0, col - c0);
                         const T2 tmp = *x; *x = *y; *y = tmp;
                     } else {
                         T2 *x = &a[(long long)c * ld + col], *y = &a[(long long)ip * ld + col];
@@ -113,19 +120,19 @@ k_lu_leaf(T2_t<T> *a, int n, int ld, long long stride, int k0, int w, int *piv, 
                 }
             }
             __syncthreads();
-            const T2 pinv = safe_inv(sp[(c - k0) * SW + t]);
+            const T2 pinv = safe_inv(P(c - k0, t));
             for (int r = c + 1 + tid; r < n; r += nt) {
-                T2 *row = &sp[(r - k0) * SW];
-                const T2 l = cmul(row[t], pinv);
-                row[t] = l;
-                for (int tt = t + 1; tt < sw; tt++) row[tt] = cfms(row[tt], l, sp[(c - k0) * SW + tt]);
+                const T2 l = cmul(P(r - k0, t), pinv);
+                P(r - k0, t) = l;
+                for (int tt = t + 1; tt < sw; tt++) P(r - k0, tt) = cfms(P(r - k0, tt), l, P(c - k0, tt));
             }
             __syncthreads();
         }
-        for (int e = tid; e < m * sw; e += nt) {
-            const int r = e / sw, t = e - r * sw;
-            a[(long long)(k0 + r) * ld + c0 + t] = sp[r * SW + t];
-        }
+        if (!G)
+            for (int e = tid; e < m * sw; e += nt) {
+                const int r = e / sw, t = e - r * sw;
+                a[(long long)(k0 + r) * ld + c0 + t] = spm[r * SW + t];
+            }
         const int c1 = c0 + sw, nr = k0 + w - c1;
         if (nr > 0) {
             // U rows of this sub-panel for the remaining leaf columns
@@ -133,7 +140,7 @@ k_lu_leaf(T2_t<T> *a, int n, int ld, long long stride, int k0, int w, int *piv, 
                 for (int t = 0; t < sw; t++) {
                     T2 v = a[(long long)(c0 + t) * ld + col];
                     for (int tp = 0; tp < t; tp++)
-                        v = cfms(v, sp[(c0 + t - k0) * SW + tp], urow[tp * 32 + (col - c1)]);
+                        v = cfms(v, P(c0 + t - k0, tp), urow[tp * 32 + (col - c1)]);
                     urow[t * 32 + (col - c1)] = v;
                     a[(long long)(c0 + t) * ld + col] = v;
                 }
@@ -145,7 +152,7 @@ k_lu_leaf(T2_t<T> *a, int n, int ld, long long stride, int k0, int w, int *piv, 
                 T2 v = a[(long long)r * ld + col];
 #pragma unroll
                 for (int t = 0; t < SW; t++)
-                    if (t < sw) v = cfms(v, sp[(r - k0) * SW + t], urow[t * 32 + (col - c1)]);
+                    if (t < sw) v = cfms(v, P(r - k0, t), urow[t * 32 + (col - c1)]);
                 a[(long long)r * ld + col] = v;
             }
         }
@@ -441,17 +448,17 @@ template <typename T> static int leaf_sw(int m, size_t *smem)
     return 0;
 }
 
-template <typename T, int SW>
+template <typename T, int SW, bool G = false>
 static int launch_leaf(pb_lu_engine *e, T2_t<T> *a, int n, int ld, long long stride, int nb,
                        int k0, int w, int *piv, int *info, size_t smem)
 {
     static std::atomic<unsigned long long> attr_set{0};   // per device, before any launch relies on it
-    PB_TRY(pb_smem_optin(k_lu_leaf<T, SW>, pb_smem_cap() - 1024, attr_set));
+    PB_TRY(pb_smem_optin(k_lu_leaf<T, SW, G>, pb_smem_cap() - 1024, attr_set));
     // the panel has m = n - k0 rows: a CTA no wider than the panel (at least 128 threads)
     // lets several small systems share an SM (batches of small structures); the pivot
     // search and the updates do not depend on the thread count, so results are unchanged
     const int m = n - k0, nt = std::min(1024, std::max(128, (m + 31) / 32 * 32));
-    k_lu_leaf<T, SW><<<nb, nt, smem, e->stream>>>(a, n, ld, stride, k0, w, piv, info);
+    k_lu_leaf<T, SW, G><<<nb, nt, smem, e->stream>>>(a, n, ld, stride, k0, w, piv, info);
     e->launches++;
     PB_CHECK_LAUNCH();
     return PB_OK;
@@ -497,6 +504,16 @@ static int lu_rec(pb_lu_engine *e, T2_t<T> *a, int n, int ld, long long stride, 
                   int k0, int w, int *piv, int *info, int sw, size_t smem)
 {
     if (w <= 32) {
+        if (sw == 0) {
+            // orders whose panel column does not fit in shared memory: while it does not,
+            // the panel is worked on in global memory, then one column at a time in shared
+            size_t sm1 = 0;
+            if (leaf_sw<T>(n - k0, &sm1) == 0)
+                return launch_leaf<T, 1, true>(e, a, n, ld, stride, nb, k0, w, piv, info,
+                                               32 * sizeof(T2_t<T>));
+            return launch_leaf<T, 1>(e, a, n, ld, stride, nb, k0, w, piv, info,
+                                     ((size_t)(n - k0) + 32) * sizeof(T2_t<T>));
+        }
         if (sw == 4) return launch_leaf<T, 4>(e, a, n, ld, stride, nb, k0, w, piv, info, smem);
         if (sw == 2) return launch_leaf<T, 2>(e, a, n, ld, stride, nb, k0, w, piv, info, smem);
         return launch_leaf<T, 1>(e, a, n, ld, stride, nb, k0, w, piv, info, smem);
@@ -526,11 +543,7 @@ int pb_lu_factor(pb_lu_engine *e, int n, int nb, T2_t<T> *a, int ld, long stride
     k_fill_int<<<ceil_div(nb, 256), 256, 0, e->stream>>>(info, -1, nb);
     e->launches++;
     size_t smem = 0;
-    const int sw = leaf_sw<T>(n, &smem);
-    if (sw == 0) {
-        pb_set_error("LU order %d exceeds the shared-memory panel capacity of this build", n);
-        return PB_ERR_UNSUP;
-    }
+    const int sw = leaf_sw<T>(n, &smem);           // 0: the first panels go through global memory
     PB_TRY(lu_rec<T>(e, a, n, ld, stride, nb, 0, n, piv, info, sw, smem));
     return check_tc(e);
 }
@@ -561,14 +574,92 @@ int pb_lu_perm(pb_lu_engine *e, int n, int nb, const int *piv, int *perm)
 
 // ---------------------------------------------------------------- triangular solves
 // One CTA (1024 threads) per (rhs, matrix). The whole vector lives in shared memory.
-template <typename TF>
+// Sum over c in [c0, c1) of row[c] * xs[c] (complex) by one warp; the result is valid in
+// lane 0. Four independent accumulators keep several loads in flight; FP32 rows are read
+// 16 bytes (two entries) at a time when row and c0 allow it. xs is in shared memory.
+__device__ __forceinline__ float2 warp_cdot(const float2 *row, const float2 *xs, int c0, int c1, int lane)
+{
+    float ax = 0.f, ay = 0.f, bx = 0.f, by = 0.f, cx = 0.f, cy = 0.f, dx = 0.f, dy = 0.f;
+    if (((c0 & 1) == 0) && ((reinterpret_cast<uintptr_t>(row) & 15) == 0)) {
+        const float4 *r4 = reinterpret_cast<const float4 *>(row);
+        const float4 *x4 = reinterpret_cast<const float4 *>(xs);
+        const int pe = c1 >> 1;                          // pairs entirely inside [c0, c1)
+        int p = (c0 >> 1) + lane;
+        for (; p + 32 < pe; p += 64) {
+            const float4 u = r4[p], v = x4[p], u2 = r4[p + 32], v2 = x4[p + 32];
+            ax = fmaf(u.x, v.x, fmaf(-u.y, v.y, ax));
+            ay = fmaf(u.x, v.y, fmaf(u.y, v.x, ay));
+            bx = fmaf(u.z, v.z, fmaf(-u.w, v.w, bx));
+            by = fmaf(u.z, v.w, fmaf(u.w, v.z, by));
+            cx = fmaf(u2.x, v2.x, fmaf(-u2.y, v2.y, cx));
+            cy = fmaf(u2.x, v2.y, fmaf(u2.y, v2.x, cy));
+            dx = fmaf(u2.z, v2.z, fmaf(-u2.w, v2.w, dx));
+            dy = fmaf(u2.z, v2.w, fmaf(u2.w, v2.z, dy));
+        }
+        if (p < pe) {
+            const float4 u = r4[p], v = x4[p];
+            ax = fmaf(u.x, v.x, fmaf(-u.y, v.y, ax));
+            ay = fmaf(u.x, v.y, fmaf(u.y, v.x, ay));
+            bx = fmaf(u.z, v.z, fmaf(-u.w, v.w, bx));
+            by = fmaf(u.z, v.w, fmaf(u.w, v.z, by));
+        }
+        const int c = 2 * pe;                            // odd c1: the last entry (if inside)
+        if (c >= c0 && c < c1 && lane == 0) {
+            cx = fmaf(row[c].x, xs[c].x, fmaf(-row[c].y, xs[c].y, cx));
+            cy = fmaf(row[c].x, xs[c].y, fmaf(row[c].y, xs[c].x, cy));
+        }
+    } else {
+        int c = c0 + lane;
+        for (; c + 32 < c1; c += 64) {
+            const float2 u = row[c], v = xs[c], u2 = row[c + 32], v2 = xs[c + 32];
+            ax = fmaf(u.x, v.x, fmaf(-u.y, v.y, ax));
+            ay = fmaf(u.x, v.y, fmaf(u.y, v.x, ay));
+            bx = fmaf(u2.x, v2.x, fmaf(-u2.y, v2.y, bx));
+            by = fmaf(u2.x, v2.y, fmaf(u2.y, v2.x, by));
+        }
+        if (c < c1) {
+            ax = fmaf(row[c].x, xs[c].x, fmaf(-row[c].y, xs[c].y, ax));
+            ay = fmaf(row[c].x, xs[c].y, fmaf(row[c].y, xs[c].x, ay));
+        }
+    }
+    float sx = (ax + bx) + (cx + dx), sy = (ay + by) + (cy + dy);
+    for (int o = 16; o > 0; o >>= 1) {
+        sx += __shfl_down_sync(0xffffffffu, sx, o);
+        sy += __shfl_down_sync(0xffffffffu, sy, o);
+    }
+    return make_float2(sx, sy);
+}
+
+__device__ __forceinline__ double2 warp_cdot(const double2 *row, const double2 *xs, int c0, int c1, int lane)
+{
+    double ax = 0, ay = 0, bx = 0, by = 0;
+    int c = c0 + lane;
+    for (; c + 32 < c1; c += 64) {
+        const double2 u = row[c], v = xs[c], u2 = row[c + 32], v2 = xs[c + 32];
+        ax = fma(u.x, v.x, fma(-u.y, v.y, ax));
+        ay = fma(u.x, v.y, fma(u.y, v.x, ay));
+        bx = fma(u2.x, v2.x, fma(-u2.y, v2.y, bx));
+        by = fma(u2.x, v2.y, fma(u2.y, v2.x, by));
+    }
+    if (c < c1) {
+        ax = fma(row[c].x, xs[c].x, fma(-row[c].y, xs[c].y, ax));
+        ay = fma(row[c].x, xs[c].y, fma(row[c].y, xs[c].x, ay));
+    }
+    double sx = ax + bx, sy = ay + by;
+    for (int o = 16; o > 0; o >>= 1) {
+        sx += __shfl_down_sync(0xffffffffu, sx, o);
+        sy += __shfl_down_sync(0xffffffffu, sy, o);
+    }
+    return make_double2(sx, sy);
+}
+
+template <typename TF, bool G>
 __global__ void __launch_bounds__(1024)
 k_lu_solve(const T2_t<TF> *lu, int n, int ld, long long stride, const int *perm,
            const double2 *r, double2 *x, int nrhs, const int *sys, const int *lu_of)
 {
     typedef T2_t<TF> T2;
     extern __shared__ __align__(16) unsigned char smraw[];
-    T2 *xs = reinterpret_cast<T2 *>(smraw);        // [n]
     __shared__ T2 diag[32][33];
     __shared__ T2 tmp[32];
     __shared__ double red[33];
@@ -580,6 +671,9 @@ k_lu_solve(const T2_t<TF> *lu, int n, int ld, long long stride, const int *perm,
     perm += (long long)fm * n;
     const double2 *rv = r + ((long long)b * nrhs + rhs) * n;
     double2 *xv = x + ((long long)b * nrhs + rhs) * n;
+    // the working vector: shared memory, or (G: FP64 orders above ~13 000, whose vector
+    // does not fit) the output vector itself
+    T2 *xs = G ? reinterpret_cast<T2 *>(xv) : reinterpret_cast<T2 *>(smraw);
 
     // scale by max |component|
     double mx = 0;
@@ -594,9 +688,26 @@ k_lu_solve(const T2_t<TF> *lu, int n, int ld, long long stride, const int *perm,
     }
     __syncthreads();
     const double scale = red[32] > 0 ? red[32] : 1.0;
-    for (int i = tid; i < n; i += blockDim.x) {
-        const double2 v = rv[perm[i]];
-        xs[i] = mk2<T2>(v.x / scale, v.y / scale);
+    if (G) {
+        // r and x may alias: read every permuted entry before the first write
+        constexpr int KMAX = 32;                  // n <= 32 * 1024 (checked by the launcher)
+        double2 v[KMAX];
+#pragma unroll
+        for (int k = 0; k < KMAX; k++) {
+            const int i = tid + k * (int)blockDim.x;
+            if (i < n) v[k] = rv[perm[i]];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < KMAX; k++) {
+            const int i = tid + k * (int)blockDim.x;
+            if (i < n) xs[i] = mk2<T2>(v[k].x / scale, v[k].y / scale);
+        }
+    } else {
+        for (int i = tid; i < n; i += blockDim.x) {
+            const double2 v = rv[perm[i]];
+            xs[i] = mk2<T2>(v.x / scale, v.y / scale);
+        }
     }
     __syncthreads();
 
@@ -605,12 +716,7 @@ k_lu_solve(const T2_t<TF> *lu, int n, int ld, long long stride, const int *perm,
         const int r = r0 + warp;
         if (r < n) {
             const T2 *row = lu + (long long)r * ld;
-            T2 acc = mk2<T2>(0, 0);
-            for (int c = lane; c < r0; c += 32) acc = cadd(acc, cmul(row[c], xs[c]));
-            for (int o = 16; o > 0; o >>= 1) {
-                acc.x += __shfl_down_sync(0xffffffffu, acc.x, o);
-                acc.y += __shfl_down_sync(0xffffffffu, acc.y, o);
-            }
+            const T2 acc = warp_cdot(row, xs, 0, r0, lane);
             if (lane == 0) tmp[warp] = csub(xs[r], acc);
             diag[warp][lane] = (r0 + lane < n) ? row[r0 + lane] : mk2<T2>(0, 0);
         }
@@ -638,12 +744,7 @@ k_lu_solve(const T2_t<TF> *lu, int n, int ld, long long stride, const int *perm,
         const int r = r0 + warp;
         if (warp < nbk) {
             const T2 *row = lu + (long long)r * ld;
-            T2 acc = mk2<T2>(0, 0);
-            for (int c = r0 + 32 + lane; c < n; c += 32) acc = cadd(acc, cmul(row[c], xs[c]));
-            for (int o = 16; o > 0; o >>= 1) {
-                acc.x += __shfl_down_sync(0xffffffffu, acc.x, o);
-                acc.y += __shfl_down_sync(0xffffffffu, acc.y, o);
-            }
+            const T2 acc = warp_cdot(row, xs, r0 + 32, n, lane);
             if (lane == 0) tmp[warp] = csub(xs[r], acc);
             diag[warp][lane] = (lane < nbk) ? row[r0 + lane] : mk2<T2>(0, 0);
         }
@@ -682,9 +783,18 @@ int pb_lu_solve_mapped(pb_lu_engine *e, int n, int nb, int nrhs, const T2_t<TF> 
     if (nb <= 0) return PB_OK;
     const size_t smem = (size_t)n * sizeof(T2_t<TF>);
     static std::atomic<unsigned long long> attr_set{0};   // per device
-    PB_TRY(pb_smem_optin(k_lu_solve<TF>, pb_smem_cap() - 20480, attr_set));
     dim3 g(nrhs, nb);
-    k_lu_solve<TF><<<g, 1024, smem, e->stream>>>(lu, n, ld, stride, perm, r, x, nrhs, sys, lu_of);
+    if (smem > (size_t)pb_smem_cap() - 20480) {
+        // the vector does not fit in shared memory: solve in place in x (FP64 only)
+        if (sizeof(T2_t<TF>) != sizeof(double2) || n > 32 * 1024) {
+            pb_set_error("triangular solve of order %d does not fit this build", n);
+            return PB_ERR_UNSUP;
+        }
+        k_lu_solve<TF, true><<<g, 1024, 0, e->stream>>>(lu, n, ld, stride, perm, r, x, nrhs, sys, lu_of);
+    } else {
+        PB_TRY(pb_smem_optin(k_lu_solve<TF, false>, pb_smem_cap() - 20480, attr_set));
+        k_lu_solve<TF, false><<<g, 1024, smem, e->stream>>>(lu, n, ld, stride, perm, r, x, nrhs, sys, lu_of);
+    }
     e->launches++;
     PB_CHECK_LAUNCH();
     return PB_OK;
@@ -762,13 +872,18 @@ __device__ __forceinline__ void atomic_max_pos(double *addr, double v)
 __global__ void __launch_bounds__(256)
 k_residual(const double2 *a, int n, int ld, long long stride, const double2 *bv,
            const double2 *xv, double2 *rv, double *rn, double *bn, double *xn, double *an,
-           int nrhs, int rows_per_block, const int *sys, double *cw)
+           int nrhs, int rows_per_block, const int *sys, double *cw, int stage)
 {
+    // stage = 1: x is staged in shared memory [nrhs][n]; 0 (orders whose x does not fit,
+    // above ~14 000 unknowns): x is read from global memory (L2 holds it)
     extern __shared__ __align__(16) unsigned char smraw[];
-    double2 *xs = reinterpret_cast<double2 *>(smraw);     // [nrhs][n]
     const int b = sys ? sys[blockIdx.y] : blockIdx.y, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const double2 *xs = stage ? reinterpret_cast<const double2 *>(smraw) : xv + (long long)b * nrhs * n;
     a += (long long)b * stride;
-    for (int e = tid; e < nrhs * n; e += blockDim.x) xs[e] = xv[(long long)b * nrhs * n + e];
+    if (stage) {
+        double2 *xw = reinterpret_cast<double2 *>(smraw);
+        for (int e = tid; e < nrhs * n; e += blockDim.x) xw[e] = xv[(long long)b * nrhs * n + e];
+    }
     __syncthreads();
     if (blockIdx.x == 0 && xn) {
         for (int q = warp; q < nrhs; q += 8) {
@@ -833,11 +948,13 @@ int pb_residual(pb_lu_engine *e, int n, int nb, int nrhs, const double2 *a, int 
     if (cw) PB_CUDA(cudaMemsetAsync(cw, 0, sizeof(double) * nb * nrhs, e->stream));
     PB_CUDA(cudaMemsetAsync(bn, 0, sizeof(double) * nb * nrhs, e->stream));
     if (an) PB_CUDA(cudaMemsetAsync(an, 0, sizeof(double) * nb, e->stream));
-    const size_t smem = (size_t)nrhs * n * sizeof(double2);
+    const size_t xbytes = (size_t)nrhs * n * sizeof(double2);
+    const int stage = xbytes <= (size_t)pb_smem_cap();
+    const size_t smem = stage ? xbytes : 0;
     PB_TRY(pb_smem_optin(k_residual, pb_smem_cap(), g_residual_attr));
     const int rpb = 64;
     dim3 g(ceil_div(n, rpb), nb);
-    k_residual<<<g, 256, smem, e->stream>>>(a, n, ld, stride, b, x, r, rn, bn, xn, an, nrhs, rpb, nullptr, cw);
+    k_residual<<<g, 256, smem, e->stream>>>(a, n, ld, stride, b, x, r, rn, bn, xn, an, nrhs, rpb, nullptr, cw, stage);
     e->launches++;
     PB_CHECK_LAUNCH();
     return PB_OK;
@@ -852,11 +969,13 @@ int pb_residual_mapped(pb_lu_engine *e, int n, int nb, int nrhs, const double2 *
     PB_CUDA(cudaMemsetAsync(bn, 0, sizeof(double) * nall * nrhs, e->stream));
     if (an) PB_CUDA(cudaMemsetAsync(an, 0, sizeof(double) * nall, e->stream));
     if (nb <= 0) return PB_OK;
-    const size_t smem = (size_t)nrhs * n * sizeof(double2);
+    const size_t xbytes = (size_t)nrhs * n * sizeof(double2);
+    const int stage = xbytes <= (size_t)pb_smem_cap();
+    const size_t smem = stage ? xbytes : 0;
     PB_TRY(pb_smem_optin(k_residual, pb_smem_cap(), g_residual_attr));
     const int rpb = 64;
     dim3 g(ceil_div(n, rpb), nb);
-    k_residual<<<g, 256, smem, e->stream>>>(a, n, ld, stride, b, x, r, rn, bn, xn, an, nrhs, rpb, sys, cw);
+    k_residual<<<g, 256, smem, e->stream>>>(a, n, ld, stride, b, x, r, rn, bn, xn, an, nrhs, rpb, sys, cw, stage);
     e->launches++;
     PB_CHECK_LAUNCH();
     return PB_OK;
@@ -866,12 +985,14 @@ int pb_matvec_mapped(pb_lu_engine *e, int n, int nb, int nrhs, const double2 *a,
                      const double2 *x, double2 *y, const int *sys)
 {
     if (nb <= 0) return PB_OK;
-    const size_t smem = (size_t)nrhs * n * sizeof(double2);
+    const size_t xbytes = (size_t)nrhs * n * sizeof(double2);
+    const int stage = xbytes <= (size_t)pb_smem_cap();
+    const size_t smem = stage ? xbytes : 0;
     PB_TRY(pb_smem_optin(k_residual, pb_smem_cap(), g_residual_attr));
     const int rpb = 64;
     dim3 g(ceil_div(n, rpb), nb);
     k_residual<<<g, 256, smem, e->stream>>>(a, n, ld, stride, nullptr, x, y, nullptr, nullptr, nullptr,
-                                            nullptr, nrhs, rpb, sys, nullptr);
+                                            nullptr, nrhs, rpb, sys, nullptr, stage);
     e->launches++;
     PB_CHECK_LAUNCH();
     return PB_OK;

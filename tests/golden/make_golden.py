@@ -225,6 +225,45 @@ def make_comp_case(name, peec_text, freqs, threads=16):
     print(name, "nseg", len(prob.seg), "z", zs["z"].ravel()[:1], "dense", zs["z_dense"].ravel()[:1], "->", out)
 
 
+def make_cfg4_full(freq=1e8, threads=8):
+    """Config 4 at full size (the 96 x 96 x 4 volume-bar stack, 74 496 cells) through the
+    reference's own CLI on its compressed path (compression = 1 1e-6) at one frequency:
+    its Zin (zin.csv, 10 significant digits) and the H-matrix / GMRES statistics of
+    peec.log. About five minutes on 8 cores. The geometry is not stored: the tests
+    rebuild it from the stored .peec text (plates are within the package's builder)."""
+    import re
+    import shutil
+    text = re.sub(r"frequency\s*=.*", "frequency = %.10g %.10g 0" % (freq, freq), configs.cfg4())
+    work = tempfile.mkdtemp(prefix="cfg4_")
+    open(os.path.join(work, "cfg4.peec"), "w").write(text)
+    subprocess.run([os.path.join(ROOT, "oracle", "_ref", "peec"), "-n", str(threads), "cfg4.peec"],
+                   cwd=work, check=True, stdout=subprocess.DEVNULL)
+    log = open(os.path.join(work, "peec.log")).read()
+    row = open(os.path.join(work, "zin.csv")).read().splitlines()[1].split(",")
+    z = complex(float(row[2]), float(row[3]))
+    m = re.search(r"compression Lp : (\d+) cells, (\d+) far blocks \+ (\d+) near blocks", log)
+    g = re.search(r"GMRES solves \(avg ([0-9.]+) iterations\)", log)
+    t = re.search(r"solve ([0-9.]+) s", log)
+    out = os.path.join(HERE, "comp", "cfg4_full.npz")
+    np.savez_compressed(out, freqs=np.array([float(row[1])]), z=np.array([[[z]]]),
+                        ncell=np.array(int(m.group(1))), far=np.array(int(m.group(2))),
+                        near=np.array(int(m.group(3))), gmres_its=np.array(float(g.group(1))),
+                        ref_solve_s=np.array(float(t.group(1))), threads=np.array(threads),
+                        peec=np.array(text))
+    shutil.rmtree(work, ignore_errors=True)
+    print("cfg4_full", z, m.groups(), g.group(1), "->", out)
+
+
+def cfg5_cases():
+    """Scaled-down config 5 (two disks, one quad and a 6 x 6 x 2 dielectric brick over the
+    ground plane): the reference's port Z and sampled entries (make_case), and its
+    plane-wave open-circuit voltage (make_pw_case), at three frequencies of the sweep."""
+    text = configs.cfg5(0, ndisk=2, nquad=1, disk_grid=(4, 16), quad_grid=8, brick=(6, 6, 2), nfreq=3,
+                        f0=1e7, df=1.275e9)
+    make_case("cfg5_small", text, [1e7, 1.285e9, 2.56e9])
+    make_pw_case("cfg5_small_pw", text, [1e7, 1.285e9, 2.56e9])
+
+
 def comp_cases():
     make_comp_case("compress_wire", sample("compress_wire.peec"), [1e6])
     make_comp_case("compress_plate", sample("compress_plate.peec"), [1e8])
@@ -268,9 +307,17 @@ def main():
     ap.add_argument("--comp-only", action="store_true", help="only the compressed-path cases")
     ap.add_argument("--src-only", action="store_true", help="only the independent-source cases")
     ap.add_argument("--post-only", action="store_true", help="only the far-field / transient cases")
+    ap.add_argument("--cfg4-only", action="store_true", help="only config 4 at full size (minutes)")
+    ap.add_argument("--cfg5-only", action="store_true", help="only the scaled-down config-5 cases")
     a = ap.parse_args()
     subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True,
                    stdout=subprocess.DEVNULL)
+    if a.cfg4_only:
+        make_cfg4_full()
+        return
+    if a.cfg5_only:
+        cfg5_cases()
+        return
     if a.src_only:
         src_cases()
         return

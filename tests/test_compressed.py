@@ -133,3 +133,23 @@ def test_two_level_large_circuit():
         z1, s1 = ctx.sweep([1e9], compress=1, pc_coarse=1)
     assert np.abs(z1 - z0).max() <= 1e-8 * np.abs(z0).max()
     assert s1["gmres_its_max"] < s0["gmres_its_max"], (s0["gmres_its_max"], s1["gmres_its_max"])
+
+
+def test_config4_full_size_matches_reference():
+    """Config 4 at full size (96 x 96 x 4 bar stack, 74 496 current cells) at 100 MHz on the
+    compressed path against the reference's own compressed solve of the same input
+    (golden comp/cfg4_full.npz: Zin to 10 digits, its block counts and GMRES iterations;
+    make_golden.py --cfg4-only). Same cluster tree and admissibility, so the same block
+    partition; Z within 1e-5 as for the smaller compressed cases."""
+    import os
+    from openpeec_b200 import abi, api, geometry
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "comp", "cfg4_full.npz"))
+    prob = geometry.build(geometry.parse_peec(str(g["peec"])))
+    assert len(prob.seg) == int(g["ncell"])
+    with api.Context(prob) as ctx:
+        z, st = ctx.sweep(g["freqs"], fill_prec=abi.PREC_MIXED, compress=1, ctol=1e-6)
+    e = float(np.max(np.abs(z - g["z"]) / np.abs(g["z"])))
+    print("cfg4 full: Z", z.ravel(), "reference", g["z"].ravel(), "rel", e, "GMRES", st["gmres_its_max"],
+          "reference GMRES", float(g["gmres_its"]), "blocks", st["hmat_far"], st["hmat_near"])
+    assert (st["hmat_far"], st["hmat_near"]) == (int(g["far"]), int(g["near"]))
+    assert e <= 1e-5, e

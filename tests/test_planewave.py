@@ -16,7 +16,7 @@ import pytest
 from conftest import load_golden
 from oracle.pyoracle import Oracle
 
-PW = ["dipole_pw", "bent_pw", "loop_pw", "loop_pw_load", "mono_pw"]
+PW = ["dipole_pw", "bent_pw", "loop_pw", "loop_pw_load", "mono_pw", "cfg5_small_pw"]
 C0 = 2.99792458e8
 
 
