@@ -574,6 +574,40 @@ def run_batch3(args):
     }
 
 
+def run_gemm(args):
+    """The LU's trailing update alone (C -= A B, complex FP32, batched): the library's
+    tcgen05 kernel against cuBLAS's BF16x9 emulation of the same update, on square
+    shapes of the top recursion levels of the benchmark's 4196-cell factorisation.
+    Complex-equivalent TFLOP/s = 8 m n k per matrix / CUDA-event time (mean of 10)."""
+    L = abi.lib()                      # before torch: this process's cuBLAS is the library's
+    import torch
+    out = []
+    for (m, nc, k, nb) in [(2048, 2048, 2048, 8), (4096, 2048, 2048, 4), (1024, 1024, 1024, 32)]:
+        row = {"m": m, "nc": nc, "k": k, "nb": nb}
+        ld = m + k
+        a = torch.randn(nb, ld, 2 * ld, device="cuda")
+        base, cs = a.data_ptr(), 8
+        pa, pb, pc = base + (k * ld) * cs, base + k * cs, base + (k * ld + k) * cs
+        for tag, kind in (("tcgen05_own", abi.LU_TC), ("cublas_bf16x9", abi.LU_TC_CUBLAS)):
+            call = lambda: L.pb_cgemm_sub_batched_dev(m, nc, k, pa, ld, pb, ld, pc, ld, ld * ld, nb, kind)
+            rc = [call() for _ in range(3)]
+            if any(r != abi.PB_OK for r in rc):
+                row[tag] = {"unavailable": abi.last_error()}
+                continue
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(10):
+                call()
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / 10
+            row[tag] = {"ms": round(ms, 3), "tflops": round(8.0 * m * nc * k * nb / (ms * 1e-3) / 1e12, 1)}
+        out.append(row)
+        del a
+    return {"gemm": out}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -592,8 +626,12 @@ def main():
                     help="--barstack: aggregation level of the two-level preconditioner (1 = leaves)")
     ap.add_argument("--barstack", default="",
                     help="NXxNYxNZ: time the compressed path on the bar stack instead (e.g. 96x96x4)")
+    ap.add_argument("--gemm", action="store_true", help="time the LU trailing-update kernels alone")
     args = ap.parse_args()
     ws, rank = dist_env()
+    if args.gemm:
+        print(json.dumps(run_gemm(args)), flush=True)
+        return
     if args.barstack:
         if rank == 0:
             print(json.dumps(run_barstack(args)), flush=True)

@@ -334,8 +334,11 @@ int  pb_cgemm_sub_batched_dev(int m, int nc, int k, const float *a_dev, int lda,
  * GPU loading it holds until exit. The first call on each device does a one-time set-up
  * (it looks the array's device address up with cudaGetSymbolAddress), so make that first
  * call before any stream capture.
- * Calls share that scratch and run on the default stream: calls that overlap on the GPU
- * (e.g. from several host threads) race, so serialise them.
+ * Calls share that scratch and run on the legacy default stream: calls that overlap on
+ * the GPU (e.g. from several host threads) race, so serialise them. The call reads seg_dev
+ * and writes lp_dev on that stream and synchronises it before returning, so the output is
+ * complete on return; the inputs must be complete before the call (a host that filled
+ * seg_dev on a non-blocking stream of its own synchronises that stream first).
  */
 int  pb_lp_fill_noalloc(int nseg, const pb_cell_t *seg_dev, int gp, double gpz, double kw,
                         int prec, double *lp_dev);

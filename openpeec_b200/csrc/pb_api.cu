@@ -575,20 +575,23 @@ int pb_cgemm_sub_batched_dev(int m, int nc, int k, const float *a_dev, int lda, 
     std::lock_guard<std::mutex> lk(mu);
     if (!eng.blas) PB_TRY(pb_lu_engine_init(&eng, nullptr));
     eng.gemm_kind = kind == PB_LU_TC ? PB_GEMM_TC : kind == PB_LU_FP32 ? PB_GEMM_FP32 : PB_GEMM_TC_BLAS;
-    float *emb = nullptr;
     if (kind == PB_LU_TC_CUBLAS) {
-        eng.emb_cap = (size_t)nb * 4 * k * nc * sizeof(float);
-        PB_CUDA(cudaMalloc(&emb, eng.emb_cap));
+        // the comparison's embedded right operand, kept between calls (grow-only)
+        static float *emb = nullptr;
+        static size_t emb_cap = 0;
+        const size_t need = (size_t)nb * 4 * k * nc * sizeof(float);
+        if (need > emb_cap) {
+            if (emb) PB_CUDA(cudaFree(emb));
+            emb = nullptr;
+            emb_cap = 0;
+            PB_CUDA(cudaMalloc(&emb, need));
+            emb_cap = need;
+        }
         eng.emb = emb;
+        eng.emb_cap = emb_cap;
     }
     int r = pb_cgemm_sub(&eng, m, nc, k, (const float2 *)a_dev, lda, (const float2 *)b_dev, ldb, (float2 *)c_dev,
                          ldc, stride, nb);
-    if (kind == PB_LU_TC_CUBLAS) {
-        cudaStreamSynchronize(nullptr);
-        cudaFree(emb);
-        eng.emb = nullptr;
-        eng.emb_cap = 0;
-    }
     if (r == PB_OK && eng.tc_used && eng.tc_err) {
         eng.tc_used = 0;
         int h = 0;

@@ -200,16 +200,21 @@ __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.
 // BF16 (value i of term j in half i of out[j]).
 __device__ __forceinline__ void split8_bf16x3(const float (&x)[8], uint4 (&out)[3])
 {
+    // two values per conversion instruction (cvt.rn.bf16x2.f32: the conversion pipe is the
+    // kernel's busiest), the BF16 -> FP32 expansion by bit operations
     uint32_t w[3][4];
 #pragma unroll
     for (int i = 0; i < 8; i += 2) {
         float r0 = x[i], r1 = x[i + 1];
 #pragma unroll
         for (int j = 0; j < 3; j++) {
-            const __nv_bfloat16 b0 = __float2bfloat16_rn(r0), b1 = __float2bfloat16_rn(r1);
-            r0 -= __bfloat162float(b0);
-            r1 -= __bfloat162float(b1);
-            w[j][i >> 1] = (uint32_t)__bfloat16_as_ushort(b0) | ((uint32_t)__bfloat16_as_ushort(b1) << 16);
+            const __nv_bfloat162 b = __floats2bfloat162_rn(r0, r1);     // .x = r0 (low half)
+            const uint32_t u = *reinterpret_cast<const uint32_t *>(&b);
+            w[j][i >> 1] = u;
+            if (j < 2) {
+                r0 -= __uint_as_float(u << 16);
+                r1 -= __uint_as_float(u & 0xffff0000u);
+            }
         }
     }
 #pragma unroll

@@ -33,12 +33,17 @@ def test_noalloc_matches_allocating_entry_point(prec, tol):
     cells = torch.from_numpy(prob.seg.view(np.uint8).copy()).cuda()
     out = torch.empty((n, n, 2), dtype=torch.float64, device="cuda")
     torch.cuda.synchronize()
-    for _ in range(2):
+    for call in range(2):
         out.fill_(np.nan)
         torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info()[0]
         r = abi.lib().pb_lp_fill_noalloc(n, cells.data_ptr(), int(prob.gp), float(prob.gpz),
                                          float(kw), int(prec), out.data_ptr())
         assert r == abi.PB_OK, abi.last_error()
+        if call == 1:
+            # after the first call (which may load the library's kernels), a call takes no
+            # device memory: the driver's free-memory count is unchanged
+            assert torch.cuda.mem_get_info()[0] == free0
         got = out.cpu().numpy()
         got = got[..., 0] + 1j * got[..., 1]
         scale = np.max(np.abs(ref))
