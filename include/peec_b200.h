@@ -172,6 +172,12 @@ typedef struct {
     int    pc_mlp_fallbacks;           /* frequencies that fell back to the plain preconditioner */
     int    pc_coarse_n;                /* coarse-space size of the two-level preconditioner */
     double t_coarse_ms;                /* its set-up time (coarse basis and matrix) [ms]   */
+    int    probe_fallbacks;/* mixed path: frequencies sent to the FP64 fall back because the
+                              conditioning probe found their port voltages sensitive above a
+                              quarter of the 1e-6 bar to perturbations of the size of the
+                              remaining backward error (counted in fp64_fallbacks too)    */
+    int    pad4_;
+    double probe_max;      /* largest probe sensitivity |dV_port| / |V_port| of the sweep   */
 } pb_sweep_stats;
 
 const char *pb_last_error(void);
@@ -204,6 +210,18 @@ int  pb_pot_fill(pb_ctx *ctx, double kw, int prec, double *p_host);
  */
 int  pb_sweep(pb_ctx *ctx, int nfreq, const double *freq, const pb_sweep_opts *opts,
               double *zmat, double *segi, pb_sweep_stats *stats);
+
+/*
+ * pb_sweep with the distribution outputs of distribution = 1 (solve.c:331-362): segi as
+ * pb_sweep, and cellq [nfreq*nport*ncell] complex (reference QIDX layout,
+ * include/peec.h:237) the cell charges of each port excitation, q = C v on the dense path
+ * (obtained without forming C = P^-1: from KCL, j w q = injection - G i, in the reduced
+ * form; the charge unknowns in the full form), the charge unknowns on the compressed path.
+ * Cells in the reference's order (first appearance of the node id among the charge
+ * sub-cells). cellq is left untouched without capacitance. Any output may be NULL.
+ */
+int  pb_sweep_dist(pb_ctx *ctx, int nfreq, const double *freq, const pb_sweep_opts *opts,
+                   double *zmat, double *segi, double *cellq, pb_sweep_stats *stats);
 
 /*
  * Plane-wave incidence (the reference's planewave key, src/input_data.c:501-519):

@@ -76,6 +76,7 @@ class PbSweepStats(C.Structure):
         ("hmat_far", C.c_int), ("hmat_near", C.c_int), ("hmat_max_rank", C.c_int),
         ("hmat_dense_far", C.c_int), ("hmat_mb", C.c_double), ("hmat_dense_mb", C.c_double),
         ("pc_mlp_fallbacks", C.c_int), ("pc_coarse_n", C.c_int), ("t_coarse_ms", C.c_double),
+        ("probe_fallbacks", C.c_int), ("pad4_", C.c_int), ("probe_max", C.c_double),
     ]
 
     def as_dict(self):
@@ -139,6 +140,8 @@ def lib():
     L.pb_pot_fill.argtypes = [_vp, C.c_double, C.c_int, _vp]
     L.pb_sweep.argtypes = [_vp, C.c_int, _vp, C.POINTER(PbSweepOpts), _vp, _vp,
                            C.POINTER(PbSweepStats)]
+    L.pb_sweep_dist.argtypes = [_vp, C.c_int, _vp, C.POINTER(PbSweepOpts), _vp, _vp, _vp,
+                                C.POINTER(PbSweepStats)]
     L.pb_planewave.argtypes = [_vp, C.c_int, _vp, C.POINTER(PbSweepOpts), C.POINTER(PbPlanewave),
                                _vp, _vp, C.POINTER(PbSweepStats)]
     L.pb_lu_decomp.argtypes = [C.c_int, _vp, _vp]

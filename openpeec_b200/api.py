@@ -65,9 +65,11 @@ class Context:
 
     def sweep(self, freqs, fill_prec=abi.PREC_MIXED, lu=abi.LU_TC, form=abi.FORM_AUTO,
               batch=0, refine_tol=0.0, refine_maxit=0, want_segi=False, zmat_out=None,
-              corr_freqs=0, verbose=0, accel=None, compress=None, ctol=None, pc_mlp=None, pc_coarse=0):
+              corr_freqs=0, verbose=0, accel=None, compress=None, ctol=None, pc_mlp=None, pc_coarse=0,
+              want_cellq=False):
         """pb_sweep. accel / compress / ctol = None take the .peec file's acceleration and
-        compression keys."""
+        compression keys. want_cellq (pb_sweep_dist) adds the cell charges
+        [nfreq, nport, ncell] of every port excitation after the segment currents."""
         accel = getattr(self.prob, "accel", 0) if accel is None else accel
         compress = getattr(self.prob, "compress", 0) if compress is None else compress
         ctol = getattr(self.prob, "ctol", 0.0) if ctol is None else ctol
@@ -83,6 +85,14 @@ class Context:
             o.pc_mlp = pc_mlp.ctypes.data
         o.pc_coarse = int(pc_coarse)
         st = abi.PbSweepStats()
+        if want_cellq:
+            q = np.zeros((len(freqs), npt, self.ncell), np.complex128)
+            _check(abi.lib().pb_sweep_dist(self.h, len(freqs), freqs.ctypes.data, C.byref(o),
+                                           z.ctypes.data, None if segi is None else segi.ctypes.data,
+                                           q.ctypes.data, C.byref(st)))
+            if want_segi:
+                return z, segi, q, st.as_dict()
+            return z, q, st.as_dict()
         _check(abi.lib().pb_sweep(self.h, len(freqs), freqs.ctypes.data, C.byref(o),
                                   z.ctypes.data, None if segi is None else segi.ctypes.data,
                                   C.byref(st)))

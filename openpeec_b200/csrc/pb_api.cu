@@ -33,7 +33,7 @@ int pb_cuda_fail(cudaError_t e, const char *what, const char *file, int line)
 int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts *opts,
                   double *zmat, double *segi, pb_sweep_stats *stats,
                   const pb_planewave_t *pw, double *voc, double *segipw,
-                  const double *rhs_fixed = nullptr, double *vnode = nullptr);
+                  const double *rhs_fixed = nullptr, double *vnode = nullptr, double *cellq = nullptr);
 
 extern "C" const char *pb_last_error(void) { return g_err.c_str(); }
 
@@ -383,6 +383,15 @@ int pb_sweep(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts *opts
     if (!c) { pb_set_error("pb_sweep: null context"); return PB_ERR_ARG; }
     PB_CUDA(cudaSetDevice(c->dev));
     return pb_sweep_impl(c, nfreq, freq, opts, zmat, segi, stats, nullptr, nullptr, nullptr);
+}
+
+int pb_sweep_dist(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts *opts, double *zmat,
+                  double *segi, double *cellq, pb_sweep_stats *stats)
+{
+    if (!c) { pb_set_error("pb_sweep_dist: null context"); return PB_ERR_ARG; }
+    PB_CUDA(cudaSetDevice(c->dev));
+    return pb_sweep_impl(c, nfreq, freq, opts, zmat, segi, stats, nullptr, nullptr, nullptr, nullptr, nullptr,
+                         cellq);
 }
 
 int pb_sweep_many(int ninst, pb_ctx *const *ctx, const int *nfreq, const double *const *freq,

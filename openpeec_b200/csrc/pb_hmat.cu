@@ -1091,7 +1091,8 @@ int pc_samples(pb_ctx *c, KBlock &kb, const std::vector<zc> &zint, double om, co
 
 int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts &o, double ctol,
                         double gtol, double *zmat, pb_sweep_stats *stats, pb_hstats *hs, float *sample_x,
-                        float *sample_t, const pb_planewave_t *pw, double *voc, double *segipw)
+                        float *sample_t, const pb_planewave_t *pw, double *voc, double *segipw, double *segi,
+                        double *cellq)
 {
     int mlp_fallbacks = 0, coarse_fallbacks = 0, coarse_n = 0;
     double t_coarse = 0;
@@ -1914,6 +1915,14 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
                     zmat[2 * (((size_t)ifr * np + i) * np + j)] = v.real();
                     zmat[2 * (((size_t)ifr * np + i) * np + j) + 1] = v.imag();
                 }
+            }
+            for (int k = 0; k < ns && segi; k++) {
+                segi[2 * (((size_t)ifr * np + j) * ns + k)] = xh[offS + k].real();
+                segi[2 * (((size_t)ifr * np + j) * ns + k) + 1] = xh[offS + k].imag();
+            }
+            for (int m = 0; m < nc && cellq; m++) {
+                cellq[2 * (((size_t)ifr * np + j) * nc + m)] = xh[offQ + m].real();
+                cellq[2 * (((size_t)ifr * np + j) * nc + m) + 1] = xh[offQ + m].imag();
             }
         }
         tock(t_gm);

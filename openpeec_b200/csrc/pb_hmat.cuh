@@ -51,10 +51,13 @@ struct pb_hstats {
 // pw != nullptr: one plane-wave excitation per frequency instead of the port excitations
 // (mna_rhs_planewave, src/mna.c:434-468): voc [nport][nfreq] open-circuit port voltages,
 // segipw [nfreq][nseg] branch currents (either may be nullptr), zmat unused.
+// Port excitations: segi [nfreq][nport][nseg] branch currents and cellq [nfreq][nport][ncell]
+// cell charges (the charge unknowns, solve.c:344-351), either may be nullptr.
 int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts &o,
                         double ctol, double gtol, double *zmat, pb_sweep_stats *stats, pb_hstats *hs,
                         float *sample_x = nullptr, float *sample_t = nullptr,
-                        const pb_planewave_t *pw = nullptr, double *voc = nullptr, double *segipw = nullptr);
+                        const pb_planewave_t *pw = nullptr, double *voc = nullptr, double *segipw = nullptr,
+                        double *segi = nullptr, double *cellq = nullptr);
 
 // Plane-wave right-hand side of the full MNA form at one frequency (freq_dev: one double in
 // device memory): -EMF on the branch rows offS + k, zero elsewhere (n rows).

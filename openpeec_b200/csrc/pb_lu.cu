@@ -872,7 +872,7 @@ __device__ __forceinline__ void atomic_max_pos(double *addr, double v)
 __global__ void __launch_bounds__(256)
 k_residual(const double2 *a, int n, int ld, long long stride, const double2 *bv,
            const double2 *xv, double2 *rv, double *rn, double *bn, double *xn, double *an,
-           int nrhs, int rows_per_block, const int *sys, double *cw, int stage)
+           int nrhs, int rows_per_block, const int *sys, double *cw, int stage, double *wv)
 {
     // stage = 1: x is staged in shared memory [nrhs][n]; 0 (orders whose x does not fit,
     // above ~14 000 unknowns): x is read from global memory (L2 holds it)
@@ -910,12 +910,12 @@ k_residual(const double2 *a, int n, int ld, long long stride, const double2 *bv,
                 const double2 av = row[c], xx = x[c];
                 sr += av.x * xx.x - av.y * xx.y;
                 si += av.x * xx.y + av.y * xx.x;
-                if (cw) sa += (fabs(av.x) + fabs(av.y)) * (fabs(xx.x) + fabs(xx.y));
+                if (cw || wv) sa += (fabs(av.x) + fabs(av.y)) * (fabs(xx.x) + fabs(xx.y));
             }
             for (int o = 16; o > 0; o >>= 1) {
                 sr += __shfl_down_sync(0xffffffffu, sr, o);
                 si += __shfl_down_sync(0xffffffffu, si, o);
-                if (cw) sa += __shfl_down_sync(0xffffffffu, sa, o);
+                if (cw || wv) sa += __shfl_down_sync(0xffffffffu, sa, o);
             }
             if (lane == 0) {
                 const long long idx = ((long long)b * nrhs + q) * n + r;
@@ -929,6 +929,7 @@ k_residual(const double2 *a, int n, int ld, long long stride, const double2 *bv,
                         const double num = fabs(res.x) + fabs(res.y), den = sa + fabs(bb.x) + fabs(bb.y);
                         atomic_max_pos(&cw[b * nrhs + q], den > 0 ? num / den : (num > 0 ? 1.0 : 0.0));
                     }
+                    if (wv) wv[idx] = sa + fabs(bb.x) + fabs(bb.y);   // (|A||x| + |b|)_r
                 } else {
                     rv[idx] = make_double2(sr, si);          // product only: r = A x
                 }
@@ -954,7 +955,8 @@ int pb_residual(pb_lu_engine *e, int n, int nb, int nrhs, const double2 *a, int 
     PB_TRY(pb_smem_optin(k_residual, pb_smem_cap(), g_residual_attr));
     const int rpb = 64;
     dim3 g(ceil_div(n, rpb), nb);
-    k_residual<<<g, 256, smem, e->stream>>>(a, n, ld, stride, b, x, r, rn, bn, xn, an, nrhs, rpb, nullptr, cw, stage);
+    k_residual<<<g, 256, smem, e->stream>>>(a, n, ld, stride, b, x, r, rn, bn, xn, an, nrhs, rpb, nullptr, cw, stage,
+                                            nullptr);
     e->launches++;
     PB_CHECK_LAUNCH();
     return PB_OK;
@@ -962,7 +964,7 @@ int pb_residual(pb_lu_engine *e, int n, int nb, int nrhs, const double2 *a, int 
 
 int pb_residual_mapped(pb_lu_engine *e, int n, int nb, int nrhs, const double2 *a, int ld, long stride,
                        const double2 *b, const double2 *x, double2 *r, double *rn, double *bn, double *xn,
-                       double *an, int nall, const int *sys, double *cw)
+                       double *an, int nall, const int *sys, double *cw, double *wv)
 {
     PB_CUDA(cudaMemsetAsync(rn, 0, sizeof(double) * nall * nrhs, e->stream));
     if (cw) PB_CUDA(cudaMemsetAsync(cw, 0, sizeof(double) * nall * nrhs, e->stream));
@@ -975,7 +977,7 @@ int pb_residual_mapped(pb_lu_engine *e, int n, int nb, int nrhs, const double2 *
     PB_TRY(pb_smem_optin(k_residual, pb_smem_cap(), g_residual_attr));
     const int rpb = 64;
     dim3 g(ceil_div(n, rpb), nb);
-    k_residual<<<g, 256, smem, e->stream>>>(a, n, ld, stride, b, x, r, rn, bn, xn, an, nrhs, rpb, sys, cw, stage);
+    k_residual<<<g, 256, smem, e->stream>>>(a, n, ld, stride, b, x, r, rn, bn, xn, an, nrhs, rpb, sys, cw, stage, wv);
     e->launches++;
     PB_CHECK_LAUNCH();
     return PB_OK;
@@ -992,7 +994,7 @@ int pb_matvec_mapped(pb_lu_engine *e, int n, int nb, int nrhs, const double2 *a,
     const int rpb = 64;
     dim3 g(ceil_div(n, rpb), nb);
     k_residual<<<g, 256, smem, e->stream>>>(a, n, ld, stride, nullptr, x, y, nullptr, nullptr, nullptr,
-                                            nullptr, nrhs, rpb, sys, nullptr, stage);
+                                            nullptr, nrhs, rpb, sys, nullptr, stage, nullptr);
     e->launches++;
     PB_CHECK_LAUNCH();
     return PB_OK;

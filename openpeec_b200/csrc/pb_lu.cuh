@@ -71,10 +71,10 @@ int pb_lu_solve_mapped(pb_lu_engine *e, int n, int nb, int nrhs,
                        const int *lu_of);
 
 // pb_residual for the nb systems sys[0..nb) of a batch of nall; the norms of the other
-// systems are left at 0.
+// systems are left at 0. wv (optional, laid out like r): (|A||x| + |b|) per row.
 int pb_residual_mapped(pb_lu_engine *e, int n, int nb, int nrhs, const double2 *a, int ld, long stride,
                        const double2 *b, const double2 *x, double2 *r, double *rn, double *bn, double *xn,
-                       double *an, int nall, const int *sys, double *cw = nullptr);
+                       double *an, int nall, const int *sys, double *cw = nullptr, double *wv = nullptr);
 
 // y = A x for the nb systems sys[0..nb) (nullptr = 0..nb), nrhs vectors each.
 int pb_matvec_mapped(pb_lu_engine *e, int n, int nb, int nrhs, const double2 *a, int ld, long stride,

@@ -208,6 +208,50 @@ __global__ void k_z_full(int nb, int np, int nx, int n, const int *pm, const dou
     z[idx] = v;
 }
 
+// Cell charges of the port excitations (solve.c:344-361), q[f][j][c] (QIDX layout).
+// Reduced form: KCL at cell c, j w q_c = b_j[c] - (G ib_j)[c] (the quantity k_z_reduced
+// multiplies by P). Full form: the charge unknowns x[offQ + c] themselves.
+__global__ void k_cellq(int nb, int np, int n, int nc, int reduced, int offQ, const int *inc_off,
+                        const int *inc_seg, const int *pc, const double2 *x, const double *freq, double2 *q)
+{
+    const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (idx >= (long long)nb * np * nc) return;
+    const int c = (int)(idx % nc);
+    const int j = (int)((idx / nc) % np);
+    const int f = (int)(idx / ((long long)nc * np));
+    const double2 *xv = x + ((long long)f * np + j) * n;
+    if (!reduced) {
+        q[idx] = xv[offQ + c];
+        return;
+    }
+    double yr = (c == pc[2 * j] ? 1.0 : 0.0) - (c == pc[2 * j + 1] ? 1.0 : 0.0), yi = 0;
+    for (int e = inc_off[c]; e < inc_off[c + 1]; e++) {
+        const int s = inc_seg[e];
+        const int k = (s > 0 ? s : -s) - 1;
+        const double sg = s > 0 ? 1.0 : -1.0;
+        yr -= sg * xv[k].x;
+        yi -= sg * xv[k].y;
+    }
+    const double om = 2 * PB_PI * freq[f];
+    q[idx] = make_double2(yi / om, -yr / om);
+}
+
+// Conditioning probe of the refined solutions: the right-hand side of a perturbation of the
+// size of the remaining componentwise backward error, db_r = eta_q (|A||x| + |b|)_r with a
+// fixed pseudo-random phase of +-1 +- j per row (per = vectors x rows of one system).
+__global__ void k_probe_rhs(long long per, const int *sys, const double *w, const double *eta, double2 *out)
+{
+    const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (e >= per) return;
+    const long long q = sys[blockIdx.y];
+    unsigned h = (unsigned)e * 2654435761u;          // integer hash of the row index
+    h ^= h >> 15;
+    h *= 2246822519u;
+    h ^= h >> 13;
+    const double a = eta[q] * w[q * per + e] * 0.7071067811865476;
+    out[q * per + e] = make_double2((h & 1u) ? a : -a, (h & 2u) ? a : -a);
+}
+
 // full form: blocks of the augmented matrix (Lp block with -zint, P block)
 __global__ void k_full_blocks(int nb, int n, int ns, int nc, int offS, int offQ,
                               const double2 *lp, long long lst, const double2 *P, long long pst,
@@ -356,7 +400,7 @@ struct PhaseTimer {
 int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts *opts_in,
                   double *zmat, double *segi, pb_sweep_stats *stats,
                   const pb_planewave_t *pw, double *voc, double *segipw,
-                  const double *rhs_fixed, double *vnode)
+                  const double *rhs_fixed, double *vnode, double *cellq)
 {
     pb_sweep_opts o;
     if (opts_in) o = *opts_in;
@@ -373,7 +417,7 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
         pb_hstats hs;
         return pb_sweep_compressed(c, nfreq, freq, o, o.ctol > 0 ? o.ctol : 1e-6,
                                    o.refine_tol > 0 ? o.refine_tol : 1e-10, pw ? nullptr : zmat, stats, &hs,
-                                   nullptr, nullptr, pw, voc, segipw);
+                                   nullptr, nullptr, pw, voc, segipw, pw ? nullptr : segi, pw ? nullptr : cellq);
     }
     if (nfreq <= 0 || freq == nullptr) { pb_set_error("pb_sweep: no frequencies"); return PB_ERR_ARG; }
     for (int i = 0; i < nfreq; i++)
@@ -465,6 +509,14 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
     PB_TRY(bFreq.alloc((size_t)B * 8));
     PB_TRY(bZ.alloc((size_t)B * np * nr * 16 + 16));
     PB_TRY(bPC.alloc((size_t)2 * (np + 1) * 4));
+    DevBuf bW(cs + 26), bEta(cs + 27), bZp(cs + 28); // conditioning probe: row weights, eta, port voltages
+    if (mixed && !rhs_fixed) {
+        PB_TRY(bW.alloc((size_t)B * nr * n * 8));
+        PB_TRY(bEta.alloc((size_t)B * 8));
+        PB_TRY(bZp.alloc((size_t)2 * B * np * nr * 16 + 16));
+    }
+    DevBuf bQ(cs + 25);                           // cell charges of one batch (distribution)
+    if (cellq && !pw && !rhs_fixed && c->capacitance && nc > 0) PB_TRY(bQ.alloc((size_t)B * np * nc * 16));
 
     // port endpoints: cells (reduced) or matrix indices (full)
     std::vector<int> pc(2 * np);
@@ -490,8 +542,8 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
     if (pw) PB_TRY(make_pw_args(pw, pwa));
 
     PhaseTimer tStatic, tCorr, tAsm, tLu, tRef, tAll;
-    double samples = 0, luflops = 0, maxres = 0;
-    int maxits = 0, refreshes = 0;
+    double samples = 0, luflops = 0, maxres = 0, probe_max = 0;
+    int maxits = 0, refreshes = 0, probe_fb = 0;
     // the static tables stay with the context between calls (cache slots 4 and 5): valid
     // while the quadrature-level signature is unchanged and the slots kept their storage
     std::vector<long> cur_sig, sig;
@@ -767,7 +819,8 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
                                               bX.as<double2>() + vo));
             const double eta_tol = std::max(1e-14, 8.0 * std::sqrt((double)n) * 1.1e-16);
             const bool cwise = (form == PB_FORM_FULL);
-            std::vector<double> prev(nb, 1e300), cwh((size_t)mb * nr, 0.0);
+            const bool probe = !rhs_fixed;
+            std::vector<double> prev(nb, 1e300), cwh((size_t)mb * nr, 0.0), etah(mb, 0.0);
             for (int q = nd; q < nb; q++) if (state[q] == 1) state[q] = 0;
             // only the systems still refining are touched after the first pass (the
             // stragglers near the FP64 fallback take up to a dozen steps, most need 2-3)
@@ -781,7 +834,8 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
                 PB_TRY(pb_residual_mapped(&c->lu, n, (int)act.size(), nr, m64, n, nn, bRhs.as<double2>() + vo,
                                           bX.as<double2>() + vo, bR.as<double2>() + vo, bRn.as<double>(),
                                           bBn.as<double>(), bXn.as<double>(), it == 1 ? bAn.as<double>() : nullptr,
-                                          mb, bSys.as<int>(), cwise ? bCw.as<double>() : nullptr));
+                                          mb, bSys.as<int>(), cwise ? bCw.as<double>() : nullptr,
+                                          probe ? bW.as<double>() : nullptr));
                 PB_CUDA(cudaMemcpyAsync(rnh.data(), bRn.p, sizeof(double) * mb * nr, cudaMemcpyDeviceToHost, st));
                 PB_CUDA(cudaMemcpyAsync(bnh.data(), bBn.p, sizeof(double) * mb * nr, cudaMemcpyDeviceToHost, st));
                 PB_CUDA(cudaMemcpyAsync(xnh.data(), bXn.p, sizeof(double) * mb * nr, cudaMemcpyDeviceToHost, st));
@@ -798,7 +852,7 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
                         eta = std::max(eta, den > 0 ? rnh[v] / den : 0.0);
                         if (cwise) eta = std::max(eta, cwh[v]);
                     }
-                    if (eta <= eta_tol) { state[nd + q] = 1; maxres = std::max(maxres, eta); }
+                    if (eta <= eta_tol) { state[nd + q] = 1; maxres = std::max(maxres, eta); etah[q] = eta; }
                     else if (eta > 0.5 * prev[nd + q] || it > maxit) state[nd + q] = 2;
                     else { prev[nd + q] = eta; active++; }
                 }
@@ -815,6 +869,62 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
                 PB_CHECK_LAUNCH();
             }
             maxits = std::max(maxits, it);
+            // Conditioning probe. A backward error at FP64 level does not bound the forward
+            // error of an ill-conditioned system (e.g. an inductive structure whose port
+            // resistance is 1e-5 of |Z| behind 1e-9 ohm bus resistors: cond ~ 1e13), and
+            // there only the reference's own elimination order reproduces its digits. Each
+            // converged system is perturbed by its remaining backward error (k_probe_rhs,
+            // solved with its FP32 factors); where the port voltages move by more than a
+            // quarter of the 1e-6 parity bar relative to the largest, the frequency takes
+            // the FP64 fall back (stats->probe_fallbacks).
+            std::vector<int> conv;
+            for (int q = 0; q < mb; q++) if (state[nd + q] == 1) conv.push_back(q);
+            if (probe && !conv.empty()) {
+                for (int q = 0; q < mb; q++) etah[q] = std::max(etah[q], 4.0 * 1.1e-16);
+                PB_CUDA(cudaMemcpyAsync(bEta.p, etah.data(), sizeof(double) * mb, cudaMemcpyHostToDevice, st));
+                PB_CUDA(cudaMemcpyAsync(bSys.p, conv.data(), sizeof(int) * conv.size(), cudaMemcpyHostToDevice, st));
+                const long long per = (long long)nr * n;
+                k_probe_rhs<<<dim3(ceil_div(per, 256), (unsigned)conv.size()), 256, 0, st>>>(
+                    per, bSys.as<int>(), bW.as<double>(), bEta.as<double>(), bR.as<double2>() + vo);
+                c->launches++;
+                PB_CHECK_LAUNCH();
+                PB_TRY(pb_lu_solve_mapped<float>(&c->lu, n, (int)conv.size(), nr, m32, n, nn, perm,
+                                                 bR.as<double2>() + vo, bD.as<double2>() + vo, bSys.as<int>(), nullptr));
+                // port voltages of x (with the port injections) and of the probe solution
+                // (linear part only) for systems nd .. nb
+                const int *pnone = bPC.as<int>() + 2 * np;
+                const int *pcx0 = pw ? pnone : bPC.as<int>();
+                double2 *zx = bZp.as<double2>(), *zy = zx + (long long)mb * np * nr;
+                for (int pass = 0; pass < 2; pass++) {
+                    const double2 *xv = (pass ? bD.as<double2>() : bX.as<double2>()) + vo;
+                    if (form == PB_FORM_REDUCED) {
+                        k_z_reduced<<<dim3(nr, np, mb), 256, 0, st>>>(np, nr, n, nc, bP.as<double2>() + (long long)nd * nc * nc,
+                                                                     (long long)nc * nc, c->d_inc_off, c->d_inc_seg,
+                                                                     bPC.as<int>(), pass ? pnone : pcx0, xv,
+                                                                     bFreq.as<double>() + nd, pass ? zy : zx);
+                    } else {
+                        k_z_full<<<ceil_div(mb * np * nr, 128), 128, 0, st>>>(mb, np, nr, n, bPC.as<int>(), xv,
+                                                                              pass ? zy : zx);
+                    }
+                    c->launches++;
+                    PB_CHECK_LAUNCH();
+                }
+                std::vector<double2> zph((size_t)2 * mb * np * nr);
+                PB_CUDA(cudaMemcpyAsync(zph.data(), zx, sizeof(double2) * zph.size(), cudaMemcpyDeviceToHost, st));
+                PB_CUDA(cudaStreamSynchronize(st));
+                const size_t per_z = (size_t)np * nr;
+                for (int q : conv) {
+                    double ax = 0, ay = 0;
+                    for (size_t t = 0; t < per_z; t++) {
+                        const double2 a = zph[(size_t)q * per_z + t], b = zph[(size_t)(mb + q) * per_z + t];
+                        ax = std::max(ax, std::hypot(a.x, a.y));
+                        ay = std::max(ay, std::hypot(b.x, b.y));
+                    }
+                    const double sens = ax > 0 ? ay / ax : 0.0;
+                    probe_max = std::max(probe_max, sens);
+                    if (sens > 2.5e-7) { state[nd + q] = 2; probe_fb++; }
+                }
+            }
         }
         if (nb > nd) {
             // FP64 fallback, batched: copy the stalled frequencies' FP64 matrices into the
@@ -904,6 +1014,15 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
                 PB_CUDA(cudaMemcpyAsync(segipw + 2 * ((size_t)(b0 + q) * ns), bX.as<double2>() + (long long)q * n + off,
                                         sizeof(double2) * ns, cudaMemcpyDeviceToHost, st));
         }
+        if (cellq && !pw && !rhs_fixed && c->capacitance && nc > 0) {
+            k_cellq<<<(int)ceil_div((long long)nb * np * nc, 256), 256, 0, st>>>(
+                nb, np, n, nc, form == PB_FORM_REDUCED, c->nunknown, c->d_inc_off, c->d_inc_seg, bPC.as<int>(),
+                bX.as<double2>(), bFreq.as<double>(), bQ.as<double2>());
+            c->launches++;
+            PB_CHECK_LAUNCH();
+            PB_CUDA(cudaMemcpyAsync(cellq + 2 * (size_t)b0 * np * nc, bQ.p, sizeof(double2) * nb * np * nc,
+                                    cudaMemcpyDeviceToHost, st));
+        }
         if (segi && !pw) {
             const int off = (form == PB_FORM_REDUCED) ? 0 : c->offS;
             for (int q = 0; q < nb; q++)
@@ -938,6 +1057,8 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
         stats->gmres_its_max = gm_max;
         stats->gmres_refactored = refactored;
         stats->gmres_its_avg = gm_solves > 0 ? (double)gm_its / gm_solves : 0.0;
+        stats->probe_fallbacks = probe_fb;
+        stats->probe_max = probe_max;
     }
     return PB_OK;
 }

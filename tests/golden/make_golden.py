@@ -12,6 +12,7 @@ reference's own sources with oracle/Makefile). For every case it stores:
     python tests/golden/make_golden.py --cfg2     # + the full 64x32 plate at 2 frequencies
     python tests/golden/make_golden.py --pw-only  # only the plane-wave cases (tests/golden/pw)
     python tests/golden/make_golden.py --comp-only  # only the compressed-path cases (tests/golden/comp)
+    python tests/golden/make_golden.py --dropin-only  # the reference CLI's output files (tests/golden/dropin)
 """
 import argparse
 import os
@@ -295,6 +296,87 @@ def pw_cases():
     make_pw_case("mono_pw", mono, [1.3e8, 1.45e8, 1.6e8])
 
 
+def run_cli(peec_text, threads=8):
+    """The reference's own CLI (oracle/_ref/peec, built from its sources) on one input:
+    its output files, as text."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "peec")
+    with tempfile.TemporaryDirectory() as d:
+        with open(os.path.join(d, "case.peec"), "w") as f:
+            f.write(peec_text)
+        subprocess.run([exe, "-n", str(threads), "case.peec"], cwd=d, check=True, stdout=subprocess.DEVNULL)
+        out = {}
+        for fn in sorted(os.listdir(d)):
+            if fn == "case.peec":
+                continue
+            with open(os.path.join(d, fn)) as f:
+                out[fn] = f.read()
+    log = out.pop("peec.log")
+    assert "normal end" in log, log[-400:]
+    out["captotal"] = "\n".join(l for l in log.splitlines() if "total capacitance" in l)
+    return out
+
+
+def with_key(text, line):
+    """Insert a key line after the title (as the reference's checks build their variants)."""
+    return "\n".join(l + ("\n" + line if l.startswith("title = ") else "") for l in text.splitlines()) + "\n"
+
+
+def skin_hf(text):
+    """skineffect = 1 before the title and a single frequency of 1 GHz."""
+    out = []
+    for l in text.splitlines():
+        if l.startswith("title = "):
+            out.append("skineffect = 1")
+        out.append("frequency = 1e9 1e9 0" if l.startswith("frequency = ") else l)
+    return "\n".join(out) + "\n"
+
+
+def dropin_cases():
+    """Reference CLI outputs (zin.csv, dist.csv, pw.csv, far.csv, tran.csv, Touchstone, the
+    total-capacitance log line) of the sample inputs on the hot path, for the drop-in
+    binary peec_gpu (openpeec_b200/dropin)."""
+    out = os.path.join(HERE, "dropin")
+    os.makedirs(out, exist_ok=True)
+    wd = sample("wire_dist.peec")
+    cases = {
+        "rlc_series": sample("rlc_series.peec"),
+        "dipole_halfwave": sample("dipole_halfwave.peec"),
+        "dipole_hw_accel": with_key(sample("dipole_halfwave.peec"), "acceleration = 1"),
+        "dipole_full": sample("dipole_full.peec"),
+        "monopole_gp": sample("monopole_gp.peec"),
+        "plate_cap": sample("plate_cap.peec"),
+        "disk_cap": sample("disk_cap.peec"),
+        "quad_square": sample("quad_square.peec"),
+        "bar_skin": sample("bar_skin.peec"),
+        "wire_skin_hf": sample("wire_skin_hf.peec"),
+        "diel_pp": sample("diel_pp.peec"),
+        "diel_debye": sample("diel_debye.peec"),
+        "strip_dipole_ret": sample("strip_dipole_ret.peec"),
+        "compress_wire": sample("compress_wire.peec"),
+        "compress_plate": sample("compress_plate.peec"),
+        "compress_cap": sample("compress_cap.peec"),
+        "wire_dist": wd,
+        "wire_dist_cap": "\n".join(("capacitance = 1\n" + l) if l.startswith("distribution = 1") else l
+                                   for l in wd.splitlines()) + "\n",
+        "twoport_dist": sample("twoport_dist.peec"),
+        "tnetwork_l_spara": sample("tnetwork_l_spara.peec"),
+        "loop_pw": sample("loop_pw.peec"),
+        "bent_pw": sample("bent_pw.peec"),
+        "dipole_ff": sample("dipole_ff.peec"),
+        "loop_tran": sample("loop_tran.peec"),
+        "tdr_resistor": sample("tdr_resistor.peec"),
+        # the sheet at 1 GHz with skin effect (the reference's "quad sheet R vs plate" pair):
+        # R is 6e-5 of |Z| behind 1e-9 ohm bus resistors, cond(A) ~ 4e13
+        "sk_plate_hf": skin_hf(sample("quad_square_ref.peec")),
+        "sk_quad_hf": skin_hf(sample("quad_square.peec")),
+    }
+    for name, text in cases.items():
+        files = run_cli(text)
+        np.savez_compressed(os.path.join(out, name + ".npz"), peec=np.array(text),
+                            names=np.array(sorted(files)), **{"f_" + k: np.array(v) for k, v in files.items()})
+        print(name, sorted(files))
+
+
 def sample(fn):
     with open(os.path.join(REF, "data", "sample", fn)) as f:
         return f.read()
@@ -309,9 +391,13 @@ def main():
     ap.add_argument("--post-only", action="store_true", help="only the far-field / transient cases")
     ap.add_argument("--cfg4-only", action="store_true", help="only config 4 at full size (minutes)")
     ap.add_argument("--cfg5-only", action="store_true", help="only the scaled-down config-5 cases")
+    ap.add_argument("--dropin-only", action="store_true", help="only the reference-CLI outputs (tests/golden/dropin)")
     a = ap.parse_args()
     subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True,
                    stdout=subprocess.DEVNULL)
+    if a.dropin_only:
+        dropin_cases()
+        return
     if a.cfg4_only:
         make_cfg4_full()
         return
