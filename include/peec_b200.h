@@ -99,9 +99,15 @@ typedef struct pb_ctx pb_ctx;
 /* Dense factorisation used inside the sweep. */
 #define PB_LU_FP64     0     /* FP64 panels + FP64 trailing updates                      */
 #define PB_LU_FP32     1     /* FP32 panels + FP32 SIMT trailing updates, FP64 refinement */
-#define PB_LU_TC       2     /* FP32 panels + tensor-core trailing updates, FP64 refinement */
-#define PB_LU_TC_CUBLAS 3    /* comparison baseline: as PB_LU_TC, with cuBLAS's BF16x9 FP32
-                                emulation in place of the library's tcgen05 update kernel  */
+#define PB_LU_TC       2     /* FP32 panels + tensor-core trailing updates, FP64 refinement;
+                                the reduced (complex-symmetric) form is factored as L D L^T
+                                without pivoting, every other system by the pivoted LU     */
+#define PB_LU_TC_CUBLAS 3    /* comparison baseline: pivoted LU as PB_LU_TC, with cuBLAS's
+                                BF16x9 FP32 emulation in place of the library's tcgen05
+                                update kernel                                              */
+#define PB_LU_TC_PIVOTED 4   /* as PB_LU_TC, always the pivoted LU (comparison)             */
+#define PB_LU_LDLT     5     /* pb_lu_decomp_batched32_dev only: the L D L^T factorisation
+                                PB_LU_TC uses for the reduced form                          */
 
 /* MNA formulation inside the sweep. */
 #define PB_FORM_AUTO    0    /* reduced when applicable, else full                       */
@@ -149,7 +155,7 @@ typedef struct {
 typedef struct {
     double t_static_ms, t_corr_ms, t_assemble_ms, t_lu_ms, t_refine_ms, t_total_ms;
     double corr_samples;    /* retardation-correction quadrature samples evaluated    */
-    double lu_flops;        /* (8/3) n^3 per frequency, summed                       */
+    double lu_flops;        /* (8/3) n^3 per LU, (4/3) n^3 per L D L^T, summed       */
     double max_resid;       /* largest final normwise backward error |r|/(|A||x|+|b|) */
     int    max_iters;       /* largest refinement iteration count                    */
     int    form_used;       /* PB_FORM_FULL or PB_FORM_REDUCED                       */
@@ -323,7 +329,10 @@ int  pb_lu_decomp_batched_dev(int n, int nb, double *a_dev, int *piv_dev, int *i
  * The mixed-precision factorisation of the sweep on device memory: nb matrices of order
  * n, row-major, complex FP32 (interleaved re/im), stride n*n, factorised in place with
  * the pivot rule of lu_decomp (src/lu.c:16-66); lu = PB_LU_TC (tensor-core trailing
- * updates), PB_LU_FP32 (SIMT updates) or PB_LU_TC_CUBLAS. info_host[b] as above.
+ * updates), PB_LU_FP32 (SIMT updates) or PB_LU_TC_CUBLAS. lu = PB_LU_LDLT: the
+ * complex-symmetric A = L D L^T without pivoting (only the lower triangle of A is read;
+ * stored as an unpivoted LU, unit L below and U = D L^T on and above the diagonal, piv the
+ * identity; PB_ERR_UNSUP above ~28 000 unknowns). info_host[b] as above.
  */
 int  pb_lu_decomp_batched32_dev(int n, int nb, float *a_dev, int *piv_dev, int *info_host, int lu);
 

@@ -32,7 +32,7 @@ MUT_DTYPE = np.dtype([("l1", "<i4"), ("l2", "<i4"), ("k", "<f8")])
 PB_LUMP_R, PB_LUMP_C, PB_LUMP_L, PB_LUMP_V = 0, 1, 2, 3
 PB_OK, PB_ERR_ARG, PB_ERR_CUDA, PB_ERR_SINGULAR, PB_ERR_NOCONV, PB_ERR_UNSUP = range(6)
 PREC_FP64, PREC_MIXED = 0, 1
-LU_FP64, LU_FP32, LU_TC, LU_TC_CUBLAS = 0, 1, 2, 3
+LU_FP64, LU_FP32, LU_TC, LU_TC_CUBLAS, LU_TC_PIVOTED, LU_LDLT = 0, 1, 2, 3, 4, 5
 FORM_AUTO, FORM_FULL, FORM_REDUCED = 0, 1, 2
 
 _vp = C.c_void_p

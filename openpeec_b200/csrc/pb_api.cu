@@ -537,11 +537,14 @@ int pb_lu_decomp_batched_dev(int n, int nb, double *a_dev, int *piv_dev, int *in
 int pb_lu_decomp_batched32_dev(int n, int nb, float *a_dev, int *piv_dev, int *info_host, int lu)
 {
     if (n <= 0 || nb <= 0 || !a_dev || !piv_dev || !info_host) { pb_set_error("pb_lu_decomp_batched32_dev: bad argument"); return PB_ERR_ARG; }
-    if (lu != PB_LU_TC && lu != PB_LU_FP32 && lu != PB_LU_TC_CUBLAS) { pb_set_error("pb_lu_decomp_batched32_dev: bad kind %d", lu); return PB_ERR_ARG; }
+    if (lu != PB_LU_TC && lu != PB_LU_FP32 && lu != PB_LU_TC_CUBLAS && lu != PB_LU_LDLT) {
+        pb_set_error("pb_lu_decomp_batched32_dev: bad kind %d", lu);
+        return PB_ERR_ARG;
+    }
     PB_TRY(need_device());
     pb_lu_engine e;
     PB_TRY(pb_lu_engine_init(&e, nullptr));
-    e.gemm_kind = lu == PB_LU_TC ? PB_GEMM_TC : lu == PB_LU_FP32 ? PB_GEMM_FP32 : PB_GEMM_TC_BLAS;
+    e.gemm_kind = (lu == PB_LU_TC || lu == PB_LU_LDLT) ? PB_GEMM_TC : lu == PB_LU_FP32 ? PB_GEMM_FP32 : PB_GEMM_TC_BLAS;
     int *info = nullptr;
     float *emb = nullptr;
     cudaError_t ce = cudaMalloc(&info, sizeof(int) * nb);
@@ -551,7 +554,9 @@ int pb_lu_decomp_batched32_dev(int n, int nb, float *a_dev, int *piv_dev, int *i
         e.emb = emb;
     }
     if (ce != cudaSuccess) { cudaFree(info); pb_lu_engine_free(&e); return pb_cuda_fail(ce, "cudaMalloc", __FILE__, __LINE__); }
-    int r = pb_lu_factor<float>(&e, n, nb, (float2 *)a_dev, n, (long)n * n, piv_dev, info);
+    int r = lu == PB_LU_LDLT ? pb_ldl_factor(&e, n, nb, (float2 *)a_dev, n, (long)n * n, piv_dev, info)
+                             : pb_lu_factor<float>(&e, n, nb, (float2 *)a_dev, n, (long)n * n, piv_dev, info);
+    if (r == PB_ERR_UNSUP) pb_set_error("pb_lu_decomp_batched32_dev: L D L^T panel of order %d does not fit", n);
     if (r == PB_OK) {
         ce = cudaMemcpy(info_host, info, sizeof(int) * nb, cudaMemcpyDeviceToHost);
         if (ce != cudaSuccess) r = pb_cuda_fail(ce, "cudaMemcpy", __FILE__, __LINE__);

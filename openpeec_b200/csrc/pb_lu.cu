@@ -275,8 +275,9 @@ static pb_set_emulation_fn set_emulation()
 // 4 x 4 per thread, k staged in shared memory 16 at a time, FP32 fused multiply-adds.
 __global__ void __launch_bounds__(256)
 k_cgemm_simt(const float2 *__restrict__ A, int lda, const float2 *__restrict__ B, int ldb,
-             float2 *__restrict__ C, int ldc, long long stride, int m, int nc, int k)
+             float2 *__restrict__ C, int ldc, long long stride, int m, int nc, int k, int lower)
 {
+    if (lower && (int)(blockIdx.y + 1) * 64 <= (int)blockIdx.x * 64) return;   // tile above the diagonal
     __shared__ float2 As[16][65];               // [kk][row], padded against bank conflicts
     __shared__ float2 Bs[16][64];               // [kk][col]
     const long long bo = (long long)blockIdx.z * stride;
@@ -365,7 +366,7 @@ static int gemm_sub_cublas_bf16x9(pb_lu_engine *e, int m, int nc, int k, const f
 }
 
 int pb_cgemm_sub(pb_lu_engine *e, int m, int nc, int k, const float2 *A, int lda, const float2 *B,
-                 int ldb, float2 *Cm, int ldc, long long stride, int nb)
+                 int ldb, float2 *Cm, int ldc, long long stride, int nb, int lower)
 {
     if (m <= 0 || nc <= 0 || k <= 0 || nb <= 0) return PB_OK;
     if (e->gemm_kind == PB_GEMM_TC && m >= 128 && nc >= 128 && k >= 16 &&
@@ -376,14 +377,14 @@ int pb_cgemm_sub(pb_lu_engine *e, int m, int nc, int k, const float2 *A, int lda
         }
         e->launches++;
         e->tc_used = 1;
-        return pb_cgemm_tc(m, nc, k, A, lda, B, ldb, Cm, ldc, stride, nb, e->tc_err, e->stream);
+        return pb_cgemm_tc(m, nc, k, A, lda, B, ldb, Cm, ldc, stride, nb, e->tc_err, e->stream, lower);
     }
     if (e->gemm_kind == PB_GEMM_TC_BLAS) {
         const int r = gemm_sub_cublas_bf16x9(e, m, nc, k, A, lda, B, ldb, Cm, ldc, stride, nb);
         if (r != PB_ERR_UNSUP) return r;
     }
     k_cgemm_simt<<<dim3(ceil_div(nc, 64), ceil_div(m, 64), nb), 256, 0, e->stream>>>(A, lda, B, ldb, Cm, ldc,
-                                                                                       stride, m, nc, k);
+                                                                                       stride, m, nc, k, lower);
     e->launches++;
     PB_CHECK_LAUNCH();
     return PB_OK;
@@ -549,6 +550,174 @@ int pb_lu_factor(pb_lu_engine *e, int n, int nb, T2_t<T> *a, int ld, long stride
 }
 template int pb_lu_factor<float>(pb_lu_engine *, int, int, float2 *, int, long, int *, int *);
 template int pb_lu_factor<double>(pb_lu_engine *, int, int, double2 *, int, long, int *, int *);
+
+// ---------------------------------------------------------------- complex-symmetric LDL^T
+// The reduced system jw Zb + G^T P G is complex symmetric (Lp and P are). Without
+// pivoting its factorisation is A = L D L^T with U = D L^T, so the U part of an LU needs
+// no triangular solve (U12 = D1 L21^T is a scaled transpose) and the trailing updates only
+// their lower triangle: about half the flops of the pivoted LU, no row swaps. The factors
+// are stored like an unpivoted LU (unit L below, U on and above the diagonal).
+
+// Leaf: columns [k0, k0+w) (w <= 32) over rows [k0, n), SW columns at a time in shared
+// memory. The U row of a column is read from the lower triangle (U[c][j] = A[j][c] before
+// scaling), so entries above the diagonal that earlier updates skipped are never read.
+template <int SW>
+__global__ void __launch_bounds__(1024)
+k_ldl_leaf(float2 *a, int n, int ld, long long stride, int k0, int w, int *info)
+{
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const int m = n - k0;
+    float2 *spm = reinterpret_cast<float2 *>(smraw);      // [m][SW], rows k0 + r
+    float2 *urow = spm + (size_t)m * SW;                   // [SW][32]
+    const int b = blockIdx.x, tid = threadIdx.x, nt = blockDim.x;
+    a += (long long)b * stride;
+    for (int s0 = 0; s0 < w; s0 += SW) {
+        const int sw = min(SW, w - s0), c0 = k0 + s0;
+        for (int e = tid; e < (n - c0) * sw; e += nt) {
+            const int r = c0 - k0 + e / sw, t = e - (e / sw) * sw;
+            spm[r * SW + t] = a[(long long)(k0 + r) * ld + c0 + t];
+        }
+        __syncthreads();
+        for (int t = 0; t < sw; t++) {
+            const int c = c0 + t, rc = c - k0;
+            const float2 d = spm[rc * SW + t];
+            if (tid == 0 && cmag1(d) < 1e-30 && info[b] < 0) info[b] = c;
+            const float2 dinv = safe_inv(d);
+            float2 u[SW];
+#pragma unroll
+            for (int tt = 0; tt < SW; tt++)
+                u[tt] = (tt > t && tt < sw) ? spm[(c0 + tt - k0) * SW + t] : mk2<float2>(0, 0);
+            __syncthreads();
+            for (int r = c + 1 + tid; r < n; r += nt) {
+                const float2 l = cmul(spm[(r - k0) * SW + t], dinv);
+                spm[(r - k0) * SW + t] = l;
+#pragma unroll
+                for (int tt = 0; tt < SW; tt++)
+                    if (tt > t && tt < sw && r >= c0 + tt)
+                        spm[(r - k0) * SW + tt] = cfms(spm[(r - k0) * SW + tt], l, u[tt]);
+            }
+            if (tid == 0)
+                for (int tt = t + 1; tt < sw; tt++) spm[rc * SW + tt] = u[tt];   // U row c = d L^T
+            __syncthreads();
+        }
+        for (int e = tid; e < (n - c0) * sw; e += nt) {
+            const int r = c0 - k0 + e / sw, t = e - (e / sw) * sw;
+            a[(long long)(k0 + r) * ld + c0 + t] = spm[r * SW + t];
+        }
+        const int c1 = c0 + sw, nr = k0 + w - c1;
+        if (nr > 0) {
+            // U rows of this sub-panel for the remaining leaf columns: U[c0+t][col] = d_t L[col][c0+t]
+            for (int e = tid; e < sw * nr; e += nt) {
+                const int t = e / nr, col = c1 + (e - t * nr);
+                const float2 v = cmul(spm[(c0 + t - k0) * SW + t], spm[(col - k0) * SW + t]);
+                urow[t * 32 + (col - c1)] = v;
+                a[(long long)(c0 + t) * ld + col] = v;
+            }
+            __syncthreads();
+            // trailing update of the remaining leaf columns, lower triangle only
+            const long long tot = (long long)(n - c1) * nr;
+            for (long long e = tid; e < tot; e += nt) {
+                const int r = c1 + (int)(e / nr), col = c1 + (int)(e % nr);
+                if (r < col) continue;
+                float2 v = a[(long long)r * ld + col];
+#pragma unroll
+                for (int t = 0; t < SW; t++)
+                    if (t < sw) v = cfms(v, spm[(r - k0) * SW + t], urow[t * 32 + (col - c1)]);
+                a[(long long)r * ld + col] = v;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// U12 = D1 L21^T: a[c][j] = a[c][c] * a[j][c] for c in [r0, r0+w1), j in [j0, j1); 32 x 32
+// tiles transposed through shared memory (coalesced reads along c, writes along j).
+__global__ void __launch_bounds__(256)
+k_sym_u(float2 *a, int ld, long long stride, int r0, int w1, int j0, int j1)
+{
+    __shared__ float2 t[32][33];
+    __shared__ float2 dg[32];
+    a += (long long)blockIdx.z * stride;
+    const int cb = r0 + blockIdx.y * 32, jb = j0 + blockIdx.x * 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    if (ty == 0) dg[tx] = (cb + tx < r0 + w1) ? a[(long long)(cb + tx) * ld + cb + tx] : mk2<float2>(0, 0);
+    for (int jj = ty; jj < 32; jj += 8) {
+        const int j = jb + jj, c = cb + tx;
+        t[jj][tx] = (j < j1 && c < r0 + w1) ? a[(long long)j * ld + c] : mk2<float2>(0, 0);
+    }
+    __syncthreads();
+    for (int cc = ty; cc < 32; cc += 8) {
+        const int c = cb + cc, j = jb + tx;
+        if (c < r0 + w1 && j < j1) a[(long long)c * ld + j] = cmul(dg[cc], t[tx][cc]);
+    }
+}
+
+static int ldl_sw(int m, size_t *smem)
+{
+    const size_t avail = (size_t)pb_smem_cap() - 1024;
+    const int opts[5] = {8, 6, 4, 2, 1};
+    for (int i = 0; i < 5; i++) {
+        const size_t need = ((size_t)m * opts[i] + (size_t)opts[i] * 32) * sizeof(float2);
+        if (need <= avail) { *smem = need; return opts[i]; }
+    }
+    return 0;
+}
+
+template <int SW>
+static int launch_ldl_leaf(pb_lu_engine *e, float2 *a, int n, int ld, long long stride, int nb, int k0, int w,
+                           int *info, size_t smem)
+{
+    static std::atomic<unsigned long long> attr_set{0};   // per device
+    PB_TRY(pb_smem_optin(k_ldl_leaf<SW>, pb_smem_cap() - 1024, attr_set));
+    const int m = n - k0, nt = std::min(1024, std::max(128, (m + 31) / 32 * 32));
+    k_ldl_leaf<SW><<<nb, nt, smem, e->stream>>>(a, n, ld, stride, k0, w, info);
+    e->launches++;
+    PB_CHECK_LAUNCH();
+    return PB_OK;
+}
+
+static int ldl_rec(pb_lu_engine *e, float2 *a, int n, int ld, long long stride, int nb, int k0, int w, int *info,
+                   int sw, size_t smem)
+{
+    if (w <= 32) {
+        switch (sw) {
+        case 8: return launch_ldl_leaf<8>(e, a, n, ld, stride, nb, k0, w, info, smem);
+        case 6: return launch_ldl_leaf<6>(e, a, n, ld, stride, nb, k0, w, info, smem);
+        case 4: return launch_ldl_leaf<4>(e, a, n, ld, stride, nb, k0, w, info, smem);
+        case 2: return launch_ldl_leaf<2>(e, a, n, ld, stride, nb, k0, w, info, smem);
+        default: return launch_ldl_leaf<1>(e, a, n, ld, stride, nb, k0, w, info, smem);
+        }
+    }
+    const int w1 = ((w / 2 + 31) / 32) * 32, w2 = w - w1;
+    PB_TRY(ldl_rec(e, a, n, ld, stride, nb, k0, w1, info, sw, smem));
+    k_sym_u<<<dim3(ceil_div(w2, 32), ceil_div(w1, 32), nb), 256, 0, e->stream>>>(a, ld, stride, k0, w1, k0 + w1,
+                                                                                 k0 + w);
+    e->launches++;
+    PB_CHECK_LAUNCH();
+    PB_TRY(pb_cgemm_sub(e, n - k0 - w1, w2, w1, a + (long long)(k0 + w1) * ld + k0, ld, a + (long long)k0 * ld + k0 + w1,
+                        ld, a + (long long)(k0 + w1) * ld + k0 + w1, ld, stride, nb, 1));
+    return ldl_rec(e, a, n, ld, stride, nb, k0 + w1, w2, info, sw, smem);
+}
+
+__global__ void k_iota_piv(int *piv, int n, int nb)
+{
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < (long long)n * nb) piv[i] = (int)(i % n);
+}
+
+int pb_ldl_factor(pb_lu_engine *e, int n, int nb, float2 *a, int ld, long stride, int *piv, int *info)
+{
+    if (n <= 0 || nb <= 0) return PB_OK;
+    size_t smem = 0;
+    const int sw = ldl_sw(n, &smem);
+    if (sw == 0) return PB_ERR_UNSUP;
+    k_fill_int<<<ceil_div(nb, 256), 256, 0, e->stream>>>(info, -1, nb);
+    k_iota_piv<<<ceil_div((long long)n * nb, 256), 256, 0, e->stream>>>(piv, n, nb);
+    e->launches += 2;
+    PB_CHECK_LAUNCH();
+    PB_TRY(ldl_rec(e, a, n, ld, stride, nb, 0, n, info, sw, smem));
+    return check_tc(e);
+}
 
 // ---------------------------------------------------------------- permutation
 __global__ void k_perm(const int *piv, int *perm, int n, int nb)

@@ -32,8 +32,10 @@ struct pb_lu_engine {
 
 // C (m x nc) -= A (m x k) * B (k x nc), complex FP32, row-major, batched with one stride,
 // on the engine's stream with the engine's kernel choice (PB_GEMM_FP32 / TC / TC_BLAS).
+// lower = 1: only entries with row >= column (C-local indices) are needed; tiles that lie
+// entirely above that diagonal are skipped (the others are computed in full).
 int pb_cgemm_sub(pb_lu_engine *e, int m, int nc, int k, const float2 *A, int lda, const float2 *B,
-                 int ldb, float2 *C, int ldc, long long stride, int nb);
+                 int ldb, float2 *C, int ldc, long long stride, int nb, int lower = 0);
 
 int pb_lu_engine_init(pb_lu_engine *e, cudaStream_t s);
 void pb_lu_engine_free(pb_lu_engine *e);
@@ -44,6 +46,14 @@ void pb_lu_engine_free(pb_lu_engine *e);
 template <typename T>
 int pb_lu_factor(pb_lu_engine *e, int n, int nb, typename cplx_t<T>::type *a, int ld,
                  long stride, int *piv, int *info);
+
+// Complex-symmetric factorisation A = L D L^T without pivoting, FP32, for nb matrices as
+// pb_lu_factor (only the lower triangle of A is read). The result is stored like an
+// unpivoted LU (unit L below the diagonal, U = D L^T on and above it) and piv is the
+// identity, so pb_lu_perm and the LU solves apply unchanged. Returns PB_ERR_UNSUP when the
+// panel does not fit in shared memory (orders above ~28 000); info as pb_lu_factor (a
+// zero diagonal). Growth is not controlled: callers refine against the FP64 matrix.
+int pb_ldl_factor(pb_lu_engine *e, int n, int nb, float2 *a, int ld, long stride, int *piv, int *info);
 
 // Row permutation perm[b*n + i] (row i of P*b comes from row perm[i]) from pivots.
 int pb_lu_perm(pb_lu_engine *e, int n, int nb, const int *piv, int *perm);

@@ -432,7 +432,8 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
     const int fill32 = (o.fill_prec == PB_PREC_MIXED);
     const double tol = o.refine_tol > 0 ? o.refine_tol : 1e-12;
     const int maxit = o.refine_maxit > 0 ? o.refine_maxit : 30;
-    c->lu.gemm_kind = (o.lu == PB_LU_TC) ? PB_GEMM_TC : (o.lu == PB_LU_TC_CUBLAS) ? PB_GEMM_TC_BLAS
+    c->lu.gemm_kind = (o.lu == PB_LU_TC || o.lu == PB_LU_TC_PIVOTED) ? PB_GEMM_TC
+                    : (o.lu == PB_LU_TC_CUBLAS) ? PB_GEMM_TC_BLAS
                     : (o.lu == PB_LU_FP32) ? PB_GEMM_FP32 : PB_GEMM_FP64;
     const long launches0 = c->launches + c->lu.launches;
 
@@ -442,6 +443,19 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
     const int n = (form == PB_FORM_REDUCED) ? ns : c->nfull;
     const cudaStream_t st = c->stream;
     if (n <= 0) { pb_set_error("pb_sweep: empty system"); return PB_ERR_ARG; }
+    // FP32 factorisation of the mixed path: the reduced system is complex symmetric, so
+    // PB_LU_TC factors it as L D L^T without pivoting (half the flops, no swaps; refinement
+    // against the FP64 matrix and the FP64 fall back cover the missing pivoting); every
+    // other case takes the pivoted LU
+    const bool sym32 = (form == PB_FORM_REDUCED && o.lu == PB_LU_TC);
+    auto factor32 = [&](int nm, float2 *a32, long long strd, int *piv, int *info) -> int {
+        if (sym32) {
+            const int r = pb_ldl_factor(&c->lu, n, nm, a32, n, strd, piv, info);
+            if (r != PB_ERR_UNSUP) return r;
+        }
+        return pb_lu_factor<float>(&c->lu, n, nm, a32, n, strd, piv, info);
+    };
+    auto flops32 = [&](int nm) { return (sym32 ? 4.0 : 8.0) / 3.0 * (double)n * n * n * nm; };
 
     // batch size from free memory
     size_t fr = 0, tot = 0;
@@ -695,11 +709,11 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
         tLu.start(st);
         if (nd > 0) PB_TRY(pb_lu_factor<double>(&c->lu, n, nd, bM64.as<double2>(), n, nn, bPiv.as<int>(), bInfo.as<int>()));
         if (mb > 0)
-            PB_TRY(pb_lu_factor<float>(&c->lu, n, nanch, bM32.as<float2>() + (nd + aoff) * nn, n, S ? S * nn : nn,
-                                       bPiv.as<int>() + (long long)nd * n, bInfo.as<int>() + nd));
+            PB_TRY(factor32(nanch, bM32.as<float2>() + (nd + aoff) * nn, S ? S * nn : nn,
+                            bPiv.as<int>() + (long long)nd * n, bInfo.as<int>() + nd));
         PB_TRY(pb_lu_perm(&c->lu, n, nd + (mb > 0 ? nanch : 0), bPiv.as<int>(), bPerm.as<int>()));
         tLu.stop(st);
-        luflops += 8.0 / 3.0 * (double)n * n * n * (nd + (mb > 0 ? nanch : 0));
+        luflops += 8.0 / 3.0 * (double)n * n * n * nd + (mb > 0 ? flops32(nanch) : 0.0);
         lu_count += nd + (mb > 0 ? nanch : 0);
         PB_CUDA(cudaMemcpyAsync(infoh.data(), bInfo.p, sizeof(int) * nb, cudaMemcpyDeviceToHost, st));
         PB_CUDA(cudaStreamSynchronize(st));
@@ -775,11 +789,10 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
                         PB_CUDA(cudaMemcpyAsync(m32 + t * nn, m32 + redo[t] * nn, sizeof(float2) * nn,
                                                 cudaMemcpyDeviceToDevice, st));
                 tLu.start(st);
-                PB_TRY(pb_lu_factor<float>(&c->lu, n, nr, m32, n, nn, bPiv.as<int>() + (long long)nd * n,
-                                           bInfo.as<int>() + nd));
+                PB_TRY(factor32(nr, m32, nn, bPiv.as<int>() + (long long)nd * n, bInfo.as<int>() + nd));
                 PB_TRY(pb_lu_perm(&c->lu, n, nr, bPiv.as<int>() + (long long)nd * n, bPerm.as<int>() + (long long)nd * n));
                 tLu.stop(st);
-                luflops += 8.0 / 3.0 * (double)n * n * n * nr;
+                luflops += flops32(nr);
                 lu_count += nr;
                 std::vector<int> rinfo(nr);
                 PB_CUDA(cudaMemcpyAsync(rinfo.data(), bInfo.as<int>() + nd, sizeof(int) * nr, cudaMemcpyDeviceToHost, st));

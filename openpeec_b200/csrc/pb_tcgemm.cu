@@ -226,8 +226,11 @@ __device__ __forceinline__ uint32_t swz(int r, int c) { return (uint32_t)(r * 12
 
 __global__ void __launch_bounds__(NTHREADS, 1)
 k_cgemm_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-           float2 *__restrict__ C, int ldc, long long stride, int m, int nc, int k, int *err)
+           float2 *__restrict__ C, int ldc, long long stride, int m, int nc, int k, int *err, int lower)
 {
+    // lower: a tile whose rows all lie above its columns is not needed (symmetric updates);
+    // the whole CTA leaves before any barrier or TMEM allocation
+    if (lower && (int)(blockIdx.y + 1) * TM <= (int)blockIdx.x * TN) return;
     extern __shared__ unsigned char smraw[];
     const uint32_t raw0 = smem_u32(smraw);
     const uint32_t sb = (raw0 + 1023u) & ~1023u;         // 1024-B aligned base (swizzle atoms)
@@ -494,7 +497,7 @@ bool pb_cgemm_tc_ok(const float2 *A, int lda, const float2 *B, int ldb, const fl
 }
 
 int pb_cgemm_tc(int m, int nc, int k, const float2 *A, int lda, const float2 *B, int ldb, float2 *C, int ldc,
-                long long stride, int nb, int *err, cudaStream_t s)
+                long long stride, int nb, int *err, cudaStream_t s, int lower)
 {
     if (m <= 0 || nc <= 0 || k <= 0 || nb <= 0) return PB_OK;
     // the TMA boxes (128 rows of A, 128 complex columns of B, 16 of k) stay within the
@@ -508,7 +511,7 @@ int pb_cgemm_tc(int m, int nc, int k, const float2 *A, int lda, const float2 *B,
     PB_TRY(make_map(&tb, B, k, nc, ldb, stride, nb, 2 * TN, TK, CU_TENSOR_MAP_SWIZZLE_NONE));
     PB_TRY(pb_smem_optin(k_cgemm_tc, SMEM_BYTES, g_tc_attr));
     const dim3 grid(ceil_div(nc, TN), ceil_div(m, TM), nb);
-    k_cgemm_tc<<<grid, NTHREADS, SMEM_BYTES, s>>>(ta, tb, C, ldc, stride, m, nc, k, err);
+    k_cgemm_tc<<<grid, NTHREADS, SMEM_BYTES, s>>>(ta, tb, C, ldc, stride, m, nc, k, err, lower);
     PB_CHECK_LAUNCH();
     return PB_OK;
 }

@@ -15,4 +15,4 @@ bool pb_cgemm_tc_ok(const float2 *A, int lda, const float2 *B, int ldb, const fl
 // are accumulated in FP32 (an FP32-accurate product). err: device int, set non-zero when
 // a pipeline wait of the kernel times out (the update is then incomplete).
 int pb_cgemm_tc(int m, int nc, int k, const float2 *A, int lda, const float2 *B, int ldb,
-                float2 *C, int ldc, long long stride, int nb, int *err, cudaStream_t s);
+                float2 *C, int ldc, long long stride, int nb, int *err, cudaStream_t s, int lower = 0);

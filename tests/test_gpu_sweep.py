@@ -64,6 +64,24 @@ def test_full_and_reduced_forms_agree(name, golden):
     assert zerr(zr, zf) <= 1e-9
 
 
+@pytest.mark.parametrize("name", ["dipole_halfwave", "cfg2_small", "cfg5_small", "plate_cap"])
+def test_symmetric_and_pivoted_fp32_factorisations_agree(golden, name):
+    """PB_LU_TC factors the complex-symmetric reduced form as L D L^T without pivoting;
+    after FP64 refinement (and the FP64 fall back where it stalls) Z equals the pivoted
+    LU's and the FP64 path's within the 1e-6 bar, and the symmetric factorisation needs half
+    the flops."""
+    prob, fx = golden(name)
+    with api.Context(prob) as ctx:
+        z64, _ = ctx.sweep(fx["freqs"], fill_prec=abi.PREC_FP64, lu=abi.LU_FP64)
+        zs, ss = ctx.sweep(fx["freqs"], fill_prec=abi.PREC_MIXED, lu=abi.LU_TC)
+        zp, sp = ctx.sweep(fx["freqs"], fill_prec=abi.PREC_MIXED, lu=abi.LU_TC_PIVOTED)
+    print(name, "sym vs fp64", zerr(zs, z64), "pivoted vs fp64", zerr(zp, z64), "fallbacks", ss["fp64_fallbacks"],
+          sp["fp64_fallbacks"], "its", ss["max_iters"], sp["max_iters"])
+    assert zerr(zs, z64) <= 1e-6 and zerr(zp, z64) <= 1e-6
+    if ss["form_used"] == abi.FORM_REDUCED and ss["fp64_fallbacks"] == 0:
+        assert ss["lu_flops"] < 0.6 * sp["lu_flops"]
+
+
 @pytest.mark.parametrize("name", ["dipole_halfwave", "cfg2_small"])
 def test_full_form_mixed_lu_refines_componentwise(golden, name):
     """The full form mixes charge rows (P ~ 1e10) with KCL rows of entries 1. After one

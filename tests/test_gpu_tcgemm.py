@@ -163,6 +163,34 @@ def test_fp32_lu_with_tc_updates(n, nb):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("n,nb", [(520, 3), (1036, 2), (517, 2), (45, 4)])
+def test_fp32_ldlt_of_complex_symmetric(n, nb):
+    """L D L^T without pivoting of complex-symmetric matrices (the reduced MNA form): only the
+    lower triangle is read (the upper one holds garbage here), the factors come back as an
+    unpivoted LU with U = D L^T, piv the identity, and L U reproduces A to FP32 level."""
+    import torch
+    rng = np.random.default_rng(7 * n)
+    a = _crand(rng, (nb, n, n))
+    a = a + np.swapaxes(a, 1, 2)                       # complex symmetric
+    a += (np.arange(n)[None, :, None] == np.arange(n)[None, None, :]) * (3.0 * np.sqrt(n))
+    g = a.copy()
+    g[:, np.triu_indices(n, 1)[0], np.triu_indices(n, 1)[1]] = 1e3 + 1e3j   # never read
+    dev = torch.from_numpy(g.view(np.float32).copy()).cuda()
+    piv = torch.zeros((nb, n), dtype=torch.int32, device="cuda")
+    info = (C.c_int * nb)()
+    r = abi.lib().pb_lu_decomp_batched32_dev(n, nb, dev.data_ptr(), piv.data_ptr(), info, abi.LU_LDLT)
+    assert r == abi.PB_OK, abi.last_error()
+    assert all(v == -1 for v in info)
+    lu = dev.cpu().numpy().view(np.complex64).reshape(nb, n, n).astype(np.complex128)
+    pv = piv.cpu().numpy()
+    for b in range(nb):
+        assert np.array_equal(pv[b], np.arange(n))
+        assert _lu_backward_error(a[b], lu[b], pv[b]) < 2e-5
+        L = np.tril(lu[b], -1) + np.eye(n)
+        assert np.allclose(np.triu(lu[b]), np.diag(np.diag(lu[b])) @ L.T, rtol=0, atol=2e-5 * np.abs(a[b]).max())
+
+
+@pytest.mark.gpu
 def test_tc_update_has_no_accumulation_drift():
     """A long accumulation (k = 2048) stays as accurate as an FP32 product: the tensor
     core truncates when it adds into its accumulator, so the kernel sums TMEM only over
