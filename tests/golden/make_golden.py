@@ -265,6 +265,27 @@ def cfg5_cases():
     make_pw_case("cfg5_small_pw", text, [1e7, 1.285e9, 2.56e9])
 
 
+def make_cfg5_full_ref(freq=1e9, threads=6):
+    """Full config 5 (15 374 current cells, 6 925 charge cells) at one frequency through the
+    reference's own CLI: port S11 (Touchstone, 10 digits), Z derived from it and the
+    plane-wave open-circuit voltage (pw.csv). The dense reference solve takes about
+    50 minutes on 6 threads (setup 15 minutes)."""
+    text = configs.cfg5(0)
+    fs = ("%.6g" % freq).replace("e+0", "e").replace("e+", "e")
+    text = "\n".join(("frequency = %s %s 0" % (fs, fs)) if l.startswith("frequency") else l
+                      for l in text.splitlines()) + "\n"
+    out = run_cli(text, threads=threads)
+    s1p = [l.split() for l in out["peec.s1p"].splitlines() if l.strip() and l[0] not in "!#"]
+    s11 = complex(float(s1p[0][1]), float(s1p[0][2]))
+    pw = out["pw.csv"].splitlines()[1].split(",")
+    voc = complex(float(pw[2]), float(pw[3]))
+    z = 50.0 * (1 + s11) / (1 - s11)
+    np.savez_compressed(os.path.join(HERE, "geom", "cfg5_full_ref.npz"), freq=np.array([freq]), s11=np.array([s11]),
+                        z=np.array([z]), voc=np.array([voc]), peec=np.array(text), s1p=np.array(out["peec.s1p"]),
+                        pw_csv=np.array(out["pw.csv"]))
+    print("cfg5 full reference: Z", z, "Voc", voc)
+
+
 def comp_cases():
     make_comp_case("compress_wire", sample("compress_wire.peec"), [1e6])
     make_comp_case("compress_plate", sample("compress_plate.peec"), [1e8])
@@ -392,11 +413,15 @@ def main():
     ap.add_argument("--cfg4-only", action="store_true", help="only config 4 at full size (minutes)")
     ap.add_argument("--cfg5-only", action="store_true", help="only the scaled-down config-5 cases")
     ap.add_argument("--dropin-only", action="store_true", help="only the reference-CLI outputs (tests/golden/dropin)")
+    ap.add_argument("--cfg5-full", action="store_true", help="full config 5 at 1 GHz through the reference CLI (~1 h)")
     a = ap.parse_args()
     subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True,
                    stdout=subprocess.DEVNULL)
     if a.dropin_only:
         dropin_cases()
+        return
+    if a.cfg5_full:
+        make_cfg5_full_ref()
         return
     if a.cfg4_only:
         make_cfg4_full()

@@ -9,15 +9,21 @@ Fixtures (tests/golden/make_golden.py --cfg5-only, from the reference's own solv
       port Z, sampled entries, plane-wave open-circuit voltage
   geom/cfg5_full.npz                     the reference builder's discretisation of the full
       config 5 (15 374 current cells, 6 925 charge cells; N = 22 299 in the reference's
-      MNA), for the full-size runs (no reference solution at this size)
+      MNA), for the full-size runs
+  geom/cfg5_full_ref.npz                 the reference CLI's port S11 (Z) and plane-wave Voc
+      of the full config 5 at 1 GHz (make_golden.py --cfg5-full)
 The dense Z and Voc of the small case against the reference are part of test_gpu_sweep.py
 and test_planewave.py (golden lists); here the compressed path is held to them, and at
 full size the two paths to each other.
 """
+import os
+
 import numpy as np
 import pytest
 
 from conftest import load_golden
+
+HERE = os.path.dirname(os.path.abspath(__file__))
 
 pytestmark = pytest.mark.gpu
 
@@ -61,17 +67,22 @@ def test_small_compressed_planewave_matches_reference():
 
 def test_full_size_dense_sweep_and_planewave():
     """Full config 5 (15 374 current cells, 6 925 charge cells) at 1 GHz on the dense
-    batched mixed-precision path: the port Z and the plane-wave Voc, refined to FP64
-    backward error without any FP64 fall-back, and the same Z from the plain FP64 path."""
+    batched mixed-precision path against the reference's own CLI on the same input
+    (geom/cfg5_full_ref.npz: S11 to 10 digits, Z derived from it, Voc; a 50-minute dense
+    reference solve): the port Z and the plane-wave Voc within 1e-6, refined to FP64
+    backward error without any FP64 fall-back, and the plain FP64 path the same."""
     from openpeec_b200 import abi, api
     prob, _ = load_golden("cfg5_full", "geom")
-    f = np.array([1e9])
+    ref = np.load(os.path.join(HERE, "golden", "geom", "cfg5_full_ref.npz"))
+    f = ref["freq"]
     pw = (30.0, 45.0, 1, 1.0, 0.0)
     with api.Context(prob) as ctx:
         zm, stm = ctx.sweep(f, fill_prec=abi.PREC_MIXED, lu=abi.LU_TC)
         vm, _ = ctx.planewave(f, pw, fill_prec=abi.PREC_MIXED)
         zp, _ = ctx.sweep(f, fill_prec=abi.PREC_FP64, lu=abi.LU_FP64)
-    print("cfg5 full 1 GHz: Z mixed", zm.ravel(), "plain", zp.ravel(), "Voc", vm.ravel(), stm)
+    print("cfg5 full 1 GHz: Z mixed", zm.ravel(), "plain", zp.ravel(), "reference", ref["z"], "Voc", vm.ravel(),
+          "reference", ref["voc"], stm)
     assert stm["n_system"] == 15374 and stm["fp64_fallbacks"] == 0
-    assert np.all(np.isfinite(vm)) and np.abs(vm).max() > 0
+    assert rel(zm.ravel(), ref["z"]) <= 1e-6 and rel(zp.ravel(), ref["z"]) <= 1e-6
+    assert rel(vm.ravel(), ref["voc"]) <= 1e-6
     assert rel(zm, zp) <= 1e-6
