@@ -899,12 +899,12 @@ k_corr(pb_fill_geom g, KArg k, const double *st, pb_epi_args ea, double2 *ig, lo
                 if (cb >= 0 && da >= 0) { const double2 pp = P[(long long)cb * nc + da]; vr -= pp.x; vi -= pp.y; }
                 if (cb >= 0 && db >= 0) { const double2 pp = P[(long long)cb * nc + db]; vr += pp.x; vi += pp.y; }
                 double2 *m = ea.m64 + f * ea.m_stride;
-                m[(long long)i * n + j] = make_double2(vr, vi);
-                m[(long long)j * n + i] = make_double2(vr, vi);
+                m[(long long)j * n + i] = make_double2(vr, vi);           // lower (i <= j)
+                if (!ea.lower) m[(long long)i * n + j] = make_double2(vr, vi);
                 if (ea.m32) {
                     float2 *m2 = ea.m32 + f * ea.m_stride;
-                    m2[(long long)i * n + j] = make_float2((float)vr, (float)vi);
                     m2[(long long)j * n + i] = make_float2((float)vr, (float)vi);
+                    if (!ea.lower) m2[(long long)i * n + j] = make_float2((float)vr, (float)vi);
                 }
             }
         };

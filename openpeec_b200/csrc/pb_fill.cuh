@@ -44,6 +44,7 @@ struct pb_epi_args {
     const double2 *pm = nullptr;    // P(f) [f][ncell][ncell]
     long long pm_stride = 0;
     const double2 *zint = nullptr;  // [f][nseg]
+    int lower = 0;                  // REDUCED: write only the lower triangle (symmetric solves)
     double omega[PB_FMAX];
 };
 

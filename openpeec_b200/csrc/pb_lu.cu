@@ -705,6 +705,12 @@ __global__ void k_iota_piv(int *piv, int n, int nb)
     if (i < (long long)n * nb) piv[i] = (int)(i % n);
 }
 
+bool pb_ldl_supported(int n)
+{
+    size_t smem = 0;
+    return n > 0 && ldl_sw(n, &smem) > 0;
+}
+
 int pb_ldl_factor(pb_lu_engine *e, int n, int nb, float2 *a, int ld, long stride, int *piv, int *info)
 {
     if (n <= 0 || nb <= 0) return PB_OK;
@@ -1147,6 +1153,254 @@ int pb_residual_mapped(pb_lu_engine *e, int n, int nb, int nrhs, const double2 *
     const int rpb = 64;
     dim3 g(ceil_div(n, rpb), nb);
     k_residual<<<g, 256, smem, e->stream>>>(a, n, ld, stride, b, x, r, rn, bn, xn, an, nrhs, rpb, sys, cw, stage, wv);
+    e->launches++;
+    PB_CHECK_LAUNCH();
+    return PB_OK;
+}
+
+// ---------------------------------------------------------------- symmetric FP64 residual
+// r = b - A x for complex-symmetric A of which only the lower triangle (with the diagonal)
+// is read: half the bytes of k_residual. Deterministic two-phase sum:
+//  phase 1, one CTA per 32-row block R of a system: the block's rows against columns
+//  c <= i (direct part, warp-reduced per row) and, transposed, the strictly lower entries
+//  against the block's x (column partials, summed over the 8 warps in fixed order): those
+//  of columns below the block go to the scratch part[R][c], those inside the block are
+//  added to the block's own rows;
+//  phase 2, per row i: y_i = yblk_i + sum over R > block(i) of part[R][i] in order of R.
+// |A||x| and the |A| row sums (|re| + |im|, as k_residual) come along when asked for.
+constexpr int SYM_RB = 32;          // rows per block
+constexpr int SYM_CW = 128;         // columns per chunk (4 per lane)
+
+template <bool AX, bool AS>
+__global__ void __launch_bounds__(256)
+k_symres_p1(const double2 *__restrict__ a, int n, long long stride, const double2 *__restrict__ xv,
+            const int *sys, int nrb, double2 *yblk, double *axblk, double *asblk, double2 *py, double *pax,
+            double *pas)
+{
+    __shared__ double2 xb[SYM_RB];
+    __shared__ double2 tp[8][SYM_CW];
+    __shared__ double tpa[AX ? 8 : 1][SYM_CW], tps[AS ? 8 : 1][SYM_CW];
+    __shared__ double2 tin[SYM_RB], ydir[SYM_RB];
+    __shared__ double tina[SYM_RB], tins[SYM_RB], ydira[SYM_RB], ydirs[SYM_RB];
+    const int s = sys ? sys[blockIdx.y] : blockIdx.y;
+    const int R = blockIdx.x, r0 = R * SYM_RB, r1 = min(n, r0 + SYM_RB);
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    a += (long long)s * stride;
+    const double2 *x = xv + (long long)s * n;
+    if (tid < SYM_RB) {
+        xb[tid] = (r0 + tid < n) ? x[r0 + tid] : make_double2(0, 0);
+        tin[tid] = make_double2(0, 0);
+        tina[tid] = tins[tid] = 0;
+    }
+    __syncthreads();
+    double dr[4] = {0, 0, 0, 0}, di[4] = {0, 0, 0, 0}, da[4] = {0, 0, 0, 0}, ds[4] = {0, 0, 0, 0};
+    for (int c0 = 0; c0 < r1; c0 += SYM_CW) {
+        double2 xc[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const int c = c0 + lane + 32 * k;
+            xc[k] = c < r1 ? x[c] : make_double2(0, 0);
+        }
+        double tr[4] = {0, 0, 0, 0}, ti[4] = {0, 0, 0, 0}, ta[4] = {0, 0, 0, 0}, ts[4] = {0, 0, 0, 0};
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int il = 4 * w + q, i = r0 + il;
+            if (i >= n) continue;
+            const double2 *row = a + (long long)i * n;
+            const double2 xi = xb[il];
+            double2 av[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const int c = c0 + lane + 32 * k;
+                av[k] = c <= i ? row[c] : make_double2(0, 0);
+            }
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const int c = c0 + lane + 32 * k;
+                const double2 v = av[k];
+                dr[q] += v.x * xc[k].x - v.y * xc[k].y;
+                di[q] += v.x * xc[k].y + v.y * xc[k].x;
+                const double m = fabs(v.x) + fabs(v.y);
+                if (AX) da[q] += m * (fabs(xc[k].x) + fabs(xc[k].y));
+                if (AS) ds[q] += m;
+                if (c < i) {                                   // strictly lower: transposed part
+                    tr[k] += v.x * xi.x - v.y * xi.y;
+                    ti[k] += v.x * xi.y + v.y * xi.x;
+                    if (AX) ta[k] += m * (fabs(xi.x) + fabs(xi.y));
+                    if (AS) ts[k] += m;
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            tp[w][lane + 32 * k] = make_double2(tr[k], ti[k]);
+            if (AX) tpa[w][lane + 32 * k] = ta[k];
+            if (AS) tps[w][lane + 32 * k] = ts[k];
+        }
+        __syncthreads();
+        if (tid < SYM_CW) {
+            const int c = c0 + tid;
+            if (c < r1) {
+                double sr = 0, si = 0, sa = 0, ss = 0;
+#pragma unroll
+                for (int v = 0; v < 8; v++) {
+                    sr += tp[v][tid].x;
+                    si += tp[v][tid].y;
+                    if (AX) sa += tpa[v][tid];
+                    if (AS) ss += tps[v][tid];
+                }
+                if (c < r0) {
+                    const long long o = ((long long)blockIdx.y * nrb + R) * n + c;
+                    py[o] = make_double2(sr, si);
+                    if (AX) pax[o] = sa;
+                    if (AS) pas[o] = ss;
+                } else {
+                    tin[c - r0] = make_double2(sr, si);
+                    if (AX) tina[c - r0] = sa;
+                    if (AS) tins[c - r0] = ss;
+                }
+            }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        for (int o = 16; o > 0; o >>= 1) {
+            dr[q] += __shfl_down_sync(0xffffffffu, dr[q], o);
+            di[q] += __shfl_down_sync(0xffffffffu, di[q], o);
+            if (AX) da[q] += __shfl_down_sync(0xffffffffu, da[q], o);
+            if (AS) ds[q] += __shfl_down_sync(0xffffffffu, ds[q], o);
+        }
+        if (lane == 0) {
+            ydir[4 * w + q] = make_double2(dr[q], di[q]);
+            ydira[4 * w + q] = da[q];
+            ydirs[4 * w + q] = ds[q];
+        }
+    }
+    __syncthreads();
+    if (tid < SYM_RB && r0 + tid < n) {
+        const long long o = (long long)blockIdx.y * n + r0 + tid;
+        yblk[o] = make_double2(ydir[tid].x + tin[tid].x, ydir[tid].y + tin[tid].y);
+        if (AX) axblk[o] = ydira[tid] + tina[tid];
+        if (AS) asblk[o] = ydirs[tid] + tins[tid];
+    }
+}
+
+template <bool AX, bool AS>
+__global__ void __launch_bounds__(256)
+k_symres_p2(int n, int nrb, const int *sys, const double2 *yblk, const double *axblk, const double *asblk,
+            const double2 *py, const double *pax, const double *pas, const double2 *bv, const double2 *xv,
+            double2 *rv, double *rn, double *bn, double *xn, double *an, double *wv)
+{
+    const int s = sys ? sys[blockIdx.y] : blockIdx.y;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double mr = 0, mb = 0, mx = 0, ms = 0;
+    if (i < n) {
+        const long long o = (long long)blockIdx.y * n + i;
+        double2 y = yblk[o];
+        double sa = AX ? axblk[o] : 0, ss = AS ? asblk[o] : 0;
+        for (int R = i / SYM_RB + 1; R < nrb; R++) {
+            const long long p = ((long long)blockIdx.y * nrb + R) * n + i;
+            const double2 t = py[p];
+            y.x += t.x;
+            y.y += t.y;
+            if (AX) sa += pax[p];
+            if (AS) ss += pas[p];
+        }
+        const long long g = (long long)s * n + i;
+        const double2 b = bv[g], xx = xv[g];
+        const double2 r = make_double2(b.x - y.x, b.y - y.y);
+        rv[g] = r;
+        mr = fmax(fabs(r.x), fabs(r.y));
+        mb = fmax(fabs(b.x), fabs(b.y));
+        mx = fmax(fabs(xx.x), fabs(xx.y));
+        ms = ss;
+        if (AX && wv) wv[g] = sa + fabs(b.x) + fabs(b.y);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        mr = fmax(mr, __shfl_down_sync(0xffffffffu, mr, o));
+        mb = fmax(mb, __shfl_down_sync(0xffffffffu, mb, o));
+        mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, o));
+        ms = fmax(ms, __shfl_down_sync(0xffffffffu, ms, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomic_max_pos(&rn[s], mr);
+        atomic_max_pos(&bn[s], mb);
+        if (xn) atomic_max_pos(&xn[s], mx);
+        if (AS && an) atomic_max_pos(&an[s], ms);
+    }
+}
+
+size_t pb_sym_residual_scratch(int n, int nb)
+{
+    const int nrb = (n + SYM_RB - 1) / SYM_RB;
+    return (size_t)nb * ((size_t)nrb * n * 32 + (size_t)n * 32);
+}
+
+int pb_sym_residual_mapped(pb_lu_engine *e, int n, int nb, const double2 *a, long stride, const double2 *b,
+                           const double2 *x, double2 *r, double *rn, double *bn, double *xn, double *an, int nall,
+                           const int *sys, double *wv, void *scratch)
+{
+    PB_CUDA(cudaMemsetAsync(rn, 0, sizeof(double) * nall, e->stream));
+    PB_CUDA(cudaMemsetAsync(bn, 0, sizeof(double) * nall, e->stream));
+    if (xn) PB_CUDA(cudaMemsetAsync(xn, 0, sizeof(double) * nall, e->stream));
+    if (an) PB_CUDA(cudaMemsetAsync(an, 0, sizeof(double) * nall, e->stream));
+    if (nb <= 0) return PB_OK;
+    const int nrb = (n + SYM_RB - 1) / SYM_RB;
+    // scratch per system: part y [nrb][n] complex, part |A||x| and |A| [nrb][n] real each,
+    // the block sums [n] complex + 2 real
+    double2 *py = reinterpret_cast<double2 *>(scratch);
+    double *pax = reinterpret_cast<double *>(py + (size_t)nb * nrb * n);
+    double *pas = pax + (size_t)nb * nrb * n;
+    double2 *yblk = reinterpret_cast<double2 *>(pas + (size_t)nb * nrb * n);
+    double *axblk = reinterpret_cast<double *>(yblk + (size_t)nb * n);
+    double *asblk = axblk + (size_t)nb * n;
+    const bool ax = wv != nullptr, as = an != nullptr;
+    const dim3 g1(nrb, nb), g2(ceil_div(n, 256), nb);
+#define PB_SYMRES(AXV, ASV)                                                                                          \
+    do {                                                                                                             \
+        k_symres_p1<AXV, ASV><<<g1, 256, 0, e->stream>>>(a, n, stride, x, sys, nrb, yblk, axblk, asblk, py, pax, pas); \
+        k_symres_p2<AXV, ASV><<<g2, 256, 0, e->stream>>>(n, nrb, sys, yblk, axblk, asblk, py, pax, pas, b, x, r, rn,  \
+                                                         bn, xn, an, wv);                                            \
+    } while (0)
+    if (ax && as) PB_SYMRES(true, true);
+    else if (ax) PB_SYMRES(true, false);
+    else if (as) PB_SYMRES(false, true);
+    else PB_SYMRES(false, false);
+#undef PB_SYMRES
+    e->launches += 2;
+    PB_CHECK_LAUNCH();
+    return PB_OK;
+}
+
+// Upper triangle := lower triangle (transpose) for nb FP64 matrices of order n (32 x 32 tiles
+// through shared memory): the symmetric systems whose fill wrote only the lower triangle,
+// before a pivoted factorisation that reads both.
+__global__ void __launch_bounds__(256)
+k_sym_mirror(double2 *a, int n, long long stride)
+{
+    __shared__ double2 t[32][33];
+    const int bx = blockIdx.x, by = blockIdx.y;     // tile column, tile row; upper tiles only
+    if (bx < by) return;
+    a += (long long)blockIdx.z * stride;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    // read the lower tile (rows bx*32.., cols by*32..), write its transpose into the upper one
+    for (int r = ty; r < 32; r += 8) {
+        const int i = bx * 32 + r, j = by * 32 + tx;
+        t[r][tx] = (i < n && j < n) ? a[(long long)i * n + j] : make_double2(0, 0);
+    }
+    __syncthreads();
+    for (int r = ty; r < 32; r += 8) {
+        const int i = by * 32 + r, j = bx * 32 + tx;       // upper entry (i, j) = lower (j, i)
+        if (i < n && j < n && j > i) a[(long long)i * n + j] = t[tx][r];
+    }
+}
+
+int pb_sym_mirror(pb_lu_engine *e, int n, int nb, double2 *a, long long stride)
+{
+    if (n <= 0 || nb <= 0) return PB_OK;
+    const int nt = (n + 31) / 32;
+    k_sym_mirror<<<dim3(nt, nt, nb), 256, 0, e->stream>>>(a, n, stride);
     e->launches++;
     PB_CHECK_LAUNCH();
     return PB_OK;

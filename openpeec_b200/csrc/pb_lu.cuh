@@ -54,6 +54,7 @@ int pb_lu_factor(pb_lu_engine *e, int n, int nb, typename cplx_t<T>::type *a, in
 // panel does not fit in shared memory (orders above ~28 000); info as pb_lu_factor (a
 // zero diagonal). Growth is not controlled: callers refine against the FP64 matrix.
 int pb_ldl_factor(pb_lu_engine *e, int n, int nb, float2 *a, int ld, long stride, int *piv, int *info);
+bool pb_ldl_supported(int n);     // the panel of order n fits (pb_ldl_factor will not return UNSUP)
 
 // Row permutation perm[b*n + i] (row i of P*b comes from row perm[i]) from pivots.
 int pb_lu_perm(pb_lu_engine *e, int n, int nb, const int *piv, int *perm);
@@ -85,6 +86,17 @@ int pb_lu_solve_mapped(pb_lu_engine *e, int n, int nb, int nrhs,
 int pb_residual_mapped(pb_lu_engine *e, int n, int nb, int nrhs, const double2 *a, int ld, long stride,
                        const double2 *b, const double2 *x, double2 *r, double *rn, double *bn, double *xn,
                        double *an, int nall, const int *sys, double *cw = nullptr, double *wv = nullptr);
+
+// pb_residual_mapped for one right-hand side of complex-symmetric systems of which only the
+// lower triangle is read (half the bytes); deterministic. Norms as pb_residual_mapped (an,
+// wv optional: then |A| row sums / (|A||x| + |b|) are formed too). scratch: device buffer
+// of pb_sym_residual_scratch(n, nb) bytes.
+size_t pb_sym_residual_scratch(int n, int nb);
+int pb_sym_residual_mapped(pb_lu_engine *e, int n, int nb, const double2 *a, long stride, const double2 *b,
+                           const double2 *x, double2 *r, double *rn, double *bn, double *xn, double *an, int nall,
+                           const int *sys, double *wv, void *scratch);
+// Upper triangle := transposed lower triangle of nb FP64 matrices (stride in elements).
+int pb_sym_mirror(pb_lu_engine *e, int n, int nb, double2 *a, long long stride);
 
 // y = A x for the nb systems sys[0..nb) (nullptr = 0..nb), nrhs vectors each.
 int pb_matvec_mapped(pb_lu_engine *e, int n, int nb, int nrhs, const double2 *a, int ld, long stride,

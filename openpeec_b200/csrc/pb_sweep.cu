@@ -456,6 +456,10 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
         return pb_lu_factor<float>(&c->lu, n, nm, a32, n, strd, piv, info);
     };
     auto flops32 = [&](int nm) { return (sym32 ? 4.0 : 8.0) / 3.0 * (double)n * n * n * nm; };
+    // symmetric storage: with one right-hand side and no LU reuse the fill writes only the
+    // lower triangle of the FP64 and FP32 systems, the refinement residual reads only that
+    // (pb_sym_residual_mapped), and the few FP64 factorisations mirror it first
+    const bool lower = sym32 && pb_ldl_supported(n) && !rhs_fixed && o.accel < 2 && (pw || np == 1);
 
     // batch size from free memory
     size_t fr = 0, tot = 0;
@@ -529,6 +533,8 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
         PB_TRY(bEta.alloc((size_t)B * 8));
         PB_TRY(bZp.alloc((size_t)2 * B * np * nr * 16 + 16));
     }
+    DevBuf bSymScr(cs + 29);                      // partial sums of the symmetric residual
+    if (lower) PB_TRY(bSymScr.alloc(pb_sym_residual_scratch(n, B)));
     DevBuf bQ(cs + 25);                           // cell charges of one batch (distribution)
     if (cellq && !pw && !rhs_fixed && c->capacitance && nc > 0) PB_TRY(bQ.alloc((size_t)B * np * nc * 16));
 
@@ -651,6 +657,7 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
                 ea.pm = bP.as<double2>() + (long long)f * nc * nc;
                 ea.pm_stride = (long long)nc * nc;
                 ea.zint = bZint.as<double2>() + (long long)f * ns;
+                ea.lower = lower ? 1 : 0;
                 PB_TRY(pb_lp_corr(c->g, nf, kw, fill32, bStLp.as<double>(), PB_EPI_REDUCED, ea, st,
                                   &c->launches, &samples));
             } else {
@@ -707,6 +714,7 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
         for (int q = 0; q < mb; q++)
             lu_of[q] = S ? std::min(nanch - 1, std::max(0, (int)std::floor((q - aoff) / (double)S + 0.5))) : q;
         tLu.start(st);
+        if (nd > 0 && lower) PB_TRY(pb_sym_mirror(&c->lu, n, nd, bM64.as<double2>(), nn));
         if (nd > 0) PB_TRY(pb_lu_factor<double>(&c->lu, n, nd, bM64.as<double2>(), n, nn, bPiv.as<int>(), bInfo.as<int>()));
         if (mb > 0)
             PB_TRY(factor32(nanch, bM32.as<float2>() + (nd + aoff) * nn, S ? S * nn : nn,
@@ -844,11 +852,18 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
                 for (int q = 0; q < mb; q++) if (state[nd + q] == 0) act.push_back(q);
                 if (act.empty()) break;
                 PB_CUDA(cudaMemcpyAsync(bSys.p, act.data(), sizeof(int) * act.size(), cudaMemcpyHostToDevice, st));
-                PB_TRY(pb_residual_mapped(&c->lu, n, (int)act.size(), nr, m64, n, nn, bRhs.as<double2>() + vo,
-                                          bX.as<double2>() + vo, bR.as<double2>() + vo, bRn.as<double>(),
-                                          bBn.as<double>(), bXn.as<double>(), it == 1 ? bAn.as<double>() : nullptr,
-                                          mb, bSys.as<int>(), cwise ? bCw.as<double>() : nullptr,
-                                          probe ? bW.as<double>() : nullptr));
+                if (lower)
+                    PB_TRY(pb_sym_residual_mapped(&c->lu, n, (int)act.size(), m64, nn, bRhs.as<double2>() + vo,
+                                                  bX.as<double2>() + vo, bR.as<double2>() + vo, bRn.as<double>(),
+                                                  bBn.as<double>(), bXn.as<double>(),
+                                                  it == 1 ? bAn.as<double>() : nullptr, mb, bSys.as<int>(),
+                                                  probe ? bW.as<double>() : nullptr, bSymScr.p));
+                else
+                    PB_TRY(pb_residual_mapped(&c->lu, n, (int)act.size(), nr, m64, n, nn, bRhs.as<double2>() + vo,
+                                              bX.as<double2>() + vo, bR.as<double2>() + vo, bRn.as<double>(),
+                                              bBn.as<double>(), bXn.as<double>(), it == 1 ? bAn.as<double>() : nullptr,
+                                              mb, bSys.as<int>(), cwise ? bCw.as<double>() : nullptr,
+                                              probe ? bW.as<double>() : nullptr));
                 PB_CUDA(cudaMemcpyAsync(rnh.data(), bRn.p, sizeof(double) * mb * nr, cudaMemcpyDeviceToHost, st));
                 PB_CUDA(cudaMemcpyAsync(bnh.data(), bBn.p, sizeof(double) * mb * nr, cudaMemcpyDeviceToHost, st));
                 PB_CUDA(cudaMemcpyAsync(xnh.data(), bXn.p, sizeof(double) * mb * nr, cudaMemcpyDeviceToHost, st));
@@ -956,6 +971,7 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
                                             bRhs.as<double2>() + (long long)q * nr * n, sizeof(double2) * nr * n,
                                             cudaMemcpyDeviceToDevice, st));
                 }
+                if (lower) PB_TRY(pb_sym_mirror(&c->lu, n, ng, scr, nn));
                 PB_TRY(pb_lu_factor<double>(&c->lu, n, ng, scr, n, nn, bPiv.as<int>(), bInfo.as<int>()));
                 lu_count += ng;
                 PB_TRY(pb_lu_perm(&c->lu, n, ng, bPiv.as<int>(), bPerm.as<int>()));
