@@ -61,11 +61,12 @@ int pb_lu_perm(pb_lu_engine *e, int n, int nb, const int *piv, int *perm);
 
 // Solve A x = r for nb matrices x nrhs right-hand sides using the factors (type TF).
 // r, x: FP64 complex [nb][nrhs][n] device (may alias). Each RHS is scaled by its
-// max-norm before conversion to TF and scaled back afterwards.
+// max-norm before conversion to TF and scaled back afterwards. operm = 1: the factors are
+// of the symmetrically permuted P A P^T (pb_sym_order), x = P^T y (x and r must not alias).
 template <typename TF>
 int pb_lu_solve_batched(pb_lu_engine *e, int n, int nb, int nrhs,
                         const typename cplx_t<TF>::type *lu, int ld, long stride,
-                        const int *perm, const double2 *r, double2 *x);
+                        const int *perm, const double2 *r, double2 *x, int operm = 0);
 
 // Explicit inverse X = A^-1 (row-major n x n, device) of one FP64 system from its factors
 // (pb_lu_factor / pb_lu_perm), for a matrix whose factors serve many solves.
@@ -79,7 +80,7 @@ template <typename TF>
 int pb_lu_solve_mapped(pb_lu_engine *e, int n, int nb, int nrhs,
                        const typename cplx_t<TF>::type *lu, int ld, long stride,
                        const int *perm, const double2 *r, double2 *x, const int *sys,
-                       const int *lu_of);
+                       const int *lu_of, int operm = 0);
 
 // pb_residual for the nb systems sys[0..nb) of a batch of nall; the norms of the other
 // systems are left at 0. wv (optional, laid out like r): (|A||x| + |b|) per row.
@@ -95,6 +96,11 @@ size_t pb_sym_residual_scratch(int n, int nb);
 int pb_sym_residual_mapped(pb_lu_engine *e, int n, int nb, const double2 *a, long stride, const double2 *b,
                            const double2 *x, double2 *r, double *rn, double *bn, double *xn, double *an, int nall,
                            const int *sys, double *wv, void *scratch);
+// Symmetric ordering for the unpivoted L D L^T: per system perm = the unknowns by decreasing
+// |A_kk| / sum_j |A_kj| (a: lower-triangle FP64 systems), and a32 (lower triangle) = the
+// permuted matrix in FP32. n <= 16384 (else PB_ERR_UNSUP); scratch as pb_sym_residual.
+int pb_sym_order(pb_lu_engine *e, int n, int nb, const double2 *a, long long stride, float2 *a32, int *perm,
+                 void *scratch);
 // Upper triangle := transposed lower triangle of nb FP64 matrices (stride in elements).
 int pb_sym_mirror(pb_lu_engine *e, int n, int nb, double2 *a, long long stride);
 

@@ -460,6 +460,9 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
     // lower triangle of the FP64 and FP32 systems, the refinement residual reads only that
     // (pb_sym_residual_mapped), and the few FP64 factorisations mirror it first
     const bool lower = sym32 && pb_ldl_supported(n) && !rhs_fixed && o.accel < 2 && (pw || np == 1);
+    // and the unpivoted factorisation runs on a static symmetric ordering of each system
+    // (decreasing diagonal dominance, pb_sym_order), formed from the FP64 lower triangle
+    const bool reorder = lower && n <= 16384;
 
     // batch size from free memory
     size_t fr = 0, tot = 0;
@@ -533,8 +536,9 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
         PB_TRY(bEta.alloc((size_t)B * 8));
         PB_TRY(bZp.alloc((size_t)2 * B * np * nr * 16 + 16));
     }
-    DevBuf bSymScr(cs + 29);                      // partial sums of the symmetric residual
+    DevBuf bSymScr(cs + 29), bOrd(cs + 30);       // partial sums of the symmetric residual; orderings
     if (lower) PB_TRY(bSymScr.alloc(pb_sym_residual_scratch(n, B)));
+    if (reorder) PB_TRY(bOrd.alloc((size_t)B * n * sizeof(int)));
     DevBuf bQ(cs + 25);                           // cell charges of one batch (distribution)
     if (cellq && !pw && !rhs_fixed && c->capacitance && nc > 0) PB_TRY(bQ.alloc((size_t)B * np * nc * 16));
 
@@ -652,7 +656,7 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
             for (int q = 0; q < nf; q++) ea.omega[q] = 2 * PB_PI * fb[f + q];
             if (form == PB_FORM_REDUCED) {
                 ea.m64 = bM64.as<double2>() + (long long)f * n * n;
-                ea.m32 = mixed ? bM32.as<float2>() + (long long)f * n * n : nullptr;
+                ea.m32 = (mixed && !reorder) ? bM32.as<float2>() + (long long)f * n * n : nullptr;
                 ea.m_stride = (long long)n * n;
                 ea.pm = bP.as<double2>() + (long long)f * nc * nc;
                 ea.pm_stride = (long long)nc * nc;
@@ -714,12 +718,18 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
         for (int q = 0; q < mb; q++)
             lu_of[q] = S ? std::min(nanch - 1, std::max(0, (int)std::floor((q - aoff) / (double)S + 0.5))) : q;
         tLu.start(st);
+        if (reorder && mb > 0)
+            PB_TRY(pb_sym_order(&c->lu, n, mb, bM64.as<double2>() + nd * nn, nn, bM32.as<float2>() + nd * nn,
+                                bOrd.as<int>() + (long long)nd * n, bSymScr.p));
         if (nd > 0 && lower) PB_TRY(pb_sym_mirror(&c->lu, n, nd, bM64.as<double2>(), nn));
         if (nd > 0) PB_TRY(pb_lu_factor<double>(&c->lu, n, nd, bM64.as<double2>(), n, nn, bPiv.as<int>(), bInfo.as<int>()));
         if (mb > 0)
             PB_TRY(factor32(nanch, bM32.as<float2>() + (nd + aoff) * nn, S ? S * nn : nn,
                             bPiv.as<int>() + (long long)nd * n, bInfo.as<int>() + nd));
         PB_TRY(pb_lu_perm(&c->lu, n, nd + (mb > 0 ? nanch : 0), bPiv.as<int>(), bPerm.as<int>()));
+        if (reorder && mb > 0)
+            PB_CUDA(cudaMemcpyAsync(bPerm.as<int>() + (long long)nd * n, bOrd.as<int>() + (long long)nd * n,
+                                    sizeof(int) * (size_t)mb * n, cudaMemcpyDeviceToDevice, st));
         tLu.stop(st);
         luflops += 8.0 / 3.0 * (double)n * n * n * nd + (mb > 0 ? flops32(nanch) : 0.0);
         lu_count += nd + (mb > 0 ? nanch : 0);
@@ -837,7 +847,7 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
             for (int q = 0; q < mb; q++)
                 if (infoh[nd + q] >= 0) state[nd + q] = 2;          // zero FP32 pivot: go FP64
             PB_TRY(pb_lu_solve_batched<float>(&c->lu, n, mb, nr, m32, n, nn, perm, bRhs.as<double2>() + vo,
-                                              bX.as<double2>() + vo));
+                                              bX.as<double2>() + vo, reorder ? 1 : 0));
             const double eta_tol = std::max(1e-14, 8.0 * std::sqrt((double)n) * 1.1e-16);
             const bool cwise = (form == PB_FORM_FULL);
             const bool probe = !rhs_fixed;
@@ -889,7 +899,8 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
                 for (int q = 0; q < mb; q++) if (state[nd + q] == 0) act.push_back(q);
                 PB_CUDA(cudaMemcpyAsync(bSys.p, act.data(), sizeof(int) * act.size(), cudaMemcpyHostToDevice, st));
                 PB_TRY(pb_lu_solve_mapped<float>(&c->lu, n, (int)act.size(), nr, m32, n, nn, perm,
-                                                 bR.as<double2>() + vo, bD.as<double2>() + vo, bSys.as<int>(), nullptr));
+                                                 bR.as<double2>() + vo, bD.as<double2>() + vo, bSys.as<int>(), nullptr,
+                                                 reorder ? 1 : 0));
                 const long long mv = (long long)nr * n;
                 k_axpy_sys<<<dim3(ceil_div(mv, 256), (unsigned)act.size()), 256, 0, st>>>(
                     bX.as<double2>() + vo, bD.as<double2>() + vo, mv, bSys.as<int>());
@@ -917,7 +928,8 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
                 c->launches++;
                 PB_CHECK_LAUNCH();
                 PB_TRY(pb_lu_solve_mapped<float>(&c->lu, n, (int)conv.size(), nr, m32, n, nn, perm,
-                                                 bR.as<double2>() + vo, bD.as<double2>() + vo, bSys.as<int>(), nullptr));
+                                                 bR.as<double2>() + vo, bD.as<double2>() + vo, bSys.as<int>(), nullptr,
+                                                 reorder ? 1 : 0));
                 // port voltages of x (with the port injections) and of the probe solution
                 // (linear part only) for systems nd .. nb
                 const int *pnone = bPC.as<int>() + 2 * np;
