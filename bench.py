@@ -286,17 +286,22 @@ def run_ours(args, ws, rank, dist):
                  "stats": {k: round(v, 3) if isinstance(v, float) else v for k, v in stp.items()}}
         zm = zs[0][1]
         acc = {"zin_rel_err_vs_plain_fp64": float(np.max(np.abs(zm - zp) / np.abs(zp)))}
-        # the LU trailing update on the library's tcgen05 kernel against cuBLAS's BF16x9
-        # emulation of the same update, on one batch (no FP64 fall-back frequencies in it)
+        # the factorisation engines on one batch (no FP64 fall-back frequencies in it): the
+        # ordered symmetric L D L^T the sweep uses, and the pivoted LU with its trailing
+        # updates on the library's tcgen05 kernel or on cuBLAS's BF16x9 emulation
         fc = zs[1][0] if len(zs) > 1 else zs[0][0]
         cmp_ = {}
-        for tag, kind in (("tcgen05_own", abi.LU_TC), ("cublas_bf16x9", abi.LU_TC_CUBLAS)):
+        for tag, kind in (("ldlt_tcgen05", abi.LU_TC), ("lu_tcgen05", abi.LU_TC_PIVOTED),
+                          ("lu_cublas_bf16x9", abi.LU_TC_CUBLAS)):
             zk, stk = ctx.sweep(fc, fill_prec=abi.PREC_MIXED, lu=kind, batch=B)
             cmp_[tag] = {"t_lu_ms": round(stk["t_lu_ms"], 2), "t_refine_ms": round(stk["t_refine_ms"], 2),
                          "fp64_fallbacks": stk["fp64_fallbacks"], "refine_max_iters": stk["max_iters"]}
             cmp_[tag]["zin"] = zk
-        cmp_["zin_rel_diff"] = float(np.max(np.abs(cmp_["tcgen05_own"].pop("zin") - cmp_["cublas_bf16x9"]["zin"])
-                                            / np.abs(cmp_["cublas_bf16x9"].pop("zin"))))
+        zr = cmp_["lu_cublas_bf16x9"]["zin"]
+        cmp_["zin_rel_diff"] = float(max(np.max(np.abs(cmp_[t]["zin"] - zr) / np.abs(zr))
+                                         for t in ("ldlt_tcgen05", "lu_tcgen05")))
+        for t in ("ldlt_tcgen05", "lu_tcgen05", "lu_cublas_bf16x9"):
+            cmp_[t].pop("zin")
         acc["lu_engine_compare"] = cmp_
         gpath = os.path.join(ROOT, "tests", "golden", "cfg2_full.npz")
         if os.path.exists(gpath) and args.grid == "64x32":
@@ -314,14 +319,15 @@ def run_ours(args, ws, rank, dist):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_dev_max / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64 (f32 correction and bf16x9 tensor-core LU; f64 static part and refinement)",
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64 (f32 correction, f32 L D L^T with bf16x6 tcgen05 updates; f64 static part and refinement)",
         "data": "synthetic (seeded geometry from the .peec text; no external data)",
         "config": {"workload": WORKLOAD if args.grid == "64x32" else "profiling case, plate grid " + args.grid,
                    "freqs_per_step": B, "n_system": len(prob.seg),
                    "form": "reduced branch-current MNA",
                    "solve": ("FP32 LU every %d frequencies + FP64 GMRES(60)" % args.accel) if args.accel >= 2
-                            else "FP32 LU per frequency + FP64 refinement", "parallelism": "frequency batches per rank" if ws > 1 else "1 GPU",
-                   "l2": "inputs larger than L2 (282 MB FP64 system matrix per frequency)",
+                            else "ordered FP32 L D L^T per frequency + FP64 refinement (FP64 LU fall back)",
+                   "parallelism": "frequency batches per rank" if ws > 1 else "1 GPU",
+                   "l2": "inputs larger than L2 (141 MB FP64 lower triangle per frequency)",
                    "e2e": "one context per sweep, created in the first timed step; frequencies in, Z out every step"},
         "e2e": {"value": total_points / e2e_t, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
