@@ -320,9 +320,13 @@ template <> struct TermOffset<double> {
     double cd[3];                 // centre (or start-point) offset
     double a2;                    // equivalent radius squared (wire kernel)
 };
+// bases of an FP32 term for EQ launches (sin/cos of kh[0], kh[8] and dkh times D), formed
+// in the set-up by the term's own lane
+#define PB_TBASE 3
 template <> struct TermOffset<float> {
     double D;                     // sqrt(|cd|^2 + a2), FP64: the term's phase kh * D
     float cdf[3], a2f, Df, Dlo, inv_rn;   // D = Df + Dlo
+    float4 tb[PB_TBASE];
 };
 template <typename R> struct Term : TermOffset<R> {
     int ty, nsub, n1, n2;
@@ -471,18 +475,22 @@ __device__ void run_term(const Term<R> &T, const KArg &k, Acc<R, F> &a, int lane
 // term are computed in FP64 by the first lanes into the warp's `base` slots.
 template <int F, int EQ, int RED, bool HAS2>
 __device__ void run_term32(const Term<float> &T, const KArg &k, Acc<float, F> &a, int lane,
-                           float4 *base)
+                           float4 *bases)
 {
     constexpr int NB = nbase<F, EQ>();
-    __syncwarp();                                   // previous term's bases no longer read
-    if (lane < NB) {
-        const double kh = EQ ? (lane < NB - 1 ? k.kh[8 * lane] : k.dkh) : k.kh[lane];
-        double sn, cs;
-        sincos(kh * T.D, &sn, &cs);
-        const float sh = (float)sn, ch = (float)cs;
-        base[lane] = make_float4(sh, ch, (float)(sn - (double)sh), (float)(cs - (double)ch));
+    // EQ launches: the term's bases were formed in the set-up (T.tb); otherwise here
+    const float4 *base = T.tb;
+    if (!EQ) {
+        __syncwarp();                               // previous term's bases no longer read
+        if (lane < NB) {
+            double sn, cs;
+            sincos(k.kh[lane] * T.D, &sn, &cs);
+            const float sh = (float)sn, ch = (float)cs;
+            bases[lane] = make_float4(sh, ch, (float)(sn - (double)sh), (float)(cs - (double)ch));
+        }
+        __syncwarp();
+        base = bases;
     }
-    __syncwarp();
     const float cd[3] = {T.cdf[0], T.cdf[1], T.cdf[2]};
     const float D = T.Df, Dlo = T.Dlo, irn = T.inv_rn;
     const int nsub = T.nsub;
@@ -729,16 +737,19 @@ __device__ void run_far2(const Term<float> *T, const KArg &k, Acc<float, F> &a, 
 {
     constexpr int NB = nbase<F, EQ>();
     const int hl = lane & 15;
-    float4 *base = bases + (lane >> 4) * NB;
-    __syncwarp();                                   // previous term's bases no longer read
-    if (T && hl < NB) {
-        const double kh = EQ ? (hl < NB - 1 ? k.kh[8 * hl] : k.dkh) : k.kh[hl];
-        double sn, cs;
-        sincos(kh * T->D, &sn, &cs);
-        const float sh = (float)sn, ch = (float)cs;
-        base[hl] = make_float4(sh, ch, (float)(sn - (double)sh), (float)(cs - (double)ch));
+    const float4 *base = T ? T->tb : nullptr;       // EQ: formed in the set-up
+    if (!EQ) {
+        float4 *bw = bases + (lane >> 4) * NB;
+        __syncwarp();                               // previous term's bases no longer read
+        if (T && hl < NB) {
+            double sn, cs;
+            sincos(k.kh[hl] * T->D, &sn, &cs);
+            const float sh = (float)sn, ch = (float)cs;
+            bw[hl] = make_float4(sh, ch, (float)(sn - (double)sh), (float)(cs - (double)ch));
+        }
+        __syncwarp();
+        base = bw;
     }
-    __syncwarp();
     if (T) {
         const float g = 0.577350269189625765f;      // 1/sqrt(3), weights 1
         const float xi = (hl & 1) ? g : -g, xj = (hl & 2) ? g : -g;
@@ -795,6 +806,7 @@ k_corr(pb_fill_geom g, KArg k, const double *st, pb_epi_args ea, double2 *ig, lo
                                                                               PB_GROUP * sizeof(TaskHdr) +
                                                                               2 * F * 32 * sizeof(double)))
                     + (size_t)wib * (PB_FMAX + 1);
+    static_assert(nbase<F, 1>() <= PB_TBASE, "EQ bases per term");
     const pb_dev_cells &set = SET == PB_SET_LP ? g.seg : g.chg;
     const int n = set.n;
     const long long T = (long long)n * (n + 1) / 2;
@@ -841,6 +853,23 @@ k_corr(pb_fill_geom g, KArg k, const double *st, pb_epi_args ea, double2 *ig, lo
                     make_term<R>(terms[2 * pl + term], si, sj, (i == j && term == 0), a1, a2, wgt, kw0, k.kwmax,
                                  set, i, j);
                     ok = 1;
+                }
+            }
+        }
+        if constexpr (sizeof(R) == 4 && EQ) {
+            // the term's phase bases, formed by its own lane (all lanes at once) rather than
+            // by a few lanes while the others wait in the sample loops: sin/cos(kh[8 g] D) per
+            // group of 8 frequencies, then sin/cos(dkh D)
+            if (ok) {
+                constexpr int NB = nbase<F, EQ>();
+                const double D = terms[2 * pl + term].D;
+                float4 *tb = terms[2 * pl + term].tb;
+#pragma unroll 1
+                for (int b = 0; b < NB; b++) {
+                    double sn, cs;
+                    sincos((b < NB - 1 ? k.kh[8 * b] : k.dkh) * D, &sn, &cs);
+                    const float sh = (float)sn, ch = (float)cs;
+                    tb[b] = make_float4(sh, ch, (float)(sn - (double)sh), (float)(cs - (double)ch));
                 }
             }
         }
@@ -950,11 +979,34 @@ k_corr(pb_fill_geom g, KArg k, const double *st, pb_epi_args ea, double2 *ig, lo
                     const int nt = tk >= 0 ? hdr[tk].nterm : 0;
                     if (tk >= 0) prefetch_p(hdr[tk], f);
                     if (nq > 0) {                          // warp-uniform; 0: two term-less pairs
+                        // at most two samples per lane (one per term): FP32 partials, no
+                        // FP64 running totals (the flush never triggers); the transposed
+                        // reduction adds the 16 lanes of a half in FP64
                         Acc<R, F> acc;
-                        acc.init(tot + lane);
+                        acc.tot = nullptr;
+                        acc.cnt = 0;
+#pragma unroll
+                        for (int ff = 0; ff < F; ff++) acc.pr[ff] = acc.pi[ff] = 0.f;
                         for (int q = 0; q < nq; q++)
                             run_far2<F, EQ, RED>(q < nt ? &terms[2 * tk + q] : nullptr, k, acc, lane, bases);
-                        reduce_halves<F>(acc, lane, cr, cim);
+                        float *fp = reinterpret_cast<float *>(tot);
+                        __syncwarp();
+#pragma unroll
+                        for (int ff = 0; ff < F; ff++) {
+                            fp[(2 * ff) * 32 + lane] = acc.pr[ff];
+                            fp[(2 * ff + 1) * 32 + lane] = acc.pi[ff];
+                        }
+                        __syncwarp();
+                        cr = cim = 0;
+                        if (hl < F) {
+                            const int h0 = lane & 16;
+#pragma unroll 8
+                            for (int l = 0; l < 16; l++) {
+                                cr += (double)fp[(2 * hl) * 32 + h0 + l];
+                                cim += (double)fp[(2 * hl + 1) * 32 + h0 + l];
+                            }
+                        }
+                        __syncwarp();
                     }
                 } else {
                     tk = -1;
