@@ -320,21 +320,27 @@ template <> struct TermOffset<double> {
     double cd[3];                 // centre (or start-point) offset
     double a2;                    // equivalent radius squared (wire kernel)
 };
-// bases of an FP32 term for EQ launches (sin/cos of kh[0], kh[8] and dkh times D), formed
-// in the set-up by the term's own lane
-#define PB_TBASE 3
 template <> struct TermOffset<float> {
     double D;                     // sqrt(|cd|^2 + a2), FP64: the term's phase kh * D
     float cdf[3], a2f, Df, Dlo, inv_rn;   // D = Df + Dlo
+};
+// bases of an FP32 term for EQ launches (sin/cos of kh[0], kh[8] and dkh times D), formed
+// in the set-up by the term's own lane; an empty base for FP64 terms
+#define PB_TBASE 3
+template <typename R> struct TermBases {};
+template <> struct TermBases<float> {
     float4 tb[PB_TBASE];
 };
-template <typename R> struct Term : TermOffset<R> {
+// 192 bytes for FP32 (a multiple of 16 without padding: three warps' groups of terms and
+// totals fit five CTAs per SM)
+template <typename R> struct Term : TermBases<R>, TermOffset<R> {
     int ty, nsub, n1, n2;
     double sc;                    // folded scale (term weight x quadrature Jacobian)
     R u1[3], v1[3], u2[3], v2[3];
     R L1, W1, L2, W2, zs;
-    const double4 *q1, *q2;
+    int qo1, qo2;                 // polygon point sets: offsets into the set's qpt
 };
+static_assert(sizeof(Term<float>) == 192, "FP32 term record layout");
 
 // Quadrature choice and geometry of neumann_pair_k's retardation term
 // (partial.c:256-317, neumann_self_k partial.c:320-328).
@@ -349,9 +355,9 @@ __device__ void make_term(Term<R> &T, const Cell &s1, const Cell &s2, int same, 
     double cdl[3], a2l = 0;
     if (ty == PT_POLY) {                                   // poly_corr, polygon.c:305-334
         T.ty = TT_POLY;
-        T.q1 = set.qpt + set.qoff[i1];
+        T.qo1 = set.qoff[i1];
         T.n1 = set.qoff[i1 + 1] - set.qoff[i1];
-        T.q2 = set.qpt + set.qoff[i2];
+        T.qo2 = set.qoff[i2];
         T.n2 = set.qoff[i2 + 1] - set.qoff[i2];
 #pragma unroll
         for (int c = 0; c < 3; c++) cdl[c] = 0.5 * (s2.x1[c] + s2.x2[c]) - 0.5 * (s1.x1[c] + s1.x2[c]);
@@ -417,7 +423,7 @@ __device__ __forceinline__ double dist64(const double *cd, const double *p, doub
 }
 
 template <typename R, int F, int EQ>
-__device__ void run_term(const Term<R> &T, const KArg &k, Acc<R, F> &a, int lane)
+__device__ void run_term(const Term<R> &T, const KArg &k, Acc<R, F> &a, int lane, const double4 *qpt)
 {
     const int nsub = T.nsub;
     const R rn = (R)nsub;
@@ -457,7 +463,7 @@ __device__ void run_term(const Term<R> &T, const KArg &k, Acc<R, F> &a, int lane
         const int S = T.n1 * T.n2;
         for (int s = lane; s < S; s += 32) {
             const int k1 = s / T.n2, k2 = s - k1 * T.n2;
-            const double4 o1 = T.q1[k1], o2 = T.q2[k2];
+            const double4 o1 = qpt[T.qo1 + k1], o2 = qpt[T.qo2 + k2];
             R p[3];
             p[0] = (R)o2.x - (R)o1.x;
             p[1] = (R)o2.y - (R)o1.y;
@@ -475,7 +481,7 @@ __device__ void run_term(const Term<R> &T, const KArg &k, Acc<R, F> &a, int lane
 // term are computed in FP64 by the first lanes into the warp's `base` slots.
 template <int F, int EQ, int RED, bool HAS2>
 __device__ void run_term32(const Term<float> &T, const KArg &k, Acc<float, F> &a, int lane,
-                           float4 *bases)
+                           float4 *bases, const double4 *qpt)
 {
     constexpr int NB = nbase<F, EQ>();
     // EQ launches: the term's bases were formed in the set-up (T.tb); otherwise here
@@ -590,7 +596,7 @@ __device__ void run_term32(const Term<float> &T, const KArg &k, Acc<float, F> &a
         const double msc = -2.0 * T.sc;
         for (int s = lane; s < S; s += 32) {
             const int k1 = s / T.n2, k2 = s - k1 * T.n2;
-            const double4 o1 = T.q1[k1], o2 = T.q2[k2];
+            const double4 o1 = qpt[T.qo1 + k1], o2 = qpt[T.qo2 + k2];
             sample32<F, EQ, RED>(a, k, base, cd, 0.f, D, Dlo, (float)o2.x - (float)o1.x, (float)o2.y - (float)o1.y,
                             T.zs * (float)o2.z - (float)o1.z, (float)(o1.w * o2.w * msc));
         }
@@ -714,10 +720,10 @@ k_pot_static(pb_fill_geom g, double kw, double *st)
 // memory. Then the warp sweeps the samples: pairs with a near term one after the other
 // with all 32 lanes (lanes split the samples), far and term-less pairs two at a time,
 // one per half-warp. The FP64 set-up so costs one lane-evaluation per term.
-#define PB_CORR_WARPS 4
-#ifndef PB_CORR_MINB
-#define PB_CORR_MINB 4      // resident blocks per SM the register budget is sized for
-#endif
+// FP64 kernels: 4 warps per CTA, 4 CTAs per SM; FP32 kernels: 3 warps per CTA, 5 CTAs per
+// SM (128 registers either way; the FP32 CTA's terms and totals take 44 KB of shared memory)
+template <typename R> constexpr int corr_warps() { return sizeof(R) == 4 ? 3 : 4; }
+template <typename R> constexpr int corr_minb() { return sizeof(R) == 4 ? 5 : 4; }
 #define PB_GROUP 16
 
 enum { PB_SET_LP = 0, PB_SET_IG = 1 };
@@ -783,20 +789,22 @@ __device__ __forceinline__ void reduce_halves(Acc<float, F> &a, int lane, double
     __syncwarp();
 }
 
-template <typename R, int F>
+template <typename R, int F, int EQ>
 constexpr size_t corr_smem_bytes()
 {
-    return (size_t)PB_CORR_WARPS * (2 * PB_GROUP * sizeof(Term<R>) + PB_GROUP * sizeof(TaskHdr) +
-                                     (sizeof(R) == 4 ? 2 * F * 32 * sizeof(double) + (PB_FMAX + 1) * sizeof(float4) : 0));
+    return (size_t)corr_warps<R>() *
+           (2 * PB_GROUP * sizeof(Term<R>) + PB_GROUP * sizeof(TaskHdr) +
+            (sizeof(R) == 4 ? 2 * F * 32 * sizeof(double) + (EQ ? 0 : (PB_FMAX + 1) * sizeof(float4)) : 0));
 }
 
 template <typename R, int F, int SET, int EPI, int EQ, int RED>
-__global__ void __launch_bounds__(32 * PB_CORR_WARPS, PB_CORR_MINB)
+__global__ void __launch_bounds__(32 * corr_warps<R>(), corr_minb<R>())
 k_corr(pb_fill_geom g, KArg k, const double *st, pb_epi_args ea, double2 *ig, long long igs)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     Term<R> *terms = reinterpret_cast<Term<R> *>(smraw) + (size_t)wib * 2 * PB_GROUP;
+    constexpr int PB_CORR_WARPS = corr_warps<R>();
     TaskHdr *hdr = reinterpret_cast<TaskHdr *>(smraw + (size_t)PB_CORR_WARPS * 2 * PB_GROUP * sizeof(Term<R>))
                    + wib * PB_GROUP;
     double *tot = reinterpret_cast<double *>(smraw + (size_t)PB_CORR_WARPS * (2 * PB_GROUP * sizeof(Term<R>) +
@@ -959,10 +967,10 @@ k_corr(pb_fill_geom g, KArg k, const double *st, pb_epi_args ea, double2 *ig, lo
                     acc.init(tot + lane);
                     for (int q = 0; q < h.nterm; q++) {
                         if constexpr (sizeof(R) == 4) {
-                            run_term32<F, EQ, RED, !PAIR_FAR>(terms[2 * tk + q], k, acc, lane, bases);
+                            run_term32<F, EQ, RED, !PAIR_FAR>(terms[2 * tk + q], k, acc, lane, bases, set.qpt);
                         } else {
                             const Term<R> tm = terms[2 * tk + q];
-                            run_term<R, F, EQ>(tm, k, acc, lane);
+                            run_term<R, F, EQ>(tm, k, acc, lane, set.qpt);
                         }
                     }
                     reduce_select<F>(acc, lane, cr, cim);
@@ -1280,11 +1288,11 @@ static int launch_corr(const pb_fill_geom &g, const KArg &k, const double *st, c
 {
     const int n = SET == PB_SET_LP ? g.seg.n : g.chg.n;
     const long long T = (long long)n * (n + 1) / 2;
-    constexpr size_t smem = corr_smem_bytes<R, F>();
+    constexpr size_t smem = corr_smem_bytes<R, F, EQ>();
     static std::atomic<unsigned long long> attr_set{0};   // per device, before any launch relies on it
     PB_TRY(pb_smem_optin(k_corr<R, F, SET, EPI, EQ, RED>, (int)smem, attr_set));
-    const int grid = grid_for((T + PB_GROUP - 1) / PB_GROUP, PB_CORR_WARPS, PB_CORR_MINB);
-    k_corr<R, F, SET, EPI, EQ, RED><<<grid, 32 * PB_CORR_WARPS, smem, s>>>(g, k, st, ea, ig, igs);
+    const int grid = grid_for((T + PB_GROUP - 1) / PB_GROUP, corr_warps<R>(), corr_minb<R>());
+    k_corr<R, F, SET, EPI, EQ, RED><<<grid, 32 * corr_warps<R>(), smem, s>>>(g, k, st, ea, ig, igs);
     PB_CHECK_LAUNCH();
     return PB_OK;
 }
