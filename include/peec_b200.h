@@ -149,7 +149,12 @@ typedef struct {
                                ancestors pc_coarse - 1 levels up otherwise) applied before the
                                plain preconditioner; 0 = the plain preconditioner alone (the
                                reference's) */
-    int pad3_;
+    int pc_exact_leaf;      /* compressed path, experiment: 1 = every leaf block of the Lp kernel
+                               block replaced by the exact S_r = ((A_LL^-1)_rr)^-1 (the leaf
+                               block that makes the block-diagonal preconditioner reproduce
+                               the diagonal blocks of the inverse; dense inverse on the GPU,
+                               for structures of a few thousand cells): the best any
+                               correction of the leaf blocks alone can do; 0 = off */
 } pb_sweep_opts;
 
 typedef struct {

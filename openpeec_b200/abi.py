@@ -57,7 +57,7 @@ class PbSweepOpts(C.Structure):
         ("fill_prec", C.c_int), ("lu", C.c_int), ("form", C.c_int), ("batch", C.c_int),
         ("refine_tol", C.c_double), ("refine_maxit", C.c_int), ("verbose", C.c_int),
         ("corr_freqs", C.c_int), ("accel", C.c_int), ("compress", C.c_int), ("pad_", C.c_int),
-        ("ctol", C.c_double), ("pc_mlp", C.c_void_p), ("pc_coarse", C.c_int), ("pad3_", C.c_int),
+        ("ctol", C.c_double), ("pc_mlp", C.c_void_p), ("pc_coarse", C.c_int), ("pc_exact_leaf", C.c_int),
     ]
 
 

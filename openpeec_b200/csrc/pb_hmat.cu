@@ -1034,6 +1034,53 @@ int apply_mlp(pb_ctx *c, KBlock &kb, const std::vector<zc> &zint, double om, con
     return PB_OK;
 }
 
+// Exact leaf blocks (pb_sweep_opts.pc_exact_leaf): every leaf block D_r of the kernel block
+// replaced by S_r = ((A_LL^-1)_rr)^-1, A_LL = scale K - diag(Z_int), from a dense inverse on
+// the device; the inverse's leaf blocks come back to the host and are inverted there.
+int exact_leaves(pb_ctx *c, KBlock &kb, const std::vector<zc> &zint, const double2 *K)
+{
+    const cudaStream_t st = c->stream;
+    const int n = kb.n;
+    std::vector<zc> A((size_t)n * n);
+    PB_CUDA(cudaMemcpyAsync(A.data(), K, sizeof(double2) * (size_t)n * n, cudaMemcpyDeviceToHost, st));
+    PB_CUDA(cudaStreamSynchronize(st));
+    for (size_t e = 0; e < A.size(); e++) A[e] *= zc(kb.scale.x, kb.scale.y);
+    for (int i = 0; i < n; i++) A[(size_t)i * n + i] -= zint[i];
+    std::vector<zc> I((size_t)n * n, zc(0, 0));
+    for (int i = 0; i < n; i++) I[(size_t)i * n + i] = 1.0;
+    Dev dA, dI, dX, piv, perm, info;
+    PB_TRY(upload(dA, A, st));
+    PB_TRY(upload(dI, I, st));
+    PB_TRY(dX.alloc(sizeof(double2) * (size_t)n * n));
+    PB_TRY(piv.alloc(sizeof(int) * n));
+    PB_TRY(perm.alloc(sizeof(int) * n));
+    PB_TRY(info.alloc(sizeof(int)));
+    PB_TRY(pb_lu_factor<double>(&c->lu, n, 1, dA.as<double2>(), n, (long)n * n, piv.as<int>(), info.as<int>()));
+    PB_TRY(pb_lu_perm(&c->lu, n, 1, piv.as<int>(), perm.as<int>()));
+    PB_TRY(pb_lu_solve_batched<double>(&c->lu, n, 1, n, dA.as<double2>(), n, (long)n * n, perm.as<int>(),
+                                       dI.as<double2>(), dX.as<double2>()));
+    std::vector<zc> X((size_t)n * n);                 // X[j*n + i] = (A^-1)_ij
+    PB_CUDA(cudaMemcpyAsync(X.data(), dX.p, sizeof(double2) * (size_t)n * n, cudaMemcpyDeviceToHost, st));
+    PB_CUDA(cudaStreamSynchronize(st));
+    for (int r = 0; r < kb.nl; r++) {
+        const int mm = kb.lof[r + 1] - kb.lof[r];
+        const int *idx = &kb.lidx[kb.lof[r]];
+        std::vector<zc> Xr((size_t)mm * mm), e(mm);
+        std::vector<int> pv(mm);
+        for (int a = 0; a < mm; a++)
+            for (int b = 0; b < mm; b++) Xr[(size_t)a * mm + b] = X[(size_t)idx[b] * n + idx[a]];
+        if (host_lu(mm, Xr.data(), pv.data()) >= 0) { pb_set_error("exact leaves: singular leaf inverse block"); return PB_ERR_SINGULAR; }
+        zc *D = &kb.dlu[kb.dof[r]];
+        for (int b = 0; b < mm; b++) {                // column b of S_r = Xr^-1
+            std::fill(e.begin(), e.end(), zc(0, 0));
+            e[b] = 1.0;
+            host_lu_solve(mm, Xr.data(), pv.data(), e.data());
+            for (int a = 0; a < mm; a++) D[(size_t)a * mm + b] = e[a];
+        }
+    }
+    return PB_OK;
+}
+
 // Training samples at one frequency: features of every current cell and the target
 // (S_r - D_r)_ii / D_ii, where S_r = ((A_LL^-1)_rr)^-1 is the leaf block that makes a
 // block-diagonal preconditioner reproduce the diagonal blocks of the inverse of the whole
@@ -1327,7 +1374,8 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
             return PB_OK;
         }
         mark("Schur init");
-        bool use_mlp = o.pc_mlp != nullptr;
+        if (o.pc_exact_leaf) PB_TRY(exact_leaves(c, kbs[0], zint, bK.as<double2>()));
+        bool use_mlp = o.pc_mlp != nullptr && !o.pc_exact_leaf;
         if (use_mlp) {
             PB_TRY(apply_mlp(c, kbs[0], zint, om, o.pc_mlp, use_mlp));
             if (!use_mlp) mlp_fallbacks++;       // prediction not finite: plain preconditioner
