@@ -187,7 +187,8 @@ typedef struct {
                               conditioning probe found their port voltages sensitive above a
                               quarter of the 1e-6 bar to perturbations of the size of the
                               remaining backward error (counted in fp64_fallbacks too)    */
-    int    pad4_;
+    int    pipelined;      /* 1 = batches were pipelined: the next batch filled on a second,
+                              lower-priority stream while the current one was solved       */
     double probe_max;      /* largest probe sensitivity |dV_port| / |V_port| of the sweep   */
 } pb_sweep_stats;
 

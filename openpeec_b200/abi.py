@@ -76,7 +76,7 @@ class PbSweepStats(C.Structure):
         ("hmat_far", C.c_int), ("hmat_near", C.c_int), ("hmat_max_rank", C.c_int),
         ("hmat_dense_far", C.c_int), ("hmat_mb", C.c_double), ("hmat_dense_mb", C.c_double),
         ("pc_mlp_fallbacks", C.c_int), ("pc_coarse_n", C.c_int), ("t_coarse_ms", C.c_double),
-        ("probe_fallbacks", C.c_int), ("pad4_", C.c_int), ("probe_max", C.c_double),
+        ("probe_fallbacks", C.c_int), ("pipelined", C.c_int), ("probe_max", C.c_double),
     ]
 
     def as_dict(self):

@@ -234,7 +234,14 @@ int pb_create(const pb_problem_t *prob, pb_ctx **out)
     if (r != PB_OK) { delete c; if (r == PB_ERR_ARG) pb_set_error("pb_create: node id out of range"); return r; }
 
     cudaGetDevice(&c->dev);
-    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    // the solve stream at the highest priority, the fill stream at the lowest: while both
+    // have work, the latency-bound factorisation and refinement kernels get SMs first and the
+    // issue-bound fill takes what is left
+    int prio_lo = 0, prio_hi = 0;
+    cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
+    if (cudaStreamCreateWithPriority(&c->stream, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&c->stream_fill, cudaStreamNonBlocking, prio_lo) != cudaSuccess) {
+        if (c->stream) cudaStreamDestroy(c->stream);
         delete c; pb_set_error("cudaStreamCreate failed"); return PB_ERR_CUDA;
     }
     const cudaStream_t s = c->stream;
@@ -301,6 +308,7 @@ void pb_destroy(pb_ctx *c)
 {
     if (!c) return;
     if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->stream_fill) cudaStreamSynchronize(c->stream_fill);
     void *ptrs[] = {c->g.seg.cell, c->g.seg.qpt, c->g.seg.qoff, c->g.chg.cell, c->g.chg.qpt,
                     c->g.chg.qoff, c->g.pv, c->g.csoff, c->g.csidx, c->g.carea, c->g.seg_ca,
                     c->g.seg_cb, c->d_inc_off, c->d_inc_seg, c->d_fe_row, c->d_fe_col, c->d_fe_off,
@@ -310,6 +318,7 @@ void pb_destroy(pb_ctx *c)
     if (c->comp_schur_reg) cudaHostUnregister(c->comp_schur_reg);
     pb_lu_engine_free(&c->lu);
     if (c->stream) cudaStreamDestroy(c->stream);
+    if (c->stream_fill) cudaStreamDestroy(c->stream_fill);
     delete c;
 }
 

@@ -10,8 +10,8 @@
 // Device storage a context keeps across sweep calls (grow-only, freed by pb_destroy), so
 // repeated sweeps of one structure do not reallocate their batch buffers.
 struct pb_cache_slot { void *p = nullptr; size_t cap = 0; };
-#define PB_CACHE_SLOTS 40
-#define PB_SLOT_COMP0  32     // slots [32, 40) hold the compressed path's dense kernel blocks
+#define PB_CACHE_SLOTS 48
+#define PB_SLOT_COMP0  40     // slots [40, 48) hold the compressed path's dense kernel blocks
 
 // One additive contribution to an MNA entry whose value scales as val * {1, jw, -jw}.
 enum { ST_CONST = 0, ST_JW = 1, ST_MJW = 2 };
@@ -61,6 +61,9 @@ struct pb_ctx {
     unsigned long long *d_count = nullptr;     // [2] quadrature-sample counters (statistics)
 
     pb_cache_slot cache[PB_CACHE_SLOTS];
+    // the dense sweep's second stream (lower priority): the next batch's fill runs on it while
+    // the current batch is factorised and refined on `stream`
+    cudaStream_t stream_fill = nullptr;
     // correction samples (Lp, P) per quadrature-level signature, for the statistics
     std::map<std::vector<long>, std::pair<double, double>> sample_counts;
     // compressed path: level signature whose static parts the held slots contain

@@ -397,6 +397,45 @@ struct PhaseTimer {
     }
 };
 
+// Phase timer of the fill stream: event pairs recorded without waiting (the host must not
+// block on the fill stream while the other stream's batch is being solved), summed once
+// the sweep is done.
+struct AsyncTimer {
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev;
+    cudaEvent_t cur = nullptr;
+    double acc = 0;
+    void start(cudaStream_t s)
+    {
+        cudaEventCreate(&cur);
+        cudaEventRecord(cur, s);
+    }
+    void stop(cudaStream_t s)
+    {
+        cudaEvent_t b = nullptr;
+        cudaEventCreate(&b);
+        cudaEventRecord(b, s);
+        ev.push_back(std::make_pair(cur, b));
+        cur = nullptr;
+    }
+    void finish()
+    {
+        for (auto &e : ev) {
+            cudaEventSynchronize(e.second);
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e.first, e.second);
+            acc += ms;
+            cudaEventDestroy(e.first);
+            cudaEventDestroy(e.second);
+        }
+        ev.clear();
+    }
+    ~AsyncTimer()
+    {
+        for (auto &e : ev) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
+        if (cur) cudaEventDestroy(cur);
+    }
+};
+
 int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts *opts_in,
                   double *zmat, double *segi, pb_sweep_stats *stats,
                   const pb_planewave_t *pw, double *voc, double *segipw,
@@ -469,27 +508,51 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
     PB_CUDA(cudaMemGetInfo(&fr, &tot));
     const double n2 = (double)n * n;
     const int tc = (o.lu == PB_LU_TC_CUBLAS);     // the library comparison needs the embedding scratch
-    double perf = n2 * 16 + (mixed ? n2 * 8 : 0) + (tc ? n2 * 4 : 0) + (double)nc * nc * 16 + (double)ns * 16
-                + (form == PB_FORM_FULL ? (double)ns * ns * 16 : 0) + 4.0 * nr * n * 16 + 8.0 * n;
+    // per frequency: the filled systems (one set per batch in flight) and the solve's storage
+    const double perf_set = n2 * 16 + (mixed ? n2 * 8 : 0) + (double)nc * nc * 16 + (double)ns * 16 + 8.0
+                          + (form == PB_FORM_FULL ? (double)ns * ns * 16 : 0);
+    const double perf_solve = (tc ? n2 * 4 : 0) + 4.0 * nr * n * 16 + 8.0 * n;
     const double fixed = (double)ns * ns * 8 + (double)nc * nc * 8 +
                          (c->retardation ? (double)PB_FMAX * c->chg.size() * c->chg.size() * 16 : 0.0);
+    double cached = 0;                           // storage this context already holds
+    for (int q = 0; q < PB_SLOT_COMP0; q++) cached += (double)c->cache[q].cap;
+    // concurrent instances (pb_sweep_many) share the free memory
+    const double avail = 0.80 * ((double)fr + cached) / pb_mem_share - fixed - 256e6;
     int B = o.batch;
     if (B <= 0) {
-        double cached = 0;                       // storage this context already holds
-        for (int q = 0; q < PB_SLOT_COMP0; q++) cached += (double)c->cache[q].cap;
-        // concurrent instances (pb_sweep_many) share the free memory
-        const double avail = 0.80 * ((double)fr + cached) / pb_mem_share - fixed - 256e6;
-        B = (int)std::max(1.0, std::floor(avail / perf));
+        B = (int)std::max(1.0, std::floor(avail / (perf_set + perf_solve)));
         B = std::min(B, 256);
     }
     B = std::max(1, std::min(B, nfreq));
+    // Pipelined batches: with more than one batch, the next batch is filled (on the context's
+    // low-priority fill stream) while the current one is factorised and refined, which needs
+    // a second set of filled systems. Taken when both sets fit with batches of >= 32
+    // frequencies (smaller batches lose more in the batched kernels than the overlap gains).
+    bool pipe = false;
+    if (nfreq > B && !rhs_fixed) {
+        int Bp = o.batch > 0 ? B : (int)std::min(256.0, std::floor(avail / (2 * perf_set + perf_solve)));
+        if ((o.batch > 0 || Bp >= 32) && (double)Bp * (2 * perf_set + perf_solve) <= avail) {
+            pipe = true;
+            B = std::max(1, std::min(Bp, nfreq));
+        }
+    }
 
     pb_cache_slot *cs = c->cache;
-    DevBuf bM64(cs + 0), bM32(cs + 1), bP(cs + 2), bLp(cs + 3), bStLp(cs + 4), bStP(cs + 5), bZint(cs + 6), bPiv(cs + 7), bPerm(cs + 8), bInfo(cs + 9), bRhs(cs + 10), bX(cs + 11), bR(cs + 12), bD(cs + 13), bRn(cs + 14), bBn(cs + 15), bFreq(cs + 16), bZ(cs + 17), bPC(cs + 18);
-    PB_TRY(bM64.alloc((size_t)B * n2 * 16));
-    // the FP32 factors; the FP64 fall-back later reuses this storage for up to B/2 FP64
-    // matrices, so it holds at least one (B = 1)
-    if (mixed) PB_TRY(bM32.alloc((size_t)std::max(B, 2) * n2 * 8));
+    DevBuf bM64a(cs + 0), bM32a(cs + 1), bPa(cs + 2), bLpa(cs + 3), bStLp(cs + 4), bStP(cs + 5), bZinta(cs + 6), bPiv(cs + 7), bPerm(cs + 8), bInfo(cs + 9), bRhs(cs + 10), bX(cs + 11), bR(cs + 12), bD(cs + 13), bRn(cs + 14), bBn(cs + 15), bFreqa(cs + 16), bZ(cs + 17), bPC(cs + 18);
+    // the second set of filled systems (pipelined batches)
+    DevBuf bM64b(cs + 31), bM32b(cs + 32), bPb(cs + 33), bLpb(cs + 34), bZintb(cs + 35), bFreqb(cs + 36);
+    for (int set = 0; set < (pipe ? 2 : 1); set++) {
+        DevBuf &m64 = set ? bM64b : bM64a, &m32 = set ? bM32b : bM32a, &pm = set ? bPb : bPa;
+        DevBuf &lpb = set ? bLpb : bLpa, &zb = set ? bZintb : bZinta, &fq = set ? bFreqb : bFreqa;
+        PB_TRY(m64.alloc((size_t)B * n2 * 16));
+        // the FP32 factors; the FP64 fall-back later reuses this storage for up to B/2 FP64
+        // matrices, so it holds at least one (B = 1)
+        if (mixed) PB_TRY(m32.alloc((size_t)std::max(B, 2) * n2 * 8));
+        PB_TRY(pm.alloc((size_t)B * nc * nc * 16 + 16));
+        if (form == PB_FORM_FULL) PB_TRY(lpb.alloc((size_t)B * ns * ns * 16 + 16));
+        PB_TRY(zb.alloc((size_t)B * ns * 16 + 16));
+        PB_TRY(fq.alloc((size_t)B * 8));
+    }
     // real-embedded right operands of the tensor-core trailing updates: the largest is
     // k x nc complex with k + nc = n, i.e. at most n^2/4 entries -> 4 * n^2/4 floats
     DevBuf bEmb(cs + 19);
@@ -502,14 +565,11 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
         c->lu.emb = bEmb.as<float>();
         c->lu.emb_cap = (size_t)B * n2 * 4;
     }
-    PB_TRY(bP.alloc((size_t)B * nc * nc * 16 + 16));
     DevBuf bIg(cs + 20);                                  // sub-cell P corrections of one fill chunk
     if (c->capacitance && nc > 0 && c->retardation)
         PB_TRY(bIg.alloc((size_t)PB_FMAX * c->chg.size() * c->chg.size() * 16));
-    if (form == PB_FORM_FULL) PB_TRY(bLp.alloc((size_t)B * ns * ns * 16 + 16));
     PB_TRY(bStLp.alloc((size_t)ns * ns * 8 + 16));
     PB_TRY(bStP.alloc((size_t)nc * nc * 8 + 16));
-    PB_TRY(bZint.alloc((size_t)B * ns * 16 + 16));
     PB_TRY(bPiv.alloc((size_t)B * n * 4));
     PB_TRY(bPerm.alloc((size_t)B * n * 4));
     PB_TRY(bInfo.alloc((size_t)B * 4));
@@ -527,7 +587,6 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
     PB_TRY(bCw.alloc((size_t)B * nr * 8));
     DevBuf bSys(cs + 24);                         // systems still refining
     PB_TRY(bSys.alloc((size_t)B * sizeof(int)));
-    PB_TRY(bFreq.alloc((size_t)B * 8));
     PB_TRY(bZ.alloc((size_t)B * np * nr * 16 + 16));
     PB_TRY(bPC.alloc((size_t)2 * (np + 1) * 4));
     DevBuf bW(cs + 26), bEta(cs + 27), bZp(cs + 28); // conditioning probe: row weights, eta, port voltages
@@ -565,7 +624,8 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
     PwArgs pwa;
     if (pw) PB_TRY(make_pw_args(pw, pwa));
 
-    PhaseTimer tStatic, tCorr, tAsm, tLu, tRef, tAll;
+    PhaseTimer tLu, tRef, tAll;
+    AsyncTimer tStatic, tCorr, tAsm;                // fill phases (possibly on the fill stream)
     double samples = 0, luflops = 0, maxres = 0, probe_max = 0;
     int maxits = 0, refreshes = 0, probe_fb = 0;
     // the static tables stay with the context between calls (cache slots 4 and 5): valid
@@ -582,13 +642,17 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
     std::vector<int> infoh(B);
     tAll.start(st);
 
-    for (int b0 = 0; b0 < nfreq; b0 += B) {
-        const int nb = std::min(B, nfreq - b0);
-        const double *fb = freq + b0;
-        PB_CUDA(cudaMemcpyAsync(bFreq.p, fb, sizeof(double) * nb, cudaMemcpyHostToDevice, st));
-        tAsm.start(st);
-        PB_TRY(pb_zint(c->g, c->skin, nb, bFreq.as<double>(), bZint.as<double2>(), st, &c->launches));
-        tAsm.stop(st);
+    // Fill of one batch (frequencies fb0 .. fb0 + nb - 1) into buffer set `set` on stream fs:
+    // internal impedances, the static tables when the quadrature levels change, the
+    // correction kernels with the reduced-form epilogue, or the full-form assembly.
+    auto fill_batch = [&](int fb0, int nb, int set, cudaStream_t fs) -> int {
+        DevBuf &bM64 = set ? bM64b : bM64a, &bM32 = set ? bM32b : bM32a, &bP = set ? bPb : bPa;
+        DevBuf &bLp = set ? bLpb : bLpa, &bZint = set ? bZintb : bZinta, &bFreq = set ? bFreqb : bFreqa;
+        const double *fb = freq + fb0;
+        PB_CUDA(cudaMemcpyAsync(bFreq.p, fb, sizeof(double) * nb, cudaMemcpyHostToDevice, fs));
+        tAsm.start(fs);
+        PB_TRY(pb_zint(c->g, c->skin, nb, bFreq.as<double>(), bZint.as<double2>(), fs, &c->launches));
+        tAsm.stop(fs);
         // fill in chunks of <= 32 frequencies with one quadrature-level signature
         int f = 0;
         while (f < nb) {
@@ -613,10 +677,10 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
             // (bit-identical) while it does not
             if (!static_valid || sig != cur_sig) {
                 c->dense_static_valid = false;
-                tStatic.start(st);
-                if (c->capacitance && nc > 0) PB_TRY(pb_pot_static(c->g, kw0, bStP.as<double>(), st, &c->launches));
-                PB_TRY(pb_lp_static(c->g, kw0, bStLp.as<double>(), st, &c->launches));
-                tStatic.stop(st);
+                tStatic.start(fs);
+                if (c->capacitance && nc > 0) PB_TRY(pb_pot_static(c->g, kw0, bStP.as<double>(), fs, &c->launches));
+                PB_TRY(pb_lp_static(c->g, kw0, bStLp.as<double>(), fs, &c->launches));
+                tStatic.stop(fs);
                 cur_sig = sig;
                 static_valid = true;
                 c->dense_sig = sig;
@@ -639,7 +703,7 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
                 skey.push_back(fill32 ? far_rule_key(c, kwmax) : -1);
                 auto it = c->sample_counts.find(skey);
                 if (it == c->sample_counts.end()) {
-                    PB_TRY(pb_count_samples(c->g, kw0, &lp_samp, &p_samp, st, c->d_count, fill32 ? kwmax : 0.0));
+                    PB_TRY(pb_count_samples(c->g, kw0, &lp_samp, &p_samp, fs, c->d_count, fill32 ? kwmax : 0.0));
                     c->sample_counts[skey] = std::make_pair(lp_samp, p_samp);
                 } else {
                     lp_samp = it->second.first;
@@ -648,10 +712,10 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
             } else {
                 lp_samp = p_samp = 0;
             }
-            tCorr.start(st);
+            tCorr.start(fs);
             if (c->capacitance && nc > 0)
                 PB_TRY(pb_pot_corr(c->g, nf, kw, fill32, bStP.as<double>(), bP.as<double2>() + (long long)f * nc * nc,
-                                   (long long)nc * nc, bIg.as<double2>(), st, &c->launches, &samples));
+                                   (long long)nc * nc, bIg.as<double2>(), fs, &c->launches, &samples));
             pb_epi_args ea;
             for (int q = 0; q < nf; q++) ea.omega[q] = 2 * PB_PI * fb[f + q];
             if (form == PB_FORM_REDUCED) {
@@ -662,24 +726,24 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
                 ea.pm_stride = (long long)nc * nc;
                 ea.zint = bZint.as<double2>() + (long long)f * ns;
                 ea.lower = lower ? 1 : 0;
-                PB_TRY(pb_lp_corr(c->g, nf, kw, fill32, bStLp.as<double>(), PB_EPI_REDUCED, ea, st,
+                PB_TRY(pb_lp_corr(c->g, nf, kw, fill32, bStLp.as<double>(), PB_EPI_REDUCED, ea, fs,
                                   &c->launches, &samples));
             } else {
                 ea.out = bLp.as<double2>() + (long long)f * ns * ns;
                 ea.out_stride = (long long)ns * ns;
-                PB_TRY(pb_lp_corr(c->g, nf, kw, fill32, bStLp.as<double>(), PB_EPI_STORE, ea, st,
+                PB_TRY(pb_lp_corr(c->g, nf, kw, fill32, bStLp.as<double>(), PB_EPI_STORE, ea, fs,
                                   &c->launches, &samples));
             }
-            tCorr.stop(st);
+            tCorr.stop(fs);
             samples += (lp_samp + (c->capacitance ? p_samp : 0)) * nf;
             f = e;
         }
         if (form == PB_FORM_FULL) {
-            tAsm.start(st);
-            PB_CUDA(cudaMemsetAsync(bM64.p, 0, (size_t)nb * n2 * 16, st));
+            tAsm.start(fs);
+            PB_CUDA(cudaMemsetAsync(bM64.p, 0, (size_t)nb * n2 * 16, fs));
             const int offQ = c->nunknown;
             const long long per = (long long)ns * ns + (c->capacitance ? (long long)nc * nc : 0);
-            if (per > 0) k_full_blocks<<<ceil_div(per * nb, 256), 256, 0, st>>>(
+            if (per > 0) k_full_blocks<<<ceil_div(per * nb, 256), 256, 0, fs>>>(
                 nb, n, ns, c->capacitance ? nc : 0, c->offS, offQ, bLp.as<double2>(), (long long)ns * ns,
                 bP.as<double2>(), (long long)nc * nc, bZint.as<double2>(), bFreq.as<double>(),
                 bM64.as<double2>(), (long long)n * n);
@@ -687,19 +751,49 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
             PB_CHECK_LAUNCH();
             const int ne = (int)c->fe_row.size();
             if (ne > 0) {
-                k_full_stamps<<<ceil_div((long long)ne * nb, 256), 256, 0, st>>>(
+                k_full_stamps<<<ceil_div((long long)ne * nb, 256), 256, 0, fs>>>(
                     nb, n, ne, c->d_fe_row, c->d_fe_col, c->d_fe_off, c->d_fe_st, bFreq.as<double>(),
                     bM64.as<double2>(), (long long)n * n);
                 c->launches++;
                 PB_CHECK_LAUNCH();
             }
             if (mixed) {
-                k_to_f32<<<1184, 256, 0, st>>>(bM64.as<double2>(), bM32.as<float2>(), (long long)nb * n * n);
+                k_to_f32<<<1184, 256, 0, fs>>>(bM64.as<double2>(), bM32.as<float2>(), (long long)nb * n * n);
                 c->launches++;
                 PB_CHECK_LAUNCH();
             }
-            tAsm.stop(st);
+            tAsm.stop(fs);
         }
+        return PB_OK;
+    };
+    // Pipelined: the next batch's fill is queued on the fill stream before this batch is
+    // solved on `st`, which waits for its own batch's fill event. Both streams only touch
+    // their own buffer set; a set is refilled only after the batch that used it has been
+    // solved (the solve ends with a host synchronisation of `st`).
+    const cudaStream_t sf = pipe ? c->stream_fill : st;
+    struct EvPair {
+        cudaEvent_t e[2] = {nullptr, nullptr};
+        ~EvPair() { for (auto x : e) if (x) cudaEventDestroy(x); }
+    } evFill;
+    if (pipe) {
+        for (int q = 0; q < 2; q++) PB_CUDA(cudaEventCreateWithFlags(&evFill.e[q], cudaEventDisableTiming));
+        PB_TRY(fill_batch(0, std::min(B, nfreq), 0, sf));
+        PB_CUDA(cudaEventRecord(evFill.e[0], sf));
+    }
+    for (int b0 = 0, set = 0; b0 < nfreq; b0 += B, set ^= 1) {
+        const int nb = std::min(B, nfreq - b0);
+        const double *fb = freq + b0;
+        if (pipe) {
+            if (b0 + B < nfreq) {
+                PB_TRY(fill_batch(b0 + B, std::min(B, nfreq - b0 - B), set ^ 1, sf));
+                PB_CUDA(cudaEventRecord(evFill.e[set ^ 1], sf));
+            }
+            PB_CUDA(cudaStreamWaitEvent(st, evFill.e[set], 0));
+        } else {
+            PB_TRY(fill_batch(b0, nb, 0, st));
+        }
+        DevBuf &bM64 = set ? bM64b : bM64a, &bM32 = set ? bM32b : bM32a, &bP = set ? bPb : bPa;
+        DevBuf &bFreq = set ? bFreqb : bFreqa;
         // Precision per frequency. Frequencies at or below fp64_hz (the highest frequency
         // whose mixed solve stalled earlier in this sweep) go straight to an FP64 LU; they
         // form a prefix of the ascending batch. The rest are factorised in FP32 and refined.
@@ -1075,6 +1169,9 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
         PB_CUDA(cudaStreamSynchronize(st));
     }
     tAll.stop(st);
+    tStatic.finish();
+    tCorr.finish();
+    tAsm.finish();
     if (stats) {
         stats->t_static_ms = tStatic.acc;
         stats->t_corr_ms = tCorr.acc;
@@ -1099,6 +1196,7 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
         stats->gmres_refactored = refactored;
         stats->gmres_its_avg = gm_solves > 0 ? (double)gm_its / gm_solves : 0.0;
         stats->probe_fallbacks = probe_fb;
+        stats->pipelined = pipe ? 1 : 0;
         stats->probe_max = probe_max;
     }
     return PB_OK;

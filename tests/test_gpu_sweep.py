@@ -242,3 +242,19 @@ def test_accel_gmres_sweep_uses_fewer_factorisations():
     assert st["lu_count"] == 3 and st["fp64_fallbacks"] == 0, st
     assert st["gmres_solves"] == 24 and st["gmres_its_max"] <= 60, st
     assert zerr(za, zp) <= 1e-6, (zerr(za, zp), st)
+
+
+@pytest.mark.parametrize("name", ["cfg2_small", "dipole_halfwave"])
+def test_pipelined_batches_match_one_batch(golden, name):
+    """Batches of 2 frequencies (pipelined: each next batch filled on the context's second,
+    lower-priority stream while the current one is solved) give the single-batch Z; the
+    correction chunks differ, so FP32 rounding differs, within the mixed path's bar."""
+    prob, fx = golden(name)
+    with api.Context(prob) as ctx:
+        z1, s1 = ctx.sweep(fx["freqs"], fill_prec=abi.PREC_MIXED, lu=abi.LU_TC)
+        z2, s2 = ctx.sweep(fx["freqs"], fill_prec=abi.PREC_MIXED, lu=abi.LU_TC, batch=2)
+        z3, s3 = ctx.sweep(fx["freqs"], fill_prec=abi.PREC_FP64, lu=abi.LU_FP64, batch=2)
+        z4, _ = ctx.sweep(fx["freqs"], fill_prec=abi.PREC_FP64, lu=abi.LU_FP64)
+    assert len(fx["freqs"]) > 2 and s2["pipelined"] == 1 and s1["pipelined"] == 0
+    assert zerr(z2, z1) <= 1e-7, zerr(z2, z1)
+    assert zerr(z3, z4) <= 1e-12, zerr(z3, z4)
