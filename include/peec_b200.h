@@ -137,7 +137,10 @@ typedef struct {
                                preconditioner, matrix-free GMRES(60) per port to the relative
                                residual refine_tol (0 = 1e-10, ACCEL_TOL); full MNA form,
                                with capacitance the charge block P is compressed too */
-    int    pad_;
+    int    aca_dense;       /* compressed path: 0 = the Lp block's ACA rows / columns and its
+                               dense blocks are evaluated on demand from the geometry (no
+                               N x N fill, the reference's hmat_entry_fn route); 1 = fill the
+                               whole block densely first and compress from it (same values) */
     double ctol;            /* ACA relative tolerance (0 = 1e-6, the reference's default) */
     const float *pc_mlp;    /* compressed path: weights (pb_mlp_nparam() floats) of the learned
                                correction of the preconditioner's leaf blocks, NULL = plain
@@ -159,7 +162,8 @@ typedef struct {
 
 typedef struct {
     double t_static_ms, t_corr_ms, t_assemble_ms, t_lu_ms, t_refine_ms, t_total_ms;
-    double corr_samples;    /* retardation-correction quadrature samples evaluated    */
+    double corr_samples;    /* retardation-correction quadrature samples evaluated (the
+                               compressed path with on-demand entries: of P only)       */
     double lu_flops;        /* (8/3) n^3 per LU, (4/3) n^3 per L D L^T, summed       */
     double max_resid;       /* largest final normwise backward error |r|/(|A||x|+|b|) */
     int    max_iters;       /* largest refinement iteration count                    */
@@ -190,6 +194,8 @@ typedef struct {
     int    pipelined;      /* 1 = batches were pipelined: the next batch filled on a second,
                               lower-priority stream while the current one was solved       */
     double probe_max;      /* largest probe sensitivity |dV_port| / |V_port| of the sweep   */
+    double hmat_entries;   /* compressed path: entries of the Lp block evaluated, summed over
+                              the frequencies (N^2 per frequency for the dense fill)        */
 } pb_sweep_stats;
 
 const char *pb_last_error(void);

@@ -56,7 +56,7 @@ class PbSweepOpts(C.Structure):
     _fields_ = [
         ("fill_prec", C.c_int), ("lu", C.c_int), ("form", C.c_int), ("batch", C.c_int),
         ("refine_tol", C.c_double), ("refine_maxit", C.c_int), ("verbose", C.c_int),
-        ("corr_freqs", C.c_int), ("accel", C.c_int), ("compress", C.c_int), ("pad_", C.c_int),
+        ("corr_freqs", C.c_int), ("accel", C.c_int), ("compress", C.c_int), ("aca_dense", C.c_int),
         ("ctol", C.c_double), ("pc_mlp", C.c_void_p), ("pc_coarse", C.c_int), ("pc_exact_leaf", C.c_int),
     ]
 
@@ -77,6 +77,7 @@ class PbSweepStats(C.Structure):
         ("hmat_dense_far", C.c_int), ("hmat_mb", C.c_double), ("hmat_dense_mb", C.c_double),
         ("pc_mlp_fallbacks", C.c_int), ("pc_coarse_n", C.c_int), ("t_coarse_ms", C.c_double),
         ("probe_fallbacks", C.c_int), ("pipelined", C.c_int), ("probe_max", C.c_double),
+        ("hmat_entries", C.c_double),
     ]
 
     def as_dict(self):

@@ -66,7 +66,7 @@ class Context:
     def sweep(self, freqs, fill_prec=abi.PREC_MIXED, lu=abi.LU_TC, form=abi.FORM_AUTO,
               batch=0, refine_tol=0.0, refine_maxit=0, want_segi=False, zmat_out=None,
               corr_freqs=0, verbose=0, accel=None, compress=None, ctol=None, pc_mlp=None, pc_coarse=0,
-              want_cellq=False, pc_exact_leaf=0):
+              want_cellq=False, pc_exact_leaf=0, aca_dense=0):
         """pb_sweep. accel / compress / ctol = None take the .peec file's acceleration and
         compression keys. want_cellq (pb_sweep_dist) adds the cell charges
         [nfreq, nport, ncell] of every port excitation after the segment currents."""
@@ -85,6 +85,7 @@ class Context:
             o.pc_mlp = pc_mlp.ctypes.data
         o.pc_coarse = int(pc_coarse)
         o.pc_exact_leaf = int(pc_exact_leaf)
+        o.aca_dense = int(aca_dense)
         st = abi.PbSweepStats()
         if want_cellq:
             q = np.zeros((len(freqs), npt, self.ncell), np.complex128)

@@ -639,41 +639,59 @@ __device__ __forceinline__ void reduce_select(Acc<double, F> &a, int lane, doubl
 }
 
 // ---------------------------------------------------------------- static kernels
+// Static part of Lp(i, j), i <= j (partial.c:392-423), as one entry.
+__device__ __forceinline__ double lp_static_entry(const pb_fill_geom &g, int i, int j, double kw)
+{
+    const double coef = PB_MU0 / (4 * PB_PI);
+    Cell si, sj, mj;
+    load_cell(si, g.seg.cell, g.pv, i, 0, g.gpz);
+    const double ai = g.seg.cell[i].aL, aj = g.seg.cell[j].aL;
+    double t1[3], t2[3];
+    tangent(si, t1);
+    double v = 0;
+    if (i == j) {                                   // partial.c:392-401
+        v = static_term(si, si, 1, ai, ai, kw);
+        if (g.gp) {
+            load_cell(mj, g.seg.cell, g.pv, i, 1, g.gpz);
+            const double tdm = t1[0] * t1[0] + t1[1] * t1[1] - t1[2] * t1[2];
+            v -= tdm * static_term(si, mj, 0, ai, ai, kw);
+        }
+    } else {                                        // partial.c:403-423
+        load_cell(sj, g.seg.cell, g.pv, j, 0, g.gpz);
+        tangent(sj, t2);
+        const double tdot = dot3(t1, t2);
+        const double tdm = t1[0] * t2[0] + t1[1] * t2[1] - t1[2] * t2[2];
+        if (tdot != 0) v = tdot * static_term(si, sj, 0, ai, aj, kw);
+        if (g.gp && tdm != 0) {
+            load_cell(mj, g.seg.cell, g.pv, j, 1, g.gpz);
+            v -= tdm * static_term(si, mj, 0, ai, aj, kw);
+        }
+    }
+    return coef * v;
+}
+
 __global__ void __launch_bounds__(128)
 k_lp_static(pb_fill_geom g, double kw, double *st)
 {
     const int n = g.seg.n;
     const long long T = (long long)n * (n + 1) / 2;
-    const double coef = PB_MU0 / (4 * PB_PI);
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < T;
          t += (long long)gridDim.x * blockDim.x) {
         int i, j;
         tri_index(t, n, i, j);
-        Cell si, sj, mj;
-        load_cell(si, g.seg.cell, g.pv, i, 0, g.gpz);
-        const double ai = g.seg.cell[i].aL, aj = g.seg.cell[j].aL;
-        double t1[3], t2[3];
-        tangent(si, t1);
-        double v = 0;
-        if (i == j) {                                   // partial.c:392-401
-            v = static_term(si, si, 1, ai, ai, kw);
-            if (g.gp) {
-                load_cell(mj, g.seg.cell, g.pv, i, 1, g.gpz);
-                const double tdm = t1[0] * t1[0] + t1[1] * t1[1] - t1[2] * t1[2];
-                v -= tdm * static_term(si, mj, 0, ai, ai, kw);
-            }
-        } else {                                        // partial.c:403-423
-            load_cell(sj, g.seg.cell, g.pv, j, 0, g.gpz);
-            tangent(sj, t2);
-            const double tdot = dot3(t1, t2);
-            const double tdm = t1[0] * t2[0] + t1[1] * t2[1] - t1[2] * t2[2];
-            if (tdot != 0) v = tdot * static_term(si, sj, 0, ai, aj, kw);
-            if (g.gp && tdm != 0) {
-                load_cell(mj, g.seg.cell, g.pv, j, 1, g.gpz);
-                v -= tdm * static_term(si, mj, 0, ai, aj, kw);
-            }
-        }
-        st[(long long)i * n + j] = coef * v;
+        st[(long long)i * n + j] = lp_static_entry(g, i, j, kw);
+    }
+}
+
+// the static part of a pair list: stl[t] = static Lp(min, max of pairs[t])
+__global__ void __launch_bounds__(128)
+k_lp_static_list(pb_fill_geom g, double kw, const int2 *pairs, const int *npair, double *stl)
+{
+    const long long T = *npair;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < T;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int2 p = pairs[t];
+        stl[t] = lp_static_entry(g, min(p.x, p.y), max(p.x, p.y), kw);
     }
 }
 
@@ -817,7 +835,7 @@ k_corr(pb_fill_geom g, KArg k, const double *st, pb_epi_args ea, double2 *ig, lo
     static_assert(nbase<F, 1>() <= PB_TBASE, "EQ bases per term");
     const pb_dev_cells &set = SET == PB_SET_LP ? g.seg : g.chg;
     const int n = set.n;
-    const long long T = (long long)n * (n + 1) / 2;
+    const long long T = EPI == PB_EPI_LIST ? (long long)*ea.npair : (long long)n * (n + 1) / 2;
     const double coef = PB_MU0 / (4 * PB_PI);
     // far pairs two at a time: each half-warp needs its own phase bases
     constexpr bool PAIR_FAR = sizeof(R) == 4 && 2 * nbase<F, EQ>() <= PB_FMAX + 1;
@@ -832,7 +850,13 @@ k_corr(pb_fill_geom g, KArg k, const double *st, pb_epi_args ea, double2 *ig, lo
         const long long t = g0 + pl;
         int i = 0, j = 0, ok = 0;
         if (t < T) {
-            tri_index(t, n, i, j);
+            if constexpr (EPI == PB_EPI_LIST) {
+                const int2 p = ea.pairs[t];
+                i = min(p.x, p.y);
+                j = max(p.x, p.y);
+            } else {
+                tri_index(t, n, i, j);
+            }
             if (kw0 > 0 && (term == 0 || g.gp)) {
                 Cell si, sj;
                 load_cell(si, set.cell, g.pv, i, 0, g.gpz);
@@ -910,7 +934,12 @@ k_corr(pb_fill_geom g, KArg k, const double *st, pb_epi_args ea, double2 *ig, lo
             }
         };
         // one entry (pair i, j) at frequency f from its correction cr + j cim
-        auto emit = [&](int i, int j, int f, double cr, double cim) {
+        auto emit = [&](int i, int j, int f, double cr, double cim, long long t) {
+            if constexpr (EPI == PB_EPI_LIST) {     // one wavenumber; static part per entry
+                const double lr = st[t] + cr;
+                ea.out[t] = make_double2(ea.lscale_re * lr - ea.lscale_im * cim, ea.lscale_re * cim + ea.lscale_im * lr);
+                return;
+            }
             if (SET == PB_SET_IG) {
                 ig[f * igs + (long long)i * n + j] = make_double2(cr, cim);
                 return;
@@ -1021,7 +1050,7 @@ k_corr(pb_fill_geom g, KArg k, const double *st, pb_epi_args ea, double2 *ig, lo
                     f = 0;
                 }
             }
-            if (tk >= 0 && f < nf) emit(hdr[tk].i, hdr[tk].j, f, cr, cim);
+            if (tk >= 0 && f < nf) emit(hdr[tk].i, hdr[tk].j, f, cr, cim, g0 + tk);
         }
         __syncwarp();
     }
@@ -1287,7 +1316,7 @@ static int launch_corr(const pb_fill_geom &g, const KArg &k, const double *st, c
                        double2 *ig, long long igs, cudaStream_t s)
 {
     const int n = SET == PB_SET_LP ? g.seg.n : g.chg.n;
-    const long long T = (long long)n * (n + 1) / 2;
+    const long long T = EPI == PB_EPI_LIST ? ea.lcap : (long long)n * (n + 1) / 2;
     constexpr size_t smem = corr_smem_bytes<R, F, EQ>();
     static std::atomic<unsigned long long> attr_set{0};   // per device, before any launch relies on it
     PB_TRY(pb_smem_optin(k_corr<R, F, SET, EPI, EQ, RED>, (int)smem, attr_set));
@@ -1361,6 +1390,32 @@ int pb_lp_corr(const pb_fill_geom &g, int nf, const double *kw, int use_fp32, co
         : launch_corr_any<PB_SET_LP, PB_EPI_REDUCED>(g, k, use_fp32, stLp, ea, nullptr, 0, s);
     if (launches) (*launches)++;
     (void)samples;
+    return r;
+}
+
+int pb_lp_entries(const pb_fill_geom &g, double kw, int use_fp32, const int2 *pairs, const int *npair_dev,
+                  long long cap, double2 scale, double *stl, double2 *out, cudaStream_t s, long *launches)
+{
+    if (cap <= 0 || g.seg.n == 0) return PB_OK;
+    k_lp_static_list<<<grid_for(cap, 128), 128, 0, s>>>(g, kw, pairs, npair_dev, stl);
+    if (launches) (*launches)++;
+    PB_CHECK_LAUNCH();
+    KArg k;
+    make_karg(k, 1, &kw, g.pmax);
+    pb_epi_args ea;
+    ea.out = out;
+    ea.pairs = pairs;
+    ea.npair = npair_dev;
+    ea.lcap = cap;
+    ea.lscale_re = scale.x;
+    ea.lscale_im = scale.y;
+    int r;
+    if (use_fp32)
+        r = k.reduce ? launch_corr<float, 1, PB_SET_LP, PB_EPI_LIST, 0, 1>(g, k, stl, ea, nullptr, 0, s)
+                     : launch_corr<float, 1, PB_SET_LP, PB_EPI_LIST, 0, 0>(g, k, stl, ea, nullptr, 0, s);
+    else
+        r = launch_corr<double, 1, PB_SET_LP, PB_EPI_LIST, 0, 0>(g, k, stl, ea, nullptr, 0, s);
+    if (launches) (*launches)++;
     return r;
 }
 

@@ -31,7 +31,7 @@ struct pb_fill_geom {
 #define PB_FAR_KL 0.1
 
 // Epilogue of the Lp correction kernel.
-enum { PB_EPI_STORE = 0, PB_EPI_REDUCED = 1 };
+enum { PB_EPI_STORE = 0, PB_EPI_REDUCED = 1, PB_EPI_LIST = 2 };
 
 struct pb_epi_args {
     // STORE: out[f][i][j] (both triangles), FP64 complex, stride per frequency
@@ -46,12 +46,27 @@ struct pb_epi_args {
     const double2 *zint = nullptr;  // [f][nseg]
     int lower = 0;                  // REDUCED: write only the lower triangle (symmetric solves)
     double omega[PB_FMAX];
+    // LIST (one wavenumber): out[t] = lscale * Lp(pairs[t]) for t < *npair, the static
+    // part read from st[t]; lcap bounds *npair and sizes the launch
+    const int2 *pairs = nullptr;
+    const int *npair = nullptr;
+    long long lcap = 0;
+    double lscale_re = 1, lscale_im = 0;
 };
 
 // FP64 static tables: stLp[i*n+j] (i <= j) = coef * sum_terms weight * static;
 // stP[ci*nc+cj] (ci <= cj) likewise for P.
 int pb_lp_static(const pb_fill_geom &g, double kw, double *stLp, cudaStream_t s, long *launches);
 int pb_pot_static(const pb_fill_geom &g, double kw, double *stP, cudaStream_t s, long *launches);
+
+// Entries of Lp at one wavenumber for an explicit list of cell pairs (the on-demand rows,
+// columns and dense blocks of the compressed path): out[t] = scale * Lp(pairs[t].x,
+// pairs[t].y) for t < *npair_dev (device count, at most cap), FP64 static part and the
+// FP32 (use_fp32) or FP64 correction. Each entry is evaluated as its (min, max) pair of
+// the dense fill (pb_lp_static + pb_lp_corr with nf = 1), so the values are the same bits.
+// stl: scratch of cap doubles.
+int pb_lp_entries(const pb_fill_geom &g, double kw, int use_fp32, const int2 *pairs, const int *npair_dev,
+                  long long cap, double2 scale, double *stl, double2 *out, cudaStream_t s, long *launches);
 
 // Correction kernels for nf <= PB_FMAX wavenumbers (kw[f] > 0). use_fp32 selects the
 // FP32 quadrature (mixed path) or FP64 (plain path). With kw == 0 (quasi-static) pass

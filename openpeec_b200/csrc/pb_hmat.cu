@@ -1,12 +1,15 @@
 // pb_hmat.cu — compressed (matrix-free) sweep for large structures, compression = 1:
 //   * cluster tree + block partition on the host (hmatrix.c:91-227, same deterministic
 //     splits as the reference, so the same blocks),
-//   * the kernel blocks Lp(f) (and, with capacitance, P(f) over the node cells) are filled
-//     densely on the device (74k cells is 89 GB in FP64, within HBM) and their far blocks
-//     are compressed by partially pivoted ACA with the
-//     reference's restarts from unrepresented rows (aca_block, hmatrix.c:265-395), one CTA
-//     per block, entries read from the dense fill; near blocks (and far blocks that do not
-//     compress) are copied out dense,
+//   * the far blocks of the kernel block Lp(f) are compressed by partially pivoted ACA with
+//     the reference's restarts from unrepresented rows (aca_block, hmatrix.c:265-395), all
+//     blocks advancing together one row / one column half-step per launch, the rows and
+//     columns they ask for evaluated on demand from the geometry (the hmat_entry_fn
+//     callback, peec.h:279, as a batched device evaluation); near blocks (and far blocks
+//     that do not compress) are evaluated densely, entry by entry; no N x N array is
+//     formed. The dense fill followed by one CTA per block over it (k_aca) stays as an
+//     option and for the experiments that need the whole block; with capacitance the P(f)
+//     block over the node cells is filled densely and compressed that way,
 //   * H-matrix x vector product in two phases, t_b = V_b^T x then one warp per row summing
 //     its leaf's blocks in a fixed order (hmat_matvec, hmatrix.c:680-778), so results do not
 //     depend on scheduling,
@@ -297,6 +300,244 @@ k_aca(const double2 *K, int n, const int *perm, const AcaBlk *blks, double2 *U, 
     if (tid == 0) rank[blockIdx.x] = (k <= 0 || k >= lim) ? -1 : k;
 }
 
+// ---- the same ACA with entries evaluated on demand. All far blocks advance together, one
+// half-step per launch: a row half-step (residual row, pivot column or a restart row) and a
+// column half-step (residual column, norms, next pivot row). Between them the entries each
+// block asks for (one row or one column of the kernel block) are evaluated from the
+// geometry by pb_lp_entries, so no dense N x N block is formed. The per-block arithmetic
+// and its order are those of k_aca, and the entries are the same bits as the dense fill's,
+// so both give the same factors.
+struct AcaSt {
+    double fro2, urmax;
+    int k, irow, jcol, probe;
+    int st;                       // 0: needs row irow, 1: needs column jcol, 2: done
+    int pad;
+    long long ent;                // offset of its requested entries in the half-step's list
+};
+
+__global__ void k_acaod_init(const AcaBlk *blks, AcaSt *S, int *rused_pool, double *urep_pool, int *rank)
+{
+    const AcaBlk B = blks[blockIdx.x];
+    for (int i = threadIdx.x; i < B.m; i += blockDim.x) {
+        rused_pool[B.soff + i] = 0;
+        urep_pool[B.soff + i] = 0;
+    }
+    if (threadIdx.x == 0) {
+        AcaSt s;
+        s.fro2 = s.urmax = 0;
+        s.k = s.irow = s.probe = 0;
+        s.jcol = -1;
+        s.st = B.lim > 0 ? 0 : 2;
+        s.pad = 0;
+        s.ent = 0;
+        S[blockIdx.x] = s;
+        if (s.st == 2) rank[blockIdx.x] = -1;
+    }
+}
+
+// Offsets of the entries the blocks in state `want` request, in block order (the lists do
+// not depend on scheduling): cnt[0] = entries requested, cnt[1] = blocks not done;
+// acc[want] accumulates the entries requested over the build.
+__global__ void __launch_bounds__(1024)
+k_acaod_scan(int nb, const AcaBlk *blks, AcaSt *S, int want, int *cnt, long long *acc)
+{
+    __shared__ long long wsum[32];
+    __shared__ long long carry;
+    __shared__ int nact;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (threadIdx.x == 0) { carry = 0; nact = 0; }
+    __syncthreads();
+    int act = 0;
+    for (int base = 0; base < nb; base += 1024) {
+        const int b = base + threadIdx.x;
+        long long len = 0;
+        if (b < nb) {
+            const int st = S[b].st;
+            act += st != 2;
+            if (st == want) len = want == 0 ? blks[b].nn : blks[b].m;
+        }
+        long long x = len;                             // inclusive scan: warp, then warps
+        for (int o = 1; o < 32; o <<= 1) {
+            const long long y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) wsum[w] = x;
+        __syncthreads();
+        if (w == 0) {
+            long long v = wsum[lane];
+            for (int o = 1; o < 32; o <<= 1) {
+                const long long y = __shfl_up_sync(0xffffffffu, v, o);
+                if (lane >= o) v += y;
+            }
+            wsum[lane] = v;
+        }
+        __syncthreads();
+        const long long excl = carry + (w > 0 ? wsum[w - 1] : 0) + x - len;
+        if (len > 0) S[b].ent = excl;
+        __syncthreads();
+        if (threadIdx.x == 1023) carry = excl + len;
+        __syncthreads();
+    }
+    atomicAdd(&nact, act);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        cnt[0] = (int)carry;
+        cnt[1] = nact;
+        acc[want] += carry;
+    }
+}
+
+// the cell pairs of each requesting block's row (want 0) or column (want 1)
+__global__ void k_acaod_pairs(const AcaBlk *blks, const AcaSt *S, const int *perm, int want, int2 *pairs)
+{
+    const AcaSt s = S[blockIdx.x];
+    if (s.st != want) return;
+    const AcaBlk B = blks[blockIdx.x];
+    if (want == 0) {
+        const int pr = perm[B.r0 + s.irow];
+        for (int j = threadIdx.x; j < B.nn; j += blockDim.x) pairs[s.ent + j] = make_int2(pr, perm[B.c0 + j]);
+    } else {
+        const int pc = perm[B.c0 + s.jcol];
+        for (int i = threadIdx.x; i < B.m; i += blockDim.x) pairs[s.ent + i] = make_int2(perm[B.r0 + i], pc);
+    }
+}
+
+// row half-step: v_k = A(irow, :) - sum_l u_l[irow] v_l from the evaluated row
+__global__ void __launch_bounds__(256)
+k_acaod_row(const AcaBlk *blks, AcaSt *S, const double2 *vals, double2 *U, double2 *V, int *rused_pool,
+            double *urep_pool, double tol, int *rank)
+{
+    __shared__ double shv[33];
+    __shared__ int shi[33];
+    AcaSt s = S[blockIdx.x];
+    if (s.st != 0) return;
+    const AcaBlk B = blks[blockIdx.x];
+    const int m = B.m, nn = B.nn, tid = threadIdx.x, bd = blockDim.x;
+    const double2 *u = U + B.uoff;
+    double2 *v = V + B.voff;
+    int *rused = rused_pool + B.soff;
+    const double *urep = urep_pool + B.soff;
+    const double2 *row = vals + s.ent;
+    const int k = s.k, irow = s.irow;
+    double rn2 = 0, amax = 0;
+    int jmax = -1;
+    for (int j = tid; j < nn; j += bd) {
+        double2 a = row[j];
+        for (int l = 0; l < k; l++) a = csub(a, cmul(u[(long long)l * m + irow], v[(long long)l * nn + j]));
+        v[(long long)k * nn + j] = a;
+        const double t2 = cabs2(a), t = sqrt(t2);
+        rn2 += t2;
+        if (t > amax) { amax = t; jmax = j; }
+    }
+    rn2 = bsum(rn2, shv);
+    bargext(amax, jmax, true, shv, shi);
+    if (tid == 0) rused[irow] = 1;
+    __syncthreads();
+    if (jmax < 0 || amax <= 0 || sqrt(rn2) <= tol * sqrt(s.fro2)) {
+        bool done = ++s.probe > PB_HM_PROBE;
+        if (!done) {
+            const int nxt = aca_unrep(rused, urep, m, tol * s.urmax, shv, shi);
+            if (nxt < 0) done = true;
+            else s.irow = nxt;
+        }
+        if (done) s.st = 2;
+    } else {
+        s.probe = 0;
+        const double2 piv = v[(long long)k * nn + jmax];
+        __syncthreads();
+        for (int j = tid; j < nn; j += bd) v[(long long)k * nn + j] = cdiv64(v[(long long)k * nn + j], piv);
+        s.jcol = jmax;
+        s.st = 1;
+    }
+    if (tid == 0) {
+        S[blockIdx.x] = s;
+        if (s.st == 2) rank[blockIdx.x] = (s.k <= 0 || s.k >= B.lim) ? -1 : s.k;
+    }
+}
+
+// column half-step: u_k = A(:, jcol) - sum_l u_l v_l[jcol], ||A_k||_F, next pivot row
+__global__ void __launch_bounds__(256)
+k_acaod_col(const AcaBlk *blks, AcaSt *S, const double2 *vals, double2 *U, const double2 *V,
+            const int *rused_pool, double *urep_pool, double tol, int *rank)
+{
+    __shared__ double shv[33];
+    __shared__ int shi[33];
+    AcaSt s = S[blockIdx.x];
+    if (s.st != 1) return;
+    const AcaBlk B = blks[blockIdx.x];
+    const int m = B.m, nn = B.nn, tid = threadIdx.x, bd = blockDim.x;
+    double2 *u = U + B.uoff;
+    const double2 *v = V + B.voff;
+    const int *rused = rused_pool + B.soff;
+    double *urep = urep_pool + B.soff;
+    const double2 *col = vals + s.ent;
+    const int k = s.k, jmax = s.jcol;
+    double un2 = 0;
+    for (int i = tid; i < m; i += bd) {
+        double2 a = col[i];
+        for (int l = 0; l < k; l++) a = csub(a, cmul(u[(long long)l * m + i], v[(long long)l * nn + jmax]));
+        u[(long long)k * m + i] = a;
+        un2 += cabs2(a);
+    }
+    double vn2 = 0;
+    for (int j = tid; j < nn; j += bd) vn2 += cabs2(v[(long long)k * nn + j]);
+    un2 = bsum(un2, shv);
+    vn2 = bsum(vn2, shv);
+    double cross = 0;
+    for (int l = 0; l < k; l++) {
+        double dur = 0, dui = 0, dvr = 0, dvi = 0;
+        for (int i = tid; i < m; i += bd) {
+            const double2 a = u[(long long)l * m + i], b = u[(long long)k * m + i];
+            dur += a.x * b.x + a.y * b.y;
+            dui += a.x * b.y - a.y * b.x;
+        }
+        for (int j = tid; j < nn; j += bd) {
+            const double2 a = v[(long long)l * nn + j], b = v[(long long)k * nn + j];
+            dvr += a.x * b.x + a.y * b.y;
+            dvi += a.x * b.y - a.y * b.x;
+        }
+        dur = bsum(dur, shv);
+        dui = bsum(dui, shv);
+        dvr = bsum(dvr, shv);
+        dvi = bsum(dvi, shv);
+        const double pr = dur * dvr - dui * dvi, pi = dur * dvi + dui * dvr;
+        cross += 2 * sqrt(pr * pr + pi * pi);
+    }
+    s.fro2 += un2 * vn2 + cross;
+    s.k = k + 1;
+    double lmax = 0, umax = 0;
+    int inext = -1;
+    const bool go = sqrt(un2) * sqrt(vn2) > tol * sqrt(s.fro2 > 0 ? s.fro2 : 1);
+    for (int i = tid; i < m; i += bd) {
+        const double t = sqrt(cabs2(u[(long long)k * m + i]));
+        if (t > urep[i]) urep[i] = t;
+        if (t > lmax) lmax = t;
+        if (go && !rused[i] && t > umax) { umax = t; inext = i; }
+    }
+    int dummy = 0;
+    bargext(lmax, dummy, true, shv, shi);
+    if (lmax > s.urmax) s.urmax = lmax;
+    bargext(umax, inext, true, shv, shi);
+    __syncthreads();
+    bool done = false;
+    if (inext < 0) {
+        if (++s.probe > PB_HM_PROBE) done = true;
+        else {
+            inext = aca_unrep(rused, urep, m, tol * s.urmax, shv, shi);
+            if (inext < 0) done = true;
+        }
+    }
+    if (!done) {
+        s.irow = inext;
+        if (s.k >= B.lim) done = true;
+    }
+    s.st = done ? 2 : 0;
+    if (tid == 0) {
+        S[blockIdx.x] = s;
+        if (done) rank[blockIdx.x] = (s.k <= 0 || s.k >= B.lim) ? -1 : s.k;
+    }
+}
+
 // dense copies: out[off + i*nn + j] = scale * K[perm[r0+i]][perm[c0+j]]
 struct DBlk { int r0, m, c0, nn; long long off; };
 __global__ void k_gather(const double2 *K, int n, const int *perm, const DBlk *blks, double2 scale, double2 *out)
@@ -308,6 +549,20 @@ __global__ void k_gather(const double2 *K, int n, const int *perm, const DBlk *b
         out[B.off + e] = cmul(scale, K[(long long)perm[B.r0 + i] * n + perm[B.c0 + j]]);
     }
 }
+
+// the cell pairs of dense blocks (on-demand entries): pairs[off + i*nn + j] in block order,
+// off relative to the first block of the launch
+__global__ void k_dense_pairs(const int *perm, const DBlk *blks, long long base, int2 *pairs)
+{
+    const DBlk B = blks[blockIdx.x];
+    const long long tot = (long long)B.m * B.nn;
+    for (long long e = threadIdx.x; e < tot; e += blockDim.x) {
+        const int i = (int)(e / B.nn), j = (int)(e % B.nn);
+        pairs[B.off - base + e] = make_int2(perm[B.r0 + i], perm[B.c0 + j]);
+    }
+}
+
+__global__ void k_set_count(int *cnt, int v) { *cnt = v; }
 
 // ================================================================ device: H x vector
 // uoff: the block's U, scaled and row by row, in the compact Urm; usrc: its columns in the
@@ -766,6 +1021,8 @@ struct KBlock {
     std::vector<int> bri, bci, cri, cci;
     std::vector<zc> bval, cval;
     Dev lof_d, lidx_d, dof_d, dlu_d, dpiv_d, bro, bcol, bv, cro, ccol, cv, wb, ub;
+    // on-demand entries: ACA state, pair list, static parts, values, counts
+    Dev od_st, od_pairs, od_stl, od_vals, od_cnt, od_acc, od_blk;
 };
 
 // tree, leaves and ACA workspace of a block (hmat_build_gen, hmatrix.c:403-421)
@@ -818,13 +1075,133 @@ int kb_setup(KBlock &kb, const double *pts, cudaStream_t st)
     return PB_OK;
 }
 
-// H-matrix of scale * K: ACA on the far blocks, dense copies of the rest, per-leaf lists,
-// and the scaled leaf-diagonal blocks for the preconditioner (dlu, host)
-int kb_compress(KBlock &kb, const double2 *K, double ctol, pb_ctx *c, pb_hstats *hs)
+// Entries of the Lp kernel block evaluated on demand at wavenumber kw (FP32 or FP64
+// correction, as the dense fill would use); entries counts what was evaluated.
+struct OnDemand {
+    double kw = 0;
+    int fill32 = 0;
+    double entries = 0;
+};
+
+// ACA of every far block with on-demand rows and columns (k_acaod_*): one row and one
+// column half-step per round for all blocks still running, until none is.
+int kb_aca_ondemand(KBlock &kb, pb_ctx *c, OnDemand &od, double ctol)
+{
+    const cudaStream_t st = c->stream;
+    const int nfar = (int)kb.ab.size();
+    if (nfar == 0) return PB_OK;
+    long long sm = 0, sn = 0;
+    for (const AcaBlk &B : kb.ab) { sm += B.m; sn += B.nn; }
+    const long long cap = std::max(sm, sn);
+    if (cap >= (1LL << 31)) { pb_set_error("compressed sweep: %lld on-demand entries per step", cap); return PB_ERR_UNSUP; }
+    PB_TRY(kb.od_st.alloc(sizeof(AcaSt) * (size_t)nfar));
+    PB_TRY(kb.od_pairs.alloc(sizeof(int2) * (size_t)cap));
+    PB_TRY(kb.od_stl.alloc(sizeof(double) * (size_t)cap));
+    PB_TRY(kb.od_vals.alloc(sizeof(double2) * (size_t)cap));
+    PB_TRY(kb.od_cnt.alloc(sizeof(int) * 2));
+    PB_TRY(kb.od_acc.alloc(sizeof(long long) * 2));
+    AcaSt *S = kb.od_st.as<AcaSt>();
+    const AcaBlk *blk = kb.aca.as<AcaBlk>();
+    int *cnt = kb.od_cnt.as<int>(), *rank = kb.rank.as<int>();
+    long long *acc = kb.od_acc.as<long long>();
+    PB_CUDA(cudaMemsetAsync(acc, 0, sizeof(long long) * 2, st));
+    k_acaod_init<<<nfar, 256, 0, st>>>(blk, S, kb.rused.as<int>(), kb.urep.as<double>(), rank);
+    c->launches++;
+    PB_CHECK_LAUNCH();
+    // every round advances each running block by a row; a block ends after at most
+    // PB_HM_MAXIT ranks, each with at most PB_HM_PROBE + 1 rows
+    const int maxit = (PB_HM_MAXIT + 1) * (PB_HM_PROBE + 2);
+    int hc[2] = {0, 0};
+    for (int it = 0;; it++) {
+        k_acaod_scan<<<1, 1024, 0, st>>>(nfar, blk, S, 0, cnt, acc);
+        c->launches++;
+        PB_CHECK_LAUNCH();
+        PB_CUDA(cudaMemcpyAsync(hc, cnt, sizeof(hc), cudaMemcpyDeviceToHost, st));
+        PB_CUDA(cudaStreamSynchronize(st));
+        if (hc[1] == 0) break;
+        if (it >= maxit) {
+            pb_set_error("compressed sweep: on-demand ACA still running after %d rounds", maxit);
+            return PB_ERR_NOCONV;
+        }
+        for (int want = 0; want < 2; want++) {
+            if (want == 1) {
+                k_acaod_scan<<<1, 1024, 0, st>>>(nfar, blk, S, 1, cnt, acc);
+                c->launches++;
+            }
+            k_acaod_pairs<<<nfar, 256, 0, st>>>(blk, S, kb.perm.as<int>(), want, kb.od_pairs.as<int2>());
+            c->launches++;
+            PB_CHECK_LAUNCH();
+            PB_TRY(pb_lp_entries(c->g, od.kw, od.fill32, kb.od_pairs.as<int2>(), cnt, want == 0 ? hc[0] : sm,
+                                 make_double2(1, 0), kb.od_stl.as<double>(), kb.od_vals.as<double2>(), st,
+                                 &c->launches));
+            if (want == 0)
+                k_acaod_row<<<nfar, 256, 0, st>>>(blk, S, kb.od_vals.as<double2>(), kb.U.as<double2>(),
+                                                  kb.V.as<double2>(), kb.rused.as<int>(), kb.urep.as<double>(), ctol,
+                                                  rank);
+            else
+                k_acaod_col<<<nfar, 256, 0, st>>>(blk, S, kb.od_vals.as<double2>(), kb.U.as<double2>(),
+                                                  kb.V.as<double2>(), kb.rused.as<int>(), kb.urep.as<double>(), ctol,
+                                                  rank);
+            c->launches++;
+            PB_CHECK_LAUNCH();
+        }
+    }
+    long long ha[2] = {0, 0};
+    PB_CUDA(cudaMemcpyAsync(ha, acc, sizeof(ha), cudaMemcpyDeviceToHost, st));
+    PB_CUDA(cudaStreamSynchronize(st));
+    od.entries += (double)(ha[0] + ha[1]);
+    return PB_OK;
+}
+
+// out[B.off + i*nn + j] = scale * K(perm[r0+i], perm[c0+j]) for dense blocks (consecutive
+// offsets), entries evaluated on demand in chunks of at most 2^24 entries (or one block)
+int kb_dense_ondemand(KBlock &kb, pb_ctx *c, OnDemand &od, const std::vector<DBlk> &blks, double2 scale,
+                      double2 *out)
+{
+    const cudaStream_t st = c->stream;
+    if (blks.empty()) return PB_OK;
+    long long big = 0, total = 0;
+    for (const DBlk &B : blks) {
+        big = std::max(big, (long long)B.m * B.nn);
+        total += (long long)B.m * B.nn;
+    }
+    const long long chunk = std::max(1LL << 24, big), buf = std::min(total, chunk);
+    if (buf >= (1LL << 31)) { pb_set_error("compressed sweep: dense block of %lld entries", big); return PB_ERR_UNSUP; }
+    PB_TRY(kb.od_pairs.alloc(sizeof(int2) * (size_t)buf));
+    PB_TRY(kb.od_stl.alloc(sizeof(double) * (size_t)buf));
+    PB_TRY(kb.od_cnt.alloc(sizeof(int) * 2));
+    for (size_t q0 = 0; q0 < blks.size();) {
+        size_t q1 = q0;
+        long long tot = 0;
+        while (q1 < blks.size() && tot + (long long)blks[q1].m * blks[q1].nn <= chunk) {
+            tot += (long long)blks[q1].m * blks[q1].nn;
+            q1++;
+        }
+        const long long base = blks[q0].off;
+        std::vector<DBlk> part(blks.begin() + q0, blks.begin() + q1);
+        PB_TRY(upload(kb.od_blk, part, st));
+        k_dense_pairs<<<(unsigned)part.size(), 256, 0, st>>>(kb.perm.as<int>(), kb.od_blk.as<DBlk>(), base,
+                                                             kb.od_pairs.as<int2>());
+        k_set_count<<<1, 1, 0, st>>>(kb.od_cnt.as<int>(), (int)tot);
+        c->launches += 2;
+        PB_CHECK_LAUNCH();
+        PB_TRY(pb_lp_entries(c->g, od.kw, od.fill32, kb.od_pairs.as<int2>(), kb.od_cnt.as<int>(), tot, scale,
+                             kb.od_stl.as<double>(), out + base, st, &c->launches));
+        od.entries += (double)tot;
+        q0 = q1;
+    }
+    return PB_OK;
+}
+
+// H-matrix of scale * K: ACA on the far blocks, dense copies of the rest; K is the dense
+// fill, or nullptr with od: entries evaluated on demand
+int kb_compress(KBlock &kb, const double2 *K, double ctol, pb_ctx *c, pb_hstats *hs, OnDemand *od)
 {
     const cudaStream_t st = c->stream;
     const int nfar = (int)kb.T.fr.size(), nnear = (int)kb.T.nr.size();
-    if (nfar > 0) {
+    if (nfar > 0 && od) {
+        PB_TRY(kb_aca_ondemand(kb, c, *od, ctol));
+    } else if (nfar > 0) {
         k_aca<<<nfar, 256, 0, st>>>(K, kb.n, kb.perm.as<int>(), kb.aca.as<AcaBlk>(), kb.U.as<double2>(),
                                     kb.V.as<double2>(), kb.rused.as<int>(), kb.urep.as<double>(), ctol,
                                     kb.rank.as<int>());
@@ -884,7 +1261,9 @@ int kb_compress(KBlock &kb, const double2 *K, double ctol, pb_ctx *c, pb_hstats 
     }
     PB_TRY(upload(kb.dblk, kb.db, st));
     PB_TRY(kb.D.alloc(sizeof(double2) * (size_t)std::max(1LL, doff)));
-    if (!kb.db.empty()) {
+    if (!kb.db.empty() && od) {
+        PB_TRY(kb_dense_ondemand(kb, c, *od, kb.db, kb.scale, kb.D.as<double2>()));
+    } else if (!kb.db.empty()) {
         k_gather<<<(unsigned)kb.db.size(), 256, 0, st>>>(K, kb.n, kb.perm.as<int>(), kb.dblk.as<DBlk>(), kb.scale,
                                                          kb.D.as<double2>());
         c->launches++;
@@ -933,9 +1312,13 @@ int kb_compress(KBlock &kb, const double2 *K, double ctol, pb_ctx *c, pb_hstats 
     Dev bLb, bLd;
     PB_TRY(upload(bLb, lb, st));
     PB_TRY(bLd.alloc(sizeof(double2) * (size_t)std::max<long long>(1, kb.dof[nl])));
-    k_gather<<<nl, 256, 0, st>>>(K, kb.n, kb.perm.as<int>(), bLb.as<DBlk>(), kb.scale, bLd.as<double2>());
-    c->launches++;
-    PB_CHECK_LAUNCH();
+    if (od) {
+        PB_TRY(kb_dense_ondemand(kb, c, *od, lb, kb.scale, bLd.as<double2>()));
+    } else {
+        k_gather<<<nl, 256, 0, st>>>(K, kb.n, kb.perm.as<int>(), bLb.as<DBlk>(), kb.scale, bLd.as<double2>());
+        c->launches++;
+        PB_CHECK_LAUNCH();
+    }
     PB_CUDA(cudaMemcpyAsync(kb.dlu.data(), bLd.p, sizeof(double2) * kb.dof[nl], cudaMemcpyDeviceToHost, st));
     PB_CUDA(cudaStreamSynchronize(st));
     return PB_OK;
@@ -1153,6 +1536,10 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
     }
     const cudaStream_t st = c->stream;
     const int fill32 = (o.fill_prec == PB_PREC_MIXED);
+    // the Lp block's entries are evaluated on demand (no dense N x N fill) unless asked for
+    // the dense fill, or an option needs the dense block (exact leaf inverses, samples)
+    const bool od_lp = !o.aca_dense && !o.pc_exact_leaf && !sample_x;
+    double od_entries = 0;
     *hs = pb_hstats();
 
     // compressed blocks: Lp over the segment midpoints (hmat_build, hmatrix.c:617-634) and,
@@ -1189,9 +1576,11 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
     Held bK(cs + 0), bSt(cs + 1), bKP(cs + 2), bStP(cs + 3), bIg(cs + 4);
     Dev bZint, bFreq, bX, bB, bR, bW, bZ, bVk, bDot, bU1;
     const size_t stat_bytes = sizeof(double) * (size_t)ns * ns, statP_bytes = sizeof(double) * (size_t)nc * nc;
-    if (cs[1].cap < stat_bytes || (cap && cs[3].cap < statP_bytes)) c->comp_static_valid = false;
-    PB_TRY(bK.alloc(sizeof(double2) * (size_t)ns * ns));
-    PB_TRY(bSt.alloc(stat_bytes));
+    if ((!od_lp && cs[1].cap < stat_bytes) || (cap && cs[3].cap < statP_bytes)) c->comp_static_valid = false;
+    if (!od_lp) {
+        PB_TRY(bK.alloc(sizeof(double2) * (size_t)ns * ns));
+        PB_TRY(bSt.alloc(stat_bytes));
+    }
     if (cap) {
         PB_TRY(bKP.alloc(sizeof(double2) * (size_t)nc * nc));
         PB_TRY(bStP.alloc(statP_bytes));
@@ -1240,34 +1629,42 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
             std::vector<long> sig;
             level_signature(c, kw, sig);
             sig.push_back(cap);
+            sig.push_back(od_lp);
             if (!c->comp_static_valid || sig != c->comp_sig) {
                 c->comp_static_valid = false;
-                PB_TRY(pb_lp_static(c->g, kw, bSt.as<double>(), st, &c->launches));
+                if (!od_lp) PB_TRY(pb_lp_static(c->g, kw, bSt.as<double>(), st, &c->launches));
                 if (cap) PB_TRY(pb_pot_static(c->g, kw, bStP.as<double>(), st, &c->launches));
                 c->comp_sig = sig;
                 c->comp_static_valid = true;
             }
-            pb_epi_args ea;
-            ea.out = bK.as<double2>();
-            ea.out_stride = (long long)ns * ns;
-            PB_TRY(pb_lp_corr(c->g, 1, &kw, fill32, bSt.as<double>(), PB_EPI_STORE, ea, st, &c->launches, nullptr));
+            if (!od_lp) {
+                pb_epi_args ea;
+                ea.out = bK.as<double2>();
+                ea.out_stride = (long long)ns * ns;
+                PB_TRY(pb_lp_corr(c->g, 1, &kw, fill32, bSt.as<double>(), PB_EPI_STORE, ea, st, &c->launches,
+                                  nullptr));
+                od_entries += (double)ns * ns;
+            }
             if (cap) {
                 PB_TRY(pb_pot_corr(c->g, 1, &kw, fill32, bStP.as<double>(), bKP.as<double2>(), (long long)nc * nc,
                                    c->retardation ? bIg.as<double2>() : nullptr, st, &c->launches, nullptr));
             }
             if (kw > 0) {
                 sig.pop_back();
+                sig.pop_back();
                 std::vector<long> skey(sig);
                 skey.push_back(fill32 ? far_rule_key(c, kw) : -1);   // FP32: lower-order rules
                 auto it = c->sample_counts.find(skey);
-                if (it == c->sample_counts.end()) {
+                if (od_lp && !cap) {
+                    lp_samp = p_samp = 0;           // no dense fill to count
+                } else if (it == c->sample_counts.end()) {
                     PB_TRY(pb_count_samples(c->g, kw, &lp_samp, &p_samp, st, c->d_count, fill32 ? kw : 0.0));
                     c->sample_counts[skey] = std::make_pair(lp_samp, p_samp);
                 } else {
                     lp_samp = it->second.first;
                     p_samp = it->second.second;
                 }
-                samples += lp_samp + (cap ? p_samp : 0);
+                samples += (od_lp ? 0 : lp_samp) + (cap ? p_samp : 0);
             }
         }
         tock(t_fill);
@@ -1275,10 +1672,14 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
         tick();
         pb_hstats hf;
         kbs[0].scale = make_double2(0, -om);        // -jw Lp (solve.c:262)
-        PB_TRY(kb_compress(kbs[0], bK.as<double2>(), ctol, c, &hf));
+        OnDemand od;
+        od.kw = kw;
+        od.fill32 = fill32;
+        PB_TRY(kb_compress(kbs[0], od_lp ? nullptr : bK.as<double2>(), ctol, c, &hf, od_lp ? &od : nullptr));
+        od_entries += od.entries;
         if (cap) {
             kbs[1].scale = make_double2(1, 0);      // P (solve.c:275)
-            PB_TRY(kb_compress(kbs[1], bKP.as<double2>(), ctol, c, &hf));
+            PB_TRY(kb_compress(kbs[1], bKP.as<double2>(), ctol, c, &hf, nullptr));
         }
         hf.max_rank = std::max(hf.max_rank, hs->max_rank);
         *hs = hf;
@@ -2004,6 +2405,7 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
         stats->hmat_dense_far = hs->ndense_far;
         stats->hmat_mb = hs->mem_mb;
         stats->hmat_dense_mb = hs->dense_mb;
+        stats->hmat_entries = od_entries;
         stats->pc_mlp_fallbacks = mlp_fallbacks;
         stats->pc_coarse_n = coarse_n;
         stats->t_coarse_ms = t_coarse;

@@ -443,9 +443,12 @@ int pb_sweep_impl(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts 
 {
     pb_sweep_opts o;
     if (opts_in) o = *opts_in;
-    else { o.fill_prec = PB_PREC_MIXED; o.lu = PB_LU_TC; o.form = PB_FORM_AUTO; o.batch = 0;
-           o.refine_tol = 0; o.refine_maxit = 0; o.verbose = 0; o.corr_freqs = 0; o.accel = 0;
-           o.compress = 0; o.pad_ = 0; o.ctol = 0; }
+    else {
+        memset(&o, 0, sizeof(o));                  // every option off, pointers null
+        o.fill_prec = PB_PREC_MIXED;
+        o.lu = PB_LU_TC;
+        o.form = PB_FORM_AUTO;
+    }
     if (o.compress) {
         if (rhs_fixed) { pb_set_error("source excitation is not built for the compressed path"); return PB_ERR_UNSUP; }
         if (nfreq <= 0 || freq == nullptr) { pb_set_error("pb_sweep: no frequencies"); return PB_ERR_ARG; }

@@ -46,6 +46,29 @@ def test_compressed_matches_reference(name):
     assert np.all(e_den <= ref_err + 2e-5), (name, e_den, ref_err)
 
 
+@pytest.mark.parametrize("name,prec", [("compress_plate", "fp64"), ("bars_small", "mixed"),
+                                       ("cap_retarded", "mixed"), ("compress_wire", "fp64")])
+def test_on_demand_aca_equals_dense_fill(name, prec):
+    """ACA with entries evaluated on demand (rows, columns and dense blocks from the geometry,
+    no N x N fill) against the dense fill followed by ACA over it: the entries are the same
+    bits, so the blocks, ranks and Z agree to rounding; the on-demand build evaluates a
+    fraction of the N^2 entries per frequency."""
+    from openpeec_b200 import abi, api
+    prob, fx = load_golden(name, "comp")
+    fp = abi.PREC_FP64 if prec == "fp64" else abi.PREC_MIXED
+    with api.Context(prob) as ctx:
+        zd, sd = ctx.sweep(fx["freqs"], fill_prec=fp, compress=1, aca_dense=1)
+        zo, so = ctx.sweep(fx["freqs"], fill_prec=fp, compress=1, aca_dense=0)
+    n, nf = len(prob.seg), len(fx["freqs"])
+    for k in ("hmat_far", "hmat_near", "hmat_max_rank", "hmat_dense_far"):
+        assert sd[k] == so[k], (k, sd[k], so[k])
+    # dense: N^2 per fill (once without retardation, else per frequency)
+    assert float(n) * n <= sd["hmat_entries"] <= float(n) * n * nf
+    assert so["hmat_entries"] > 0
+    assert np.all(rel(zo, zd) <= 1e-12), rel(zo, zd)
+    print(name, prec, "on-demand entries %.3g of %.3g dense" % (so["hmat_entries"], sd["hmat_entries"]))
+
+
 def test_compressed_mixed_fill_agrees():
     from openpeec_b200 import abi, api
     prob, fx = load_golden("compress_plate", "comp")
@@ -153,3 +176,5 @@ def test_config4_full_size_matches_reference():
           "reference GMRES", float(g["gmres_its"]), "blocks", st["hmat_far"], st["hmat_near"])
     assert (st["hmat_far"], st["hmat_near"]) == (int(g["far"]), int(g["near"]))
     assert e <= 1e-5, e
+    # entries on demand: well under the N^2 of a dense fill
+    assert 0 < st["hmat_entries"] < 0.25 * float(len(prob.seg)) ** 2 * len(g["freqs"]), st["hmat_entries"]
