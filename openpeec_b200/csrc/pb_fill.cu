@@ -683,13 +683,15 @@ k_lp_static(pb_fill_geom g, double kw, double *st)
     }
 }
 
-// the static part of a pair list: stl[t] = static Lp(min, max of pairs[t])
+// the static part of a pair list: stl[t] = static Lp(min, max of pairs[t]) for every t, or
+// for t = idx[u] only
 __global__ void __launch_bounds__(128)
-k_lp_static_list(pb_fill_geom g, double kw, const int2 *pairs, const int *npair, double *stl)
+k_lp_static_list(pb_fill_geom g, double kw, const int2 *pairs, const int *idx, const int *npair, double *stl)
 {
     const long long T = *npair;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < T;
-         t += (long long)gridDim.x * blockDim.x) {
+    for (long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x; u < T;
+         u += (long long)gridDim.x * blockDim.x) {
+        const long long t = idx ? idx[u] : u;
         const int2 p = pairs[t];
         stl[t] = lp_static_entry(g, min(p.x, p.y), max(p.x, p.y), kw);
     }
@@ -1393,13 +1395,21 @@ int pb_lp_corr(const pb_fill_geom &g, int nf, const double *kw, int use_fp32, co
     return r;
 }
 
-int pb_lp_entries(const pb_fill_geom &g, double kw, int use_fp32, const int2 *pairs, const int *npair_dev,
-                  long long cap, double2 scale, double *stl, double2 *out, cudaStream_t s, long *launches)
+int pb_lp_entries_static(const pb_fill_geom &g, double kw, const int2 *pairs, const int *idx, const int *nidx_dev,
+                         long long cap, double *stl, cudaStream_t s, long *launches)
 {
     if (cap <= 0 || g.seg.n == 0) return PB_OK;
-    k_lp_static_list<<<grid_for(cap, 128), 128, 0, s>>>(g, kw, pairs, npair_dev, stl);
+    k_lp_static_list<<<grid_for(cap, 128), 128, 0, s>>>(g, kw, pairs, idx, nidx_dev, stl);
     if (launches) (*launches)++;
     PB_CHECK_LAUNCH();
+    return PB_OK;
+}
+
+int pb_lp_entries_corr(const pb_fill_geom &g, double kw, int use_fp32, const int2 *pairs, const int *npair_dev,
+                       long long cap, double2 scale, const double *stl, double2 *out, cudaStream_t s,
+                       long *launches)
+{
+    if (cap <= 0 || g.seg.n == 0) return PB_OK;
     KArg k;
     make_karg(k, 1, &kw, g.pmax);
     pb_epi_args ea;
@@ -1417,6 +1427,13 @@ int pb_lp_entries(const pb_fill_geom &g, double kw, int use_fp32, const int2 *pa
         r = launch_corr<double, 1, PB_SET_LP, PB_EPI_LIST, 0, 0>(g, k, stl, ea, nullptr, 0, s);
     if (launches) (*launches)++;
     return r;
+}
+
+int pb_lp_entries(const pb_fill_geom &g, double kw, int use_fp32, const int2 *pairs, const int *npair_dev,
+                  long long cap, double2 scale, double *stl, double2 *out, cudaStream_t s, long *launches)
+{
+    PB_TRY(pb_lp_entries_static(g, kw, pairs, nullptr, npair_dev, cap, stl, s, launches));
+    return pb_lp_entries_corr(g, kw, use_fp32, pairs, npair_dev, cap, scale, stl, out, s, launches);
 }
 
 int pb_pot_corr(const pb_fill_geom &g, int nf, const double *kw, int use_fp32, const double *stP,

@@ -67,6 +67,14 @@ int pb_pot_static(const pb_fill_geom &g, double kw, double *stP, cudaStream_t s,
 // stl: scratch of cap doubles.
 int pb_lp_entries(const pb_fill_geom &g, double kw, int use_fp32, const int2 *pairs, const int *npair_dev,
                   long long cap, double2 scale, double *stl, double2 *out, cudaStream_t s, long *launches);
+// The two halves of pb_lp_entries, for callers that keep static parts between wavenumbers:
+// static parts stl[t] of the listed pairs (idx != nullptr: only of t = idx[u], u < *nidx_dev,
+// at most cap), then out[t] = scale * (stl[t] + correction) for t < *npair_dev.
+int pb_lp_entries_static(const pb_fill_geom &g, double kw, const int2 *pairs, const int *idx, const int *nidx_dev,
+                         long long cap, double *stl, cudaStream_t s, long *launches);
+int pb_lp_entries_corr(const pb_fill_geom &g, double kw, int use_fp32, const int2 *pairs, const int *npair_dev,
+                       long long cap, double2 scale, const double *stl, double2 *out, cudaStream_t s,
+                       long *launches);
 
 // Correction kernels for nf <= PB_FMAX wavenumbers (kw[f] > 0). use_fp32 selects the
 // FP32 quadrature (mixed path) or FP64 (plain path). With kw == 0 (quasi-static) pass

@@ -130,8 +130,9 @@ void pb_htree_build(pb_htree &t, int n, const double *pts)
 // ================================================================ device: ACA
 struct AcaBlk {
     int r0, m, c0, nn;
-    long long uoff, voff, soff;
+    long long uoff, voff, soff;   // soff: sum of m over the blocks before (row prefix)
     int lim, pad;
+    long long noff;               // sum of nn over the blocks before (column prefix)
 };
 
 __device__ __forceinline__ double cabs2(double2 a) { return a.x * a.x + a.y * a.y; }
@@ -311,8 +312,9 @@ struct AcaSt {
     double fro2, urmax;
     int k, irow, jcol, probe;
     int st;                       // 0: needs row irow, 1: needs column jcol, 2: done
-    int pad;
-    long long ent;                // offset of its requested entries in the half-step's list
+    int slot;                     // its row / column in the static-part cache (-1: none)
+    int hit, pad;                 // hit: the static parts come from the cache
+    long long ent, ment;          // offsets in the half-step's entry list and miss list
 };
 
 __global__ void k_acaod_init(const AcaBlk *blks, AcaSt *S, int *rused_pool, double *urep_pool, int *rank)
@@ -328,77 +330,139 @@ __global__ void k_acaod_init(const AcaBlk *blks, AcaSt *S, int *rused_pool, doub
         s.k = s.irow = s.probe = 0;
         s.jcol = -1;
         s.st = B.lim > 0 ? 0 : 2;
-        s.pad = 0;
-        s.ent = 0;
+        s.slot = -1;
+        s.hit = s.pad = 0;
+        s.ent = s.ment = 0;
         S[blockIdx.x] = s;
         if (s.st == 2) rank[blockIdx.x] = -1;
     }
 }
 
+// exclusive scan of x over a 1024-thread block (wsum: 32 slots); returns the prefix and
+// adds the block total to carry (all threads see the same carry afterwards)
+__device__ long long scan1024(long long x, long long *wsum, long long &carry)
+{
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    long long v = x;
+    for (int o = 1; o < 32; o <<= 1) {
+        const long long y = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += y;
+    }
+    if (lane == 31) wsum[w] = v;
+    __syncthreads();
+    if (w == 0) {
+        long long q = wsum[lane];
+        for (int o = 1; o < 32; o <<= 1) {
+            const long long y = __shfl_up_sync(0xffffffffu, q, o);
+            if (lane >= o) q += y;
+        }
+        wsum[lane] = q;
+    }
+    __syncthreads();
+    const long long excl = carry + (w > 0 ? wsum[w - 1] : 0) + v - x;
+    const long long tot = wsum[31];
+    __syncthreads();
+    carry += tot;
+    return excl;
+}
+
 // Offsets of the entries the blocks in state `want` request, in block order (the lists do
-// not depend on scheduling): cnt[0] = entries requested, cnt[1] = blocks not done;
-// acc[want] accumulates the entries requested over the build.
+// not depend on scheduling), and the static-part cache look-up: a row (column) whose static
+// parts are cached is a hit; otherwise it takes a free slot, if any, and its entries go to
+// the miss list too. cnt[0] = entries requested, cnt[1] = blocks not done, cnt[2] = misses;
+// acc[want] accumulates the entries requested, acc[2 + want] the misses.
 __global__ void __launch_bounds__(1024)
-k_acaod_scan(int nb, const AcaBlk *blks, AcaSt *S, int want, int *cnt, long long *acc)
+k_acaod_scan(int nb, const AcaBlk *blks, AcaSt *S, int want, int rc, int *cidx, int *cnum, int *cnt,
+             long long *acc)
 {
     __shared__ long long wsum[32];
-    __shared__ long long carry;
     __shared__ int nact;
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    if (threadIdx.x == 0) { carry = 0; nact = 0; }
+    long long carry = 0, mcarry = 0;
+    if (threadIdx.x == 0) nact = 0;
     __syncthreads();
     int act = 0;
     for (int base = 0; base < nb; base += 1024) {
         const int b = base + threadIdx.x;
-        long long len = 0;
+        long long len = 0, mlen = 0;
+        int slot = -1, hit = 0;
         if (b < nb) {
             const int st = S[b].st;
             act += st != 2;
-            if (st == want) len = want == 0 ? blks[b].nn : blks[b].m;
-        }
-        long long x = len;                             // inclusive scan: warp, then warps
-        for (int o = 1; o < 32; o <<= 1) {
-            const long long y = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= o) x += y;
-        }
-        if (lane == 31) wsum[w] = x;
-        __syncthreads();
-        if (w == 0) {
-            long long v = wsum[lane];
-            for (int o = 1; o < 32; o <<= 1) {
-                const long long y = __shfl_up_sync(0xffffffffu, v, o);
-                if (lane >= o) v += y;
+            if (st == want) {
+                len = want == 0 ? blks[b].nn : blks[b].m;
+                if (rc > 0) {
+                    const int key = want == 0 ? S[b].irow : S[b].jcol;
+                    int *ci = cidx + ((long long)b * 2 + want) * rc;
+                    const int nc = cnum[b * 2 + want];
+                    for (int q = 0; q < nc && !hit; q++)
+                        if (ci[q] == key) { slot = q; hit = 1; }
+                    if (!hit && nc < rc) {
+                        slot = nc;
+                        ci[nc] = key;
+                        cnum[b * 2 + want] = nc + 1;
+                    }
+                }
+                mlen = hit ? 0 : len;
             }
-            wsum[lane] = v;
         }
-        __syncthreads();
-        const long long excl = carry + (w > 0 ? wsum[w - 1] : 0) + x - len;
-        if (len > 0) S[b].ent = excl;
-        __syncthreads();
-        if (threadIdx.x == 1023) carry = excl + len;
-        __syncthreads();
+        const long long e = scan1024(len, wsum, carry);
+        const long long me = scan1024(mlen, wsum, mcarry);
+        if (len > 0) {
+            S[b].ent = e;
+            S[b].ment = me;
+            S[b].slot = slot;
+            S[b].hit = hit;
+        }
     }
     atomicAdd(&nact, act);
     __syncthreads();
     if (threadIdx.x == 0) {
         cnt[0] = (int)carry;
         cnt[1] = nact;
+        cnt[2] = (int)mcarry;
         acc[want] += carry;
+        acc[2 + want] += mcarry;
     }
 }
 
-// the cell pairs of each requesting block's row (want 0) or column (want 1)
-__global__ void k_acaod_pairs(const AcaBlk *blks, const AcaSt *S, const int *perm, int want, int2 *pairs)
+// static parts between the cache and the entry list: hits read their row (column) from it,
+// new slots store theirs after the misses were evaluated
+__global__ void k_acaod_cache(const AcaBlk *blks, const AcaSt *S, int want, int rc, double *crow, double *ccol,
+                              double *stl)
+{
+    const AcaSt s = S[blockIdx.x];
+    if (s.st != want || s.slot < 0) return;
+    const AcaBlk B = blks[blockIdx.x];
+    const int len = want == 0 ? B.nn : B.m;
+    double *c = want == 0 ? crow + (long long)rc * B.noff + (long long)s.slot * B.nn
+                          : ccol + (long long)rc * B.soff + (long long)s.slot * B.m;
+    if (s.hit)
+        for (int j = threadIdx.x; j < len; j += blockDim.x) stl[s.ent + j] = c[j];
+    else
+        for (int j = threadIdx.x; j < len; j += blockDim.x) c[j] = stl[s.ent + j];
+}
+
+// the cell pairs of each requesting block's row (want 0) or column (want 1), and the
+// positions of those whose static parts must be evaluated
+__global__ void k_acaod_pairs(const AcaBlk *blks, const AcaSt *S, const int *perm, int want, int2 *pairs,
+                              int *miss)
 {
     const AcaSt s = S[blockIdx.x];
     if (s.st != want) return;
     const AcaBlk B = blks[blockIdx.x];
+    const bool ms = !s.hit;
     if (want == 0) {
         const int pr = perm[B.r0 + s.irow];
-        for (int j = threadIdx.x; j < B.nn; j += blockDim.x) pairs[s.ent + j] = make_int2(pr, perm[B.c0 + j]);
+        for (int j = threadIdx.x; j < B.nn; j += blockDim.x) {
+            pairs[s.ent + j] = make_int2(pr, perm[B.c0 + j]);
+            if (ms) miss[s.ment + j] = (int)(s.ent + j);
+        }
     } else {
         const int pc = perm[B.c0 + s.jcol];
-        for (int i = threadIdx.x; i < B.m; i += blockDim.x) pairs[s.ent + i] = make_int2(perm[B.r0 + i], pc);
+        for (int i = threadIdx.x; i < B.m; i += blockDim.x) {
+            pairs[s.ent + i] = make_int2(perm[B.r0 + i], pc);
+            if (ms) miss[s.ment + i] = (int)(s.ent + i);
+        }
     }
 }
 
@@ -1007,7 +1071,7 @@ struct KBlock {
     int nl = 0;
     std::vector<int> leaf_of, leaf_lo, leaf_hi;
     std::vector<AcaBlk> ab;
-    long long uo = 0, vo = 0, so = 0;
+    long long uo = 0, vo = 0, so = 0, no = 0;
     Dev perm, aca, rank, U, V, rused, urep, leaf_of_d, Urm, leaf_lo_d, leaf_hi_d;
     // per build
     std::vector<DBlk> db;
@@ -1021,8 +1085,14 @@ struct KBlock {
     std::vector<int> bri, bci, cri, cci;
     std::vector<zc> bval, cval;
     Dev lof_d, lidx_d, dof_d, dlu_d, dpiv_d, bro, bcol, bv, cro, ccol, cv, wb, ub;
-    // on-demand entries: ACA state, pair list, static parts, values, counts
-    Dev od_st, od_pairs, od_stl, od_vals, od_cnt, od_acc, od_blk;
+    // on-demand entries: ACA state, pair list, miss list, static parts, values, counts
+    Dev od_st, od_pairs, od_miss, od_stl, od_vals, od_cnt, od_acc, od_blk;
+    // static parts kept between frequencies (valid while the quadrature levels stay): of
+    // up to rc rows and rc columns per far block (keys cidx, counts cnum, values srow /
+    // scol), of the near blocks and of the leaf blocks
+    int rc = -1;
+    Dev cidx, cnum, srow, scol, nstat, lstat;
+    bool nstat_ok = false, lstat_ok = false;
 };
 
 // tree, leaves and ACA workspace of a block (hmat_build_gen, hmatrix.c:403-421)
@@ -1045,7 +1115,7 @@ int kb_setup(KBlock &kb, const double *pts, cudaStream_t st)
     }
     const int nfar = (int)kb.T.fr.size();
     kb.ab.resize(nfar);
-    kb.uo = kb.vo = kb.so = 0;
+    kb.uo = kb.vo = kb.so = kb.no = 0;
     for (int b = 0; b < nfar; b++) {
         AcaBlk &B = kb.ab[b];
         B.r0 = kb.T.lo[kb.T.fr[b]];
@@ -1056,10 +1126,12 @@ int kb_setup(KBlock &kb, const double *pts, cudaStream_t st)
         B.uoff = kb.uo;
         B.voff = kb.vo;
         B.soff = kb.so;
+        B.noff = kb.no;
         B.pad = 0;
         kb.uo += (long long)B.lim * B.m;
         kb.vo += (long long)B.lim * B.nn;
         kb.so += B.m;
+        kb.no += B.nn;
     }
     PB_TRY(upload(kb.perm, kb.T.perm, st));
     PB_TRY(upload(kb.aca, kb.ab, st));
@@ -1080,8 +1152,19 @@ int kb_setup(KBlock &kb, const double *pts, cudaStream_t st)
 struct OnDemand {
     double kw = 0;
     int fill32 = 0;
-    double entries = 0;
+    bool reset = false;           // the quadrature levels changed: cached static parts void
+    double entries = 0, static_evals = 0;
 };
+
+// rows and columns per far block whose static parts are kept: as many as fit in 8 GB, at
+// most 64 (ACA ranks here stay below 40 plus restarts)
+static int cache_rows(long long sm, long long sn)
+{
+    const double per = 8.0 * (double)(sm + sn);
+    if (per <= 0) return 0;
+    const int r = (int)std::min(64.0, std::floor(8e9 / per));
+    return r >= 8 ? r : 0;
+}
 
 // ACA of every far block with on-demand rows and columns (k_acaod_*): one row and one
 // column half-step per round for all blocks still running, until none is.
@@ -1096,25 +1179,45 @@ int kb_aca_ondemand(KBlock &kb, pb_ctx *c, OnDemand &od, double ctol)
     if (cap >= (1LL << 31)) { pb_set_error("compressed sweep: %lld on-demand entries per step", cap); return PB_ERR_UNSUP; }
     PB_TRY(kb.od_st.alloc(sizeof(AcaSt) * (size_t)nfar));
     PB_TRY(kb.od_pairs.alloc(sizeof(int2) * (size_t)cap));
+    PB_TRY(kb.od_miss.alloc(sizeof(int) * (size_t)cap));
     PB_TRY(kb.od_stl.alloc(sizeof(double) * (size_t)cap));
     PB_TRY(kb.od_vals.alloc(sizeof(double2) * (size_t)cap));
-    PB_TRY(kb.od_cnt.alloc(sizeof(int) * 2));
-    PB_TRY(kb.od_acc.alloc(sizeof(long long) * 2));
+    PB_TRY(kb.od_cnt.alloc(sizeof(int) * 3));
+    PB_TRY(kb.od_acc.alloc(sizeof(long long) * 4));
+    if (kb.rc < 0) {                            // first build: the static-part cache, if it fits
+        kb.rc = cache_rows(sm, sn);
+        if (kb.rc > 0) {
+            const bool ok = kb.cidx.alloc(sizeof(int) * 2 * (size_t)nfar * kb.rc) == PB_OK &&
+                            kb.cnum.alloc(sizeof(int) * 2 * (size_t)nfar) == PB_OK &&
+                            kb.srow.alloc(sizeof(double) * (size_t)kb.rc * sn) == PB_OK &&
+                            kb.scol.alloc(sizeof(double) * (size_t)kb.rc * sm) == PB_OK;
+            if (!ok) {                          // no room: evaluate every static part
+                cudaGetLastError();
+                kb.rc = 0;
+            }
+        }
+        od.reset = true;
+    }
+    if (od.reset && kb.rc > 0) PB_CUDA(cudaMemsetAsync(kb.cnum.p, 0, sizeof(int) * 2 * (size_t)nfar, st));
     AcaSt *S = kb.od_st.as<AcaSt>();
     const AcaBlk *blk = kb.aca.as<AcaBlk>();
     int *cnt = kb.od_cnt.as<int>(), *rank = kb.rank.as<int>();
     long long *acc = kb.od_acc.as<long long>();
-    PB_CUDA(cudaMemsetAsync(acc, 0, sizeof(long long) * 2, st));
+    PB_CUDA(cudaMemsetAsync(acc, 0, sizeof(long long) * 4, st));
     k_acaod_init<<<nfar, 256, 0, st>>>(blk, S, kb.rused.as<int>(), kb.urep.as<double>(), rank);
     c->launches++;
     PB_CHECK_LAUNCH();
+    auto scan = [&](int want) {
+        k_acaod_scan<<<1, 1024, 0, st>>>(nfar, blk, S, want, kb.rc, kb.rc > 0 ? kb.cidx.as<int>() : nullptr,
+                                          kb.rc > 0 ? kb.cnum.as<int>() : nullptr, cnt, acc);
+        c->launches++;
+    };
     // every round advances each running block by a row; a block ends after at most
     // PB_HM_MAXIT ranks, each with at most PB_HM_PROBE + 1 rows
     const int maxit = (PB_HM_MAXIT + 1) * (PB_HM_PROBE + 2);
-    int hc[2] = {0, 0};
+    int hc[3] = {0, 0, 0};
     for (int it = 0;; it++) {
-        k_acaod_scan<<<1, 1024, 0, st>>>(nfar, blk, S, 0, cnt, acc);
-        c->launches++;
+        scan(0);
         PB_CHECK_LAUNCH();
         PB_CUDA(cudaMemcpyAsync(hc, cnt, sizeof(hc), cudaMemcpyDeviceToHost, st));
         PB_CUDA(cudaStreamSynchronize(st));
@@ -1124,16 +1227,23 @@ int kb_aca_ondemand(KBlock &kb, pb_ctx *c, OnDemand &od, double ctol)
             return PB_ERR_NOCONV;
         }
         for (int want = 0; want < 2; want++) {
-            if (want == 1) {
-                k_acaod_scan<<<1, 1024, 0, st>>>(nfar, blk, S, 1, cnt, acc);
-                c->launches++;
-            }
-            k_acaod_pairs<<<nfar, 256, 0, st>>>(blk, S, kb.perm.as<int>(), want, kb.od_pairs.as<int2>());
+            if (want == 1) scan(1);
+            const long long lcap = want == 0 ? hc[0] : sm;
+            k_acaod_pairs<<<nfar, 256, 0, st>>>(blk, S, kb.perm.as<int>(), want, kb.od_pairs.as<int2>(),
+                                                kb.od_miss.as<int>());
             c->launches++;
             PB_CHECK_LAUNCH();
-            PB_TRY(pb_lp_entries(c->g, od.kw, od.fill32, kb.od_pairs.as<int2>(), cnt, want == 0 ? hc[0] : sm,
-                                 make_double2(1, 0), kb.od_stl.as<double>(), kb.od_vals.as<double2>(), st,
-                                 &c->launches));
+            PB_TRY(pb_lp_entries_static(c->g, od.kw, kb.od_pairs.as<int2>(), kb.od_miss.as<int>(), cnt + 2,
+                                        want == 0 ? hc[2] : sm, kb.od_stl.as<double>(), st, &c->launches));
+            if (kb.rc > 0) {
+                k_acaod_cache<<<nfar, 256, 0, st>>>(blk, S, want, kb.rc, kb.srow.as<double>(), kb.scol.as<double>(),
+                                                    kb.od_stl.as<double>());
+                c->launches++;
+                PB_CHECK_LAUNCH();
+            }
+            PB_TRY(pb_lp_entries_corr(c->g, od.kw, od.fill32, kb.od_pairs.as<int2>(), cnt, lcap,
+                                      make_double2(1, 0), kb.od_stl.as<double>(), kb.od_vals.as<double2>(), st,
+                                      &c->launches));
             if (want == 0)
                 k_acaod_row<<<nfar, 256, 0, st>>>(blk, S, kb.od_vals.as<double2>(), kb.U.as<double2>(),
                                                   kb.V.as<double2>(), kb.rused.as<int>(), kb.urep.as<double>(), ctol,
@@ -1146,17 +1256,20 @@ int kb_aca_ondemand(KBlock &kb, pb_ctx *c, OnDemand &od, double ctol)
             PB_CHECK_LAUNCH();
         }
     }
-    long long ha[2] = {0, 0};
+    long long ha[4] = {0, 0, 0, 0};
     PB_CUDA(cudaMemcpyAsync(ha, acc, sizeof(ha), cudaMemcpyDeviceToHost, st));
     PB_CUDA(cudaStreamSynchronize(st));
     od.entries += (double)(ha[0] + ha[1]);
+    od.static_evals += (double)(ha[2] + ha[3]);
     return PB_OK;
 }
 
 // out[B.off + i*nn + j] = scale * K(perm[r0+i], perm[c0+j]) for dense blocks (consecutive
-// offsets), entries evaluated on demand in chunks of at most 2^24 entries (or one block)
+// offsets), entries evaluated on demand in chunks of at most 2^24 entries (or one block).
+// stat: where the static parts are kept (indexed from the first block's offset), valid
+// from an earlier call (stat_ok) or written now; nullptr: a scratch buffer.
 int kb_dense_ondemand(KBlock &kb, pb_ctx *c, OnDemand &od, const std::vector<DBlk> &blks, double2 scale,
-                      double2 *out)
+                      double2 *out, double *stat, bool stat_ok)
 {
     const cudaStream_t st = c->stream;
     if (blks.empty()) return PB_OK;
@@ -1168,8 +1281,9 @@ int kb_dense_ondemand(KBlock &kb, pb_ctx *c, OnDemand &od, const std::vector<DBl
     const long long chunk = std::max(1LL << 24, big), buf = std::min(total, chunk);
     if (buf >= (1LL << 31)) { pb_set_error("compressed sweep: dense block of %lld entries", big); return PB_ERR_UNSUP; }
     PB_TRY(kb.od_pairs.alloc(sizeof(int2) * (size_t)buf));
-    PB_TRY(kb.od_stl.alloc(sizeof(double) * (size_t)buf));
-    PB_TRY(kb.od_cnt.alloc(sizeof(int) * 2));
+    if (!stat) PB_TRY(kb.od_stl.alloc(sizeof(double) * (size_t)buf));
+    PB_TRY(kb.od_cnt.alloc(sizeof(int) * 3));
+    const long long base0 = blks[0].off;
     for (size_t q0 = 0; q0 < blks.size();) {
         size_t q1 = q0;
         long long tot = 0;
@@ -1185,8 +1299,14 @@ int kb_dense_ondemand(KBlock &kb, pb_ctx *c, OnDemand &od, const std::vector<DBl
         k_set_count<<<1, 1, 0, st>>>(kb.od_cnt.as<int>(), (int)tot);
         c->launches += 2;
         PB_CHECK_LAUNCH();
-        PB_TRY(pb_lp_entries(c->g, od.kw, od.fill32, kb.od_pairs.as<int2>(), kb.od_cnt.as<int>(), tot, scale,
-                             kb.od_stl.as<double>(), out + base, st, &c->launches));
+        double *stl = stat ? stat + (base - base0) : kb.od_stl.as<double>();
+        if (!stat || !stat_ok) {
+            PB_TRY(pb_lp_entries_static(c->g, od.kw, kb.od_pairs.as<int2>(), nullptr, kb.od_cnt.as<int>(), tot, stl,
+                                        st, &c->launches));
+            od.static_evals += (double)tot;
+        }
+        PB_TRY(pb_lp_entries_corr(c->g, od.kw, od.fill32, kb.od_pairs.as<int2>(), kb.od_cnt.as<int>(), tot, scale,
+                                  stl, out + base, st, &c->launches));
         od.entries += (double)tot;
         q0 = q1;
     }
@@ -1262,7 +1382,17 @@ int kb_compress(KBlock &kb, const double2 *K, double ctol, pb_ctx *c, pb_hstats 
     PB_TRY(upload(kb.dblk, kb.db, st));
     PB_TRY(kb.D.alloc(sizeof(double2) * (size_t)std::max(1LL, doff)));
     if (!kb.db.empty() && od) {
-        PB_TRY(kb_dense_ondemand(kb, c, *od, kb.db, kb.scale, kb.D.as<double2>()));
+        // near blocks: the same every frequency, static parts kept; far blocks kept dense:
+        // evaluated afresh
+        const std::vector<DBlk> nearb(kb.db.begin(), kb.db.begin() + nnear), fard(kb.db.begin() + nnear, kb.db.end());
+        long long nent = 0;
+        for (const DBlk &B : nearb) nent += (long long)B.m * B.nn;
+        if (od->reset || kb.nstat.cap < sizeof(double) * (size_t)std::max(1LL, nent)) kb.nstat_ok = false;
+        if (nent > 0) PB_TRY(kb.nstat.alloc(sizeof(double) * (size_t)nent));
+        PB_TRY(kb_dense_ondemand(kb, c, *od, nearb, kb.scale, kb.D.as<double2>(), kb.nstat.as<double>(),
+                                 kb.nstat_ok));
+        kb.nstat_ok = true;
+        PB_TRY(kb_dense_ondemand(kb, c, *od, fard, kb.scale, kb.D.as<double2>(), nullptr, false));
     } else if (!kb.db.empty()) {
         k_gather<<<(unsigned)kb.db.size(), 256, 0, st>>>(K, kb.n, kb.perm.as<int>(), kb.dblk.as<DBlk>(), kb.scale,
                                                          kb.D.as<double2>());
@@ -1313,7 +1443,10 @@ int kb_compress(KBlock &kb, const double2 *K, double ctol, pb_ctx *c, pb_hstats 
     PB_TRY(upload(bLb, lb, st));
     PB_TRY(bLd.alloc(sizeof(double2) * (size_t)std::max<long long>(1, kb.dof[nl])));
     if (od) {
-        PB_TRY(kb_dense_ondemand(kb, c, *od, lb, kb.scale, bLd.as<double2>()));
+        if (od->reset || kb.lstat.cap < sizeof(double) * (size_t)std::max<long long>(1, kb.dof[nl])) kb.lstat_ok = false;
+        PB_TRY(kb.lstat.alloc(sizeof(double) * (size_t)std::max<long long>(1, kb.dof[nl])));
+        PB_TRY(kb_dense_ondemand(kb, c, *od, lb, kb.scale, bLd.as<double2>(), kb.lstat.as<double>(), kb.lstat_ok));
+        kb.lstat_ok = true;
     } else {
         k_gather<<<nl, 256, 0, st>>>(K, kb.n, kb.perm.as<int>(), bLb.as<DBlk>(), kb.scale, bLd.as<double2>());
         c->launches++;
@@ -1539,7 +1672,9 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
     // the Lp block's entries are evaluated on demand (no dense N x N fill) unless asked for
     // the dense fill, or an option needs the dense block (exact leaf inverses, samples)
     const bool od_lp = !o.aca_dense && !o.pc_exact_leaf && !sample_x;
-    double od_entries = 0;
+    double od_entries = 0, od_static = 0;
+    std::vector<long> od_sig;                   // quadrature levels of the kept static parts
+    bool od_reset = true;
     *hs = pb_hstats();
 
     // compressed blocks: Lp over the segment midpoints (hmat_build, hmatrix.c:617-634) and,
@@ -1630,6 +1765,10 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
             level_signature(c, kw, sig);
             sig.push_back(cap);
             sig.push_back(od_lp);
+            if (sig != od_sig) {
+                od_sig = sig;
+                od_reset = true;
+            }
             if (!c->comp_static_valid || sig != c->comp_sig) {
                 c->comp_static_valid = false;
                 if (!od_lp) PB_TRY(pb_lp_static(c->g, kw, bSt.as<double>(), st, &c->launches));
@@ -1675,8 +1814,14 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
         OnDemand od;
         od.kw = kw;
         od.fill32 = fill32;
+        od.reset = od_reset;
+        od_reset = false;
         PB_TRY(kb_compress(kbs[0], od_lp ? nullptr : bK.as<double2>(), ctol, c, &hf, od_lp ? &od : nullptr));
         od_entries += od.entries;
+        od_static += od.static_evals;
+        if (o.verbose && od_lp)
+            fprintf(stderr, "[compressed f=%.5g] on-demand entries %.4g, static parts evaluated %.4g\n", f,
+                    od.entries, od.static_evals);
         if (cap) {
             kbs[1].scale = make_double2(1, 0);      // P (solve.c:275)
             PB_TRY(kb_compress(kbs[1], bKP.as<double2>(), ctol, c, &hf, nullptr));
