@@ -160,6 +160,130 @@ k_lu_leaf(T2_t<T> *a, int n, int ld, long long stride, int k0, int w, int *piv, 
     }
 }
 
+// ---------------------------------------------------------------- cooperative leaf panel
+// Barrier among the P CTAs of one matrix (mb[0] arrivals, mb[1] generation), bounded: a
+// wait longer than about a second sets *err and returns false, and the kernel returns.
+__device__ __forceinline__ bool panel_bar(unsigned *mb, int P, unsigned &gen, int *err, int *ok_s)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        __threadfence();
+        const unsigned g = gen;
+        if (atomicAdd(&mb[0], 1u) == (unsigned)P - 1) {
+            atomicExch(&mb[0], 0u);
+            __threadfence();
+            atomicExch(&mb[1], g + 1);
+        } else {
+            long long it = 0;
+            while (atomicAdd(&mb[1], 0u) == g) {
+                if (++it > (1LL << 23) || ((it & 1023) == 0 && atomicAdd(err, 0) != 0)) {
+                    ok = 0;
+                    atomicExch(err, 1);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        *ok_s = ok;
+    }
+    __syncthreads();
+    gen++;
+    return *ok_s != 0;
+}
+
+// The leaf panel of k_lu_leaf for a few large matrices: the panel's rows [k0, n) are split
+// over the P CTAs of a matrix (blockIdx.y), RS rows each, held in shared memory for the
+// whole panel (all w <= 32 columns). Per column: every CTA's candidate (largest |re|+|im|,
+// first index), one barrier, the same global choice in every CTA, the owners of the pivot
+// row and of row c publish them, a second barrier, the swap and the rank-1 update of the
+// CTA's own rows. The arithmetic of every entry is that of k_lu_leaf (the same cfms
+// sequence), so the factors are the same; the panel's row traffic is spread over P SMs
+// instead of one. Needs all P * nb CTAs resident (cooperative launch).
+template <typename T>
+__global__ void __launch_bounds__(256)
+k_lu_leaf_coop(T2_t<T> *a, int n, int ld, long long stride, int k0, int w, int *piv, int *info, int P, int RS,
+               unsigned *bar, double *part_m, int *part_i, T2_t<T> *rows, int *err)
+{
+    typedef T2_t<T> T2;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    __shared__ double red_m[33];
+    __shared__ int red_i[33];
+    __shared__ T2 pr[32];
+    __shared__ double s_bm;
+    __shared__ int s_bi, ok_s;
+    T2 *S = reinterpret_cast<T2 *>(smraw);        // [RS][32]
+    const int p = blockIdx.x, b = blockIdx.y, tid = threadIdx.x, nt = blockDim.x;
+    a += (long long)b * stride;
+    piv += (long long)b * n;
+    unsigned *mb = bar + 2 * b;
+    double *pm = part_m + (long long)b * P;
+    int *pi = part_i + (long long)b * P;
+    T2 *prow = rows + (long long)b * 64, *crow = prow + 32;
+    const int r0 = k0 + p * RS, r1 = min(n, r0 + RS), nr = max(0, r1 - r0);
+    for (int e = tid; e < nr * w; e += nt) {
+        const int r = e / w, t = e - r * w;
+        S[r * 32 + t] = a[(long long)(r0 + r) * ld + k0 + t];
+    }
+    __syncthreads();
+    unsigned gen = 0;
+    for (int t = 0; t < w; t++) {
+        const int c = k0 + t;
+        double bm = -1.0;
+        int bi = INT_MAX;
+        for (int r = max(c, r0) + tid; r < r1; r += nt) {
+            const double mm = cmag1(S[(r - r0) * 32 + t]);
+            if (mm > bm) { bm = mm; bi = r; }
+        }
+        block_argmax(bm, bi, red_m, red_i);
+        if (tid == 0) { pm[p] = bm; pi[p] = bi; }
+        if (!panel_bar(mb, P, gen, err, &ok_s)) return;
+        if (tid < 32) {                                // the same choice in every CTA
+            double m = -1.0;
+            int i = INT_MAX;
+            for (int q = tid; q < P; q += 32) argmax_pair(m, i, __ldcg(&pm[q]), __ldcg(&pi[q]));
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const double m2 = __shfl_down_sync(0xffffffffu, m, o);
+                const int i2 = __shfl_down_sync(0xffffffffu, i, o);
+                argmax_pair(m, i, m2, i2);
+            }
+            if (tid == 0) { s_bm = m; s_bi = i; }
+        }
+        __syncthreads();
+        const int ip = (s_bi == INT_MAX) ? c : s_bi;
+        if (ip >= r0 && ip < r1)
+            for (int tt = tid; tt < w; tt += nt) prow[tt] = S[(ip - r0) * 32 + tt];
+        if (ip != c && c >= r0 && c < r1)
+            for (int tt = tid; tt < w; tt += nt) crow[tt] = S[(c - r0) * 32 + tt];
+        if (!panel_bar(mb, P, gen, err, &ok_s)) return;
+        for (int tt = tid; tt < w; tt += nt) pr[tt] = __ldcg(&prow[tt]);
+        if (ip != c && ip >= r0 && ip < r1)
+            for (int tt = tid; tt < w; tt += nt) S[(ip - r0) * 32 + tt] = __ldcg(&crow[tt]);
+        __syncthreads();
+        if (c >= r0 && c < r1)
+            for (int tt = tid; tt < w; tt += nt) S[(c - r0) * 32 + tt] = pr[tt];
+        if (p == 0 && tid == 0) {
+            piv[c] = ip;
+            if (s_bm < 1e-30 && info[b] < 0) info[b] = c;
+        }
+        __syncthreads();
+        const T2 pinv = safe_inv(pr[t]);
+        for (int r = max(c + 1, r0) + tid; r < r1; r += nt) {
+            T2 *row = S + (r - r0) * 32;
+            const T2 l = cmul(row[t], pinv);
+            row[t] = l;
+            for (int tt = t + 1; tt < w; tt++) row[tt] = cfms(row[tt], l, pr[tt]);
+        }
+        __syncthreads();
+    }
+    for (int e = tid; e < nr * w; e += nt) {
+        const int r = e / w, t = e - r * w;
+        a[(long long)(r0 + r) * ld + k0 + t] = S[r * 32 + t];
+    }
+}
+
 // ---------------------------------------------------------------- row swaps
 template <typename T>
 __global__ void k_swap_rows(T2_t<T> *a, int ld, long long stride, const int *piv, int n,
@@ -401,7 +525,8 @@ static int check_tc(pb_lu_engine *e)
     PB_CUDA(cudaStreamSynchronize(e->stream));
     if (h) {
         PB_CUDA(cudaMemsetAsync(e->tc_err, 0, sizeof(int), e->stream));
-        pb_set_error("tensor-core trailing update: a pipeline wait timed out; the factorisation is invalid");
+        pb_set_error("factorisation: a device wait timed out (tensor-core pipeline or panel barrier); "
+                     "the factors are invalid");
         return PB_ERR_CUDA;
     }
     return PB_OK;
@@ -432,6 +557,9 @@ void pb_lu_engine_free(pb_lu_engine *e)
     e->blas = nullptr;
     if (e->tc_err) cudaFree(e->tc_err);
     e->tc_err = nullptr;
+    if (e->coop) cudaFree(e->coop);
+    e->coop = nullptr;
+    e->coop_cap = 0;
 }
 
 // ---------------------------------------------------------------- recursion
@@ -462,6 +590,57 @@ static int launch_leaf(pb_lu_engine *e, T2_t<T> *a, int n, int ld, long long str
     k_lu_leaf<T, SW, G><<<nb, nt, smem, e->stream>>>(a, n, ld, stride, k0, w, piv, info);
     e->launches++;
     PB_CHECK_LAUNCH();
+    return PB_OK;
+}
+
+// The cooperative panel for nb matrices of panel height m, if it applies: one CTA per SM
+// at most, P >= 4 CTAs per matrix of at least 32 rows each, the CTA's rows within shared
+// memory. launched = false: the one-CTA panel should run.
+template <typename T>
+static int launch_leaf_coop(pb_lu_engine *e, T2_t<T> *a, int n, int ld, long long stride, int nb, int k0, int w,
+                            int *piv, int *info, bool &launched)
+{
+    launched = false;
+    const int m = n - k0;
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (m < 1024 || nb > nsm / 4) return PB_OK;
+    const int P = std::min(nsm / nb, (m + 31) / 32);
+    if (P < 4) return PB_OK;
+    const int RS = (m + P - 1) / P;
+    const size_t es = sizeof(T2_t<T>), smem = (size_t)RS * 32 * es;
+    if (smem + 4096 > (size_t)pb_smem_cap()) return PB_OK;
+    static std::atomic<unsigned long long> attr_set{0};   // per device
+    PB_TRY(pb_smem_optin(k_lu_leaf_coop<T>, pb_smem_cap() - 1024, attr_set));
+    int per_sm = 0;
+    PB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_lu_leaf_coop<T>, 256, smem));
+    if (per_sm * nsm < P * nb) return PB_OK;
+    // scratch: barriers, candidates, the two published rows
+    const size_t need = 16 * (size_t)nb + (8 + 4) * (size_t)P * nb + 64 * es * nb + 64;
+    if (e->coop_cap < need) {
+        if (e->coop) cudaFree(e->coop);
+        e->coop = nullptr;
+        e->coop_cap = 0;
+        PB_CUDA(cudaMalloc(&e->coop, need));
+        e->coop_cap = need;
+    }
+    if (!e->tc_err) {
+        PB_CUDA(cudaMalloc(&e->tc_err, sizeof(int)));
+        PB_CUDA(cudaMemsetAsync(e->tc_err, 0, sizeof(int), e->stream));
+    }
+    char *base = (char *)e->coop;
+    unsigned *bar = (unsigned *)base;
+    T2_t<T> *rows = (T2_t<T> *)(base + 16 * (size_t)nb);
+    double *pm = (double *)((char *)rows + 64 * es * nb);
+    int *pi = (int *)(pm + (size_t)P * nb);
+    PB_CUDA(cudaMemsetAsync(bar, 0, 8 * (size_t)nb, e->stream));
+    int Pv = P, RSv = RS;
+    void *args[] = {&a, &n, &ld, &stride, &k0, &w, &piv, &info, &Pv, &RSv, &bar, &pm, &pi, &rows, &e->tc_err};
+    PB_CUDA(cudaLaunchCooperativeKernel((void *)k_lu_leaf_coop<T>, dim3(P, nb), dim3(256), args, smem, e->stream));
+    e->launches++;
+    e->tc_used = 1;                     // check_tc reads the wait-timeout flag
+    launched = true;
     return PB_OK;
 }
 
@@ -505,6 +684,9 @@ static int lu_rec(pb_lu_engine *e, T2_t<T> *a, int n, int ld, long long stride, 
                   int k0, int w, int *piv, int *info, int sw, size_t smem)
 {
     if (w <= 32) {
+        bool co = false;
+        PB_TRY(launch_leaf_coop<T>(e, a, n, ld, stride, nb, k0, w, piv, info, co));
+        if (co) return PB_OK;
         if (sw == 0) {
             // orders whose panel column does not fit in shared memory: while it does not,
             // the panel is worked on in global memory, then one column at a time in shared

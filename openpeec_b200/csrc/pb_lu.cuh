@@ -28,6 +28,8 @@ struct pb_lu_engine {
     int tc_disabled = 0;       // set if the library rejects the emulated compute type
     int *tc_err = nullptr;     // device flag: a pipeline wait of the tensor-core kernel timed out
     int tc_used = 0;           // the tensor-core kernel ran since the flag was last checked
+    void *coop = nullptr;      // scratch of the cooperative leaf panel (barriers, candidates, rows)
+    size_t coop_cap = 0;       // bytes
 };
 
 // C (m x nc) -= A (m x k) * B (k x nc), complex FP32, row-major, batched with one stride,

@@ -49,6 +49,22 @@ def test_lu_solve(n):
     assert np.max(np.abs(a @ x - b)) <= 1e-10 * np.max(np.abs(b)) * n
 
 
+@pytest.mark.parametrize("n", [1100, 2050])
+def test_cooperative_panels_match_reference_rule(n):
+    """Orders whose panels are 1024 rows or more take the cooperative panel (rows split over
+    many CTAs, candidates exchanged through a bounded grid barrier): the same pivot sequence
+    as the reference's rule and the same factors as the one-CTA panel would give."""
+    a = rand_c(n, 7 + n)
+    info, lu, piv = api.lu_decomp(a)
+    assert info == -1
+    r_info, r_lu, r_piv = Oracle.lu_decomp(a)
+    assert np.array_equal(piv, r_piv)
+    assert np.max(np.abs(lu - r_lu)) <= 1e-9 * max(1.0, np.max(np.abs(r_lu)))
+    a[:, n // 2] = 0                                   # zero column: zero pivot at n // 2
+    info, _, _ = api.lu_decomp(a)
+    assert info == n // 2, info
+
+
 def test_lu_singular_row():
     a = rand_c(6, 3)
     a[:, 2] = 0                                       # column 2 all zero -> zero pivot at k = 2
