@@ -316,6 +316,7 @@ void pb_destroy(pb_ctx *c)
     for (void *p : ptrs) if (p) cudaFree(p);
     for (auto &slot : c->cache) if (slot.p) cudaFree(slot.p);
     if (c->comp_schur_reg) cudaHostUnregister(c->comp_schur_reg);
+    pb_comp_state_free(c);
     pb_lu_engine_free(&c->lu);
     if (c->stream) cudaStreamDestroy(c->stream);
     if (c->stream_fill) cudaStreamDestroy(c->stream_fill);

@@ -76,6 +76,9 @@ struct pb_ctx {
     const void *dense_static_ptr[2] = {nullptr, nullptr};
     // compressed path: host copy of the dense circuit Schur complement, page-locked once
     // (cudaHostRegister) so that its per-frequency upload runs at full link speed
+    // compressed path: cluster trees, ACA workspaces and the kept static parts of the kernel
+    // blocks, held between calls (owned by pb_hmat.cu, released by pb_comp_state_free)
+    void *comp_state = nullptr;
     std::vector<std::complex<double>> comp_schur;
     void *comp_schur_reg = nullptr;
 

@@ -1650,7 +1650,21 @@ int pc_samples(pb_ctx *c, KBlock &kb, const std::vector<zc> &zint, double om, co
     }
     return PB_OK;
 }
+
+// the compressed path's state held by the context between calls
+struct CompState {
+    std::vector<KBlock> kbs;
+    bool ready = false;
+    std::vector<long> od_sig;     // quadrature levels of the kept static parts
+};
 }  // namespace
+
+void pb_comp_state_free(pb_ctx *c)
+{
+    if (!c || !c->comp_state) return;
+    delete static_cast<CompState *>(c->comp_state);
+    c->comp_state = nullptr;
+}
 
 int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep_opts &o, double ctol,
                         double gtol, double *zmat, pb_sweep_stats *stats, pb_hstats *hs, float *sample_x,
@@ -1673,14 +1687,20 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
     // the dense fill, or an option needs the dense block (exact leaf inverses, samples)
     const bool od_lp = !o.aca_dense && !o.pc_exact_leaf && !sample_x;
     double od_entries = 0, od_static = 0;
-    std::vector<long> od_sig;                   // quadrature levels of the kept static parts
-    bool od_reset = true;
+    bool od_reset = false;
     *hs = pb_hstats();
 
     // compressed blocks: Lp over the segment midpoints (hmat_build, hmatrix.c:617-634) and,
     // with capacitance, P over the cell points (hmat_build_pot, potential.c:158-165)
-    std::vector<KBlock> kbs(1 + cap);
-    {
+    if (!c->comp_state) c->comp_state = new CompState;
+    CompState &cst = *static_cast<CompState *>(c->comp_state);
+    std::vector<KBlock> &kbs = cst.kbs;
+    if (!cst.ready || (int)kbs.size() != 1 + cap) {
+        cst.ready = false;
+        kbs.clear();
+        kbs.resize(1 + cap);
+    }
+    if (!cst.ready) {
         std::vector<double> pts(3 * (size_t)ns);
         for (int i = 0; i < ns; i++)
             for (int q = 0; q < 3; q++) pts[3 * i + q] = 0.5 * (c->seg[i].x1[q] + c->seg[i].x2[q]);
@@ -1688,7 +1708,7 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
         kbs[0].n = ns;
         PB_TRY(kb_setup(kbs[0], pts.data(), st));
     }
-    if (cap) {
+    if (!cst.ready && cap) {
         // cell point: length-weighted centroid of its sub-cell midpoints (potential.c:98-111)
         std::vector<double> cpt(3 * (size_t)nc);
         for (int i = 0; i < nc; i++) {
@@ -1704,6 +1724,7 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
         kbs[1].n = nc;
         PB_TRY(kb_setup(kbs[1], cpt.data(), st));
     }
+    cst.ready = true;
 
     // dense kernel blocks and their static parts stay with the context between calls; the
     // static parts are valid while the quadrature-level signature does not change
@@ -1765,8 +1786,8 @@ int pb_sweep_compressed(pb_ctx *c, int nfreq, const double *freq, const pb_sweep
             level_signature(c, kw, sig);
             sig.push_back(cap);
             sig.push_back(od_lp);
-            if (sig != od_sig) {
-                od_sig = sig;
+            if (sig != cst.od_sig) {
+                cst.od_sig = sig;
                 od_reset = true;
             }
             if (!c->comp_static_valid || sig != c->comp_sig) {

@@ -35,6 +35,9 @@ long far_rule_key(const pb_ctx *c, double kwmax);
 void pb_htree_build(pb_htree &t, int n, const double *pts);
 
 // Statistics of the last compressed sweep.
+// Releases the compressed path's per-context state (trees, workspaces, kept static parts).
+void pb_comp_state_free(pb_ctx *c);
+
 struct pb_hstats {
     int nfar = 0, nnear = 0, ndense_far = 0, max_rank = 0;
     double mem_mb = 0, dense_mb = 0;
