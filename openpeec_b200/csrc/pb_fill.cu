@@ -285,7 +285,29 @@ __device__ __forceinline__ void accum(Acc<double, F> &a, const KArg &k, double r
 // One (possibly mirrored) pair term reduced to what its sample loop needs, in the
 // precision of that loop. Built from the FP64 cells just before the loop so that the
 // cells are not live during it.
-enum { TT_RIBBON = 0, TT_WIRE = 1, TT_POLY = 2, TT_RIBBON2 = 3, TT_RIBBON3 = 4 };
+enum { TT_RIBBON = 0, TT_WIRE = 1, TT_POLY = 2, TT_RIBBON2 = 3, TT_RIBBON3 = 4, TT_WIRE48 = 5 };
+
+// Separated wire pairs on the FP32 path: centre distance >= PB_WFAR_RATIO lmax and
+// k lmax <= PB_WFAR_KL at every wavenumber of the launch. There the reference's rule
+// (gauss_kernel mode 1: nsub = 2 + k lmax sub-intervals per segment, 8 Gauss-Legendre
+// points in each, 256 samples at nsub = 2) is replaced by 4 points along the whole first
+// segment and 8 along the whole second (32 samples, one per lane). On the smooth far
+// integrand the difference is below 1e-9 of the entry, orders under the FP32 rounding of
+// the correction (measured against the reference's rule in tests/test_far_rules.py).
+#define PB_WFAR_RATIO 3.0
+#define PB_WFAR_KL 0.5
+__device__ __forceinline__ bool wire_far32(const Cell &s1, const Cell &s2, double kwmax)
+{
+    const double lmax = fmax(s1.len, s2.len);
+    if (!(kwmax * lmax <= PB_WFAR_KL)) return false;
+    double d2 = 0;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        const double d = 0.5 * (s2.x1[c] + s2.x2[c]) - 0.5 * (s1.x1[c] + s1.x2[c]);
+        d2 += d * d;
+    }
+    return d2 >= (PB_WFAR_RATIO * lmax) * (PB_WFAR_RATIO * lmax);
+}
 
 // Separated ribbon pairs on the FP32 path: a single sub-square (nsub = 1) and k * lmax <=
 // PB_FAR_KL at every wavenumber of the launch (lmax: the largest cell dimension). There
@@ -398,6 +420,13 @@ __device__ void make_term(Term<R> &T, const Cell &s1, const Cell &s2, int same, 
         a2l = aeff * aeff;
         T.sc = scale * s1.len * b.len * 0.25 / ((double)nsub * nsub);
         T.nsub = nsub;
+        if constexpr (sizeof(R) == 4) {
+            if (!wire_self && wire_far32(s1, b, kwmax)) {      // 4 x 8 points, no sub-intervals
+                T.ty = TT_WIRE48;
+                T.sc = scale * s1.len * b.len * 0.25;           // weights sum to 4 as well
+                T.nsub = 1;
+            }
+        }
     }
     if constexpr (sizeof(R) == 4) {
         T.D = sqrt(cdl[0] * cdl[0] + cdl[1] * cdl[1] + cdl[2] * cdl[2] + a2l);
@@ -570,6 +599,12 @@ __device__ void run_term32(const Term<float> &T, const KArg &k, Acc<float, F> &a
                                      fmaf(b2, T.v2[2], Q[2]), (float)(wijm * cWG3[q]));
             }
         }
+    } else if (T.ty == TT_WIRE48) {                 // separated wires: 4 x 8 points, one per lane
+        const int lj = lane & 7, li = lane >> 3;
+        const float v = 0.5f * (1.f + (float)cXG8[lj]), u = 0.5f * (1.f + cXG4f[li]);
+        const float w = (float)(cWG4[li] * cWG8[lj] * (-2.0 * T.sc));
+        sample32<F, EQ, RED>(a, k, base, cd, T.a2f, D, Dlo, fmaf(-T.u1[0], u, T.u2[0] * v),
+                             fmaf(-T.u1[1], u, T.u2[1] * v), fmaf(-T.u1[2], u, T.u2[2] * v), w);
     } else if (T.ty == TT_WIRE) {                   // gauss_kernel mode 1, partial.c:61-99
         const int lj = lane & 7, li = lane >> 3;
         const float hj = 0.5f * (1.f + (float)cXG8[lj]);
@@ -1113,6 +1148,7 @@ __device__ __forceinline__ long long pair_samples(const Cell &s1, const Cell &s2
         return 256LL * n * n;
     }
     const int n = corr_nsub(s1, s2, kw);
+    if (kwf > 0 && !same && wire_far32(s1, s2, kwf)) return 32;      // the FP32 path's 4 x 8 rule
     return 64LL * n * n;
 }
 

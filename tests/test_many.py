@@ -50,3 +50,21 @@ def test_many_rejects_repeated_context():
         with pytest.raises(api.PbError) as e:
             api.sweep_many([c, c], [p.freqs()[:2], p.freqs()[:2]])
         assert e.value.code == abi.PB_ERR_ARG
+
+
+@pytest.mark.parametrize("inst", [0, 7, 11])
+def test_config3_instance_mixed_matches_fp64(inst):
+    """Full config-3 instances (64 log frequencies 50 MHz-3 GHz): the mixed path (FP32
+    correction, with the 4 x 8 rule on separated wire pairs, FP32 factorisation, FP64
+    refinement) against the plain FP64 path (the reference's 8 x 8 rule, FP64 LU): Z within
+    1e-6 at every frequency."""
+    from openpeec_b200 import abi, api, configs, geometry
+    prob = geometry.build(geometry.parse_peec(configs.cfg3_instance(0, inst)))
+    f = prob.freqs()
+    with api.Context(prob) as c:
+        z64, _ = c.sweep(f, fill_prec=abi.PREC_FP64, lu=abi.LU_FP64)
+        zmx, st = c.sweep(f, fill_prec=abi.PREC_MIXED, lu=abi.LU_TC)
+    e = np.abs(zmx - z64).reshape(len(f), -1).max(1) / np.abs(z64).reshape(len(f), -1).max(1)
+    print("instance", inst, len(prob.seg), "segments, worst", e.max())
+    assert e.max() <= 1e-6, (e.max(), int(e.argmax()))
+
