@@ -942,6 +942,28 @@ __device__ __forceinline__ float2 warp_cdot(const float2 *row, const float2 *xs,
         const float4 *x4 = reinterpret_cast<const float4 *>(xs);
         const int pe = c1 >> 1;                          // pairs entirely inside [c0, c1)
         int p = (c0 >> 1) + lane;
+        // four 16-byte row loads in flight per lane: the solve streams the factors from HBM
+        // with one CTA per system, so the loads a warp keeps in flight set its bandwidth
+        for (; p + 96 < pe; p += 128) {
+            const float4 u0 = r4[p], u1 = r4[p + 32], u2 = r4[p + 64], u3 = r4[p + 96];
+            const float4 v0 = x4[p], v1 = x4[p + 32], v2 = x4[p + 64], v3 = x4[p + 96];
+            ax = fmaf(u0.x, v0.x, fmaf(-u0.y, v0.y, ax));
+            ay = fmaf(u0.x, v0.y, fmaf(u0.y, v0.x, ay));
+            bx = fmaf(u0.z, v0.z, fmaf(-u0.w, v0.w, bx));
+            by = fmaf(u0.z, v0.w, fmaf(u0.w, v0.z, by));
+            cx = fmaf(u1.x, v1.x, fmaf(-u1.y, v1.y, cx));
+            cy = fmaf(u1.x, v1.y, fmaf(u1.y, v1.x, cy));
+            dx = fmaf(u1.z, v1.z, fmaf(-u1.w, v1.w, dx));
+            dy = fmaf(u1.z, v1.w, fmaf(u1.w, v1.z, dy));
+            ax = fmaf(u2.x, v2.x, fmaf(-u2.y, v2.y, ax));
+            ay = fmaf(u2.x, v2.y, fmaf(u2.y, v2.x, ay));
+            bx = fmaf(u2.z, v2.z, fmaf(-u2.w, v2.w, bx));
+            by = fmaf(u2.z, v2.w, fmaf(u2.w, v2.z, by));
+            cx = fmaf(u3.x, v3.x, fmaf(-u3.y, v3.y, cx));
+            cy = fmaf(u3.x, v3.y, fmaf(u3.y, v3.x, cy));
+            dx = fmaf(u3.z, v3.z, fmaf(-u3.w, v3.w, dx));
+            dy = fmaf(u3.z, v3.w, fmaf(u3.w, v3.z, dy));
+        }
         for (; p + 32 < pe; p += 64) {
             const float4 u = r4[p], v = x4[p], u2 = r4[p + 32], v2 = x4[p + 32];
             ax = fmaf(u.x, v.x, fmaf(-u.y, v.y, ax));
