@@ -323,7 +323,10 @@ int  pb_sources(pb_ctx *ctx, int nfreq, const double *freq, const pb_sweep_opts 
  * (reference lu_decomp, src/lu.c:16-66): row-major a[n*n] complex is replaced by L\U,
  * piv[k] = row swapped with row k at step k. Returns -1 on success or the 0-based row of
  * the first zero pivot (max |re|+|im| < 1e-30), exactly like the reference; returns -2
- * on a CUDA error.
+ * on a CUDA error. The complex entries are (re, im) double pairs, the layout of the
+ * reference's d_complex_t; this C ABI takes double * so that it needs no reference header.
+ * The reference-prototype entry point, lu_decomp(int, d_complex_t *, int *), is the
+ * drop-in shim's (openpeec_b200/dropin/peec_shim.c), which casts and calls this one.
  */
 int  pb_lu_decomp(int n, double *a, int *piv);
 /* Forward/back substitution with the factors of pb_lu_decomp (reference lu_solve,

@@ -10,8 +10,9 @@
 // Device storage a context keeps across sweep calls (grow-only, freed by pb_destroy), so
 // repeated sweeps of one structure do not reallocate their batch buffers.
 struct pb_cache_slot { void *p = nullptr; size_t cap = 0; };
-#define PB_CACHE_SLOTS 48
+#define PB_CACHE_SLOTS 56
 #define PB_SLOT_COMP0  40     // slots [40, 48) hold the compressed path's dense kernel blocks
+#define PB_SLOT_POST0  48     // slots [48, 56) hold the far-field buffers (pb_farfield)
 
 // One additive contribution to an MNA entry whose value scales as val * {1, jw, -jw}.
 enum { ST_CONST = 0, ST_JW = 1, ST_MJW = 2 };

@@ -599,18 +599,17 @@ __device__ void run_term32(const Term<float> &T, const KArg &k, Acc<float, F> &a
                                      fmaf(b2, T.v2[2], Q[2]), (float)(wijm * cWG3[q]));
             }
         }
-    } else if (T.ty == TT_WIRE48) {                 // separated wires: 4 x 8 points, one per lane
-        const int lj = lane & 7, li = lane >> 3;
-        const float v = 0.5f * (1.f + (float)cXG8[lj]), u = 0.5f * (1.f + cXG4f[li]);
-        const float w = (float)(cWG4[li] * cWG8[lj] * (-2.0 * T.sc));
-        sample32<F, EQ, RED>(a, k, base, cd, T.a2f, D, Dlo, fmaf(-T.u1[0], u, T.u2[0] * v),
-                             fmaf(-T.u1[1], u, T.u2[1] * v), fmaf(-T.u1[2], u, T.u2[2] * v), w);
-    } else if (T.ty == TT_WIRE) {                   // gauss_kernel mode 1, partial.c:61-99
+    } else if (T.ty == TT_WIRE || T.ty == TT_WIRE48) {
+        // gauss_kernel mode 1 (partial.c:61-99): 8 x 8 points per sub-square, two samples
+        // per lane; separated wires (TT_WIRE48): 4 x 8 points over the whole segments, one
+        // per lane. One sample call site for both keeps the kernel's code (and its
+        // instruction-cache footprint) the size it had with the reference's rule alone.
+        const bool w48 = T.ty == TT_WIRE48;
         const int lj = lane & 7, li = lane >> 3;
         const float hj = 0.5f * (1.f + (float)cXG8[lj]);
-        const float hi0 = 0.5f * (1.f + (float)cXG8[li]), hi1 = 0.5f * (1.f + (float)cXG8[li + 4]);
+        const float hi0 = 0.5f * (1.f + (w48 ? cXG4f[li] : (float)cXG8[li])), hi1 = 0.5f * (1.f + (float)cXG8[li + 4]);
         const double wj = cWG8[lj] * (-2.0 * T.sc);
-        const float w0 = (float)(cWG8[li] * wj), w1 = (float)(cWG8[li + 4] * wj);
+        const float w0 = (float)((w48 ? cWG4[li] : cWG8[li]) * wj), w1 = (float)(cWG8[li + 4] * wj);
         const float a2 = T.a2f;
         float U1[3], U2[3];
 #pragma unroll
@@ -620,10 +619,12 @@ __device__ void run_term32(const Term<float> &T, const KArg &k, Acc<float, F> &a
             for (int i2 = 0; i2 < nsub; i2++) {
                 const float v = ((float)i2 + hj) * irn;
                 const float P0 = U2[0] * v, P1 = U2[1] * v, P2 = U2[2] * v;
-                sample32<F, EQ, RED>(a, k, base, cd, a2, D, Dlo, fmaf(-U1[0], ua, P0), fmaf(-U1[1], ua, P1),
-                                fmaf(-U1[2], ua, P2), w0);
-                sample32<F, EQ, RED>(a, k, base, cd, a2, D, Dlo, fmaf(-U1[0], ub, P0), fmaf(-U1[1], ub, P1),
-                                fmaf(-U1[2], ub, P2), w1);
+#pragma unroll 1
+                for (int h = 0; h < (w48 ? 1 : 2); h++) {
+                    const float uu = h ? ub : ua;
+                    sample32<F, EQ, RED>(a, k, base, cd, a2, D, Dlo, fmaf(-U1[0], uu, P0), fmaf(-U1[1], uu, P1),
+                                         fmaf(-U1[2], uu, P2), h ? w1 : w0);
+                }
             }
         }
     } else {                                        // poly_corr, polygon.c:305-334

@@ -21,6 +21,29 @@ struct Dev1 {
     template <typename T> T *as() const { return (T *)p; }
 };
 
+// A buffer held by the context between calls (grown when too small, freed by pb_destroy):
+// no cudaMalloc / cudaFree, which synchronises the device, on repeated calls.
+struct Held1 {
+    pb_cache_slot *s;
+    void *p = nullptr;
+    explicit Held1(pb_cache_slot *slot) : s(slot) {}
+    int alloc(size_t b)
+    {
+        if (b == 0) b = 16;
+        if (s->cap < b) {
+            if (s->p) cudaFree(s->p);
+            s->p = nullptr;
+            s->cap = 0;
+            cudaError_t e = cudaMalloc(&s->p, b);
+            if (e != cudaSuccess) { s->p = nullptr; return pb_cuda_fail(e, "cudaMalloc", __FILE__, __LINE__); }
+            s->cap = b;
+        }
+        p = s->p;
+        return PB_OK;
+    }
+    template <typename T> T *as() const { return (T *)p; }
+};
+
 __device__ __forceinline__ double sinc_d(double x)                 // farfield.c:37-40
 {
     return fabs(x) < 1e-8 ? 1.0 : sin(x) / x;
@@ -150,7 +173,8 @@ extern "C" int pb_farfield(pb_ctx *c, int nfreq, const double *freq, const doubl
         }
         geo[(size_t)m * 8 + 6] = s.len;
     }
-    Dev1 dgeo, dcur, dfreq, det, dep, duu;
+    pb_cache_slot *cs = c->cache + PB_SLOT_POST0;
+    Held1 dgeo(cs + 0), dcur(cs + 1), dfreq(cs + 2), det(cs + 3), dep(cs + 4), duu(cs + 5);
     PB_TRY(dgeo.alloc(sizeof(double) * geo.size()));
     PB_TRY(dcur.alloc(sizeof(double2) * (size_t)nfreq * ns));
     PB_TRY(dfreq.alloc(sizeof(double) * nfreq));
