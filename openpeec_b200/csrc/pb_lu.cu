@@ -1090,14 +1090,18 @@ k_lu_solve(const T2_t<TF> *lu, int n, int ld, long long stride, const int *perm,
     }
     __syncthreads();
 
-    // forward: unit lower
+    // forward: unit lower (each warp takes rows warp, warp + nwarps, ... of a 32-row block:
+    // small systems run on 256-thread CTAs, so that more of them share an SM)
+    const int nwarps = (int)(blockDim.x >> 5);
     for (int r0 = 0; r0 < n; r0 += 32) {
-        const int r = r0 + warp;
-        if (r < n) {
-            const T2 *row = lu + (long long)r * ld;
-            const T2 acc = warp_cdot(row, xs, 0, r0, lane);
-            if (lane == 0) tmp[warp] = csub(xs[r], acc);
-            diag[warp][lane] = (r0 + lane < n) ? row[r0 + lane] : mk2<T2>(0, 0);
+        for (int wr = warp; wr < 32; wr += nwarps) {
+            const int r = r0 + wr;
+            if (r < n) {
+                const T2 *row = lu + (long long)r * ld;
+                const T2 acc = warp_cdot(row, xs, 0, r0, lane);
+                if (lane == 0) tmp[wr] = csub(xs[r], acc);
+                diag[wr][lane] = (r0 + lane < n) ? row[r0 + lane] : mk2<T2>(0, 0);
+            }
         }
         __syncthreads();
         if (warp == 0) {
@@ -1120,12 +1124,12 @@ k_lu_solve(const T2_t<TF> *lu, int n, int ld, long long stride, const int *perm,
     const int nblk = (n + 31) / 32;
     for (int bk = nblk - 1; bk >= 0; bk--) {
         const int r0 = bk * 32, nbk = min(32, n - r0);
-        const int r = r0 + warp;
-        if (warp < nbk) {
+        for (int wr = warp; wr < nbk; wr += nwarps) {
+            const int r = r0 + wr;
             const T2 *row = lu + (long long)r * ld;
             const T2 acc = warp_cdot(row, xs, r0 + 32, n, lane);
-            if (lane == 0) tmp[warp] = csub(xs[r], acc);
-            diag[warp][lane] = (lane < nbk) ? row[r0 + lane] : mk2<T2>(0, 0);
+            if (lane == 0) tmp[wr] = csub(xs[r], acc);
+            diag[wr][lane] = (lane < nbk) ? row[r0 + lane] : mk2<T2>(0, 0);
         }
         __syncthreads();
         if (warp == 0) {
@@ -1174,8 +1178,9 @@ int pb_lu_solve_mapped(pb_lu_engine *e, int n, int nb, int nrhs, const T2_t<TF> 
         k_lu_solve<TF, true><<<g, 1024, 0, e->stream>>>(lu, n, ld, stride, perm, r, x, nrhs, sys, lu_of, 0);
     } else {
         PB_TRY(pb_smem_optin(k_lu_solve<TF, false>, pb_smem_cap() - 20480, attr_set));
-        k_lu_solve<TF, false><<<g, 1024, smem, e->stream>>>(lu, n, ld, stride, perm, r, x, nrhs, sys, lu_of,
-                                                            operm);
+        // the same rows and dot products either way (results do not depend on it)
+        const int nt = n <= 512 ? 256 : 1024;
+        k_lu_solve<TF, false><<<g, nt, smem, e->stream>>>(lu, n, ld, stride, perm, r, x, nrhs, sys, lu_of, operm);
     }
     e->launches++;
     PB_CHECK_LAUNCH();
