@@ -366,14 +366,46 @@ __device__ long long scan1024(long long x, long long *wsum, long long &carry)
     return excl;
 }
 
-// Offsets of the entries the blocks in state `want` request, in block order (the lists do
-// not depend on scheduling), and the static-part cache look-up: a row (column) whose static
-// parts are cached is a hit; otherwise it takes a free slot, if any, and its entries go to
-// the miss list too. cnt[0] = entries requested, cnt[1] = blocks not done, cnt[2] = misses;
+// The static-part cache look-up of every block in state `want`, one thread per block: a
+// row (column) whose static parts are cached is a hit; otherwise it takes a free slot, if
+// any, and its entries go to the miss list too. lens[b], lens[nb + b]: entries and misses
+// requested; lens[2 nb + b]: 1 while the block runs.
+__global__ void k_acaod_lookup(int nb, const AcaBlk *blks, AcaSt *S, int want, int rc, int *cidx, int *cnum,
+                               long long *lens)
+{
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb) return;
+    const int st = S[b].st;
+    long long len = 0, mlen = 0;
+    if (st == want) {
+        int slot = -1, hit = 0;
+        len = want == 0 ? blks[b].nn : blks[b].m;
+        if (rc > 0) {
+            const int key = want == 0 ? S[b].irow : S[b].jcol;
+            int *ci = cidx + ((long long)b * 2 + want) * rc;
+            const int nc = cnum[b * 2 + want];
+            for (int q = 0; q < nc && !hit; q++)
+                if (ci[q] == key) { slot = q; hit = 1; }
+            if (!hit && nc < rc) {
+                slot = nc;
+                ci[nc] = key;
+                cnum[b * 2 + want] = nc + 1;
+            }
+        }
+        mlen = hit ? 0 : len;
+        S[b].slot = slot;
+        S[b].hit = hit;
+    }
+    lens[b] = len;
+    lens[nb + b] = mlen;
+    lens[2LL * nb + b] = st != 2;
+}
+
+// Offsets of the looked-up entries and misses, in block order (the lists do not depend on
+// scheduling): cnt[0] = entries requested, cnt[1] = blocks not done, cnt[2] = misses;
 // acc[want] accumulates the entries requested, acc[2 + want] the misses.
 __global__ void __launch_bounds__(1024)
-k_acaod_scan(int nb, const AcaBlk *blks, AcaSt *S, int want, int rc, int *cidx, int *cnum, int *cnt,
-             long long *acc)
+k_acaod_scan(int nb, AcaSt *S, int want, const long long *lens, int *cnt, long long *acc)
 {
     __shared__ long long wsum[32];
     __shared__ int nact;
@@ -384,34 +416,16 @@ k_acaod_scan(int nb, const AcaBlk *blks, AcaSt *S, int want, int rc, int *cidx, 
     for (int base = 0; base < nb; base += 1024) {
         const int b = base + threadIdx.x;
         long long len = 0, mlen = 0;
-        int slot = -1, hit = 0;
         if (b < nb) {
-            const int st = S[b].st;
-            act += st != 2;
-            if (st == want) {
-                len = want == 0 ? blks[b].nn : blks[b].m;
-                if (rc > 0) {
-                    const int key = want == 0 ? S[b].irow : S[b].jcol;
-                    int *ci = cidx + ((long long)b * 2 + want) * rc;
-                    const int nc = cnum[b * 2 + want];
-                    for (int q = 0; q < nc && !hit; q++)
-                        if (ci[q] == key) { slot = q; hit = 1; }
-                    if (!hit && nc < rc) {
-                        slot = nc;
-                        ci[nc] = key;
-                        cnum[b * 2 + want] = nc + 1;
-                    }
-                }
-                mlen = hit ? 0 : len;
-            }
+            len = lens[b];
+            mlen = lens[nb + b];
+            act += (int)lens[2LL * nb + b];
         }
         const long long e = scan1024(len, wsum, carry);
         const long long me = scan1024(mlen, wsum, mcarry);
         if (len > 0) {
             S[b].ent = e;
             S[b].ment = me;
-            S[b].slot = slot;
-            S[b].hit = hit;
         }
     }
     atomicAdd(&nact, act);
@@ -1086,7 +1100,7 @@ struct KBlock {
     std::vector<zc> bval, cval;
     Dev lof_d, lidx_d, dof_d, dlu_d, dpiv_d, bro, bcol, bv, cro, ccol, cv, wb, ub;
     // on-demand entries: ACA state, pair list, miss list, static parts, values, counts
-    Dev od_st, od_pairs, od_miss, od_stl, od_vals, od_cnt, od_acc, od_blk;
+    Dev od_st, od_pairs, od_miss, od_stl, od_vals, od_cnt, od_acc, od_blk, od_lens;
     // static parts kept between frequencies (valid while the quadrature levels stay): of
     // up to rc rows and rc columns per far block (keys cidx, counts cnum, values srow /
     // scol), of the near blocks and of the leaf blocks
@@ -1207,10 +1221,14 @@ int kb_aca_ondemand(KBlock &kb, pb_ctx *c, OnDemand &od, double ctol)
     k_acaod_init<<<nfar, 256, 0, st>>>(blk, S, kb.rused.as<int>(), kb.urep.as<double>(), rank);
     c->launches++;
     PB_CHECK_LAUNCH();
+    PB_TRY(kb.od_lens.alloc(sizeof(long long) * 3 * (size_t)nfar));
     auto scan = [&](int want) {
-        k_acaod_scan<<<1, 1024, 0, st>>>(nfar, blk, S, want, kb.rc, kb.rc > 0 ? kb.cidx.as<int>() : nullptr,
-                                          kb.rc > 0 ? kb.cnum.as<int>() : nullptr, cnt, acc);
-        c->launches++;
+        k_acaod_lookup<<<ceil_div(nfar, 256), 256, 0, st>>>(nfar, blk, S, want, kb.rc,
+                                                             kb.rc > 0 ? kb.cidx.as<int>() : nullptr,
+                                                             kb.rc > 0 ? kb.cnum.as<int>() : nullptr,
+                                                             kb.od_lens.as<long long>());
+        k_acaod_scan<<<1, 1024, 0, st>>>(nfar, S, want, kb.od_lens.as<long long>(), cnt, acc);
+        c->launches += 2;
     };
     // every round advances each running block by a row; a block ends after at most
     // PB_HM_MAXIT ranks, each with at most PB_HM_PROBE + 1 rows
